@@ -1,0 +1,337 @@
+#!/usr/bin/env python3
+"""Benchmark: cell-steps/s of the fused FP64 NEMOLite2D stepper at 4096^2.
+
+Workload (one instance per GPU): 4096 x 4096 T-points, dx = dy = 1 km, depth
+100 m plus 32 seeded Gaussian bumps (amplitude U(+-40) m, width U(20,200) km,
+floor 10 m), rdt 20 s, cbfr 1.5e-4, visc 0.1 m^2/s, tidal SSH clamp at the
+open boundary (amplitude 0.2 m, period 12.42 h).  One bench step = 100 model
+time steps (one record interval) + the device checksums of sshn/u/v, so the
+default 10 timed steps are the 1000-step run with a record every 100 steps.
+The state is reset to rest after warm-up, so the timed region is steps
+1..100*K from rest.  Inputs (9 x 134 MB per step) are far larger than L2.
+
+`value`: device-timed, state resident in HBM.  `e2e`: the same metric
+through the C ABI with pinned host buffers: every step uploads the state
+(nemo_set_state), steps, reads the state back (nemo_retrieve) and the
+checksums.  `--impl reference` times the CPU restatement of the reference
+(oracle/, OpenMP over all host cores) on the same grid.
+
+Multi-GPU (torchrun): independent replicas, one per GPU (the stepper does not
+shard); value = all ranks' cell-steps / max-over-ranks time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "nemolite2d-cuda_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+N = 4096
+STEPS_PER_ITER = 100
+WORKLOAD = dict(jpi=N, jpj=N, dx=1000.0, dy=1000.0, dep_const=100.0, rdt=20.0, cbfr=0.00015,
+                visc=0.1, amp_tide=0.2, tide_phase=0.0, nbump=32, seed=1234, bump_amp=40.0,
+                bump_wmin=20e3, bump_wmax=200e3, hmin=10.0)
+BYTES_PER_CELL_STEP = 72  # read sshn, un, vn, ht, hu, hv; write sshn, un, vn (FP64)
+METRIC = "cell-steps/s at 4096^2 FP64 (% of HBM peak)"
+CONFIG = {"workload": "plain fused FP64 stepper, one 4096x4096 instance per GPU, seeded "
+                      "32-bump bathymetry, 1000 steps from rest, checksums every 100 steps",
+          "grid": [N, N], "steps_per_bench_step": STEPS_PER_ITER, "dtype": "f64",
+          "l2": "inputs larger than L2 (1.2 GB touched per model step)"}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--tile", type=str, default="")
+    ap.add_argument("--n", type=int, default=N,
+                    help="grid side (profiling of smaller cases only; the bench line is 4096)")
+    return ap.parse_args()
+
+
+def cells():
+    return WORKLOAD["jpi"] * WORKLOAD["jpj"]
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic():
+    """DRAM bytes per fused launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "fused_step_4096.txt")
+    if not os.path.exists(path):
+        return None
+    with open(path) as fh:
+        for line in fh:
+            if line.startswith("dram_bytes_per_launch:"):
+                return float(line.split(":", 1)[1].split()[0])
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", "bench_clocks_%d.csv" % index)
+
+    def start(self):
+        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.fh, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as fh:
+            for line in fh:
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    smax = float(f[2])
+                except ValueError:
+                    continue
+                for k, n in enumerate(names):
+                    if f[5 + k].lower() == "active":
+                        reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+def cpu_oracle_rate(budget_s=12.0, max_steps=8):
+    """Oracle (OpenMP, all host cores) on the bench grid: (cell-steps/s, steps, threads)."""
+    from oracle import oracle
+    th = host_cores()
+    oracle.set_threads(th)
+    okw = dict(WORKLOAD)
+    m = oracle.Model(**okw)
+    t0 = time.perf_counter()
+    m.step(1)
+    t1 = time.perf_counter()
+    per = t1 - t0
+    n = max(1, min(max_steps, int(budget_s / max(per, 1e-3))))
+    t0 = time.perf_counter()
+    m.run(2, n)
+    dt = time.perf_counter() - t0
+    m.close()
+    oracle.set_threads(1)
+    return cells() * n / dt, n, th
+
+
+def run_reference(args, rank):
+    """CPU restatement of original/nemolite2d.f90 (the reference's CPU path)."""
+    if rank != 0:
+        return
+    from oracle import oracle
+    th = host_cores()
+    oracle.set_threads(th)
+    m = oracle.Model(**WORKLOAD)
+    istp = 1
+    for _ in range(args.warmup):
+        m.step(istp)
+        istp += 1
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        m.step(istp)
+        istp += 1
+    dt = time.perf_counter() - t0
+    v = cells() * args.steps / dt
+    sample = ("%d model steps of the 4096^2 bench grid (steps %d..%d), oracle port of "
+              "original/nemolite2d.f90, OpenMP %d threads" % (args.steps, args.warmup + 1,
+                                                               args.warmup + args.steps, th))
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "cell-steps/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * dt / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(CONFIG, bench_step="1 model time step"),
+            "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": th, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.n != N:
+        WORKLOAD["jpi"] = WORKLOAD["jpj"] = args.n
+        CONFIG["grid"] = [args.n, args.n]
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank)
+
+    import numpy as np
+    import torch
+    import nemo_b200
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    stream = torch.cuda.Stream()
+    m = nemo_b200.Model(strict=False, stream=stream.cuda_stream, device=local, **WORKLOAD)
+    if args.tile:
+        tx, ty = (int(x) for x in args.tile.split("x"))
+        m.set_tile(tx, ty)
+    jpi, jpj = m.jpi, m.jpj
+    rest = (np.zeros((jpj, jpi)), np.zeros((jpj, jpi + 1)), np.zeros((jpj + 1, jpi)))
+
+    # warm-up, then back to rest so the timed steps are 1..100*K
+    for w in range(args.warmup):
+        m.step_n(1 + STEPS_PER_ITER * w, STEPS_PER_ITER)
+        m.checksums()
+    m.set_state(*rest)
+    torch.cuda.synchronize()
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(local)
+    records = []
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    t_start.record(stream)
+    for k in range(args.steps):
+        ev[k][0].record(stream)
+        m.step_n(1 + STEPS_PER_ITER * k, STEPS_PER_ITER)
+        ev[k][1].record(stream)
+        records.append(m.checksums())
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    total_ms = t_start.elapsed_time(t_end)
+    fused_ms = sum(a.elapsed_time(b) for a, b in ev)
+    t_max = total_ms
+    if dist is not None:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+    total_cell_steps = cells() * STEPS_PER_ITER * args.steps * world
+    value = total_cell_steps / (t_max / 1e3)
+    launch_s = fused_ms / 1e3 / (STEPS_PER_ITER * args.steps)
+    peak, peak_kind = load_peaks()
+    achieved = BYTES_PER_CELL_STEP * cells() / launch_s / 1e9
+    traffic = load_traffic()
+
+    # ---- end to end through the C ABI with pinned host buffers --------------
+    e2e = None
+    if not args.no_e2e:
+        # pinned host state; each step uploads it, steps, and reads it back
+        hbuf = [torch.zeros(a.shape, dtype=torch.float64, pin_memory=True).numpy() for a in rest]
+        fields = (nemo_b200.SSHN, nemo_b200.UN, nemo_b200.VN)
+        bi = sum(a.nbytes for a in hbuf)
+        bo = sum(a.nbytes for a in hbuf) + 3 * 8
+        k_e2e = max(1, min(args.steps, 5))
+        barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for k in range(k_e2e):
+            m.set_state(*hbuf)
+            m.step_n(1 + STEPS_PER_ITER * k, STEPS_PER_ITER)
+            for f, o in zip(fields, hbuf):
+                m.field(f, out=o)
+            m.checksums()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        e_ms = e0.elapsed_time(e1)
+        if dist is not None:
+            t = torch.tensor([e_ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e_ms = float(t.item())
+        e2e = {"value": cells() * STEPS_PER_ITER * k_e2e * world / (e_ms / 1e3),
+               "unit": "cell-steps/s", "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo,
+               "steps": k_e2e}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        rate, n, th = cpu_oracle_rate()
+        cpu = {"value": rate, "unit": "cell-steps/s", "cores": th, "kind": "port",
+               "sample": "%d model steps (2..%d) of the 4096^2 bench grid, oracle port of "
+                         "original/nemolite2d.f90, OpenMP %d threads" % (n, n + 1, th)}
+
+    if rank == 0:
+        tx, ty = m.get_tile()
+        line = {"metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64", "data": "synthetic",
+                "config": dict(CONFIG, parallelism="replicas x%d" % world, tile=[tx, ty]),
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
+                             "unit": "GB/s", "frac": achieved / peak,
+                             "peak_source": peak_kind, "traffic": traffic,
+                             "kernel": "k_fused_step", "launch_us": launch_s * 1e6,
+                             "algorithmic_bytes_per_launch": BYTES_PER_CELL_STEP * cells()},
+                "gpu_launches": args.steps * (STEPS_PER_ITER + 2),
+                "checksums_last": [float(x) for x in records[-1]],
+                "clocks": clk, "e2e": e2e, "cpu_baseline": cpu}
+        print(json.dumps(line), flush=True)
+    m.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,170 @@
+/*
+ * nemo_b200.h -- C ABI of the B200 (sm_100a) NEMOLite2D time-stepper.
+ *
+ * Two layers:
+ *
+ *  1. The handle API (nemo_*).  Every call returns an int status (NEMO_OK = 0)
+ *     and never throws.  A context owns all device memory of one model
+ *     instance and one CUDA stream; there is no global state.
+ *
+ *  2. Drop-in symbols with the exact names and signatures of the reference's
+ *     CUDA library (cuda/cuda_nemolite2d.cu:234-270), bound from Fortran by
+ *     cuda/nemolite2d.f90:62-127 (explicit bind(C) interfaces) and :138,
+ *     :174, :486-489 (implicit interfaces with gfortran's trailing
+ *     underscore).  They drive one process-wide default context.
+ *
+ * Field layout at the ABI edge is the reference's: Fortran column-major
+ * arrays with the reference's bounds (ji fastest).
+ *   T fields  (1:jpi, 1:jpj)   sshn, ssha, ht, xt, yt
+ *   U fields  (0:jpi, 1:jpj)   un, ua, sshn_u, hu
+ *   V fields  (1:jpi, 0:jpj)   vn, va, sshn_v, hv
+ * (original/nemolite2d.f90:290-306).  Device storage is pitched and padded;
+ * conversion happens in the copy routines below.
+ */
+#ifndef NEMO_B200_H
+#define NEMO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------- */
+enum {
+  NEMO_OK = 0,
+  NEMO_ERR_INVALID = 1,     /* bad argument (size, field id, null pointer) */
+  NEMO_ERR_CUDA = 2,        /* a CUDA runtime call failed */
+  NEMO_ERR_ALLOC = 3,       /* device or pinned allocation failed */
+  NEMO_ERR_STATE = 4,       /* call out of order (e.g. no context) */
+  NEMO_ERR_TIMEOUT = 5,     /* a bounded device-side wait gave up */
+  NEMO_ERR_UNSUPPORTED = 6  /* feature not available in this build/device */
+};
+
+/* ---- field identifiers ---------------------------------------------------- */
+enum {
+  NEMO_SSHN = 0, NEMO_UN = 1, NEMO_VN = 2,
+  NEMO_SSHA = 3, NEMO_UA = 4, NEMO_VA = 5,
+  NEMO_SSHN_U = 6, NEMO_SSHN_V = 7,
+  NEMO_HT = 8, NEMO_HU = 9, NEMO_HV = 10,
+  NEMO_XT = 11, NEMO_YT = 12,
+  NEMO_NFIELDS = 13
+};
+
+/* Model parameters.  The first block is the reference's &namctl
+ * (original/nemolite2d.f90:100-118; jpi/jpj are the namelist's jpiglo-2,
+ * :133-137) and the argument list of cuda_setup_model_params_
+ * (cuda/cuda_nemolite2d.cu:236-246).  The second block extends the
+ * reference's hard-coded physics; nemo_default_params() sets values that
+ * reproduce the reference exactly (amp_tide 0.2, phase 0, latitude 50,
+ * uniform depth). */
+typedef struct nemo_params {
+  int jpi, jpj;
+  double dx, dy, dep_const;
+  int nit000, nitend, irecord;
+  double rdt, cbfr, visc;
+  /* extensions */
+  double amp_tide;      /* original/nemolite2d.f90:629 hard-codes 0.2 */
+  double tide_phase;    /* radians added to omega_tide*rtime */
+  double lat;           /* gphiu/gphiv, :220-221 hard-code 50 */
+  int nbump;            /* 0: uniform dep_const; >0: seeded Gaussian bumps */
+  uint64_t seed;
+  double bump_amp, bump_wmin, bump_wmax, hmin, hmax;
+  /* execution */
+  void* stream;         /* cudaStream_t to run on; NULL: the context makes one */
+  int device;           /* CUDA device ordinal; -1: current device */
+} nemo_params;
+
+typedef struct nemo_ctx nemo_ctx;
+
+/* Defaults of original/nemolite2d.f90:107-118 plus the extension defaults. */
+int nemo_default_params(nemo_params* p);
+
+/* grid + allocation + initialisation (original/nemolite2d.f90:145-371);
+ * replaces cuda_setup_model_params_ + cuda_initialise_grid_
+ * (cuda/cuda_nemolite2d.cu:418-446, :282-416).  jpi, jpj >= 2. */
+int nemo_create(const nemo_params* p, nemo_ctx** out);
+/* Frees everything the context owns; replaces cuda_finalise_ (:595-645),
+ * without its cudaDeviceReset. */
+int nemo_destroy(nemo_ctx* ctx);
+
+/* ---- per-routine boundary (original/nemolite2d.f90:375-386) ---------------
+ * Same semantics and order as the reference's routines; asynchronous on the
+ * context's stream. */
+int nemo_continuity(nemo_ctx* ctx);                /* :390-410; cu:448-476 */
+int nemo_momentum(nemo_ctx* ctx);                  /* :414-613; cu:478-482 */
+int nemo_momentum_u(nemo_ctx* ctx);                /* :430-517 */
+int nemo_momentum_v(nemo_ctx* ctx);                /* :519-609 */
+int nemo_bc(nemo_ctx* ctx, double rtime);          /* :617-700; cu:484-531 */
+int nemo_bc_ssh(nemo_ctx* ctx, double rtime);      /* :626-645 */
+int nemo_bc_solid_u(nemo_ctx* ctx);                /* :647-652 */
+int nemo_bc_solid_v(nemo_ctx* ctx);                /* :655-660 */
+int nemo_bc_flather_u(nemo_ctx* ctx);              /* :668-680 */
+int nemo_bc_flather_v(nemo_ctx* ctx);              /* :683-695 */
+int nemo_next(nemo_ctx* ctx);                      /* :704-769; cu:533-563 */
+/* step (:375-386) without output: rtime = istp*rdt, then the four routines. */
+int nemo_step(nemo_ctx* ctx, int istp);
+
+/* ---- fused path -----------------------------------------------------------
+ * Advances n steps istp0 .. istp0+n-1 with one fused launch per step
+ * (continuity + momentum + bc + next in a single pass over HBM).  Results
+ * equal nemo_step() called n times. */
+int nemo_step_n(nemo_ctx* ctx, int istp0, int n);
+
+/* Checksums SUM(ABS(f(1:jpi,1:jpj))) (shared/.../field_mod.f90:935-956,
+ * original/nemolite2d.f90:82-85) of sshn, un (=ua after next) and vn (=va),
+ * in out[0..2], computed on the device with a fixed reduction order. */
+int nemo_checksums(nemo_ctx* ctx, double out[3]);
+int nemo_checksum(nemo_ctx* ctx, int field, double* out);
+
+/* Copies one field's Fortran-bounded region to/from host memory (column
+ * major, leading dimension ld >= the field's x extent).  Replaces
+ * cuda_retrieve_results_ / cuda_retrieve_grid_constants_ (cu:565-593).
+ * These synchronise the context's stream. */
+int nemo_retrieve(nemo_ctx* ctx, int field, double* host, long ld);
+/* Overwrites sshn, un, vn (dense, Fortran extents) and re-derives
+ * sshn_u/sshn_v with the post-`next` interpolation (:736-764); the
+ * open-boundary row sshn_v(:,0), which the reference never updates after
+ * initialisation, keeps its value. */
+int nemo_set_state(nemo_ctx* ctx, const double* sshn, const double* un,
+                   const double* vn);
+
+int nemo_sync(nemo_ctx* ctx);
+int nemo_get_dims(nemo_ctx* ctx, int* jpi, int* jpj);
+/* Device address and pitch (in doubles) of a field's storage; element
+ * (ji,jj) lives at ptr[(jj+1)*pitch + (ji+1)].  For device-side consumers. */
+int nemo_device_field(nemo_ctx* ctx, int field, double** ptr, long* pitch);
+/* Tile shape of the fused kernel (columns per CTA x rows per CTA); 0 picks
+ * the tuned default. */
+int nemo_set_tile(nemo_ctx* ctx, int tile_x, int tile_y);
+int nemo_get_tile(nemo_ctx* ctx, int* tile_x, int* tile_y);
+const char* nemo_status_string(int status);
+/* 1 when this library was built with -fmad=false (bit-exact build). */
+int nemo_build_is_strict(void);
+
+/* ---- drop-in symbols (cuda/cuda_nemolite2d.cu:234-270) --------------------
+ * One default context.  Errors are printed to stderr and kept in a sticky
+ * status readable with nemo_compat_last_status() (the reference threw a C++
+ * exception through the Fortran frames instead, cuda_utils.cuh:14-24). */
+void cuda_setup_model_params_(int jpi, int jpj, double dx, double dy,
+                              double dep_const, int nit000, int nitend,
+                              int irecord, double rdt, double cbfr,
+                              double visc);
+void cuda_initialise_grid_(void);
+void cuda_continuity_(void);
+void cuda_momentum_(void);
+void cuda_boundary_conditions_(double rtime);
+void cuda_next_(void);
+void cuda_retrieve_grid_constants_(double* out_xt, double* out_yt,
+                                   double* out_ht, int jpi, int jpj);
+void cuda_retrieve_results_(double* out_sshn, double* out_un, double* out_vn,
+                            double* out_ua, double* out_va, int jpi, int jpj);
+void cuda_finalise_(void);
+int nemo_compat_last_status(void);
+nemo_ctx* nemo_compat_context(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,668 @@
+// C ABI of the NEMOLite2D stepper: context lifecycle, the per-routine
+// boundary, the fused path, checksums and field copies, plus the drop-in
+// cuda_*_ symbols of the reference library (cuda/cuda_nemolite2d.cu:234-270).
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <new>
+#include <vector>
+
+#include "nemo_internal.h"
+
+using namespace nemo;
+
+struct nemo_ctx {
+  nemo_params p;
+  Layout L;
+  Consts C;
+  int device;
+  cudaStream_t stream;
+  bool own_stream;
+  double* slab;
+  StateSet set[2];
+  int n_idx;              // set[n_idx] holds sshn/un/vn, set[1-n_idx] ssha/ua/va
+  double *sshn_u, *sshn_v, *ht, *hu, *hv;
+  double* ck_partials;    // 4*jpj
+  double* ck_out;         // 4
+  double* ck_host;        // pinned, 4
+  bool a_mirrors_n;       // after a fused step the reference's a-fields equal n
+  bool uv_stale;          // stored sshn_u/sshn_v lag behind sshn
+  int tile_x, tile_y;
+};
+
+namespace {
+
+#define CK(call)                                     \
+  do {                                               \
+    cudaError_t e_ = (call);                         \
+    if (e_ != cudaSuccess) return status_from(e_);   \
+  } while (0)
+
+int status_from(cudaError_t e) {
+  if (e == cudaSuccess) return NEMO_OK;
+  if (e == cudaErrorMemoryAllocation) return NEMO_ERR_ALLOC;
+  return NEMO_ERR_CUDA;
+}
+
+int set_device(nemo_ctx* c) {
+  if (c->device >= 0) CK(cudaSetDevice(c->device));
+  return NEMO_OK;
+}
+
+StateSet& nset(nemo_ctx* c) { return c->set[c->n_idx]; }
+StateSet& aset(nemo_ctx* c) { return c->set[1 - c->n_idx]; }
+
+RoutinePtrs rptrs(nemo_ctx* c) {
+  RoutinePtrs r;
+  r.sshn = nset(c).ssh;
+  r.un = nset(c).u;
+  r.vn = nset(c).v;
+  r.ssha = aset(c).ssh;
+  r.ua = aset(c).u;
+  r.va = aset(c).v;
+  r.sshn_u = c->sshn_u;
+  r.sshn_v = c->sshn_v;
+  r.ht = c->ht;
+  r.hu = c->hu;
+  r.hv = c->hv;
+  return r;
+}
+
+size_t field_bytes(const Layout& L) { return (size_t)L.elems() * sizeof(double); }
+
+// Before a per-routine kernel: bring stored sshn_u/sshn_v up to date, and
+// materialise the a-fields if the last step was fused.
+int prepare_routine(nemo_ctx* c, bool writes_a) {
+  if (c->uv_stale) {
+    CK(launch_derive_sshn_uv(c->L, c->C, nset(c).ssh, c->sshn_u, c->sshn_v, c->stream));
+    c->uv_stale = false;
+  }
+  if (writes_a && c->a_mirrors_n) {
+    size_t b = field_bytes(c->L);
+    CK(cudaMemcpyAsync(aset(c).ssh, nset(c).ssh, b, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(aset(c).u, nset(c).u, b, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(aset(c).v, nset(c).v, b, cudaMemcpyDeviceToDevice, c->stream));
+    c->a_mirrors_n = false;
+  }
+  return NEMO_OK;
+}
+
+// Fortran bounds of each field: x from i0 (nx points), y from j0 (ny points).
+bool field_window(const nemo_ctx* c, int f, int* i0, int* nx, int* j0, int* ny) {
+  const int jpi = c->L.jpi, jpj = c->L.jpj;
+  *i0 = 1; *nx = jpi; *j0 = 1; *ny = jpj;
+  switch (f) {
+    case NEMO_SSHN: case NEMO_SSHA: case NEMO_HT: case NEMO_XT: case NEMO_YT: return true;
+    case NEMO_UN: case NEMO_UA: case NEMO_SSHN_U: case NEMO_HU: *i0 = 0; *nx = jpi + 1; return true;
+    case NEMO_VN: case NEMO_VA: case NEMO_SSHN_V: case NEMO_HV: *j0 = 0; *ny = jpj + 1; return true;
+    default: return false;
+  }
+}
+
+double* field_storage(nemo_ctx* c, int f) {
+  switch (f) {
+    case NEMO_SSHN: return nset(c).ssh;
+    case NEMO_UN: return nset(c).u;
+    case NEMO_VN: return nset(c).v;
+    case NEMO_SSHA: return c->a_mirrors_n ? nset(c).ssh : aset(c).ssh;
+    case NEMO_UA: return c->a_mirrors_n ? nset(c).u : aset(c).u;
+    case NEMO_VA: return c->a_mirrors_n ? nset(c).v : aset(c).v;
+    case NEMO_SSHN_U: return c->sshn_u;
+    case NEMO_SSHN_V: return c->sshn_v;
+    case NEMO_HT: return c->ht;
+    case NEMO_HU: return c->hu;
+    case NEMO_HV: return c->hv;
+    default: return nullptr;
+  }
+}
+
+bool valid_params(const nemo_params* p) {
+  if (!p) return false;
+  if (p->jpi < 2 || p->jpj < 2 || p->jpi > (1 << 17) || p->jpj > (1 << 17)) return false;
+  if (!(p->dx > 0.0) || !(p->dy > 0.0) || !(p->rdt > 0.0)) return false;
+  if (p->nbump < 0 || p->nbump > 4096) return false;
+  if (p->nbump > 0 && !(p->bump_wmin > 0.0 && p->bump_wmax >= p->bump_wmin)) return false;
+  return true;
+}
+
+}  // namespace
+
+namespace nemo {
+
+Consts make_consts(const nemo_params& p) {
+  Consts C;
+  // original/nemolite2d.f90:210-217 (uniform grid) and :263-279 (areas)
+  C.e1t = C.e1u = C.e1v = p.dx;
+  C.e2t = C.e2u = C.e2v = p.dy;
+  C.e12t = C.e1t * C.e2t;
+  C.e12u = C.e1u * C.e2u;
+  C.e12v = C.e1v * C.e2v;
+  C.two_dx = C.e1v + C.e1v;
+  C.two_dy = C.e2u + C.e2u;
+  C.rdt = p.rdt;
+  C.visc = p.visc;
+  C.g = kG;
+  const double d2r = kPi / 180.0;
+  C.fcor = 2.0 * kOmega * sin(p.lat * d2r);
+  C.cfric = 1.0 + p.cbfr * p.rdt;
+  C.r_e1t = 1.0 / C.e1t;
+  C.r_e2t = 1.0 / C.e2t;
+  C.r_e12t = 1.0 / C.e12t;
+  C.r_e12u = 1.0 / C.e12u;
+  C.r_e12v = 1.0 / C.e12v;
+  C.r_2dx = 1.0 / C.two_dx;
+  C.r_2dy = 1.0 / C.two_dy;
+  C.r_cfric = 1.0 / C.cfric;
+  return C;
+}
+
+// amp*sin(omega_tide*rtime + phase), omega_tide as original/nemolite2d.f90:630
+double tide_value(const nemo_params& p, int istp) {
+  const double omega_tide = 2.0 * 3.14159 / (12.42 * 3600.0);
+  double rtime = (double)istp * p.rdt;
+  return p.amp_tide * sin(omega_tide * rtime + p.tide_phase);
+}
+
+static double tide_at_time(const nemo_params& p, double rtime) {
+  const double omega_tide = 2.0 * 3.14159 / (12.42 * 3600.0);
+  return p.amp_tide * sin(omega_tide * rtime + p.tide_phase);
+}
+
+// Seeded Gaussian bumps: SplitMix64 (Steele, Lea & Flood 2014) draws centre,
+// amplitude and width of each bump; each bump is separable and tabulated on
+// the half-grid x_k = k*dx/2 with the host libm exp.
+static uint64_t smix_next(uint64_t* s) {
+  uint64_t z = (*s += 0x9E3779B97F4A7C15ULL);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  return z ^ (z >> 31);
+}
+static double smix_unif(uint64_t* s) { return (double)(smix_next(s) >> 11) * 0x1.0p-53; }
+
+void depth_tables(const nemo_params& p, double* ax, double* gy) {
+  const int nkx = 2 * p.jpi + 2, nky = 2 * p.jpj + 2;
+  uint64_t s = p.seed;
+  const double lx = (double)p.jpi * p.dx, ly = (double)p.jpj * p.dy;
+  const double hdx = 0.5 * p.dx, hdy = 0.5 * p.dy;
+  for (int b = 0; b < p.nbump; ++b) {
+    double xc = smix_unif(&s) * lx;
+    double yc = smix_unif(&s) * ly;
+    double amp = p.bump_amp * (2.0 * smix_unif(&s) - 1.0);
+    double w = p.bump_wmin + (p.bump_wmax - p.bump_wmin) * smix_unif(&s);
+    for (int k = 0; k < nkx; ++k) {
+      double t = ((double)k * hdx - xc) / w;
+      ax[(size_t)b * nkx + k] = amp * exp(-(t * t));
+    }
+    for (int k = 0; k < nky; ++k) {
+      double t = ((double)k * hdy - yc) / w;
+      gy[(size_t)b * nky + k] = exp(-(t * t));
+    }
+  }
+}
+
+}  // namespace nemo
+
+extern "C" {
+
+int nemo_default_params(nemo_params* p) {
+  if (!p) return NEMO_ERR_INVALID;
+  memset(p, 0, sizeof(*p));
+  // original/nemolite2d.f90:107-118 (jpiglo = jpjglo = 258)
+  p->jpi = 256;
+  p->jpj = 256;
+  p->dx = 1000.0;
+  p->dy = 1000.0;
+  p->dep_const = 100.0;
+  p->nit000 = 1;
+  p->nitend = 1000;
+  p->irecord = 1;
+  p->rdt = 10.0;
+  p->cbfr = 0.001;
+  p->visc = 100.0;
+  p->amp_tide = 0.2;
+  p->tide_phase = 0.0;
+  p->lat = 50.0;
+  p->nbump = 0;
+  p->seed = 1234;
+  p->bump_amp = 40.0;
+  p->bump_wmin = 20.0e3;
+  p->bump_wmax = 200.0e3;
+  p->hmin = 10.0;
+  p->hmax = 1.0e30;
+  p->stream = nullptr;
+  p->device = -1;
+  return NEMO_OK;
+}
+
+int nemo_destroy(nemo_ctx* c) {
+  if (!c) return NEMO_ERR_INVALID;
+  if (c->device >= 0) cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->slab) cudaFree(c->slab);
+  if (c->ck_host) cudaFreeHost(c->ck_host);
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return NEMO_OK;
+}
+
+int nemo_create(const nemo_params* p, nemo_ctx** out) {
+  if (!out) return NEMO_ERR_INVALID;
+  *out = nullptr;
+  if (!valid_params(p)) return NEMO_ERR_INVALID;
+  nemo_ctx* c = new (std::nothrow) nemo_ctx();
+  if (!c) return NEMO_ERR_ALLOC;
+  c->p = *p;
+  c->device = p->device;
+  c->L.jpi = p->jpi;
+  c->L.jpj = p->jpj;
+  c->L.pitch = layout_pitch(p->jpi);
+  c->L.rows = (long)p->jpj + 3;
+  c->C = make_consts(*p);
+  c->tile_x = 128;
+  c->tile_y = 64;
+  int st = set_device(c);
+  if (st) { delete c; return st; }
+  cudaError_t e;
+  if (p->stream) {
+    c->stream = (cudaStream_t)p->stream;
+    c->own_stream = false;
+  } else {
+    e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { delete c; return status_from(e); }
+    c->own_stream = true;
+  }
+  const size_t fe = (size_t)c->L.elems();
+  const size_t ck = 4 * (size_t)p->jpj + 4;
+  const size_t total = 11 * fe + ck;
+  e = cudaMalloc(&c->slab, total * sizeof(double));
+  if (e != cudaSuccess) { c->slab = nullptr; nemo_destroy(c); cudaGetLastError(); return NEMO_ERR_ALLOC; }
+  e = cudaMallocHost(&c->ck_host, 4 * sizeof(double));
+  if (e != cudaSuccess) { c->ck_host = nullptr; nemo_destroy(c); cudaGetLastError(); return NEMO_ERR_ALLOC; }
+  double* q = c->slab;
+  for (int s = 0; s < 2; ++s) {
+    c->set[s].ssh = q; q += fe;
+    c->set[s].u = q; q += fe;
+    c->set[s].v = q; q += fe;
+  }
+  c->sshn_u = q; q += fe;
+  c->sshn_v = q; q += fe;
+  c->ht = q; q += fe;
+  c->hu = q; q += fe;
+  c->hv = q; q += fe;
+  c->ck_partials = q; q += 4 * (size_t)p->jpj;
+  c->ck_out = q;
+  c->n_idx = 0;
+  c->a_mirrors_n = false;
+  c->uv_stale = false;
+
+  // allocation (:310-318): everything starts at zero
+  e = cudaMemsetAsync(c->slab, 0, total * sizeof(double), c->stream);
+  if (e != cudaSuccess) { nemo_destroy(c); return status_from(e); }
+  // grid: depth (:238-254 or seeded bumps)
+  double* tab = nullptr;
+  if (p->nbump > 0) {
+    const size_t nax = (size_t)p->nbump * (2 * p->jpi + 2), ngy = (size_t)p->nbump * (2 * p->jpj + 2);
+    std::vector<double> h(nax + ngy);
+    depth_tables(*p, h.data(), h.data() + nax);
+    e = cudaMalloc(&tab, (nax + ngy) * sizeof(double));
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(tab, h.data(), (nax + ngy) * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess)
+      e = launch_depth(c->L, p->dep_const, p->nbump, tab, tab + nax, p->hmin, p->hmax, c->ht, c->hu, c->hv, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (tab) cudaFree(tab);
+  } else {
+    e = launch_depth(c->L, p->dep_const, 0, nullptr, nullptr, p->hmin, p->hmax, c->ht, c->hu, c->hv, c->stream);
+  }
+  // initialisation (:331-365): sshn = un = vn = 0, sshn_u/sshn_v averaged
+  if (e == cudaSuccess)
+    e = launch_init_sshn_uv(c->L, c->C, nset(c).ssh, c->sshn_u, c->sshn_v, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) { nemo_destroy(c); return status_from(e); }
+  *out = c;
+  return NEMO_OK;
+}
+
+int nemo_continuity(nemo_ctx* c) {
+  if (!c) return NEMO_ERR_STATE;
+  int st = set_device(c); if (st) return st;
+  st = prepare_routine(c, true); if (st) return st;
+  CK(launch_continuity(c->L, c->C, rptrs(c), c->stream));
+  return NEMO_OK;
+}
+
+int nemo_momentum_u(nemo_ctx* c) {
+  if (!c) return NEMO_ERR_STATE;
+  int st = set_device(c); if (st) return st;
+  st = prepare_routine(c, true); if (st) return st;
+  CK(launch_momentum_u(c->L, c->C, rptrs(c), c->stream));
+  return NEMO_OK;
+}
+
+int nemo_momentum_v(nemo_ctx* c) {
+  if (!c) return NEMO_ERR_STATE;
+  int st = set_device(c); if (st) return st;
+  st = prepare_routine(c, true); if (st) return st;
+  CK(launch_momentum_v(c->L, c->C, rptrs(c), c->stream));
+  return NEMO_OK;
+}
+
+int nemo_momentum(nemo_ctx* c) {
+  int st = nemo_momentum_u(c);
+  return st ? st : nemo_momentum_v(c);
+}
+
+int nemo_bc_ssh(nemo_ctx* c, double rtime) {
+  if (!c) return NEMO_ERR_STATE;
+  int st = set_device(c); if (st) return st;
+  st = prepare_routine(c, true); if (st) return st;
+  CK(launch_bc_ssh(c->L, tide_at_time(c->p, rtime), aset(c).ssh, c->stream));
+  return NEMO_OK;
+}
+
+int nemo_bc_solid_u(nemo_ctx* c) {
+  if (!c) return NEMO_ERR_STATE;
+  int st = set_device(c); if (st) return st;
+  st = prepare_routine(c, true); if (st) return st;
+  CK(launch_bc_solid_u(c->L, aset(c).u, c->stream));
+  return NEMO_OK;
+}
+
+int nemo_bc_solid_v(nemo_ctx* c) {
+  if (!c) return NEMO_ERR_STATE;
+  int st = set_device(c); if (st) return st;
+  st = prepare_routine(c, true); if (st) return st;
+  CK(launch_bc_solid_v(c->L, aset(c).v, c->stream));
+  return NEMO_OK;
+}
+
+int nemo_bc_flather_u(nemo_ctx* c) {
+  if (!c) return NEMO_ERR_STATE;
+  int st = set_device(c); if (st) return st;
+  st = prepare_routine(c, true); if (st) return st;
+  CK(launch_bc_flather_u(c->L, rptrs(c), c->stream));
+  return NEMO_OK;
+}
+
+int nemo_bc_flather_v(nemo_ctx* c) {
+  if (!c) return NEMO_ERR_STATE;
+  int st = set_device(c); if (st) return st;
+  st = prepare_routine(c, true); if (st) return st;
+  CK(launch_bc_flather_v(c->L, rptrs(c), c->stream));
+  return NEMO_OK;
+}
+
+int nemo_bc(nemo_ctx* c, double rtime) {
+  int st;
+  if ((st = nemo_bc_ssh(c, rtime))) return st;
+  if ((st = nemo_bc_solid_u(c))) return st;
+  if ((st = nemo_bc_solid_v(c))) return st;
+  if ((st = nemo_bc_flather_u(c))) return st;
+  return nemo_bc_flather_v(c);
+}
+
+int nemo_next(nemo_ctx* c) {
+  if (!c) return NEMO_ERR_STATE;
+  int st = set_device(c); if (st) return st;
+  st = prepare_routine(c, true); if (st) return st;
+  CK(launch_copy_next(c->L, rptrs(c), c->stream));
+  CK(launch_derive_sshn_uv(c->L, c->C, nset(c).ssh, c->sshn_u, c->sshn_v, c->stream));
+  return NEMO_OK;
+}
+
+int nemo_step(nemo_ctx* c, int istp) {
+  if (!c) return NEMO_ERR_STATE;
+  double rtime = (double)istp * c->p.rdt;  // original/nemolite2d.f90:378
+  int st;
+  if ((st = nemo_continuity(c))) return st;
+  if ((st = nemo_momentum(c))) return st;
+  if ((st = nemo_bc(c, rtime))) return st;
+  return nemo_next(c);
+}
+
+int nemo_step_n(nemo_ctx* c, int istp0, int n) {
+  if (!c) return NEMO_ERR_STATE;
+  if (n < 0) return NEMO_ERR_INVALID;
+  if (n == 0) return NEMO_OK;
+  int st = set_device(c); if (st) return st;
+  for (int k = 0; k < n; ++k) {
+    FusedArgs a;
+    a.sshn = nset(c).ssh;
+    a.un = nset(c).u;
+    a.vn = nset(c).v;
+    a.ht = c->ht;
+    a.hu = c->hu;
+    a.hv = c->hv;
+    a.sshv0 = c->sshn_v;
+    a.ssha = aset(c).ssh;
+    a.ua = aset(c).u;
+    a.va = aset(c).v;
+    a.tide = tide_value(c->p, istp0 + k);
+    CK(launch_fused_step(c->L, c->C, a, c->tile_x, c->tile_y, c->stream));
+    c->n_idx = 1 - c->n_idx;  // next: the new state becomes "now"
+  }
+  c->a_mirrors_n = true;
+  c->uv_stale = true;
+  return NEMO_OK;
+}
+
+int nemo_checksum(nemo_ctx* c, int field, double* out) {
+  if (!c || !out) return NEMO_ERR_INVALID;
+  double* f = field_storage(c, field);
+  if (!f || field == NEMO_XT || field == NEMO_YT) return NEMO_ERR_INVALID;
+  int st = set_device(c); if (st) return st;
+  if ((field == NEMO_SSHN_U || field == NEMO_SSHN_V) && (st = prepare_routine(c, false))) return st;
+  const double* fl[1] = {f};
+  CK(launch_checksums(c->L, fl, 1, c->ck_partials, c->ck_out, c->stream));
+  CK(cudaMemcpyAsync(c->ck_host, c->ck_out, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  *out = c->ck_host[0];
+  return NEMO_OK;
+}
+
+int nemo_checksums(nemo_ctx* c, double out[3]) {
+  if (!c || !out) return NEMO_ERR_INVALID;
+  int st = set_device(c); if (st) return st;
+  const double* fl[3] = {nset(c).ssh, nset(c).u, nset(c).v};
+  CK(launch_checksums(c->L, fl, 3, c->ck_partials, c->ck_out, c->stream));
+  CK(cudaMemcpyAsync(c->ck_host, c->ck_out, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (int k = 0; k < 3; ++k) out[k] = c->ck_host[k];
+  return NEMO_OK;
+}
+
+int nemo_retrieve(nemo_ctx* c, int field, double* host, long ld) {
+  if (!c || !host) return NEMO_ERR_INVALID;
+  int i0, nx, j0, ny;
+  if (!field_window(c, field, &i0, &nx, &j0, &ny)) return NEMO_ERR_INVALID;
+  if (ld < nx) return NEMO_ERR_INVALID;
+  if (field == NEMO_XT || field == NEMO_YT) {
+    // grid, :224-233: xt(1,:) = 0 + 0.5*e1t, xt(ji) = xt(ji-1) + dx (same for yt)
+    const double dx = c->p.dx, dy = c->p.dy;
+    for (int jj = 0; jj < ny; ++jj) {
+      double yv = 0.0 + 0.5 * dy;
+      for (int k = 1; k <= jj; ++k) yv = yv + dy;
+      double xv = 0.0 + 0.5 * dx;
+      for (int ii = 0; ii < nx; ++ii) {
+        if (ii > 0) xv = xv + dx;
+        host[(long)jj * ld + ii] = (field == NEMO_XT) ? xv : yv;
+      }
+    }
+    return NEMO_OK;
+  }
+  int st = set_device(c); if (st) return st;
+  if ((field == NEMO_SSHN_U || field == NEMO_SSHN_V) && (st = prepare_routine(c, false))) return st;
+  double* f = field_storage(c, field);
+  const double* src = f + c->L.idx(i0, j0);
+  CK(cudaMemcpy2DAsync(host, (size_t)ld * sizeof(double), src, (size_t)c->L.pitch * sizeof(double),
+                       (size_t)nx * sizeof(double), (size_t)ny, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return NEMO_OK;
+}
+
+int nemo_set_state(nemo_ctx* c, const double* sshn, const double* un, const double* vn) {
+  if (!c || !sshn || !un || !vn) return NEMO_ERR_INVALID;
+  int st = set_device(c); if (st) return st;
+  if ((st = prepare_routine(c, true))) return st;
+  const Layout& L = c->L;
+  const size_t P = (size_t)L.pitch * sizeof(double);
+  CK(cudaMemcpy2DAsync(nset(c).ssh + L.idx(1, 1), P, sshn, (size_t)L.jpi * sizeof(double),
+                       (size_t)L.jpi * sizeof(double), (size_t)L.jpj, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpy2DAsync(nset(c).u + L.idx(0, 1), P, un, (size_t)(L.jpi + 1) * sizeof(double),
+                       (size_t)(L.jpi + 1) * sizeof(double), (size_t)L.jpj, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpy2DAsync(nset(c).v + L.idx(1, 0), P, vn, (size_t)L.jpi * sizeof(double),
+                       (size_t)L.jpi * sizeof(double), (size_t)(L.jpj + 1), cudaMemcpyHostToDevice, c->stream));
+  CK(launch_derive_sshn_uv(L, c->C, nset(c).ssh, c->sshn_u, c->sshn_v, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->uv_stale = false;
+  return NEMO_OK;
+}
+
+int nemo_sync(nemo_ctx* c) {
+  if (!c) return NEMO_ERR_STATE;
+  int st = set_device(c); if (st) return st;
+  CK(cudaStreamSynchronize(c->stream));
+  return NEMO_OK;
+}
+
+int nemo_get_dims(nemo_ctx* c, int* jpi, int* jpj) {
+  if (!c || !jpi || !jpj) return NEMO_ERR_INVALID;
+  *jpi = c->L.jpi;
+  *jpj = c->L.jpj;
+  return NEMO_OK;
+}
+
+int nemo_device_field(nemo_ctx* c, int field, double** ptr, long* pitch) {
+  if (!c || !ptr || !pitch) return NEMO_ERR_INVALID;
+  double* f = field_storage(c, field);
+  if (!f) return NEMO_ERR_INVALID;
+  if (field == NEMO_SSHN_U || field == NEMO_SSHN_V) {
+    int st = set_device(c); if (st) return st;
+    if ((st = prepare_routine(c, false))) return st;
+  }
+  *ptr = f;
+  *pitch = c->L.pitch;
+  return NEMO_OK;
+}
+
+int nemo_set_tile(nemo_ctx* c, int tx, int ty) {
+  if (!c) return NEMO_ERR_STATE;
+  if (tx == 0) tx = 128;
+  if (ty == 0) ty = 64;
+  if (!(tx == 64 || tx == 128 || tx == 256) || ty < 1 || ty > 4096) return NEMO_ERR_INVALID;
+  c->tile_x = tx;
+  c->tile_y = ty;
+  return NEMO_OK;
+}
+
+int nemo_get_tile(nemo_ctx* c, int* tx, int* ty) {
+  if (!c || !tx || !ty) return NEMO_ERR_INVALID;
+  *tx = c->tile_x;
+  *ty = c->tile_y;
+  return NEMO_OK;
+}
+
+const char* nemo_status_string(int s) {
+  switch (s) {
+    case NEMO_OK: return "ok";
+    case NEMO_ERR_INVALID: return "invalid argument";
+    case NEMO_ERR_CUDA: return "CUDA runtime error";
+    case NEMO_ERR_ALLOC: return "allocation failed";
+    case NEMO_ERR_STATE: return "invalid state";
+    case NEMO_ERR_TIMEOUT: return "device wait timed out";
+    case NEMO_ERR_UNSUPPORTED: return "unsupported";
+    default: return "unknown status";
+  }
+}
+
+int nemo_build_is_strict(void) {
+#ifdef NEMO_STRICT_BUILD
+  return 1;
+#else
+  return 0;
+#endif
+}
+
+// ---- drop-in symbols: one default context, as the reference's globals -----
+static nemo_params g_params;
+static bool g_params_set = false;
+static nemo_ctx* g_ctx = nullptr;
+static int g_status = NEMO_OK;
+
+static void compat_fail(const char* where, int st) {
+  if (st == NEMO_OK) return;
+  if (g_status == NEMO_OK) g_status = st;
+  fprintf(stderr, "[nemo_b200] %s: %s\n", where, nemo_status_string(st));
+}
+
+int nemo_compat_last_status(void) { return g_status; }
+nemo_ctx* nemo_compat_context(void) { return g_ctx; }
+
+void cuda_setup_model_params_(int jpi, int jpj, double dx, double dy, double dep_const,
+                              int nit000, int nitend, int irecord, double rdt, double cbfr,
+                              double visc) {
+  nemo_default_params(&g_params);
+  g_params.jpi = jpi;
+  g_params.jpj = jpj;
+  g_params.dx = dx;
+  g_params.dy = dy;
+  g_params.dep_const = dep_const;
+  g_params.nit000 = nit000;
+  g_params.nitend = nitend;
+  g_params.irecord = irecord;
+  g_params.rdt = rdt;
+  g_params.cbfr = cbfr;
+  g_params.visc = visc;
+  g_params_set = true;
+  g_status = NEMO_OK;
+}
+
+void cuda_initialise_grid_(void) {
+  if (!g_params_set) {
+    // the reference only printed here (cuda/cuda_nemolite2d.cu:298-303)
+    compat_fail("cuda_initialise_grid_ (have you set up model params?)", NEMO_ERR_STATE);
+    return;
+  }
+  if (g_ctx) { nemo_destroy(g_ctx); g_ctx = nullptr; }
+  compat_fail("cuda_initialise_grid_", nemo_create(&g_params, &g_ctx));
+}
+
+void cuda_continuity_(void) { compat_fail("cuda_continuity_", g_ctx ? nemo_continuity(g_ctx) : NEMO_ERR_STATE); }
+void cuda_momentum_(void) { compat_fail("cuda_momentum_", g_ctx ? nemo_momentum(g_ctx) : NEMO_ERR_STATE); }
+void cuda_boundary_conditions_(double rtime) {
+  compat_fail("cuda_boundary_conditions_", g_ctx ? nemo_bc(g_ctx, rtime) : NEMO_ERR_STATE);
+}
+void cuda_next_(void) { compat_fail("cuda_next_", g_ctx ? nemo_next(g_ctx) : NEMO_ERR_STATE); }
+
+void cuda_retrieve_grid_constants_(double* xt, double* yt, double* ht, int jpi, int jpj) {
+  if (!g_ctx || jpi != g_ctx->L.jpi || jpj != g_ctx->L.jpj) {
+    compat_fail("cuda_retrieve_grid_constants_", g_ctx ? NEMO_ERR_INVALID : NEMO_ERR_STATE);
+    return;
+  }
+  compat_fail("cuda_retrieve_grid_constants_", nemo_retrieve(g_ctx, NEMO_XT, xt, jpi));
+  compat_fail("cuda_retrieve_grid_constants_", nemo_retrieve(g_ctx, NEMO_YT, yt, jpi));
+  compat_fail("cuda_retrieve_grid_constants_", nemo_retrieve(g_ctx, NEMO_HT, ht, jpi));
+}
+
+void cuda_retrieve_results_(double* sshn, double* un, double* vn, double* ua, double* va, int jpi,
+                            int jpj) {
+  if (!g_ctx || jpi != g_ctx->L.jpi || jpj != g_ctx->L.jpj) {
+    compat_fail("cuda_retrieve_results_", g_ctx ? NEMO_ERR_INVALID : NEMO_ERR_STATE);
+    return;
+  }
+  compat_fail("cuda_retrieve_results_", nemo_retrieve(g_ctx, NEMO_SSHN, sshn, jpi));
+  compat_fail("cuda_retrieve_results_", nemo_retrieve(g_ctx, NEMO_UN, un, jpi + 1));
+  compat_fail("cuda_retrieve_results_", nemo_retrieve(g_ctx, NEMO_VN, vn, jpi));
+  compat_fail("cuda_retrieve_results_", nemo_retrieve(g_ctx, NEMO_UA, ua, jpi + 1));
+  compat_fail("cuda_retrieve_results_", nemo_retrieve(g_ctx, NEMO_VA, va, jpi));
+}
+
+void cuda_finalise_(void) {
+  if (g_ctx) nemo_destroy(g_ctx);
+  g_ctx = nullptr;
+  g_params_set = false;
+}
+
+}  // extern "C"

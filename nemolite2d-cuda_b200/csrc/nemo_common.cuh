@@ -1,0 +1,102 @@
+// Shared device definitions: storage layout, run constants and the exact
+// arithmetic helpers used by the NEMOLite2D kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace nemo {
+
+// original/nemolite2d.f90:15-18
+constexpr double kPi = 3.1415926535897932;
+constexpr double kG = 9.80665;
+constexpr double kOmega = 7.292116e-05;
+
+// Storage of every 2-D field: one pitched array over ji in [-1, pitch-2],
+// jj in [-1, jpj+1]; element (ji,jj) at base[(jj+1)*pitch + ji+1].  Fortran
+// bounds (0:jpi,1:jpj) etc. are windows of it, so the C-grid staggering
+// needs no per-field index arithmetic.  pitch is a multiple of 32 doubles,
+// so rows start on 256-byte boundaries and ji odd starts a 16-byte pair.
+struct Layout {
+  int jpi, jpj;
+  long pitch;
+  long rows;  // jpj + 3
+  __host__ __device__ __forceinline__ long idx(int ji, int jj) const {
+    return (long)(jj + 1) * pitch + (ji + 1);
+  }
+  __host__ __device__ long elems() const { return rows * pitch; }
+};
+
+inline long layout_pitch(int jpi) { return ((long)(jpi + 4) + 31) / 32 * 32; }
+
+// Per-run constants.  The reference's grid is uniform (original/nemolite2d.f90
+// :210-217): every e1* equals dx, every e2* equals dy, every e12* equals
+// dx*dy.  Products, sums and sines are formed on the host exactly as the
+// Fortran forms them, so device and host agree bit for bit.
+struct Consts {
+  double e1t, e2t, e1u, e2u, e1v, e2v;
+  double e12t, e12u, e12v;
+  double two_dx, two_dy;     // e1v(i)+e1v(i+1), e2u(j)+e2u(j+1)
+  double rdt, visc, g;
+  double fcor;               // 2*omega*SIN(gphi*d2r), :503, :594
+  double cfric;              // 1 + cbfr*rdt, :514, :606
+  // round-to-nearest reciprocals for the corrected constant divisions
+  double r_e1t, r_e2t, r_e12t, r_e12u, r_e12v, r_2dx, r_2dy, r_cfric;
+};
+
+// Mask of original/nemolite2d.f90:184-202: 1 water, 0 land (west, east and
+// north walls), -1 open water outside the domain (south row).
+__host__ __device__ __forceinline__ int ptmask(int ji, int jj, int jpi, int jpj) {
+  if (ji <= 0 || ji >= jpi + 1 || jj >= jpj + 1) return 0;
+  if (jj <= 0) return -1;
+  return 1;
+}
+
+// Quotient a/b correctly rounded, given rb = RN(1/b) formed on the host.
+// Markstein's theorem (IBM J. Res. Dev. 34(1), 1990): with q = RN(a*rb) and
+// the exact remainder r = a - b*q (one fma), RN(q + r*rb) = RN(a/b) whenever
+// no intermediate underflows or overflows.  Quotients whose exponent is
+// below 2^-959, or infinite/NaN, take the IEEE division instead.  Writing
+// the last step as -fma(-r, rb, -q) keeps the sign of a zero quotient.
+__device__ __forceinline__ double div_const(double a, double b, double rb) {
+  double q = __dmul_rn(a, rb);
+  unsigned e = ((unsigned)__double2hiint(q) >> 20) & 0x7ffu;
+  if (e - 64u >= 0x7ffu - 64u) return a / b;
+  double r = fma(-q, b, a);
+  return -fma(-r, rb, -q);
+}
+
+constexpr unsigned long long kSign = 0x8000000000000000ull;
+
+// (+0 * other) + main, exactly: main unless main is a zero, in which case
+// the zero is negative only when both operands are negative.
+__device__ __forceinline__ double zplus(double main, double other) {
+  unsigned long long mb = (unsigned long long)__double_as_longlong(main);
+  unsigned long long ob = (unsigned long long)__double_as_longlong(other);
+  unsigned long long r = (mb << 1) ? mb : (mb & ob & kSign);
+  return __longlong_as_double((long long)r);
+}
+
+__device__ __forceinline__ bool sign_clear(double w) { return __double2hiint(w) >= 0; }
+
+// First-order upwind value across a face with normal velocity w, lo/hi the
+// values on the low/high-index side.  Equals, bit for bit,
+//   (0.5 + SIGN(0.5,w))*lo + (0.5 - SIGN(0.5,w))*hi
+// (original/nemolite2d.f90:454-471, :542-559) for finite operands: the two
+// coefficients are exactly 1 and +0.
+__device__ __forceinline__ double upwind(double w, double lo, double hi) {
+  bool pos = sign_clear(w);
+  return pos ? zplus(lo, hi) : zplus(hi, lo);
+}
+// (0.5 - SIGN(0.5,w))*hi alone (the slip-wall forms at :460, :548)
+__device__ __forceinline__ double upwind_hi_only(double w, double hi) {
+  unsigned long long hb = (unsigned long long)__double_as_longlong(hi);
+  return sign_clear(w) ? __longlong_as_double((long long)(hb & kSign)) : hi;
+}
+// (0.5 + SIGN(0.5,w))*lo alone (:467, :555)
+__device__ __forceinline__ double upwind_lo_only(double w, double lo) {
+  unsigned long long lb = (unsigned long long)__double_as_longlong(lo);
+  return sign_clear(w) ? lo : __longlong_as_double((long long)(lb & kSign));
+}
+
+}  // namespace nemo

@@ -1,0 +1,62 @@
+// Host-side internals shared by the library's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "nemo_b200.h"
+#include "nemo_common.cuh"
+
+namespace nemo {
+
+// Device pointers of one state set (the reference's "n" or "a" fields).
+struct StateSet {
+  double* ssh;
+  double* u;
+  double* v;
+};
+
+struct RoutinePtrs {
+  double *sshn, *un, *vn, *ssha, *ua, *va, *sshn_u, *sshn_v, *ht, *hu, *hv;
+};
+
+// ---- launchers (asynchronous on `s`) -------------------------------------
+cudaError_t launch_depth(const Layout& L, double dep_const, int nbump, const double* ax,
+                         const double* gy, double hmin, double hmax, double* ht,
+                         double* hu, double* hv, cudaStream_t s);
+cudaError_t launch_init_sshn_uv(const Layout& L, const Consts& C, const double* sshn,
+                                double* sshn_u, double* sshn_v, cudaStream_t s);
+cudaError_t launch_continuity(const Layout& L, const Consts& C, const RoutinePtrs& p,
+                              cudaStream_t s);
+cudaError_t launch_momentum_u(const Layout& L, const Consts& C, const RoutinePtrs& p,
+                              cudaStream_t s);
+cudaError_t launch_momentum_v(const Layout& L, const Consts& C, const RoutinePtrs& p,
+                              cudaStream_t s);
+cudaError_t launch_bc_ssh(const Layout& L, double value, double* ssha, cudaStream_t s);
+cudaError_t launch_bc_solid_u(const Layout& L, double* ua, cudaStream_t s);
+cudaError_t launch_bc_solid_v(const Layout& L, double* va, cudaStream_t s);
+cudaError_t launch_bc_flather_u(const Layout& L, const RoutinePtrs& p, cudaStream_t s);
+cudaError_t launch_bc_flather_v(const Layout& L, const RoutinePtrs& p, cudaStream_t s);
+cudaError_t launch_copy_next(const Layout& L, const RoutinePtrs& p, cudaStream_t s);
+cudaError_t launch_derive_sshn_uv(const Layout& L, const Consts& C, const double* sshn,
+                                  double* sshn_u, double* sshn_v, cudaStream_t s);
+
+struct FusedArgs {
+  const double *sshn, *un, *vn, *ht, *hu, *hv;
+  const double* sshv0;  // stored sshn_v array (only its row jj=0 is read)
+  double *ssha, *ua, *va;
+  double tide;          // clamped SSH value for this step
+};
+cudaError_t launch_fused_step(const Layout& L, const Consts& C, const FusedArgs& a,
+                              int tile_x, int tile_y, cudaStream_t s);
+
+// Sums |f(1:jpi,1:jpj)| of nf fields into out[0..nf-1] (device), fixed order.
+// row_partials: nf*jpj doubles of scratch.
+cudaError_t launch_checksums(const Layout& L, const double* const* fields, int nf,
+                             double* row_partials, double* out, cudaStream_t s);
+
+// Host helpers.
+void depth_tables(const nemo_params& p, double* ax, double* gy);  // sizes nbump*(2*jpi+2), nbump*(2*jpj+2)
+double tide_value(const nemo_params& p, int istp);
+Consts make_consts(const nemo_params& p);
+
+}  // namespace nemo

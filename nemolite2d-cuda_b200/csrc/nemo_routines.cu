@@ -1,0 +1,393 @@
+// Per-routine kernels: one thread per grid point, each a statement-for-
+// statement rendering of one loop nest of original/nemolite2d.f90 (same
+// bounds, CYCLE conditions and left-to-right evaluation).  They serve the
+// routine-boundary API (continuity / momentum / bc / next called one by one,
+// as cuda/nemolite2d.f90:486-489 does) and initialisation.
+#include "nemo_internal.h"
+
+namespace nemo {
+namespace {
+
+constexpr int BX = 32, BY = 8;
+
+inline dim3 grid_for(int ni, int nj) {
+  return dim3((unsigned)((ni + BX - 1) / BX), (unsigned)((nj + BY - 1) / BY));
+}
+
+// SIGN(a,b), gfortran semantics
+__device__ __forceinline__ double fsign(double a, double b) { return copysign(fabs(a), b); }
+
+// Seeded bathymetry (no reference counterpart): depth at half-grid point
+// (kx,ky) = clamp(H0 + sum_b ax[b][kx]*gy[b][ky]), summed in b order with
+// separate roundings; uniform dep_const when nbump == 0 (:238-254).
+__device__ double depth_at(int kx, int ky, int nkx, int nky, double dep_const, int nbump,
+                           const double* ax, const double* gy, double hmin, double hmax) {
+  if (nbump <= 0) return dep_const;
+  double acc = 0.0;
+  for (int b = 0; b < nbump; ++b)
+    acc = __dadd_rn(acc, __dmul_rn(ax[(long)b * nkx + kx], gy[(long)b * nky + ky]));
+  double h = __dadd_rn(dep_const, acc);
+  h = h < hmin ? hmin : h;
+  h = h > hmax ? hmax : h;
+  return h;
+}
+
+__global__ void k_depth(Layout L, double dep_const, int nbump, const double* ax,
+                        const double* gy, double hmin, double hmax, double* ht, double* hu,
+                        double* hv) {
+  int ji = blockIdx.x * BX + threadIdx.x;     // 0..jpi
+  int jj = blockIdx.y * BY + threadIdx.y;     // 0..jpj
+  if (ji > L.jpi || jj > L.jpj) return;
+  int nkx = 2 * L.jpi + 2, nky = 2 * L.jpj + 2;
+  if (ji >= 1 && jj >= 1)
+    ht[L.idx(ji, jj)] = depth_at(2 * ji - 1, 2 * jj - 1, nkx, nky, dep_const, nbump, ax, gy, hmin, hmax);
+  if (jj >= 1)
+    hu[L.idx(ji, jj)] = depth_at(2 * ji, 2 * jj - 1, nkx, nky, dep_const, nbump, ax, gy, hmin, hmax);
+  if (ji >= 1)
+    hv[L.idx(ji, jj)] = depth_at(2 * ji - 1, 2 * jj, nkx, nky, dep_const, nbump, ax, gy, hmin, hmax);
+}
+
+// initialisation, original/nemolite2d.f90:337-353 (min/max-clamped averages)
+__global__ void k_init_sshn_uv(Layout L, Consts C, const double* sshn, double* sshn_u,
+                               double* sshn_v) {
+  int ji = blockIdx.x * BX + threadIdx.x;  // 0..jpi
+  int jj = blockIdx.y * BY + threadIdx.y;  // 0..jpj
+  const int jpi = L.jpi, jpj = L.jpj;
+  if (ji > jpi || jj > jpj) return;
+  if (jj >= 1) {
+    int i1 = min(ji + 1, jpi), i2 = max(ji, 1);
+    double r = C.e12t * sshn[L.idx(i1, jj)] + C.e12t * sshn[L.idx(i2, jj)];
+    sshn_u[L.idx(ji, jj)] = 0.5 * r / C.e12u;
+  }
+  if (ji >= 1) {
+    int j1 = min(jj + 1, jpj), j2 = max(jj, 1);
+    double r = C.e12t * sshn[L.idx(ji, j1)] + C.e12t * sshn[L.idx(ji, j2)];
+    sshn_v[L.idx(ji, jj)] = 0.5 * r / C.e12v;
+  }
+}
+
+// continuity, :397-405
+__global__ void k_continuity(Layout L, Consts C, RoutinePtrs p) {
+  int ji = 1 + blockIdx.x * BX + threadIdx.x;
+  int jj = 1 + blockIdx.y * BY + threadIdx.y;
+  if (ji > L.jpi || jj > L.jpj) return;
+  double r1 = (p.sshn_u[L.idx(ji, jj)] + p.hu[L.idx(ji, jj)]) * p.un[L.idx(ji, jj)];
+  double r2 = (p.sshn_u[L.idx(ji - 1, jj)] + p.hu[L.idx(ji - 1, jj)]) * p.un[L.idx(ji - 1, jj)];
+  double r3 = (p.sshn_v[L.idx(ji, jj)] + p.hv[L.idx(ji, jj)]) * p.vn[L.idx(ji, jj)];
+  double r4 = (p.sshn_v[L.idx(ji, jj - 1)] + p.hv[L.idx(ji, jj - 1)]) * p.vn[L.idx(ji, jj - 1)];
+  p.ssha[L.idx(ji, jj)] = p.sshn[L.idx(ji, jj)] + (r2 - r1 + r4 - r3) * C.rdt / C.e12t;
+}
+
+// momentum, u equation, :431-517 (ssha_u is identically zero, :37, :315)
+__global__ void k_momentum_u(Layout L, Consts C, RoutinePtrs p) {
+  int ji = 1 + blockIdx.x * BX + threadIdx.x;  // 1..jpi-1
+  int jj = 1 + blockIdx.y * BY + threadIdx.y;  // 1..jpj
+  const int jpi = L.jpi, jpj = L.jpj;
+  if (ji > jpi - 1 || jj > jpj) return;
+#define PT(a, b) ptmask((a), (b), jpi, jpj)
+#define F(arr, a, b) p.arr[L.idx((a), (b))]
+  if (PT(ji, jj) + PT(ji + 1, jj) <= 0) return;
+  if (PT(ji, jj) <= 0 || PT(ji + 1, jj) <= 0) return;
+
+  double u_e = 0.5 * (F(un, ji, jj) + F(un, ji + 1, jj)) * C.e2t;
+  double depe = F(ht, ji + 1, jj) + F(sshn, ji + 1, jj);
+  double u_w = 0.5 * (F(un, ji, jj) + F(un, ji - 1, jj)) * C.e2t;
+  double depw = F(ht, ji, jj) + F(sshn, ji, jj);
+
+  double v_sc = 0.5 * (F(vn, ji, jj - 1) + F(vn, ji + 1, jj - 1));
+  double v_s = 0.5 * v_sc * (C.e1v + C.e1v);
+  double deps = 0.5 * (F(hv, ji, jj - 1) + F(sshn_v, ji, jj - 1) + F(hv, ji + 1, jj - 1) +
+                       F(sshn_v, ji + 1, jj - 1));
+  double v_nc = 0.5 * (F(vn, ji, jj) + F(vn, ji + 1, jj));
+  double v_n = 0.5 * v_nc * (C.e1v + C.e1v);
+  double depn = 0.5 * (F(hv, ji, jj) + F(sshn_v, ji, jj) + F(hv, ji + 1, jj) + F(sshn_v, ji + 1, jj));
+
+  double uu_w = (0.5 - fsign(0.5, u_w)) * F(un, ji, jj) + (0.5 + fsign(0.5, u_w)) * F(un, ji - 1, jj);
+  double uu_e = (0.5 + fsign(0.5, u_e)) * F(un, ji, jj) + (0.5 - fsign(0.5, u_e)) * F(un, ji + 1, jj);
+  double uu_s, uu_n;
+  if (PT(ji, jj - 1) <= 0 || PT(ji + 1, jj - 1) <= 0)
+    uu_s = (0.5 - fsign(0.5, v_s)) * F(un, ji, jj);
+  else
+    uu_s = (0.5 - fsign(0.5, v_s)) * F(un, ji, jj) + (0.5 + fsign(0.5, v_s)) * F(un, ji, jj - 1);
+  if (PT(ji, jj + 1) <= 0 || PT(ji + 1, jj + 1) <= 0)
+    uu_n = (0.5 + fsign(0.5, v_n)) * F(un, ji, jj);
+  else
+    uu_n = (0.5 + fsign(0.5, v_n)) * F(un, ji, jj) + (0.5 - fsign(0.5, v_n)) * F(un, ji, jj + 1);
+
+  double adv = uu_w * u_w * depw - uu_e * u_e * depe + uu_s * v_s * deps - uu_n * v_n * depn;
+
+  double dudx_e = (F(un, ji + 1, jj) - F(un, ji, jj)) / C.e1t * (F(ht, ji + 1, jj) + F(sshn, ji + 1, jj));
+  double dudx_w = (F(un, ji, jj) - F(un, ji - 1, jj)) / C.e1t * (F(ht, ji, jj) + F(sshn, ji, jj));
+  double dudy_s, dudy_n;
+  if (PT(ji, jj - 1) <= 0 || PT(ji + 1, jj - 1) <= 0)
+    dudy_s = 0.0;
+  else
+    dudy_s = (F(un, ji, jj) - F(un, ji, jj - 1)) / (C.e2u + C.e2u) *
+             (F(hu, ji, jj) + F(sshn_u, ji, jj) + F(hu, ji, jj - 1) + F(sshn_u, ji, jj - 1));
+  if (PT(ji, jj + 1) <= 0 || PT(ji + 1, jj + 1) <= 0)
+    dudy_n = 0.0;
+  else
+    dudy_n = (F(un, ji, jj + 1) - F(un, ji, jj)) / (C.e2u + C.e2u) *
+             (F(hu, ji, jj) + F(sshn_u, ji, jj) + F(hu, ji, jj + 1) + F(sshn_u, ji, jj + 1));
+
+  double vis = (dudx_e - dudx_w) * C.e2u + (dudy_n - dudy_s) * C.e1u * 0.5;
+  vis = C.visc * vis;
+  double cor = 0.5 * (C.fcor * (v_sc + v_nc)) * C.e12u * (F(hu, ji, jj) + F(sshn_u, ji, jj));
+  double hpg = -(C.g * (F(hu, ji, jj) + F(sshn_u, ji, jj)) * C.e2u * (F(sshn, ji + 1, jj) - F(sshn, ji, jj)));
+  F(ua, ji, jj) = (F(un, ji, jj) * (F(hu, ji, jj) + F(sshn_u, ji, jj)) +
+                   C.rdt * (adv + vis + cor + hpg) / C.e12u) /
+                  (F(hu, ji, jj) + 0.0) / C.cfric;
+}
+
+// momentum, v equation, :520-609
+__global__ void k_momentum_v(Layout L, Consts C, RoutinePtrs p) {
+  int ji = 1 + blockIdx.x * BX + threadIdx.x;  // 1..jpi
+  int jj = 1 + blockIdx.y * BY + threadIdx.y;  // 1..jpj-1
+  const int jpi = L.jpi, jpj = L.jpj;
+  if (ji > jpi || jj > jpj - 1) return;
+  // the reference tests pt(ji+1,jj) here (:523); kept verbatim
+  if (PT(ji, jj) + PT(ji + 1, jj) <= 0) return;
+  if (PT(ji, jj) <= 0 || PT(ji, jj + 1) <= 0) return;
+
+  double v_n = 0.5 * (F(vn, ji, jj) + F(vn, ji, jj + 1)) * C.e1t;
+  double depn = F(ht, ji, jj + 1) + F(sshn, ji, jj + 1);
+  double v_s = 0.5 * (F(vn, ji, jj) + F(vn, ji, jj - 1)) * C.e1t;
+  double deps = F(ht, ji, jj) + F(sshn, ji, jj);
+
+  double u_wc = 0.5 * (F(un, ji - 1, jj) + F(un, ji - 1, jj + 1));
+  double u_w = 0.5 * u_wc * (C.e2u + C.e2u);
+  double depw = 0.50 * (F(hu, ji - 1, jj) + F(sshn_u, ji - 1, jj) + F(hu, ji - 1, jj + 1) +
+                        F(sshn_u, ji - 1, jj + 1));
+  double u_ec = 0.5 * (F(un, ji, jj) + F(un, ji, jj + 1));
+  double u_e = 0.5 * u_ec * (C.e2u + C.e2u);
+  double depe = 0.50 * (F(hu, ji, jj) + F(sshn_u, ji, jj) + F(hu, ji, jj + 1) + F(sshn_u, ji, jj + 1));
+
+  double vv_s = (0.5 - fsign(0.5, v_s)) * F(vn, ji, jj) + (0.5 + fsign(0.5, v_s)) * F(vn, ji, jj - 1);
+  double vv_n = (0.5 + fsign(0.5, v_n)) * F(vn, ji, jj) + (0.5 - fsign(0.5, v_n)) * F(vn, ji, jj + 1);
+  double vv_w, vv_e;
+  if (PT(ji - 1, jj) <= 0 || PT(ji - 1, jj + 1) <= 0)
+    vv_w = (0.5 - fsign(0.5, u_w)) * F(vn, ji, jj);
+  else
+    vv_w = (0.5 - fsign(0.5, u_w)) * F(vn, ji, jj) + (0.5 + fsign(0.5, u_w)) * F(vn, ji - 1, jj);
+  if (PT(ji + 1, jj) <= 0 || PT(ji + 1, jj + 1) <= 0)
+    vv_e = (0.5 + fsign(0.5, u_e)) * F(vn, ji, jj);
+  else
+    vv_e = (0.5 + fsign(0.5, u_e)) * F(vn, ji, jj) + (0.5 - fsign(0.5, u_e)) * F(vn, ji + 1, jj);
+
+  double adv = vv_w * u_w * depw - vv_e * u_e * depe + vv_s * v_s * deps - vv_n * v_n * depn;
+
+  double dvdy_n = (F(vn, ji, jj + 1) - F(vn, ji, jj)) / C.e2t * (F(ht, ji, jj + 1) + F(sshn, ji, jj + 1));
+  double dvdy_s = (F(vn, ji, jj) - F(vn, ji, jj - 1)) / C.e2t * (F(ht, ji, jj) + F(sshn, ji, jj));
+  double dvdx_w, dvdx_e;
+  if (PT(ji - 1, jj) <= 0 || PT(ji - 1, jj + 1) <= 0)
+    dvdx_w = 0.0;
+  else
+    dvdx_w = (F(vn, ji, jj) - F(vn, ji - 1, jj)) / (C.e1v + C.e1v) *
+             (F(hv, ji, jj) + F(sshn_v, ji, jj) + F(hv, ji - 1, jj) + F(sshn_v, ji - 1, jj));
+  if (PT(ji + 1, jj) <= 0 || PT(ji + 1, jj + 1) <= 0)
+    dvdx_e = 0.0;
+  else
+    dvdx_e = (F(vn, ji + 1, jj) - F(vn, ji, jj)) / (C.e1v + C.e1v) *
+             (F(hv, ji, jj) + F(sshn_v, ji, jj) + F(hv, ji + 1, jj) + F(sshn_v, ji + 1, jj));
+
+  double vis = (dvdy_n - dvdy_s) * C.e1v + (dvdx_e - dvdx_w) * C.e2v * 0.5;
+  vis = C.visc * vis;
+  double cor = -0.5 * (C.fcor * (u_ec + u_wc)) * C.e12v * (F(hv, ji, jj) + F(sshn_v, ji, jj));
+  double hpg = -(C.g * (F(hv, ji, jj) + F(sshn_v, ji, jj)) * C.e1v * (F(sshn, ji, jj + 1) - F(sshn, ji, jj)));
+  F(va, ji, jj) = (F(vn, ji, jj) * (F(hv, ji, jj) + F(sshn_v, ji, jj)) +
+                   C.rdt * (adv + vis + cor + hpg) / C.e12v) /
+                  ((F(hv, ji, jj) + 0.0)) / C.cfric;
+}
+
+// bc: clamped SSH, :631-644 (value = amp*sin(omega_tide*rtime) from the host)
+__global__ void k_bc_ssh(Layout L, double value, double* ssha) {
+  int ji = 1 + blockIdx.x * BX + threadIdx.x;
+  int jj = 1 + blockIdx.y * BY + threadIdx.y;
+  const int jpi = L.jpi, jpj = L.jpj;
+  if (ji > jpi || jj > jpj) return;
+  if (PT(ji, jj) <= 0) return;
+  if (PT(ji, jj - 1) < 0 || PT(ji, jj + 1) < 0 || PT(ji + 1, jj) < 0 || PT(ji - 1, jj) < 0)
+    ssha[L.idx(ji, jj)] = value;
+}
+
+// bc: solid u, :648-652
+__global__ void k_bc_solid_u(Layout L, double* ua) {
+  int ji = blockIdx.x * BX + threadIdx.x;      // 0..jpi
+  int jj = 1 + blockIdx.y * BY + threadIdx.y;  // 1..jpj
+  const int jpi = L.jpi, jpj = L.jpj;
+  if (ji > jpi || jj > jpj) return;
+  if (PT(ji, jj) * PT(ji + 1, jj) == 0) ua[L.idx(ji, jj)] = 0.0;
+}
+
+// bc: solid v, :656-660
+__global__ void k_bc_solid_v(Layout L, double* va) {
+  int ji = 1 + blockIdx.x * BX + threadIdx.x;  // 1..jpi
+  int jj = blockIdx.y * BY + threadIdx.y;      // 0..jpj
+  const int jpi = L.jpi, jpj = L.jpj;
+  if (ji > jpi || jj > jpj) return;
+  if (PT(ji, jj) * PT(ji, jj + 1) == 0) va[L.idx(ji, jj)] = 0.0;
+}
+
+// bc: Flather u, :669-680.  The reference sweeps ji in order, in place; one
+// thread per row keeps that order.
+__global__ void k_bc_flather_u(Layout L, RoutinePtrs p) {
+  int jj = 1 + blockIdx.x * blockDim.x + threadIdx.x;  // 1..jpj
+  const int jpi = L.jpi, jpj = L.jpj;
+  if (jj > jpj) return;
+  for (int ji = 0; ji <= jpi; ++ji) {
+    if (PT(ji, jj) + PT(ji + 1, jj) <= -1) continue;
+    if (PT(ji, jj) < 0) {
+      int jiu = ji + 1;
+      F(ua, ji, jj) = F(ua, jiu, jj) + sqrt(kG / F(hu, ji, jj)) * (F(sshn_u, ji, jj) - F(sshn_u, jiu, jj));
+    } else if (PT(ji + 1, jj) < 0) {
+      int jiu = ji - 1;
+      F(ua, ji, jj) = F(ua, jiu, jj) + sqrt(kG / F(hu, ji, jj)) * (F(sshn_u, ji, jj) - F(sshn_u, jiu, jj));
+    }
+  }
+}
+
+// bc: Flather v, :684-695.  In-place dependence runs along jj, so one thread
+// per column sweeps jj in the reference's order.
+__global__ void k_bc_flather_v(Layout L, RoutinePtrs p) {
+  int ji = 1 + blockIdx.x * blockDim.x + threadIdx.x;  // 1..jpi
+  const int jpi = L.jpi, jpj = L.jpj;
+  if (ji > jpi) return;
+  for (int jj = 0; jj <= jpj; ++jj) {
+    if (PT(ji, jj) + PT(ji, jj + 1) <= -1) continue;
+    if (PT(ji, jj) < 0) {
+      int jiv = jj + 1;
+      F(va, ji, jj) = F(va, ji, jiv) + sqrt(kG / F(hv, ji, jj)) * (F(sshn_v, ji, jj) - F(sshn_v, ji, jiv));
+    } else if (PT(ji, jj + 1) < 0) {
+      int jiv = jj - 1;
+      F(va, ji, jj) = F(va, ji, jiv) + sqrt(kG / F(hv, ji, jj)) * (F(sshn_v, ji, jj) - F(sshn_v, ji, jiv));
+    }
+  }
+}
+
+// next, copies, :712-732
+__global__ void k_copy_next(Layout L, RoutinePtrs p) {
+  int ji = blockIdx.x * BX + threadIdx.x;  // 0..jpi
+  int jj = blockIdx.y * BY + threadIdx.y;  // 0..jpj
+  const int jpi = L.jpi, jpj = L.jpj;
+  if (ji > jpi || jj > jpj) return;
+  if (jj >= 1) F(un, ji, jj) = F(ua, ji, jj);
+  if (ji >= 1) F(vn, ji, jj) = F(va, ji, jj);
+  if (ji >= 1 && jj >= 1) F(sshn, ji, jj) = F(ssha, ji, jj);
+}
+
+// next, sshn_u/sshn_v re-interpolation, :736-764
+__global__ void k_derive_sshn_uv(Layout L, Consts C, const double* sshn, double* sshn_u,
+                                 double* sshn_v) {
+  int ji = blockIdx.x * BX + threadIdx.x;  // 0..jpi
+  int jj = blockIdx.y * BY + threadIdx.y;  // 0..jpj
+  const int jpi = L.jpi, jpj = L.jpj;
+  if (ji > jpi || jj > jpj) return;
+  if (jj >= 1 && !(PT(ji, jj) + PT(ji + 1, jj) <= 0)) {
+    double v;
+    bool set = true;
+    if (PT(ji, jj) * PT(ji + 1, jj) > 0) {
+      double r = C.e12t * sshn[L.idx(ji, jj)] + C.e12t * sshn[L.idx(ji + 1, jj)];
+      v = 0.5 * r / C.e12u;
+    } else if (PT(ji, jj) <= 0) {
+      v = sshn[L.idx(ji + 1, jj)];
+    } else if (PT(ji + 1, jj) <= 0) {
+      v = sshn[L.idx(ji, jj)];
+    } else {
+      set = false;
+      v = 0.0;
+    }
+    if (set) sshn_u[L.idx(ji, jj)] = v;
+  }
+  if (ji >= 1 && !(PT(ji, jj) + PT(ji, jj + 1) <= 0)) {
+    double v;
+    bool set = true;
+    if (PT(ji, jj) * PT(ji, jj + 1) > 0) {
+      double r = C.e12t * sshn[L.idx(ji, jj)] + C.e12t * sshn[L.idx(ji, jj + 1)];
+      v = 0.5 * r / C.e12v;
+    } else if (PT(ji, jj) <= 0) {
+      v = sshn[L.idx(ji, jj + 1)];
+    } else if (PT(ji, jj + 1) <= 0) {
+      v = sshn[L.idx(ji, jj)];
+    } else {
+      set = false;
+      v = 0.0;
+    }
+    if (set) sshn_v[L.idx(ji, jj)] = v;
+  }
+}
+#undef PT
+#undef F
+
+}  // namespace
+
+cudaError_t launch_depth(const Layout& L, double dep_const, int nbump, const double* ax,
+                         const double* gy, double hmin, double hmax, double* ht, double* hu,
+                         double* hv, cudaStream_t s) {
+  k_depth<<<grid_for(L.jpi + 1, L.jpj + 1), dim3(BX, BY), 0, s>>>(L, dep_const, nbump, ax, gy,
+                                                                   hmin, hmax, ht, hu, hv);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_init_sshn_uv(const Layout& L, const Consts& C, const double* sshn,
+                                double* sshn_u, double* sshn_v, cudaStream_t s) {
+  k_init_sshn_uv<<<grid_for(L.jpi + 1, L.jpj + 1), dim3(BX, BY), 0, s>>>(L, C, sshn, sshn_u, sshn_v);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_continuity(const Layout& L, const Consts& C, const RoutinePtrs& p,
+                              cudaStream_t s) {
+  k_continuity<<<grid_for(L.jpi, L.jpj), dim3(BX, BY), 0, s>>>(L, C, p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_momentum_u(const Layout& L, const Consts& C, const RoutinePtrs& p,
+                              cudaStream_t s) {
+  if (L.jpi < 2) return cudaSuccess;
+  k_momentum_u<<<grid_for(L.jpi - 1, L.jpj), dim3(BX, BY), 0, s>>>(L, C, p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_momentum_v(const Layout& L, const Consts& C, const RoutinePtrs& p,
+                              cudaStream_t s) {
+  if (L.jpj < 2) return cudaSuccess;
+  k_momentum_v<<<grid_for(L.jpi, L.jpj - 1), dim3(BX, BY), 0, s>>>(L, C, p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_bc_ssh(const Layout& L, double value, double* ssha, cudaStream_t s) {
+  k_bc_ssh<<<grid_for(L.jpi, L.jpj), dim3(BX, BY), 0, s>>>(L, value, ssha);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_bc_solid_u(const Layout& L, double* ua, cudaStream_t s) {
+  k_bc_solid_u<<<grid_for(L.jpi + 1, L.jpj), dim3(BX, BY), 0, s>>>(L, ua);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_bc_solid_v(const Layout& L, double* va, cudaStream_t s) {
+  k_bc_solid_v<<<grid_for(L.jpi, L.jpj + 1), dim3(BX, BY), 0, s>>>(L, va);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_bc_flather_u(const Layout& L, const RoutinePtrs& p, cudaStream_t s) {
+  k_bc_flather_u<<<(L.jpj + 127) / 128, 128, 0, s>>>(L, p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_bc_flather_v(const Layout& L, const RoutinePtrs& p, cudaStream_t s) {
+  k_bc_flather_v<<<(L.jpi + 127) / 128, 128, 0, s>>>(L, p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_copy_next(const Layout& L, const RoutinePtrs& p, cudaStream_t s) {
+  k_copy_next<<<grid_for(L.jpi + 1, L.jpj + 1), dim3(BX, BY), 0, s>>>(L, p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_derive_sshn_uv(const Layout& L, const Consts& C, const double* sshn,
+                                  double* sshn_u, double* sshn_v, cudaStream_t s) {
+  k_derive_sshn_uv<<<grid_for(L.jpi + 1, L.jpj + 1), dim3(BX, BY), 0, s>>>(L, C, sshn, sshn_u, sshn_v);
+  return cudaGetLastError();
+}
+
+}  // namespace nemo

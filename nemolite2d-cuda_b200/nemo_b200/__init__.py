@@ -1,0 +1,265 @@
+"""Python host side of the B200 NEMOLite2D stepper, over its C ABI.
+
+Mirrors the reference's routine boundary (original/nemolite2d.f90:375-386:
+continuity, momentum, bc, next) and the drop-in CUDA-library symbols of
+cuda/cuda_nemolite2d.cu:234-270, through ctypes bindings of
+lib/libnemo_b200.so (or lib/libnemo_b200_strict.so, the -fmad=false build).
+
+There is no CPU fallback: if the shared library is missing or cannot load,
+importing or constructing anything raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.dirname(_HERE)
+LIB_DIR = os.path.join(PKG_DIR, "lib")
+
+SSHN, UN, VN, SSHA, UA, VA, SSHN_U, SSHN_V, HT, HU, HV, XT, YT = range(13)
+FIELD_NAMES = {SSHN: "sshn", UN: "un", VN: "vn", SSHA: "ssha", UA: "ua", VA: "va",
+               SSHN_U: "sshn_u", SSHN_V: "sshn_v", HT: "ht", HU: "hu", HV: "hv",
+               XT: "xt", YT: "yt"}
+T_FIELDS = (SSHN, SSHA, HT, XT, YT)
+U_FIELDS = (UN, UA, SSHN_U, HU)
+V_FIELDS = (VN, VA, SSHN_V, HV)
+
+STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA runtime error", 3: "allocation failed",
+          4: "invalid state", 5: "device wait timed out", 6: "unsupported"}
+
+# Every symbol include/nemo_b200.h declares.
+EXPORTED = [
+    "nemo_default_params", "nemo_create", "nemo_destroy", "nemo_continuity", "nemo_momentum",
+    "nemo_momentum_u", "nemo_momentum_v", "nemo_bc", "nemo_bc_ssh", "nemo_bc_solid_u",
+    "nemo_bc_solid_v", "nemo_bc_flather_u", "nemo_bc_flather_v", "nemo_next", "nemo_step",
+    "nemo_step_n", "nemo_checksums", "nemo_checksum", "nemo_retrieve", "nemo_set_state",
+    "nemo_sync", "nemo_get_dims", "nemo_device_field", "nemo_set_tile", "nemo_get_tile",
+    "nemo_status_string", "nemo_build_is_strict",
+    "cuda_setup_model_params_", "cuda_initialise_grid_", "cuda_continuity_", "cuda_momentum_",
+    "cuda_boundary_conditions_", "cuda_next_", "cuda_retrieve_grid_constants_",
+    "cuda_retrieve_results_", "cuda_finalise_", "nemo_compat_last_status", "nemo_compat_context",
+]
+
+
+class NemoError(RuntimeError):
+    def __init__(self, status, where):
+        super().__init__("%s failed: %s (status %d)" % (where, STATUS.get(status, "?"), status))
+        self.status = status
+
+
+class Params(ctypes.Structure):
+    _fields_ = [
+        ("jpi", ctypes.c_int), ("jpj", ctypes.c_int),
+        ("dx", ctypes.c_double), ("dy", ctypes.c_double), ("dep_const", ctypes.c_double),
+        ("nit000", ctypes.c_int), ("nitend", ctypes.c_int), ("irecord", ctypes.c_int),
+        ("rdt", ctypes.c_double), ("cbfr", ctypes.c_double), ("visc", ctypes.c_double),
+        ("amp_tide", ctypes.c_double), ("tide_phase", ctypes.c_double), ("lat", ctypes.c_double),
+        ("nbump", ctypes.c_int), ("seed", ctypes.c_uint64),
+        ("bump_amp", ctypes.c_double), ("bump_wmin", ctypes.c_double),
+        ("bump_wmax", ctypes.c_double), ("hmin", ctypes.c_double), ("hmax", ctypes.c_double),
+        ("stream", ctypes.c_void_p), ("device", ctypes.c_int),
+    ]
+
+
+def lib_path(strict=False):
+    return os.path.join(LIB_DIR, "libnemo_b200_strict.so" if strict else "libnemo_b200.so")
+
+
+_libs = {}
+
+
+def load(strict=False):
+    """Load (once) and type the shared library.  Raises if it is missing."""
+    if strict in _libs:
+        return _libs[strict]
+    path = lib_path(strict)
+    if not os.path.exists(path):
+        raise ImportError("nemo_b200: %s is not built (run `make -C %s`); no fallback exists"
+                          % (path, PKG_DIR))
+    L = ctypes.CDLL(path)
+    vp, ip, dp = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+    P = ctypes.POINTER
+    L.nemo_default_params.argtypes = [P(Params)]
+    L.nemo_create.argtypes = [P(Params), P(vp)]
+    for n in ("nemo_destroy", "nemo_continuity", "nemo_momentum", "nemo_momentum_u",
+              "nemo_momentum_v", "nemo_bc_solid_u", "nemo_bc_solid_v", "nemo_bc_flather_u",
+              "nemo_bc_flather_v", "nemo_next", "nemo_sync"):
+        getattr(L, n).argtypes = [vp]
+    L.nemo_bc.argtypes = [vp, dp]
+    L.nemo_bc_ssh.argtypes = [vp, dp]
+    L.nemo_step.argtypes = [vp, ip]
+    L.nemo_step_n.argtypes = [vp, ip, ip]
+    L.nemo_checksums.argtypes = [vp, P(dp)]
+    L.nemo_checksum.argtypes = [vp, ip, P(dp)]
+    L.nemo_retrieve.argtypes = [vp, ip, P(dp), ctypes.c_long]
+    L.nemo_set_state.argtypes = [vp, P(dp), P(dp), P(dp)]
+    L.nemo_get_dims.argtypes = [vp, P(ip), P(ip)]
+    L.nemo_device_field.argtypes = [vp, ip, P(P(dp)), P(ctypes.c_long)]
+    L.nemo_set_tile.argtypes = [vp, ip, ip]
+    L.nemo_get_tile.argtypes = [vp, P(ip), P(ip)]
+    L.nemo_status_string.argtypes = [ip]
+    L.nemo_status_string.restype = ctypes.c_char_p
+    L.nemo_build_is_strict.restype = ip
+    L.cuda_setup_model_params_.argtypes = [ip, ip, dp, dp, dp, ip, ip, ip, dp, dp, dp]
+    L.cuda_setup_model_params_.restype = None
+    for n in ("cuda_initialise_grid_", "cuda_continuity_", "cuda_momentum_", "cuda_next_",
+              "cuda_finalise_"):
+        getattr(L, n).argtypes = []
+        getattr(L, n).restype = None
+    L.cuda_boundary_conditions_.argtypes = [dp]
+    L.cuda_boundary_conditions_.restype = None
+    L.cuda_retrieve_grid_constants_.argtypes = [P(dp), P(dp), P(dp), ip, ip]
+    L.cuda_retrieve_grid_constants_.restype = None
+    L.cuda_retrieve_results_.argtypes = [P(dp)] * 5 + [ip, ip]
+    L.cuda_retrieve_results_.restype = None
+    L.nemo_compat_context.restype = vp
+    _libs[strict] = L
+    return L
+
+
+def _dptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def check(status, where):
+    if status != 0:
+        raise NemoError(status, where)
+
+
+def default_params(strict=False, **kw):
+    p = Params()
+    load(strict).nemo_default_params(ctypes.byref(p))
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise AttributeError("unknown parameter %r" % k)
+        setattr(p, k, v)
+    return p
+
+
+def field_shape(field, jpi, jpj):
+    """(ny, nx): C-order view of the field's Fortran-bounded column-major block."""
+    if field in T_FIELDS:
+        return (jpj, jpi)
+    if field in U_FIELDS:
+        return (jpj, jpi + 1)
+    if field in V_FIELDS:
+        return (jpj + 1, jpi)
+    raise ValueError("unknown field %r" % field)
+
+
+class Model:
+    """One model instance on one GPU (a nemo_ctx)."""
+
+    def __init__(self, params=None, strict=False, **kw):
+        self.lib = load(strict)
+        self.strict = strict
+        self.p = params if params is not None else default_params(strict, **kw)
+        h = ctypes.c_void_p()
+        check(self.lib.nemo_create(ctypes.byref(self.p), ctypes.byref(h)), "nemo_create")
+        self.h = h
+        self.jpi, self.jpj = self.p.jpi, self.p.jpj
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.nemo_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # per-routine boundary
+    def continuity(self):
+        check(self.lib.nemo_continuity(self.h), "nemo_continuity")
+
+    def momentum(self):
+        check(self.lib.nemo_momentum(self.h), "nemo_momentum")
+
+    def momentum_u(self):
+        check(self.lib.nemo_momentum_u(self.h), "nemo_momentum_u")
+
+    def momentum_v(self):
+        check(self.lib.nemo_momentum_v(self.h), "nemo_momentum_v")
+
+    def bc(self, rtime):
+        check(self.lib.nemo_bc(self.h, rtime), "nemo_bc")
+
+    def bc_ssh(self, rtime):
+        check(self.lib.nemo_bc_ssh(self.h, rtime), "nemo_bc_ssh")
+
+    def bc_solid_u(self):
+        check(self.lib.nemo_bc_solid_u(self.h), "nemo_bc_solid_u")
+
+    def bc_solid_v(self):
+        check(self.lib.nemo_bc_solid_v(self.h), "nemo_bc_solid_v")
+
+    def bc_flather_u(self):
+        check(self.lib.nemo_bc_flather_u(self.h), "nemo_bc_flather_u")
+
+    def bc_flather_v(self):
+        check(self.lib.nemo_bc_flather_v(self.h), "nemo_bc_flather_v")
+
+    def next(self):
+        check(self.lib.nemo_next(self.h), "nemo_next")
+
+    def step(self, istp):
+        check(self.lib.nemo_step(self.h, istp), "nemo_step")
+
+    # fused path
+    def step_n(self, istp0, n):
+        check(self.lib.nemo_step_n(self.h, istp0, n), "nemo_step_n")
+
+    def set_tile(self, tx, ty):
+        check(self.lib.nemo_set_tile(self.h, tx, ty), "nemo_set_tile")
+
+    def get_tile(self):
+        a, b = ctypes.c_int(), ctypes.c_int()
+        check(self.lib.nemo_get_tile(self.h, ctypes.byref(a), ctypes.byref(b)), "nemo_get_tile")
+        return a.value, b.value
+
+    def sync(self):
+        check(self.lib.nemo_sync(self.h), "nemo_sync")
+
+    def checksums(self):
+        out = np.zeros(3, dtype=np.float64)
+        check(self.lib.nemo_checksums(self.h, _dptr(out)), "nemo_checksums")
+        return out
+
+    def checksum(self, field):
+        out = np.zeros(1, dtype=np.float64)
+        check(self.lib.nemo_checksum(self.h, field, _dptr(out)), "nemo_checksum")
+        return float(out[0])
+
+    def field(self, f, out=None):
+        shape = field_shape(f, self.jpi, self.jpj)
+        if out is None:
+            out = np.empty(shape, dtype=np.float64)
+        assert out.shape == shape and out.dtype == np.float64 and out.flags.c_contiguous
+        check(self.lib.nemo_retrieve(self.h, f, _dptr(out), shape[1]), "nemo_retrieve")
+        return out
+
+    def set_state(self, sshn, un, vn):
+        a = [np.ascontiguousarray(x, dtype=np.float64) for x in (sshn, un, vn)]
+        for f, x in zip((SSHN, UN, VN), a):
+            assert x.shape == field_shape(f, self.jpi, self.jpj), (f, x.shape)
+        check(self.lib.nemo_set_state(self.h, *[_dptr(x) for x in a]), "nemo_set_state")
+
+    def device_field(self, f):
+        ptr = ctypes.POINTER(ctypes.c_double)()
+        pitch = ctypes.c_long()
+        check(self.lib.nemo_device_field(self.h, f, ctypes.byref(ptr), ctypes.byref(pitch)),
+              "nemo_device_field")
+        return ctypes.cast(ptr, ctypes.c_void_p).value, pitch.value
+
+
+def is_strict_build(strict):
+    return bool(load(strict).nemo_build_is_strict())

@@ -1,0 +1,263 @@
+"""Parity of the CUDA stepper with the oracle and the reference's golden vectors.
+
+Two builds of the same sources are checked:
+  * lib/libnemo_b200_strict.so (-fmad=false): bit-for-bit equal (sign of zero
+    included) to the oracle and to the golden vectors executed from
+    original/nemolite2d.f90, through both the per-routine path and the fused
+    path;
+  * lib/libnemo_b200.so (default, FMA contraction on): relative max-norm
+    error max|gpu - ref| / max|ref| <= 1e-12 per field after every record.
+"""
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, GOLDEN_CASES
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12
+STATE = [("sshn", 0), ("un", 1), ("vn", 2)]
+ALL = STATE + [("ssha", 3), ("ua", 4), ("va", 5), ("sshn_u", 6), ("sshn_v", 7)]
+
+
+@pytest.fixture(scope="module")
+def nb():
+    import nemo_b200
+    nemo_b200.load(False)
+    nemo_b200.load(True)
+    return nemo_b200
+
+
+def bits(a):
+    return np.ascontiguousarray(a).view(np.int64)
+
+
+def relerr(a, b):
+    d = np.max(np.abs(a - b)) if a.size else 0.0
+    s = np.max(np.abs(b)) if b.size else 0.0
+    return d / s if s > 0 else d
+
+
+def golden_params(z):
+    return dict(jpi=int(z["jpi"]), jpj=int(z["jpj"]), dx=float(z["nml_dx"]), dy=float(z["nml_dy"]),
+                dep_const=float(z["nml_dep_const"]), rdt=float(z["nml_rdt"]),
+                cbfr=float(z["nml_cbfr"]), visc=float(z["nml_visc"]))
+
+
+@pytest.mark.parametrize("case", GOLDEN_CASES)
+@pytest.mark.parametrize("path", ["routine", "fused"])
+def test_strict_build_matches_golden_bitwise(nb, case, path):
+    z = np.load("%s/%s.npz" % (GOLDEN, case))
+    m = nb.Model(strict=True, **golden_params(z))
+    fields = ALL if path == "routine" else ALL
+    last = 0
+    for r in z["records"]:
+        r = int(r)
+        if r > 0:
+            if path == "routine":
+                for istp in range(last + 1, r + 1):
+                    m.step(istp)
+            else:
+                m.step_n(last + 1, r - last)
+            last = r
+        for name, fid in fields:
+            np.testing.assert_array_equal(bits(m.field(fid)), bits(z["s%05d_%s" % (r, name)]),
+                                          err_msg="%s %s step %d %s" % (case, path, r, name))
+
+
+@pytest.mark.parametrize("jpi,jpj,tile", [(257, 131, (128, 64)), (130, 300, (64, 7)),
+                                          (2, 2, (64, 1)), (3, 5, (128, 2)), (96, 33, (256, 16))])
+def test_strict_fused_matches_oracle_ragged_bathymetry(nb, oracle_mod, jpi, jpj, tile):
+    kw = dict(jpi=jpi, jpj=jpj, rdt=20.0, cbfr=0.00015, visc=0.1, amp_tide=0.5,
+              tide_phase=0.3, nbump=12, seed=77, bump_amp=30.0, bump_wmin=3e3, bump_wmax=40e3,
+              hmin=20.0)
+    m = nb.Model(strict=True, **kw)
+    m.set_tile(*tile)
+    o = oracle_mod.Model(**kw)
+    for name, fid in [("ht", nb.HT), ("hu", nb.HU), ("hv", nb.HV)]:
+        np.testing.assert_array_equal(bits(m.field(fid)), bits(o.field(fid)), err_msg=name)
+    istp = 1
+    for nsteps in (1, 7, 25):
+        m.step_n(istp, nsteps)
+        o.run(istp, nsteps)
+        istp += nsteps
+        for name, fid in STATE:
+            np.testing.assert_array_equal(bits(m.field(fid)), bits(o.field(fid)),
+                                          err_msg="%dx%d step %d %s" % (jpi, jpj, istp - 1, name))
+
+
+def test_strict_routines_one_by_one_from_random_state(nb, oracle_mod):
+    """Each routine of the per-routine boundary against the oracle's routine."""
+    jpi, jpj = 70, 45
+    kw = dict(jpi=jpi, jpj=jpj, rdt=20.0, cbfr=0.00015, visc=0.1, amp_tide=1.0, nbump=5,
+              seed=3, bump_amp=20.0, bump_wmin=5e3, bump_wmax=20e3)
+    rng = np.random.default_rng(11)
+    sshn = rng.normal(0, 0.1, (jpj, jpi))
+    un = rng.normal(0, 0.2, (jpj, jpi + 1))
+    vn = rng.normal(0, 0.2, (jpj + 1, jpi))
+    m = nb.Model(strict=True, **kw)
+    o = oracle_mod.Model(**kw)
+    m.set_state(sshn, un, vn)
+    o.set_state(sshn, un, vn)
+    rtime = 37 * 20.0
+    steps = [("continuity", lambda: (m.continuity(), o.continuity())),
+             ("momentum_u", lambda: (m.momentum_u(), o.momentum_u())),
+             ("momentum_v", lambda: (m.momentum_v(), o.momentum_v())),
+             ("bc_ssh", lambda: (m.bc_ssh(rtime), o.bc_ssh(rtime))),
+             ("bc_solid_u", lambda: (m.bc_solid_u(), o.bc_solid_u())),
+             ("bc_solid_v", lambda: (m.bc_solid_v(), o.bc_solid_v())),
+             ("bc_flather_u", lambda: (m.bc_flather_u(), o.bc_flather_u())),
+             ("bc_flather_v", lambda: (m.bc_flather_v(), o.bc_flather_v())),
+             ("next", lambda: (m.next(), o.next()))]
+    for label, fn in steps:
+        fn()
+        for name, fid in ALL:
+            np.testing.assert_array_equal(bits(m.field(fid)), bits(o.field(fid)),
+                                          err_msg="after %s: %s" % (label, name))
+
+
+def test_strict_fused_equals_routine_path_from_random_state(nb):
+    jpi, jpj = 200, 150
+    kw = dict(jpi=jpi, jpj=jpj, rdt=20.0, cbfr=0.00015, visc=0.1, amp_tide=1.0, nbump=8,
+              seed=5, bump_amp=30.0, bump_wmin=5e3, bump_wmax=50e3)
+    rng = np.random.default_rng(2)
+    st = (rng.normal(0, 0.1, (jpj, jpi)), rng.normal(0, 0.3, (jpj, jpi + 1)),
+          rng.normal(0, 0.3, (jpj + 1, jpi)))
+    a = nb.Model(strict=True, **kw)
+    b = nb.Model(strict=True, **kw)
+    a.set_state(*st)
+    b.set_state(*st)
+    a.step_n(10, 15)
+    for istp in range(10, 25):
+        b.step(istp)
+    for name, fid in ALL:
+        np.testing.assert_array_equal(bits(a.field(fid)), bits(b.field(fid)), err_msg=name)
+
+
+def test_default_build_config0_within_tolerance_every_record(nb, oracle_mod):
+    """128^2, rdt 20, cbfr 1.5e-4, visc 0.1, 2000 steps, records every 100."""
+    kw = dict(jpi=128, jpj=128, rdt=20.0, cbfr=0.00015, visc=0.1, amp_tide=0.2)
+    m = nb.Model(strict=False, **kw)
+    o = oracle_mod.Model(**kw)
+    for rec in range(20):
+        m.step_n(1 + 100 * rec, 100)
+        o.run(1 + 100 * rec, 100)
+        for name, fid in STATE:
+            e = relerr(m.field(fid), o.field(fid))
+            assert e <= TOL, "step %d %s rel err %.3e" % (100 * (rec + 1), name, e)
+        ck = m.checksums()
+        ref = [o.checksum(f, "seq") for f in (oracle_mod.SSHN, oracle_mod.UA, oracle_mod.VA)]
+        np.testing.assert_allclose(ck, ref, rtol=1e-11)
+
+
+def test_strict_checksums_bitwise_tree_order(nb, oracle_mod):
+    kw = dict(jpi=300, jpj=77, rdt=20.0, cbfr=0.00015, visc=0.1, amp_tide=0.2)
+    m = nb.Model(strict=True, **kw)
+    o = oracle_mod.Model(**kw)
+    m.step_n(1, 60)
+    o.run(1, 60)
+    ck = m.checksums()
+    for k, f in enumerate((oracle_mod.SSHN, oracle_mod.UN, oracle_mod.VN)):
+        assert ck[k] == o.checksum(f, "tree")
+        assert abs(ck[k] - o.checksum(f, "seq")) <= 1e-13 * abs(ck[k])
+    assert m.checksum(nb.UA) == ck[1] and m.checksum(nb.VA) == ck[2]
+
+
+@pytest.mark.parametrize("tile", [(64, 1), (64, 16), (128, 64), (256, 5), (256, 256)])
+def test_tile_shape_does_not_change_results(nb, tile):
+    kw = dict(jpi=333, jpj=210, rdt=20.0, cbfr=0.00015, visc=0.1, amp_tide=0.6, nbump=6,
+              seed=9, bump_amp=25.0, bump_wmin=5e3, bump_wmax=60e3)
+    ref = nb.Model(strict=False, **kw)
+    ref.set_tile(128, 64)
+    m = nb.Model(strict=False, **kw)
+    m.set_tile(*tile)
+    ref.step_n(1, 40)
+    m.step_n(1, 40)
+    for name, fid in STATE:
+        np.testing.assert_array_equal(bits(m.field(fid)), bits(ref.field(fid)), err_msg=name)
+
+
+def test_config1_size_against_openmp_oracle(nb, oracle_mod):
+    """4096^2 with 32 seeded bumps: strict bitwise and default within tolerance."""
+    kw = dict(jpi=4096, jpj=4096, rdt=20.0, cbfr=0.00015, visc=0.1, amp_tide=0.2, nbump=32,
+              seed=1234, bump_amp=40.0, bump_wmin=20e3, bump_wmax=200e3, hmin=10.0)
+    import os
+    oracle_mod.set_threads(max(1, len(os.sched_getaffinity(0))))
+    o = oracle_mod.Model(**kw)
+    o.run(1, 12)
+    oracle_mod.set_threads(1)
+    s = nb.Model(strict=True, **kw)
+    s.step_n(1, 12)
+    d = nb.Model(strict=False, **kw)
+    d.step_n(1, 12)
+    for name, fid in STATE:
+        ref = o.field(fid)
+        np.testing.assert_array_equal(bits(s.field(fid)), bits(ref), err_msg=name)
+        assert relerr(d.field(fid), ref) <= TOL
+    del s
+
+
+def test_long_run_properties_at_4096(nb):
+    """1000 fused steps at 4096^2: finite, walls exactly zero, clamped row exact."""
+    kw = dict(jpi=4096, jpj=4096, rdt=20.0, cbfr=0.00015, visc=0.1, amp_tide=0.2, nbump=32,
+              seed=1234, bump_amp=40.0, bump_wmin=20e3, bump_wmax=200e3, hmin=10.0)
+    m = nb.Model(strict=False, **kw)
+    m.step_n(1, 1000)
+    ck = m.checksums()
+    assert np.all(np.isfinite(ck)) and np.all(ck > 0)
+    u = m.field(nb.UN)
+    v = m.field(nb.VN)
+    s = m.field(nb.SSHN)
+    assert not np.any(u[:, 0]) and not np.any(u[:, -1]) and not np.any(v[-1, :])
+    om = 2.0 * 3.14159 / (12.42 * 3600.0)
+    assert np.all(s[0] == 0.2 * np.sin(om * (1000 * 20.0)))
+
+
+def test_compat_symbols_drive_the_reference_sequence(nb, oracle_mod):
+    """cuda_setup_model_params_ / cuda_initialise_grid_ / per-step calls /
+    cuda_retrieve_results_ as cuda/nemolite2d.f90 drives them."""
+    import ctypes
+    L = nb.load(True)
+    jpi, jpj, rdt = 40, 30, 20.0
+    L.cuda_setup_model_params_(jpi, jpj, 1000.0, 1000.0, 100.0, 1, 20, 5, rdt, 0.00015, 0.1)
+    L.cuda_initialise_grid_()
+    assert L.nemo_compat_last_status() == 0
+    o = oracle_mod.Model(jpi=jpi, jpj=jpj, rdt=rdt, cbfr=0.00015, visc=0.1)
+    P = ctypes.POINTER(ctypes.c_double)
+    for istp in range(1, 21):
+        rtime = istp * rdt
+        L.cuda_continuity_()
+        L.cuda_momentum_()
+        L.cuda_boundary_conditions_(rtime)
+        L.cuda_next_()
+        o.step(istp)
+    out = {k: np.empty(s) for k, s in [("sshn", (jpj, jpi)), ("un", (jpj, jpi + 1)),
+                                       ("vn", (jpj + 1, jpi)), ("ua", (jpj, jpi + 1)),
+                                       ("va", (jpj + 1, jpi))]}
+    L.cuda_retrieve_results_(*[out[k].ctypes.data_as(P) for k in ("sshn", "un", "vn", "ua", "va")],
+                             jpi, jpj)
+    xt, yt, ht = (np.empty((jpj, jpi)) for _ in range(3))
+    L.cuda_retrieve_grid_constants_(xt.ctypes.data_as(P), yt.ctypes.data_as(P),
+                                    ht.ctypes.data_as(P), jpi, jpj)
+    assert L.nemo_compat_last_status() == 0
+    for k, fid in [("sshn", 0), ("un", 1), ("vn", 2), ("ua", 4), ("va", 5)]:
+        np.testing.assert_array_equal(bits(out[k]), bits(o.field(fid)), err_msg=k)
+    np.testing.assert_array_equal(xt, o.field(oracle_mod.XT))
+    np.testing.assert_array_equal(yt, o.field(oracle_mod.YT))
+    np.testing.assert_array_equal(ht, o.field(oracle_mod.HT))
+    L.cuda_finalise_()
+    assert not L.nemo_compat_context()
+
+
+def test_invalid_arguments_fail_loudly(nb):
+    with pytest.raises(nb.NemoError):
+        nb.Model(jpi=1, jpj=10)
+    with pytest.raises(nb.NemoError):
+        nb.Model(jpi=10, jpj=0)
+    m = nb.Model(jpi=10, jpj=10)
+    with pytest.raises(nb.NemoError):
+        m.set_tile(100, 4)
+    with pytest.raises(nb.NemoError):
+        m.step_n(1, -1)
+    with pytest.raises(nb.NemoError):
+        m.checksum(nb.XT)
