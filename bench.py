@@ -54,7 +54,8 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--tile", type=str, default="")
+    ap.add_argument("--schedule", type=str, default="",
+                    help="warps,occupancy,rows of the fused kernel (default: tuned)")
     ap.add_argument("--n", type=int, default=N,
                     help="grid side (profiling of smaller cases only; the bench line is 4096)")
     return ap.parse_args()
@@ -227,9 +228,8 @@ def main():
 
     stream = torch.cuda.Stream()
     m = nemo_b200.Model(strict=False, stream=stream.cuda_stream, device=local, **WORKLOAD)
-    if args.tile:
-        tx, ty = (int(x) for x in args.tile.split("x"))
-        m.set_tile(tx, ty)
+    if args.schedule:
+        m.set_schedule(*(int(x) for x in args.schedule.split(",")))
     jpi, jpj = m.jpi, m.jpj
     rest = (np.zeros((jpj, jpi)), np.zeros((jpj, jpi + 1)), np.zeros((jpj + 1, jpi)))
 
@@ -313,12 +313,14 @@ def main():
                          "original/nemolite2d.f90, OpenMP %d threads" % (n, n + 1, th)}
 
     if rank == 0:
-        tx, ty = m.get_tile()
+        sched = m.get_schedule()
         line = {"metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64", "data": "synthetic",
-                "config": dict(CONFIG, parallelism="replicas x%d" % world, tile=[tx, ty]),
+                "config": dict(CONFIG, parallelism="replicas x%d" % world,
+                               schedule={"warps": sched[0], "occupancy": sched[1],
+                                         "rows": sched[2]}),
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
                              "unit": "GB/s", "frac": achieved / peak,
                              "peak_source": peak_kind, "traffic": traffic,

@@ -135,10 +135,18 @@ int nemo_get_dims(nemo_ctx* ctx, int* jpi, int* jpj);
 /* Device address and pitch (in doubles) of a field's storage; element
  * (ji,jj) lives at ptr[(jj+1)*pitch + (ji+1)].  For device-side consumers. */
 int nemo_device_field(nemo_ctx* ctx, int field, double** ptr, long* pitch);
-/* Tile shape of the fused kernel (columns per CTA x rows per CTA); 0 picks
- * the tuned default. */
-int nemo_set_tile(nemo_ctx* ctx, int tile_x, int tile_y);
-int nemo_get_tile(nemo_ctx* ctx, int* tile_x, int* tile_y);
+/* Launch schedule of the fused kernel: warps per CTA (2, 4, 8; a warp covers
+ * 30 columns), register budget as resident warps per SM (0 = compiler's
+ * choice, 16, 20; 8-warp CTAs take 0 or 16) and rows marched per CTA
+ * (0: one wave, row blocks sized so every CTA is resident at once).  In the
+ * -fmad=false build every schedule gives bit-identical results. */
+typedef struct nemo_schedule {
+  int warps;
+  int occupancy;
+  int rows;
+} nemo_schedule;
+int nemo_set_schedule(nemo_ctx* ctx, const nemo_schedule* s);
+int nemo_get_schedule(nemo_ctx* ctx, nemo_schedule* s);
 const char* nemo_status_string(int status);
 /* 1 when this library was built with -fmad=false (bit-exact build). */
 int nemo_build_is_strict(void);

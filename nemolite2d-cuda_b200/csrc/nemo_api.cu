@@ -29,7 +29,7 @@ struct nemo_ctx {
   double* ck_host;        // pinned, 4
   bool a_mirrors_n;       // after a fused step the reference's a-fields equal n
   bool uv_stale;          // stored sshn_u/sshn_v lag behind sshn
-  int tile_x, tile_y;
+  nemo_schedule sched;
 };
 
 namespace {
@@ -260,8 +260,9 @@ int nemo_create(const nemo_params* p, nemo_ctx** out) {
   c->L.pitch = layout_pitch(p->jpi);
   c->L.rows = (long)p->jpj + 3;
   c->C = make_consts(*p);
-  c->tile_x = 128;
-  c->tile_y = 64;
+  c->sched.warps = 2;
+  c->sched.occupancy = 20;
+  c->sched.rows = 0;
   int st = set_device(c);
   if (st) { delete c; return st; }
   cudaError_t e;
@@ -440,7 +441,7 @@ int nemo_step_n(nemo_ctx* c, int istp0, int n) {
     a.ua = aset(c).u;
     a.va = aset(c).v;
     a.tide = tide_value(c->p, istp0 + k);
-    CK(launch_fused_step(c->L, c->C, a, c->tile_x, c->tile_y, c->stream));
+    CK(launch_fused_step(c->L, c->C, a, c->sched.warps, c->sched.occupancy, c->sched.rows, c->stream));
     c->n_idx = 1 - c->n_idx;  // next: the new state becomes "now"
   }
   c->a_mirrors_n = true;
@@ -547,20 +548,17 @@ int nemo_device_field(nemo_ctx* c, int field, double** ptr, long* pitch) {
   return NEMO_OK;
 }
 
-int nemo_set_tile(nemo_ctx* c, int tx, int ty) {
+int nemo_set_schedule(nemo_ctx* c, const nemo_schedule* s) {
   if (!c) return NEMO_ERR_STATE;
-  if (tx == 0) tx = 128;
-  if (ty == 0) ty = 64;
-  if (!(tx == 64 || tx == 128 || tx == 256) || ty < 1 || ty > 4096) return NEMO_ERR_INVALID;
-  c->tile_x = tx;
-  c->tile_y = ty;
+  if (!s || !fused_variant_ok(s->warps, s->occupancy) || s->rows < 0 || s->rows > 65536)
+    return NEMO_ERR_INVALID;
+  c->sched = *s;
   return NEMO_OK;
 }
 
-int nemo_get_tile(nemo_ctx* c, int* tx, int* ty) {
-  if (!c || !tx || !ty) return NEMO_ERR_INVALID;
-  *tx = c->tile_x;
-  *ty = c->tile_y;
+int nemo_get_schedule(nemo_ctx* c, nemo_schedule* s) {
+  if (!c || !s) return NEMO_ERR_INVALID;
+  *s = c->sched;
   return NEMO_OK;
 }
 

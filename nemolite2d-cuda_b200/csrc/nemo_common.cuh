@@ -52,30 +52,27 @@ __host__ __device__ __forceinline__ int ptmask(int ji, int jj, int jpi, int jpj)
   return 1;
 }
 
+// True for a nonzero |q| < 2^-959 and for an infinite or NaN q: the cases
+// where the corrected quotient below is not proven exact.  +-0 is exact.
+__device__ __forceinline__ bool quotient_out_of_range(double q) {
+  unsigned t = ((unsigned)__double2hiint(q) << 1) | (unsigned)(__double2loint(q) != 0);
+  return (t - 1u) < ((64u << 21) - 1u) || t >= (0x7ffu << 21);
+}
+
 // Quotient a/b correctly rounded, given rb = RN(1/b) formed on the host.
 // Markstein's theorem (IBM J. Res. Dev. 34(1), 1990): with q = RN(a*rb) and
 // the exact remainder r = a - b*q (one fma), RN(q + r*rb) = RN(a/b) whenever
-// no intermediate underflows or overflows.  Quotients whose exponent is
-// below 2^-959, or infinite/NaN, take the IEEE division instead.  Writing
-// the last step as -fma(-r, rb, -q) keeps the sign of a zero quotient.
+// no intermediate underflows or overflows.  Quotients outside the proven
+// range take the IEEE division instead.  Writing the last step as
+// -fma(-r, rb, -q) keeps the sign of a zero quotient.
 __device__ __forceinline__ double div_const(double a, double b, double rb) {
   double q = __dmul_rn(a, rb);
-  unsigned e = ((unsigned)__double2hiint(q) >> 20) & 0x7ffu;
-  if (e - 64u >= 0x7ffu - 64u) return a / b;
+  if (quotient_out_of_range(q)) return a / b;
   double r = fma(-q, b, a);
   return -fma(-r, rb, -q);
 }
 
 constexpr unsigned long long kSign = 0x8000000000000000ull;
-
-// (+0 * other) + main, exactly: main unless main is a zero, in which case
-// the zero is negative only when both operands are negative.
-__device__ __forceinline__ double zplus(double main, double other) {
-  unsigned long long mb = (unsigned long long)__double_as_longlong(main);
-  unsigned long long ob = (unsigned long long)__double_as_longlong(other);
-  unsigned long long r = (mb << 1) ? mb : (mb & ob & kSign);
-  return __longlong_as_double((long long)r);
-}
 
 __device__ __forceinline__ bool sign_clear(double w) { return __double2hiint(w) >= 0; }
 
@@ -83,10 +80,12 @@ __device__ __forceinline__ bool sign_clear(double w) { return __double2hiint(w) 
 // values on the low/high-index side.  Equals, bit for bit,
 //   (0.5 + SIGN(0.5,w))*lo + (0.5 - SIGN(0.5,w))*hi
 // (original/nemolite2d.f90:454-471, :542-559) for finite operands: the two
-// coefficients are exactly 1 and +0.
+// coefficients are exactly 1 and +0, so the value is main + (+0*other) with
+// (main, other) = (lo, hi) when w's sign bit is clear, else (hi, lo); one
+// fma forms that sum with a single rounding and the IEEE signed-zero rule.
 __device__ __forceinline__ double upwind(double w, double lo, double hi) {
-  bool pos = sign_clear(w);
-  return pos ? zplus(lo, hi) : zplus(hi, lo);
+  const bool pos = sign_clear(w);
+  return fma(0.0, pos ? hi : lo, pos ? lo : hi);
 }
 // (0.5 - SIGN(0.5,w))*hi alone (the slip-wall forms at :460, :548)
 __device__ __forceinline__ double upwind_hi_only(double w, double hi) {

@@ -1,315 +1,356 @@
 // Fused NEMOLite2D step: continuity + momentum (u, v) + all boundary
 // conditions + next in one pass over HBM (original/nemolite2d.f90:375-769).
 //
-// Each thread owns a pair of T columns (i, i+1), i odd, so every load and
-// store of its own columns is one 16-byte access, and marches north over a
-// strip of rows.  Per row it reads the next row of sshn, un, vn, ht, hu, hv
-// and writes ssha, ua, va of the current row into the other state buffer
-// (the reference's `next` copies become a buffer swap).  Quantities the
-// reference evaluates twice -- the upwind flux through a face shared by two
-// velocity points, the velocity gradients, the interpolated sshn_u/sshn_v --
-// are evaluated once here and carried: south-face values in registers from
-// the previous row, the x-face between the two owned columns reused
-// directly.  Each of these reuses is an identical expression tree (only
-// commutations of + and * differ), so results are bit-identical to the
-// reference when contraction is off.  Divisions by grid constants use the
-// corrected-reciprocal quotient (div_const), which is the correctly rounded
-// quotient; divisions by the depth fields stay IEEE divisions.
+// Work decomposition: one warp owns a strip of 30 T columns and marches north
+// over a block of rows; lane l holds column c0+l-1, so lanes 0 and 31 are
+// halo lanes whose results are only used by their neighbours.  Per row each
+// lane loads its own sshn, un, vn, ht, hu, hv (one row ahead, prefetched),
+// and the values of columns c-1 / c+1 come from warp shuffles: no shared
+// memory, no block barriers.  The reference's `next` copies become a swap of
+// the two state buffers.
 //
-// Masks are the reference geometry's (walls at ji=0, jpi+1 and jj=jpj+1,
-// open boundary at jj=0), evaluated from the indices.
+// Every quantity the reference evaluates twice -- the upwind flux through a
+// face shared by two velocity points, the velocity gradients, sshn_u/sshn_v
+// -- is evaluated once (x-faces by the lane east of the face, y-faces
+// carried in registers from the previous row).  Each reuse is an identical
+// expression tree up to commutation of + and *, so with contraction off the
+// results are bit-identical to the reference.
+//
+// Divisions by grid constants use the corrected-reciprocal quotient; its
+// operand check is accumulated over a row, and a row in which any lane has a
+// quotient outside the safe exponent range is recomputed with IEEE division
+// (warp-uniform, so the common path stays branch-free).  Divisions by the
+// depth fields are IEEE divisions.
+//
+// Masks are those of the reference geometry (walls at ji=0, jpi+1 and
+// jj=jpj+1, open boundary at jj=0), evaluated from the indices.
 #include "nemo_internal.h"
 
 namespace nemo {
 namespace {
 
-struct Row {
-  double s[4];   // sshn at i-1 .. i+2
-  double u[4];   // un   at i-1 .. i+2
-  double v[4];   // vn   at i-1 .. i+2
-  double ht[3];  // ht   at i   .. i+2
-  double hu[3];  // hu   at i-1 .. i+1
-  double hv[4];  // hv   at i-1 .. i+2
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int COLS_PER_WARP = 30;
+
+struct Cell {
+  double s, u, v, ht, hu, hv;
 };
 
-__device__ __forceinline__ double ld1(const double* p) { return __ldg(p); }
-__device__ __forceinline__ void ld2(const double* p, double& a, double& b) {
-  double2 t = __ldg(reinterpret_cast<const double2*>(p));
-  a = t.x;
-  b = t.y;
+__device__ __forceinline__ void load_cell(Cell& x, const FusedArgs& A, long o) {
+  x.s = __ldg(A.sshn + o);
+  x.u = __ldg(A.un + o);
+  x.v = __ldg(A.vn + o);
+  x.ht = __ldg(A.ht + o);
+  x.hu = __ldg(A.hu + o);
+  x.hv = __ldg(A.hv + o);
 }
 
-__device__ __forceinline__ void load_row(Row& r, const FusedArgs& A, long base) {
-  // base = index of (i, row); i odd so base is even (16-byte aligned)
-  r.s[0] = ld1(A.sshn + base - 1);
-  ld2(A.sshn + base, r.s[1], r.s[2]);
-  r.s[3] = ld1(A.sshn + base + 2);
-  r.u[0] = ld1(A.un + base - 1);
-  ld2(A.un + base, r.u[1], r.u[2]);
-  r.u[3] = ld1(A.un + base + 2);
-  r.v[0] = ld1(A.vn + base - 1);
-  ld2(A.vn + base, r.v[1], r.v[2]);
-  r.v[3] = ld1(A.vn + base + 2);
-  ld2(A.ht + base, r.ht[0], r.ht[1]);
-  r.ht[2] = ld1(A.ht + base + 2);
-  r.hu[0] = ld1(A.hu + base - 1);
-  ld2(A.hu + base, r.hu[1], r.hu[2]);
-  r.hv[0] = ld1(A.hv + base - 1);
-  ld2(A.hv + base, r.hv[1], r.hv[2]);
-  r.hv[3] = ld1(A.hv + base + 2);
+__device__ __forceinline__ double dn(double x) { return __shfl_down_sync(FULL, x, 1); }
+__device__ __forceinline__ double up(double x) { return __shfl_up_sync(FULL, x, 1); }
+
+// a/b given rb = RN(1/b): the corrected-reciprocal quotient (see div_const)
+// with its range check reduced to what finite states need: `bad` collects
+// nonzero quotients below 2^-959, where the row is redone with IEEE
+// division.  Exact zeros (most of a domain at rest) are exact here.  An
+// infinite or NaN operand gives a non-finite quotient on both paths.
+template <bool SAFE>
+__device__ __forceinline__ double qdiv(double a, double b, double rb, bool& bad) {
+  if (SAFE) return a / b;
+  double q = __dmul_rn(a, rb);
+  const unsigned hi2 = (unsigned)__double2hiint(q) << 1;
+  const unsigned lo = (unsigned)__double2loint(q);
+  bad |= (hi2 < (64u << 21)) & ((hi2 | lo) != 0u);
+  double r = fma(-q, b, a);
+  return -fma(-r, rb, -q);
 }
 
-// sshn_u at column c of a row from sshn(c), sshn(c+1) (:736-746)
-__device__ __forceinline__ double interp_u(const Consts& C, int c, int jpi, double s0, double s1) {
+__device__ __forceinline__ double interp_u(const Consts& C, int c, int jpi, double s0, double s1,
+                                          bool safe, bool& bad) {
   if (c == 0) return s1;
   if (c == jpi) return s0;
-  return div_const(0.5 * (C.e12t * s0 + C.e12t * s1), C.e12u, C.r_e12u);
-}
-// sshn_v between rows jj and jj+1 (jj in 1..jpj; :752-763); jj == 0 is the
-// stored open-boundary row and is handled by the caller.
-__device__ __forceinline__ double interp_v(const Consts& C, int jj, int jpj, double s0, double s1) {
-  if (jj == jpj) return s0;
-  return div_const(0.5 * (C.e12t * s0 + C.e12t * s1), C.e12v, C.r_e12v);
+  double a = 0.5 * (C.e12t * s0 + C.e12t * s1);
+  return safe ? qdiv<true>(a, C.e12u, C.r_e12u, bad) : qdiv<false>(a, C.e12u, C.r_e12u, bad);
 }
 
-__global__ void __launch_bounds__(128)
+__device__ __forceinline__ double interp_v(const Consts& C, int jj, int jpj, double s0, double s1,
+                                          bool safe, bool& bad) {
+  if (jj == jpj) return s0;
+  double a = 0.5 * (C.e12t * s0 + C.e12t * s1);
+  return safe ? qdiv<true>(a, C.e12v, C.r_e12v, bad) : qdiv<false>(a, C.e12v, C.r_e12v, bad);
+}
+
+// Values carried from row j-1 to row j for one column.
+struct Carry {
+  double su, Hu;       // sshn_u and hu+sshn_u at (c, j)
+  double s_e;          // sshn(c+1, j)
+  double Fuy_s;        // upwind flux through the south face of u(c,j)
+  double dudy_s;       // dudy_s of u(c,j)
+  double vnc_s;        // v_sc of u(c,j)
+  double Fvy_s;        // upwind flux through the south face of v(c,j)
+  double Dvy_s;        // dvdy_s of v(c,j)
+  double cf_s;         // (sshn_v + hv)*vn at (c, j-1)
+};
+
+struct RowOut {
+  double ssha, ua, va, sv;
+  Carry next;
+};
+
+// One row of the step for one lane: outputs at (c, j) and the carry to j+1.
+// EDGE = false is the interior form: the caller guarantees that no lane of
+// the warp sits on column 0, 1 or jpi and that j is neither 1 nor jpj, so
+// every mask of the reference geometry is inactive.
+template <bool SAFE, bool EDGE>
+__device__ __forceinline__ void row(const Consts& C, int c, int j, int jpi, int jpj, double tide,
+                                    const Cell& cur, const Cell& nx, const Carry& k, RowOut& o,
+                                    bool& bad) {
+  const bool south = EDGE && (j == 1), north = EDGE && (j == jpj);
+  const bool west0 = EDGE && (c == 0), west1 = EDGE && (c == 1), east = EDGE && (c == jpi);
+  // sshn_v at (c, j), sshn_u at (c, j+1)
+  const double sv = EDGE ? interp_v(C, j, jpj, cur.s, nx.s, SAFE, bad)
+                         : interp_v(C, 0, 1, cur.s, nx.s, SAFE, bad);
+  const double Hv = cur.hv + sv;
+  const double s_e_n = dn(nx.s);
+  const double su_n = EDGE ? interp_u(C, c, jpi, nx.s, s_e_n, SAFE, bad)
+                           : interp_u(C, 1, 0, nx.s, s_e_n, SAFE, bad);
+  const double Hu_n = nx.hu + su_n;
+
+  // x-face of the u equation at T(c,j), between u(c-1,j) and u(c,j)
+  const double u_w = up(cur.u);
+  const double uw = 0.5 * (cur.u + u_w) * C.e2t;
+  const double dep = cur.ht + cur.s;
+  const double Fx = upwind(uw, u_w, cur.u) * uw * dep;
+  const double Dx = qdiv<SAFE>(cur.u - u_w, C.e1t, C.r_e1t, bad) * dep;
+
+  // corner (c,j): east face of v(c,j), north face of u(c,j)
+  const double uec = 0.5 * (cur.u + nx.u);
+  const double ue = 0.5 * uec * C.two_dy;
+  const double Sn = (k.Hu + nx.hu) + su_n;
+  const double v_e = dn(cur.v);
+  const double uuv = west0 ? upwind_hi_only(ue, v_e)
+                          : east ? upwind_lo_only(ue, cur.v) : upwind(ue, cur.v, v_e);
+  const double Fvx = uuv * ue * (0.5 * Sn);
+  const double Gx = qdiv<SAFE>(v_e - cur.v, C.two_dx, C.r_2dx, bad);
+  const double vnc = 0.5 * (cur.v + v_e);
+  const double vn_ = 0.5 * vnc * C.two_dx;
+  const double Re = (Hv + dn(cur.hv)) + dn(sv);
+  const double uuu = north ? upwind_lo_only(vn_, cur.u) : upwind(vn_, cur.u, nx.u);
+  const double Fuy = uuu * vn_ * (0.5 * Re);
+  const double Gy = qdiv<SAFE>(nx.u - cur.u, C.two_dy, C.r_2dy, bad);
+
+  // y-face of the v equation at T(c,j+1), between v(c,j) and v(c,j+1)
+  const double vs = 0.5 * (nx.v + cur.v) * C.e1t;
+  const double depn = nx.ht + nx.s;
+  const double Fvy_n = upwind(vs, cur.v, nx.v) * vs * depn;
+  const double Dvy_n = qdiv<SAFE>(nx.v - cur.v, C.e2t, C.r_e2t, bad) * depn;
+
+  // continuity (:399-403), clamped SSH row (:631-644)
+  const double r1 = k.Hu * cur.u;
+  const double r2 = up(r1);
+  const double r3 = Hv * cur.v;
+  const double ssh = cur.s + qdiv<SAFE>((r2 - r1 + k.cf_s - r3) * C.rdt, C.e12t, C.r_e12t, bad);
+  o.ssha = south ? tide : ssh;
+
+  // u equation (:439-514); u(jpi,j) is the east wall (:650)
+  {
+    const double Fx_e = dn(Fx);
+    const double Dx_e = dn(Dx);
+    const double adv = Fx - Fx_e + k.Fuy_s - Fuy;
+    const double dudy_n = north ? 0.0 : Gy * Sn;
+    const double dudy_s = south ? 0.0 : k.dudy_s;
+    double vis = (Dx_e - Dx) * C.e2u + (dudy_n - dudy_s) * C.e1u * 0.5;
+    vis = C.visc * vis;
+    const double cor = 0.5 * (C.fcor * (k.vnc_s + vnc)) * C.e12u * k.Hu;
+    const double hpg = -(C.g * k.Hu * C.e2u * (k.s_e - cur.s));
+    const double num = cur.u * k.Hu + qdiv<SAFE>(C.rdt * (adv + vis + cor + hpg), C.e12u, C.r_e12u, bad);
+    const double q = num / (cur.hu + 0.0);
+    o.ua = east ? 0.0 : qdiv<SAFE>(q, C.cfric, C.r_cfric, bad);
+  }
+  // v equation (:527-606); v(c,jpj) is the north wall (:658)
+  {
+    const double Fvx_w = up(Fvx);
+    const double Gx_w = up(Gx);
+    const double hv_w = up(cur.hv);
+    const double sv_w = up(sv);
+    const double uec_w = up(uec);
+    const double adv = Fvx_w - Fvx + k.Fvy_s - Fvy_n;
+    const double dvdx_e = east ? 0.0 : Gx * Re;
+    const double dvdx_w = west1 ? 0.0 : Gx_w * ((Hv + hv_w) + sv_w);
+    double vis = (Dvy_n - k.Dvy_s) * C.e1v + (dvdx_e - dvdx_w) * C.e2v * 0.5;
+    vis = C.visc * vis;
+    const double cor = -(0.5 * (C.fcor * (uec + uec_w)) * C.e12v * Hv);
+    const double hpg = -(C.g * Hv * C.e1v * (nx.s - cur.s));
+    const double num = cur.v * Hv + qdiv<SAFE>(C.rdt * (adv + vis + cor + hpg), C.e12v, C.r_e12v, bad);
+    const double q = num / (cur.hv + 0.0);
+    o.va = north ? 0.0 : qdiv<SAFE>(q, C.cfric, C.r_cfric, bad);
+  }
+  o.sv = sv;
+  // carry to row j+1
+  o.next.su = su_n;
+  o.next.Hu = Hu_n;
+  o.next.s_e = s_e_n;
+  o.next.Fuy_s = Fuy;
+  o.next.dudy_s = Gy * ((Hu_n + cur.hu) + k.su);  // dudy_s of u(c,j+1)
+  o.next.vnc_s = vnc;
+  o.next.Fvy_s = Fvy_n;
+  o.next.Dvy_s = Dvy_n;
+  o.next.cf_s = r3;
+}
+
+// Carried values at row J0 from rows J0-1 (p) and J0 (q).
+template <bool SAFE>
+__device__ __forceinline__ void prologue(const Consts& C, int c, int J0, int jpi, int jpj,
+                                         double sv_p_stored, const Cell& p, const Cell& q,
+                                         Carry& k, double& sv_p, bool& bad) {
+  k.s_e = dn(q.s);
+  k.su = interp_u(C, c, jpi, q.s, k.s_e, SAFE, bad);
+  k.Hu = q.hu + k.su;
+  sv_p = (J0 == 1) ? sv_p_stored : interp_v(C, J0 - 1, jpj, p.s, q.s, SAFE, bad);
+  const double Hv_p = p.hv + sv_p;
+  // corner (c, J0-1): south face of u(c, J0)
+  const double vnc = 0.5 * (p.v + dn(p.v));
+  const double vn_ = 0.5 * vnc * C.two_dx;
+  const double dep = 0.5 * ((Hv_p + dn(p.hv)) + dn(sv_p));
+  const double uu = (J0 == 1) ? upwind_hi_only(vn_, q.u) : upwind(vn_, p.u, q.u);
+  k.Fuy_s = uu * vn_ * dep;
+  k.vnc_s = vnc;
+  const double s_e_p = dn(p.s);
+  if (J0 == 1) {
+    k.dudy_s = 0.0;
+  } else {
+    const double su_p = interp_u(C, c, jpi, p.s, s_e_p, SAFE, bad);
+    const double gy = qdiv<SAFE>(q.u - p.u, C.two_dy, C.r_2dy, bad);
+    k.dudy_s = gy * ((k.Hu + p.hu) + su_p);
+  }
+  // T(c, J0): south face of v(c, J0)
+  const double vs = 0.5 * (q.v + p.v) * C.e1t;
+  const double depc = q.ht + q.s;
+  k.Fvy_s = upwind(vs, p.v, q.v) * vs * depc;
+  k.Dvy_s = qdiv<SAFE>(q.v - p.v, C.e2t, C.r_e2t, bad) * depc;
+  k.cf_s = Hv_p * p.v;
+}
+
+// NWARPS warps per CTA; MINB > 0 asks the compiler to fit MINB CTAs per SM
+// (register cap 65536 / (32*NWARPS*MINB)).
+template <int NWARPS, int MINB>
+__global__ void __launch_bounds__(32 * NWARPS, MINB)
 k_fused_step(Layout L, Consts C, FusedArgs A, int tile_y) {
   const int jpi = L.jpi, jpj = L.jpj;
-  const int i = 1 + 2 * (int)(blockIdx.x * blockDim.x + threadIdx.x);
-  if (i > jpi) return;
-  const bool two = (i + 1 <= jpi);
+  const int lane = threadIdx.x & 31;
+  const int warp = (int)(blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5));
+  const int c0 = 1 + COLS_PER_WARP * warp;
+  if (c0 > jpi) return;  // whole warp idle
   const int J0 = 1 + (int)blockIdx.y * tile_y;
   if (J0 > jpj) return;
   const int J1 = min(J0 + tile_y - 1, jpj);
+  const int c = c0 + lane - 1;
+  const int cl = min(c, jpi + 1);  // lanes beyond the halo column read column jpi+1
+  const bool store = (lane >= 1) && (lane <= COLS_PER_WARP) && (c <= jpi);
 
-  Row cur, nx;
-  // ---- prologue: carried values for row J0 from rows J0-1 and J0 ---------
-  double su_c[3], Hu_c[3];        // sshn_u and hu+sshn_u at row j, cols i-1..i+1
-  double Fuy_s[2], dudy_s[2];     // u-eq south-face flux and dudy_s for row j
-  double vnc_s[2];                // v_sc of u(c,j)
-  double Fvy_s[2], Dvy_s[2];      // v-eq south-face flux and dvdy_s for row j
-  double cf_s[2];                 // continuity south flux (sshn_v+hv)*vn at jj-1
-  double sv0[2] = {0.0, 0.0}, hv0[2] = {0.0, 0.0};  // open boundary row (Flather)
+  // lanes span columns c0-1 .. c0+30; the interior row form applies when
+  // none of them is 0, 1 or jpi
+  const bool edge_warp = (c0 - 1 <= 1) || (c0 + COLS_PER_WARP >= jpi);
+
+  Cell p, cur, nx;
+  load_cell(p, A, L.idx(cl, J0 - 1));
+  load_cell(cur, A, L.idx(cl, J0));
+  const double sv_stored = (J0 == 1) ? __ldg(A.sshv0 + L.idx(cl, 0)) : 0.0;
+  Carry k;
+  double sv0;
   {
-    Row pr;
-    load_row(pr, A, L.idx(i, J0 - 1));
-    load_row(cur, A, L.idx(i, J0));
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      su_c[k] = interp_u(C, i + k - 1, jpi, cur.s[k], cur.s[k + 1]);
-      Hu_c[k] = cur.hu[k] + su_c[k];
-    }
-    double sv_p[4], Hv_p[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      if (J0 == 1)
-        sv_p[k] = __ldg(A.sshv0 + L.idx(i + k - 1, 0));
-      else
-        sv_p[k] = interp_v(C, J0 - 1, jpj, pr.s[k], cur.s[k]);
-      Hv_p[k] = pr.hv[k] + sv_p[k];
-    }
-#pragma unroll
-    for (int l = 0; l < 2; ++l) {
-      // corner (i+l, J0-1): south face of u(i+l, J0)
-      double vnc = 0.5 * (pr.v[l + 1] + pr.v[l + 2]);
-      double vn_ = 0.5 * vnc * C.two_dx;
-      double dep = 0.5 * ((Hv_p[l + 1] + pr.hv[l + 2]) + sv_p[l + 2]);
-      double uu = (J0 == 1) ? upwind_hi_only(vn_, cur.u[l + 1])
-                            : upwind(vn_, pr.u[l + 1], cur.u[l + 1]);
-      Fuy_s[l] = uu * vn_ * dep;
-      vnc_s[l] = vnc;
-      if (J0 == 1) {
-        dudy_s[l] = 0.0;
-      } else {
-        double su_p = interp_u(C, i + l, jpi, pr.s[l + 1], pr.s[l + 2]);
-        double gy = div_const(cur.u[l + 1] - pr.u[l + 1], C.two_dy, C.r_2dy);
-        dudy_s[l] = gy * ((Hu_c[l + 1] + pr.hu[l + 1]) + su_p);
-      }
-      // T(i+l, J0): south face of v(i+l, J0)
-      double vlo = pr.v[l + 1], vhi = cur.v[l + 1];
-      double vs = 0.5 * (vhi + vlo) * C.e1t;
-      double depc = cur.ht[l] + cur.s[l + 1];
-      Fvy_s[l] = upwind(vs, vlo, vhi) * vs * depc;
-      Dvy_s[l] = div_const(vhi - vlo, C.e2t, C.r_e2t) * depc;
-      cf_s[l] = Hv_p[l + 1] * pr.v[l + 1];
-      if (J0 == 1) {
-        sv0[l] = sv_p[l + 1];
-        hv0[l] = pr.hv[l + 1];
-      }
-    }
+    bool bad = false;
+    prologue<false>(C, c, J0, jpi, jpj, sv_stored, p, cur, k, sv0, bad);
+    if (__any_sync(FULL, bad)) prologue<true>(C, c, J0, jpi, jpj, sv_stored, p, cur, k, sv0, bad);
   }
+  const double hv0 = p.hv;
+  load_cell(nx, A, L.idx(cl, J0 + 1));
 
+  const long pitch = L.pitch;
+  long o_ld = L.idx(cl, J0 + 2);  // prefetch row
+  const long o_last = L.idx(cl, jpj + 1);
+  long o_st = L.idx(c, J0);
+#pragma unroll 1
   for (int j = J0; j <= J1; ++j) {
-    load_row(nx, A, L.idx(i, j + 1));
-    const bool south = (j == 1), north = (j == jpj);
+    Cell pf;
+    load_cell(pf, A, o_ld < o_last ? o_ld : o_last);  // row j+2 (clamped to jpj+1)
+    o_ld += pitch;
 
-    // sshn_v and hv+sshn_v at row j, cols i-1..i+2
-    double sv[4], Hv[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      sv[k] = interp_v(C, j, jpj, cur.s[k], nx.s[k]);
-      Hv[k] = cur.hv[k] + sv[k];
+    RowOut o;
+    bool bad = false;
+    if (edge_warp || j == 1 || j == jpj)
+      row<false, true>(C, c, j, jpi, jpj, A.tide, cur, nx, k, o, bad);
+    else
+      row<false, false>(C, c, j, jpi, jpj, A.tide, cur, nx, k, o, bad);
+    if (__any_sync(FULL, bad)) {
+      bool b2 = false;
+      row<true, true>(C, c, j, jpi, jpj, A.tide, cur, nx, k, o, b2);
     }
-    // sshn_u and hu+sshn_u at row j+1, cols i-1..i+1
-    double su_n[3], Hu_n[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      su_n[k] = interp_u(C, i + k - 1, jpi, nx.s[k], nx.s[k + 1]);
-      Hu_n[k] = nx.hu[k] + su_n[k];
-    }
-
-    // x-faces of the u equation at T(c,j), c = i .. i+2 (between u(c-1), u(c))
-    double Fx[3], Dx[3];
-#pragma unroll
-    for (int l = 0; l < 3; ++l) {
-      double ulo = cur.u[l], uhi = cur.u[l + 1];
-      double uw = 0.5 * (uhi + ulo) * C.e2t;
-      double dep = cur.ht[l] + cur.s[l + 1];
-      Fx[l] = upwind(uw, ulo, uhi) * uw * dep;
-      Dx[l] = div_const(uhi - ulo, C.e1t, C.r_e1t) * dep;
-    }
-
-    // corners (c, j), c = i-1 .. i+1: east face of v(c,j); north face of u(c,j)
-    double Fvx[3], Gx[3], uec[3], Sn[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      const int c = i + k - 1;
-      uec[k] = 0.5 * (cur.u[k] + nx.u[k]);
-      double ue = 0.5 * uec[k] * C.two_dy;
-      Sn[k] = (Hu_c[k] + nx.hu[k]) + su_n[k];
-      double depe = 0.5 * Sn[k];
-      double vlo = cur.v[k], vhi = cur.v[k + 1];
-      double uu = (c == 0) ? upwind_hi_only(ue, vhi)
-                           : (c == jpi) ? upwind_lo_only(ue, vlo) : upwind(ue, vlo, vhi);
-      Fvx[k] = uu * ue * depe;
-      Gx[k] = div_const(vhi - vlo, C.two_dx, C.r_2dx);
-    }
-    double Fuy[2], Re[2], vnc[2], Gy[2];
-#pragma unroll
-    for (int l = 0; l < 2; ++l) {
-      const int k = l + 1;  // corner index of column i+l
-      vnc[l] = 0.5 * (cur.v[k] + cur.v[k + 1]);
-      double vn_ = 0.5 * vnc[l] * C.two_dx;
-      Re[l] = (Hv[k] + cur.hv[k + 1]) + sv[k + 1];
-      double depn = 0.5 * Re[l];
-      double ulo = cur.u[k], uhi = nx.u[k];
-      double uu = north ? upwind_lo_only(vn_, ulo) : upwind(vn_, ulo, uhi);
-      Fuy[l] = uu * vn_ * depn;
-      Gy[l] = div_const(uhi - ulo, C.two_dy, C.r_2dy);
-    }
-
-    // v-eq faces at T(c, j+1), c = i, i+1 (between v(c,j) and v(c,j+1))
-    double Fvy_n[2], Dvy_n[2];
-#pragma unroll
-    for (int l = 0; l < 2; ++l) {
-      double vlo = cur.v[l + 1], vhi = nx.v[l + 1];
-      double vs = 0.5 * (vhi + vlo) * C.e1t;
-      double dep = nx.ht[l] + nx.s[l + 1];
-      Fvy_n[l] = upwind(vs, vlo, vhi) * vs * dep;
-      Dvy_n[l] = div_const(vhi - vlo, C.e2t, C.r_e2t) * dep;
-    }
-
-    double ssha[2], ua[2], va[2];
-#pragma unroll
-    for (int l = 0; l < 2; ++l) {
-      const int c = i + l;
-      // continuity (:399-403) and the clamped SSH row (:631-644)
-      double r1 = Hu_c[l + 1] * cur.u[l + 1];
-      double r2 = Hu_c[l] * cur.u[l];
-      double r3 = Hv[l + 1] * cur.v[l + 1];
-      double r4 = cf_s[l];
-      double ssh = cur.s[l + 1] + div_const((r2 - r1 + r4 - r3) * C.rdt, C.e12t, C.r_e12t);
-      ssha[l] = south ? A.tide : ssh;
-      cf_s[l] = r3;
-
-      // u equation (:439-514); u(jpi,j) is the east wall (:650)
-      {
-        double adv = Fx[l] - Fx[l + 1] + Fuy_s[l] - Fuy[l];
-        double dudy_n = north ? 0.0 : Gy[l] * Sn[l + 1];
-        double dudy_sl = south ? 0.0 : dudy_s[l];
-        double vis = (Dx[l + 1] - Dx[l]) * C.e2u + (dudy_n - dudy_sl) * C.e1u * 0.5;
-        vis = C.visc * vis;
-        double Hu = Hu_c[l + 1];
-        double cor = 0.5 * (C.fcor * (vnc_s[l] + vnc[l])) * C.e12u * Hu;
-        double hpg = -(C.g * Hu * C.e2u * (cur.s[l + 2] - cur.s[l + 1]));
-        double num = cur.u[l + 1] * Hu +
-                     div_const(C.rdt * (adv + vis + cor + hpg), C.e12u, C.r_e12u);
-        double q = num / (cur.hu[l + 1] + 0.0);
-        ua[l] = (c == jpi) ? 0.0 : div_const(q, C.cfric, C.r_cfric);
-      }
-      // v equation (:527-606); v(c,jpj) is the north wall (:658)
-      {
-        double adv = Fvx[l] - Fvx[l + 1] + Fvy_s[l] - Fvy_n[l];
-        double dvdx_e = (c == jpi) ? 0.0 : Gx[l + 1] * Re[l];
-        double dvdx_w = (c == 1) ? 0.0 : Gx[l] * ((Hv[l + 1] + cur.hv[l]) + sv[l]);
-        double vis = (Dvy_n[l] - Dvy_s[l]) * C.e1v + (dvdx_e - dvdx_w) * C.e2v * 0.5;
-        vis = C.visc * vis;
-        double Hv_ = Hv[l + 1];
-        double cor = -(0.5 * (C.fcor * (uec[l + 1] + uec[l])) * C.e12v * Hv_);
-        double hpg = -(C.g * Hv_ * C.e1v * (nx.s[l + 1] - cur.s[l + 1]));
-        double num = cur.v[l + 1] * Hv_ +
-                     div_const(C.rdt * (adv + vis + cor + hpg), C.e12v, C.r_e12v);
-        double q = num / (cur.hv[l + 1] + 0.0);
-        va[l] = north ? 0.0 : div_const(q, C.cfric, C.r_cfric);
+    if (store) {
+      A.ssha[o_st] = o.ssha;
+      A.ua[o_st] = o.ua;
+      A.va[o_st] = o.va;
+      if (edge_warp && c == 1) A.ua[o_st - 1] = 0.0;  // u(0,j), west wall (:650)
+      if (j == 1) {
+        // Flather open boundary (:684-695): v(c,0) = v(c,1) + sqrt(g/hv(c,0))*(sshn_v(c,0) - sshn_v(c,1))
+        A.va[o_st - pitch] = o.va + sqrt(kG / hv0) * (sv0 - o.sv);
       }
     }
-
-    // ---- stores ----------------------------------------------------------
-    const long o = L.idx(i, j);
-    if (two) {
-      *reinterpret_cast<double2*>(A.ssha + o) = make_double2(ssha[0], ssha[1]);
-      *reinterpret_cast<double2*>(A.ua + o) = make_double2(ua[0], ua[1]);
-      *reinterpret_cast<double2*>(A.va + o) = make_double2(va[0], va[1]);
-    } else {
-      A.ssha[o] = ssha[0];
-      A.ua[o] = ua[0];
-      A.va[o] = va[0];
-    }
-    if (i == 1) A.ua[o - 1] = 0.0;  // u(0,j), west wall (:650)
-    if (south) {
-      // Flather open boundary, v(c,0) = v(c,1) + sqrt(g/hv)*(sshn_v(c,0)-sshn_v(c,1))  (:684-695)
-      const long o0 = L.idx(i, 0);
-      double f0 = va[0] + sqrt(kG / hv0[0]) * (sv0[0] - sv[1]);
-      double f1 = va[1] + sqrt(kG / hv0[1]) * (sv0[1] - sv[2]);
-      if (two) {
-        *reinterpret_cast<double2*>(A.va + o0) = make_double2(f0, f1);
-      } else {
-        A.va[o0] = f0;
-      }
-    }
-
-    // ---- carry to row j+1 ------------------------------------------------
-#pragma unroll
-    for (int l = 0; l < 2; ++l) {
-      Fuy_s[l] = Fuy[l];
-      // dudy_s of u(c, j+1): ((un(j+1)-un(j))/(e2u+e2u)) * (Hu(j+1) + hu(j) + sshn_u(j))
-      dudy_s[l] = Gy[l] * ((Hu_n[l + 1] + cur.hu[l + 1]) + su_c[l + 1]);
-      vnc_s[l] = vnc[l];
-      Fvy_s[l] = Fvy_n[l];
-      Dvy_s[l] = Dvy_n[l];
-    }
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      su_c[k] = su_n[k];
-      Hu_c[k] = Hu_n[k];
-    }
+    o_st += pitch;
+    k = o.next;
     cur = nx;
+    nx = pf;
   }
 }
 
 }  // namespace
 
-cudaError_t launch_fused_step(const Layout& L, const Consts& C, const FusedArgs& a, int tile_x,
-                              int tile_y, cudaStream_t s) {
-  // tile_x = T columns per CTA (two per thread)
-  int threads = tile_x / 2;
-  if (threads < 32) threads = 32;
-  if (threads > 128) threads = 128;
-  int cols_per_cta = 2 * threads;
-  dim3 grid((unsigned)((L.jpi + cols_per_cta - 1) / cols_per_cta),
-            (unsigned)((L.jpj + tile_y - 1) / tile_y));
-  k_fused_step<<<grid, threads, 0, s>>>(L, C, a, tile_y);
+template <int NW, int MB>
+static cudaError_t launch_variant(const Layout& L, const Consts& C, const FusedArgs& a, int tile_y,
+                                  cudaStream_t s) {
+  const int cols_per_cta = COLS_PER_WARP * NW;
+  const int gx = (L.jpi + cols_per_cta - 1) / cols_per_cta;
+  if (tile_y <= 0) {
+    // single wave: as many row blocks as the resident CTA slots allow
+    static int slots = 0;  // CTAs of this variant resident on the whole device
+    if (slots == 0) {
+      int dev = 0, sms = 0, per_sm = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fused_step<NW, MB>, 32 * NW, 0);
+      slots = sms * (per_sm > 0 ? per_sm : 1);
+    }
+    int nrb = slots / gx;
+    if (nrb < 1) nrb = 1;
+    tile_y = (L.jpj + nrb - 1) / nrb;
+  }
+  dim3 grid((unsigned)gx, (unsigned)((L.jpj + tile_y - 1) / tile_y));
+  k_fused_step<NW, MB><<<grid, 32 * NW, 0, s>>>(L, C, a, tile_y);
   return cudaGetLastError();
 }
 
+// warps: 2, 4 or 8 per CTA; occ: register budget as resident warps per SM
+// (0: compiler's choice, 16 or 20).
+cudaError_t launch_fused_step(const Layout& L, const Consts& C, const FusedArgs& a, int warps,
+                              int occ, int tile_y, cudaStream_t s) {
+  switch (warps * 100 + occ) {
+    case 200: return launch_variant<2, 1>(L, C, a, tile_y, s);
+    case 216: return launch_variant<2, 8>(L, C, a, tile_y, s);
+    case 220: return launch_variant<2, 10>(L, C, a, tile_y, s);
+    case 400: return launch_variant<4, 1>(L, C, a, tile_y, s);
+    case 416: return launch_variant<4, 4>(L, C, a, tile_y, s);
+    case 420: return launch_variant<4, 5>(L, C, a, tile_y, s);
+    case 800: return launch_variant<8, 1>(L, C, a, tile_y, s);
+    case 816: return launch_variant<8, 2>(L, C, a, tile_y, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace nemo
+
+namespace nemo {
+bool fused_variant_ok(int warps, int occ) {
+  if (warps == 2 || warps == 4) return occ == 0 || occ == 16 || occ == 20;
+  if (warps == 8) return occ == 0 || occ == 16;
+  return false;
+}
 }  // namespace nemo

@@ -46,8 +46,11 @@ struct FusedArgs {
   double *ssha, *ua, *va;
   double tide;          // clamped SSH value for this step
 };
-cudaError_t launch_fused_step(const Layout& L, const Consts& C, const FusedArgs& a,
-                              int tile_x, int tile_y, cudaStream_t s);
+// warps per CTA (2, 4, 8), register budget as resident warps per SM (0, 16,
+// 20; 8 warps supports 0 and 16), rows per CTA.
+cudaError_t launch_fused_step(const Layout& L, const Consts& C, const FusedArgs& a, int warps,
+                              int occ, int tile_y, cudaStream_t s);
+bool fused_variant_ok(int warps, int occ);
 
 // Sums |f(1:jpi,1:jpj)| of nf fields into out[0..nf-1] (device), fixed order.
 // row_partials: nf*jpj doubles of scratch.

@@ -34,7 +34,7 @@ EXPORTED = [
     "nemo_momentum_u", "nemo_momentum_v", "nemo_bc", "nemo_bc_ssh", "nemo_bc_solid_u",
     "nemo_bc_solid_v", "nemo_bc_flather_u", "nemo_bc_flather_v", "nemo_next", "nemo_step",
     "nemo_step_n", "nemo_checksums", "nemo_checksum", "nemo_retrieve", "nemo_set_state",
-    "nemo_sync", "nemo_get_dims", "nemo_device_field", "nemo_set_tile", "nemo_get_tile",
+    "nemo_sync", "nemo_get_dims", "nemo_device_field", "nemo_set_schedule", "nemo_get_schedule",
     "nemo_status_string", "nemo_build_is_strict",
     "cuda_setup_model_params_", "cuda_initialise_grid_", "cuda_continuity_", "cuda_momentum_",
     "cuda_boundary_conditions_", "cuda_next_", "cuda_retrieve_grid_constants_",
@@ -60,6 +60,10 @@ class Params(ctypes.Structure):
         ("bump_wmax", ctypes.c_double), ("hmin", ctypes.c_double), ("hmax", ctypes.c_double),
         ("stream", ctypes.c_void_p), ("device", ctypes.c_int),
     ]
+
+
+class Schedule(ctypes.Structure):
+    _fields_ = [("warps", ctypes.c_int), ("occupancy", ctypes.c_int), ("rows", ctypes.c_int)]
 
 
 def lib_path(strict=False):
@@ -96,8 +100,8 @@ def load(strict=False):
     L.nemo_set_state.argtypes = [vp, P(dp), P(dp), P(dp)]
     L.nemo_get_dims.argtypes = [vp, P(ip), P(ip)]
     L.nemo_device_field.argtypes = [vp, ip, P(P(dp)), P(ctypes.c_long)]
-    L.nemo_set_tile.argtypes = [vp, ip, ip]
-    L.nemo_get_tile.argtypes = [vp, P(ip), P(ip)]
+    L.nemo_set_schedule.argtypes = [vp, P(Schedule)]
+    L.nemo_get_schedule.argtypes = [vp, P(Schedule)]
     L.nemo_status_string.argtypes = [ip]
     L.nemo_status_string.restype = ctypes.c_char_p
     L.nemo_build_is_strict.restype = ip
@@ -218,13 +222,14 @@ class Model:
     def step_n(self, istp0, n):
         check(self.lib.nemo_step_n(self.h, istp0, n), "nemo_step_n")
 
-    def set_tile(self, tx, ty):
-        check(self.lib.nemo_set_tile(self.h, tx, ty), "nemo_set_tile")
+    def set_schedule(self, warps=4, occupancy=0, rows=64):
+        s = Schedule(warps, occupancy, rows)
+        check(self.lib.nemo_set_schedule(self.h, ctypes.byref(s)), "nemo_set_schedule")
 
-    def get_tile(self):
-        a, b = ctypes.c_int(), ctypes.c_int()
-        check(self.lib.nemo_get_tile(self.h, ctypes.byref(a), ctypes.byref(b)), "nemo_get_tile")
-        return a.value, b.value
+    def get_schedule(self):
+        s = Schedule()
+        check(self.lib.nemo_get_schedule(self.h, ctypes.byref(s)), "nemo_get_schedule")
+        return (s.warps, s.occupancy, s.rows)
 
     def sync(self):
         check(self.lib.nemo_sync(self.h), "nemo_sync")
