@@ -133,11 +133,13 @@ int nemo_set_state(nemo_ctx* ctx, const double* sshn, const double* un,
 int nemo_sync(nemo_ctx* ctx);
 int nemo_get_dims(nemo_ctx* ctx, int* jpi, int* jpj);
 /* Device address and pitch (in doubles) of a field's storage; element
- * (ji,jj) lives at ptr[(jj+1)*pitch + (ji+1)].  For device-side consumers. */
+ * (ji,jj) lives at ptr[(jj+1)*pitch + (ji+2)].  For device-side consumers. */
 int nemo_device_field(nemo_ctx* ctx, int field, double** ptr, long* pitch);
 /* Launch schedule of the fused kernel: warps per CTA (2, 4, 8; a warp covers
  * 30 columns), register budget as resident warps per SM (0 = compiler's
- * choice, 16, 20; 8-warp CTAs take 0 or 16) and rows marched per CTA
+ * choice, 16, 20, 24; 8-warp CTAs take 0, 16 or 24; a negative value, -16,
+ * -20, -24 for 2-warp and -20 for 4-warp CTAs, selects the same budget
+ * without the register prefetch of the next row) and rows marched per CTA
  * (0: one wave, row blocks sized so every CTA is resident at once).  In the
  * -fmad=false build every schedule gives bit-identical results. */
 typedef struct nemo_schedule {

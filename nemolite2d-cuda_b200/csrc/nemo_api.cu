@@ -261,8 +261,8 @@ int nemo_create(const nemo_params* p, nemo_ctx** out) {
   c->L.rows = (long)p->jpj + 3;
   c->C = make_consts(*p);
   c->sched.warps = 2;
-  c->sched.occupancy = 20;
-  c->sched.rows = 0;
+  c->sched.occupancy = -24;
+  c->sched.rows = 16;
   int st = set_device(c);
   if (st) { delete c; return st; }
   cudaError_t e;
@@ -441,7 +441,8 @@ int nemo_step_n(nemo_ctx* c, int istp0, int n) {
     a.ua = aset(c).u;
     a.va = aset(c).v;
     a.tide = tide_value(c->p, istp0 + k);
-    CK(launch_fused_step(c->L, c->C, a, c->sched.warps, c->sched.occupancy, c->sched.rows, c->stream));
+    CK(launch_fused_step(c->L, c->C, a, c->sched.warps, c->sched.occupancy, c->sched.rows,
+                         c->stream));
     c->n_idx = 1 - c->n_idx;  // next: the new state becomes "now"
   }
   c->a_mirrors_n = true;

@@ -12,22 +12,23 @@ constexpr double kPi = 3.1415926535897932;
 constexpr double kG = 9.80665;
 constexpr double kOmega = 7.292116e-05;
 
-// Storage of every 2-D field: one pitched array over ji in [-1, pitch-2],
-// jj in [-1, jpj+1]; element (ji,jj) at base[(jj+1)*pitch + ji+1].  Fortran
+// Storage of every 2-D field: one pitched array over ji in [-2, pitch-3],
+// jj in [-1, jpj+1]; element (ji,jj) at base[(jj+1)*pitch + ji+2].  Fortran
 // bounds (0:jpi,1:jpj) etc. are windows of it, so the C-grid staggering
 // needs no per-field index arithmetic.  pitch is a multiple of 32 doubles,
-// so rows start on 256-byte boundaries and ji odd starts a 16-byte pair.
+// so rows start on 256-byte boundaries and every even ji starts a 16-byte
+// pair; the pitch leaves room for the pair (jpi+1, jpi+2).
 struct Layout {
   int jpi, jpj;
   long pitch;
   long rows;  // jpj + 3
   __host__ __device__ __forceinline__ long idx(int ji, int jj) const {
-    return (long)(jj + 1) * pitch + (ji + 1);
+    return (long)(jj + 1) * pitch + (ji + 2);
   }
   __host__ __device__ long elems() const { return rows * pitch; }
 };
 
-inline long layout_pitch(int jpi) { return ((long)(jpi + 4) + 31) / 32 * 32; }
+inline long layout_pitch(int jpi) { return ((long)(jpi + 6) + 31) / 32 * 32; }
 
 // Per-run constants.  The reference's grid is uniform (original/nemolite2d.f90
 // :210-217): every e1* equals dx, every e2* equals dy, every e12* equals

@@ -232,7 +232,9 @@ __device__ __forceinline__ void prologue(const Consts& C, int c, int J0, int jpi
 
 // NWARPS warps per CTA; MINB > 0 asks the compiler to fit MINB CTAs per SM
 // (register cap 65536 / (32*NWARPS*MINB)).
-template <int NWARPS, int MINB>
+// PF: 1 prefetches row j+2 into registers while row j is computed; 0 loads
+// row j+1 at the top of each iteration (fewer live registers).
+template <int NWARPS, int MINB, int PF>
 __global__ void __launch_bounds__(32 * NWARPS, MINB)
 k_fused_step(Layout L, Consts C, FusedArgs A, int tile_y) {
   const int jpi = L.jpi, jpj = L.jpj;
@@ -263,16 +265,20 @@ k_fused_step(Layout L, Consts C, FusedArgs A, int tile_y) {
     if (__any_sync(FULL, bad)) prologue<true>(C, c, J0, jpi, jpj, sv_stored, p, cur, k, sv0, bad);
   }
   const double hv0 = p.hv;
-  load_cell(nx, A, L.idx(cl, J0 + 1));
+  if (PF) load_cell(nx, A, L.idx(cl, J0 + 1));
 
   const long pitch = L.pitch;
-  long o_ld = L.idx(cl, J0 + 2);  // prefetch row
+  long o_ld = L.idx(cl, J0 + 1 + PF);  // next row to load
   const long o_last = L.idx(cl, jpj + 1);
   long o_st = L.idx(c, J0);
 #pragma unroll 1
   for (int j = J0; j <= J1; ++j) {
     Cell pf;
-    load_cell(pf, A, o_ld < o_last ? o_ld : o_last);  // row j+2 (clamped to jpj+1)
+    if (PF) {
+      load_cell(pf, A, o_ld < o_last ? o_ld : o_last);  // row j+2 (clamped to jpj+1)
+    } else {
+      load_cell(nx, A, o_ld);  // row j+1 <= jpj+1
+    }
     o_ld += pitch;
 
     RowOut o;
@@ -298,13 +304,13 @@ k_fused_step(Layout L, Consts C, FusedArgs A, int tile_y) {
     o_st += pitch;
     k = o.next;
     cur = nx;
-    nx = pf;
+    if (PF) nx = pf;
   }
 }
 
 }  // namespace
 
-template <int NW, int MB>
+template <int NW, int MB, int PF>
 static cudaError_t launch_variant(const Layout& L, const Consts& C, const FusedArgs& a, int tile_y,
                                   cudaStream_t s) {
   const int cols_per_cta = COLS_PER_WARP * NW;
@@ -316,7 +322,7 @@ static cudaError_t launch_variant(const Layout& L, const Consts& C, const FusedA
       int dev = 0, sms = 0, per_sm = 0;
       cudaGetDevice(&dev);
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fused_step<NW, MB>, 32 * NW, 0);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fused_step<NW, MB, PF>, 32 * NW, 0);
       slots = sms * (per_sm > 0 ? per_sm : 1);
     }
     int nrb = slots / gx;
@@ -324,23 +330,31 @@ static cudaError_t launch_variant(const Layout& L, const Consts& C, const FusedA
     tile_y = (L.jpj + nrb - 1) / nrb;
   }
   dim3 grid((unsigned)gx, (unsigned)((L.jpj + tile_y - 1) / tile_y));
-  k_fused_step<NW, MB><<<grid, 32 * NW, 0, s>>>(L, C, a, tile_y);
+  k_fused_step<NW, MB, PF><<<grid, 32 * NW, 0, s>>>(L, C, a, tile_y);
   return cudaGetLastError();
 }
 
 // warps: 2, 4 or 8 per CTA; occ: register budget as resident warps per SM
-// (0: compiler's choice, 16 or 20).
+// (0: compiler's choice, 16, 20, 24); a negative occ selects the variant
+// without the register prefetch of the next row.
 cudaError_t launch_fused_step(const Layout& L, const Consts& C, const FusedArgs& a, int warps,
                               int occ, int tile_y, cudaStream_t s) {
   switch (warps * 100 + occ) {
-    case 200: return launch_variant<2, 1>(L, C, a, tile_y, s);
-    case 216: return launch_variant<2, 8>(L, C, a, tile_y, s);
-    case 220: return launch_variant<2, 10>(L, C, a, tile_y, s);
-    case 400: return launch_variant<4, 1>(L, C, a, tile_y, s);
-    case 416: return launch_variant<4, 4>(L, C, a, tile_y, s);
-    case 420: return launch_variant<4, 5>(L, C, a, tile_y, s);
-    case 800: return launch_variant<8, 1>(L, C, a, tile_y, s);
-    case 816: return launch_variant<8, 2>(L, C, a, tile_y, s);
+    case 200: return launch_variant<2, 1, 1>(L, C, a, tile_y, s);
+    case 216: return launch_variant<2, 8, 1>(L, C, a, tile_y, s);
+    case 220: return launch_variant<2, 10, 1>(L, C, a, tile_y, s);
+    case 224: return launch_variant<2, 12, 1>(L, C, a, tile_y, s);
+    case 200 - 16: return launch_variant<2, 8, 0>(L, C, a, tile_y, s);
+    case 200 - 20: return launch_variant<2, 10, 0>(L, C, a, tile_y, s);
+    case 200 - 24: return launch_variant<2, 12, 0>(L, C, a, tile_y, s);
+    case 400: return launch_variant<4, 1, 1>(L, C, a, tile_y, s);
+    case 416: return launch_variant<4, 4, 1>(L, C, a, tile_y, s);
+    case 420: return launch_variant<4, 5, 1>(L, C, a, tile_y, s);
+    case 424: return launch_variant<4, 6, 1>(L, C, a, tile_y, s);
+    case 400 - 20: return launch_variant<4, 5, 0>(L, C, a, tile_y, s);
+    case 800: return launch_variant<8, 1, 1>(L, C, a, tile_y, s);
+    case 816: return launch_variant<8, 2, 1>(L, C, a, tile_y, s);
+    case 824: return launch_variant<8, 3, 1>(L, C, a, tile_y, s);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -349,8 +363,10 @@ cudaError_t launch_fused_step(const Layout& L, const Consts& C, const FusedArgs&
 
 namespace nemo {
 bool fused_variant_ok(int warps, int occ) {
-  if (warps == 2 || warps == 4) return occ == 0 || occ == 16 || occ == 20;
-  if (warps == 8) return occ == 0 || occ == 16;
+  if (warps == 2) return occ == 0 || occ == 16 || occ == 20 || occ == 24 || occ == -16 ||
+                         occ == -20 || occ == -24;
+  if (warps == 4) return occ == 0 || occ == 16 || occ == 20 || occ == 24 || occ == -20;
+  if (warps == 8) return occ == 0 || occ == 16 || occ == 24;
   return false;
 }
 }  // namespace nemo

@@ -47,7 +47,8 @@ struct FusedArgs {
   double tide;          // clamped SSH value for this step
 };
 // warps per CTA (2, 4, 8), register budget as resident warps per SM (0, 16,
-// 20; 8 warps supports 0 and 16), rows per CTA.
+// 20, 24; negative: same budget without the next-row register prefetch), rows
+// per CTA (0: one wave).
 cudaError_t launch_fused_step(const Layout& L, const Consts& C, const FusedArgs& a, int warps,
                               int occ, int tile_y, cudaStream_t s);
 bool fused_variant_ok(int warps, int occ);

@@ -67,7 +67,9 @@ def test_strict_build_matches_golden_bitwise(nb, case, path):
 
 @pytest.mark.parametrize("jpi,jpj,tile", [(257, 131, (4, 0, 64)), (130, 300, (2, 20, 7)),
                                           (2, 2, (2, 0, 1)), (3, 5, (4, 16, 2)), (96, 33, (8, 16, 16)),
-                                          (61, 29, (4, 20, 3))])
+                                          (61, 29, (4, 24, 3)), (125, 40, (2, -16, 0)),
+                                          (62, 9, (2, 0, 0)), (63, 12, (8, 24, 5)),
+                                          (70, 21, (4, -20, 4))])
 def test_strict_fused_matches_oracle_ragged_bathymetry(nb, oracle_mod, jpi, jpj, tile):
     kw = dict(jpi=jpi, jpj=jpj, rdt=20.0, cbfr=0.00015, visc=0.1, amp_tide=0.5,
               tide_phase=0.3, nbump=12, seed=77, bump_amp=30.0, bump_wmin=3e3, bump_wmax=40e3,
@@ -115,6 +117,34 @@ def test_strict_routines_one_by_one_from_random_state(nb, oracle_mod):
         for name, fid in ALL:
             np.testing.assert_array_equal(bits(m.field(fid)), bits(o.field(fid)),
                                           err_msg="after %s: %s" % (label, name))
+
+
+@pytest.mark.parametrize("strict", [True, False])
+def test_tiny_values_take_the_exact_division_path(nb, oracle_mod, strict):
+    """A state whose values reach the subnormal range: quotients below 2^-959
+    must be recomputed with IEEE division, so the strict build stays
+    bit-identical to the oracle there too."""
+    jpi, jpj = 150, 90
+    kw = dict(jpi=jpi, jpj=jpj, rdt=20.0, cbfr=0.00015, visc=0.1, amp_tide=0.0)
+    rng = np.random.default_rng(5)
+    def tiny(shape):
+        mag = 10.0 ** rng.uniform(-322, -280, shape)
+        x = mag * rng.choice([-1.0, 1.0], shape)
+        x[rng.random(shape) < 0.3] = 0.0
+        return x
+    st = (tiny((jpj, jpi)), tiny((jpj, jpi + 1)), tiny((jpj + 1, jpi)))
+    m = nb.Model(strict=strict, **kw)
+    o = oracle_mod.Model(**kw)
+    m.set_state(*st)
+    o.set_state(*st)
+    m.step_n(1, 6)
+    o.run(1, 6)
+    for name, fid in STATE:
+        a, b = m.field(fid), o.field(fid)
+        if strict:
+            np.testing.assert_array_equal(bits(a), bits(b), err_msg=name)
+        else:
+            assert relerr(a, b) <= TOL, name
 
 
 def test_strict_fused_equals_routine_path_from_random_state(nb):
@@ -165,7 +195,7 @@ def test_strict_checksums_bitwise_tree_order(nb, oracle_mod):
 
 
 @pytest.mark.parametrize("sched", [(2, 0, 1), (2, 16, 16), (4, 0, 64), (4, 20, 5), (8, 16, 256),
-                                   (8, 0, 33)])
+                                   (8, 0, 33), (2, 24, 0), (2, -24, 16)])
 def test_schedule_does_not_change_results(nb, sched):
     """Strict build: bit-identical for every schedule.  Default build: each
     register-budget variant is compiled separately and may contract multiply-
