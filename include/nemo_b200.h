@@ -153,6 +153,25 @@ const char* nemo_status_string(int status);
 /* 1 when this library was built with -fmad=false (bit-exact build). */
 int nemo_build_is_strict(void);
 
+/* ---- allocation-free checksums ----------------------------------------------
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc
+ * (all device memory owned by their own pool, or a loop that must not pay a
+ * cudaMalloc's implicit device synchronisation): the checksums of
+ * nemo_checksums, in the same fixed reduction order, from plain device
+ * pointers, allocating nothing.  fields[k] points at element (1,1) of field k
+ * (column major, leading dimension ld doubles); out is a device array of
+ * nfields doubles; stream is a cudaStream_t (NULL: default stream).
+ * Limits: nfields <= 4, ny <= NEMO_NOALLOC_MAX_ROWS (larger ny returns
+ * NEMO_ERR_INVALID with a message on stderr).  Scratch is a fixed 512 KiB
+ * device array inside the library, held on every GPU that loads it until the
+ * process exits, and shared by all calls: calls that overlap on the GPU (for
+ * instance on two streams at once) race on it.  The first call on each
+ * device looks up the array's device address with that device current; make
+ * that first call before any stream capture. */
+#define NEMO_NOALLOC_MAX_ROWS 16384
+int nemo_checksums_noalloc(const double* const* fields, int nfields, int nx, int ny,
+                           long ld, double* out, void* stream);
+
 /* ---- drop-in symbols (cuda/cuda_nemolite2d.cu:234-270) --------------------
  * One default context.  Errors are printed to stderr and kept in a sticky
  * status readable with nemo_compat_last_status() (the reference threw a C++

@@ -35,7 +35,7 @@ EXPORTED = [
     "nemo_bc_solid_v", "nemo_bc_flather_u", "nemo_bc_flather_v", "nemo_next", "nemo_step",
     "nemo_step_n", "nemo_checksums", "nemo_checksum", "nemo_retrieve", "nemo_set_state",
     "nemo_sync", "nemo_get_dims", "nemo_device_field", "nemo_set_schedule", "nemo_get_schedule",
-    "nemo_status_string", "nemo_build_is_strict",
+    "nemo_status_string", "nemo_build_is_strict", "nemo_checksums_noalloc",
     "cuda_setup_model_params_", "cuda_initialise_grid_", "cuda_continuity_", "cuda_momentum_",
     "cuda_boundary_conditions_", "cuda_next_", "cuda_retrieve_grid_constants_",
     "cuda_retrieve_results_", "cuda_finalise_", "nemo_compat_last_status", "nemo_compat_context",
@@ -118,6 +118,8 @@ def load(strict=False):
     L.cuda_retrieve_results_.argtypes = [P(dp)] * 5 + [ip, ip]
     L.cuda_retrieve_results_.restype = None
     L.nemo_compat_context.restype = vp
+    L.nemo_checksums_noalloc.argtypes = [P(ctypes.c_void_p), ip, ip, ip, ctypes.c_long,
+                                         ctypes.c_void_p, ctypes.c_void_p]
     _libs[strict] = L
     return L
 
