@@ -153,6 +153,65 @@ const char* nemo_status_string(int status);
 /* 1 when this library was built with -fmad=false (bit-exact build). */
 int nemo_build_is_strict(void);
 
+/* ---- autotuning of the single-grid schedule ---------------------------------
+ * No counterpart in the reference.  Times every compiled schedule variant
+ * over `steps` fused steps (the model state is saved first and restored
+ * afterwards, so results are unaffected), installs the fastest and returns
+ * it.  With the environment variable NEMO_TUNE_CACHE naming a file, results
+ * are stored there per (GPU, grid size) and nemo_create applies a stored
+ * schedule. */
+int nemo_autotune(nemo_ctx* ctx, int steps, nemo_schedule* best, double* best_ms_per_step);
+
+/* ---- batched ensemble (no reference counterpart) ----------------------------
+ * Many independent model instances of uneven size advanced together: one
+ * persistent launch per step runs a work list of (member, column strip, row
+ * block) items over every member, and the n launches of nemo_ens_step_n are
+ * captured once in a CUDA graph and replayed.  Each member follows exactly
+ * the single-grid arithmetic (same kernels, same results as a nemo_ctx with
+ * the member's parameters). */
+typedef struct nemo_member {
+  int jpi, jpj;
+  double amp_tide, tide_phase;
+  double dep_const;
+  int nbump;
+  uint64_t seed;
+  double bump_amp, bump_wmin, bump_wmax, hmin, hmax;
+} nemo_member;
+
+typedef struct nemo_ens nemo_ens;
+
+typedef struct nemo_ens_schedule {
+  int warps;      /* warps per CTA: 2 or 4 */
+  int occupancy;  /* register budget, as nemo_schedule.occupancy */
+  int rows;       /* rows per work item */
+  int order;      /* work-list order: 0 member by member, 1 largest member first */
+  int ctas;       /* persistent grid size; 0: every resident CTA slot */
+} nemo_ens_schedule;
+
+/* The batched configuration's member recipe: sides log-uniform in
+ * [side_min, side_max], aspect ratio log-uniform in [0.5, 2], depth 100 m with
+ * 8 Gaussian bumps clamped to [50, 150] m, tidal amplitude
+ * amp_scale * U[0.5, 1.5] m and phase U[0, 2*pi), all drawn from seed. */
+int nemo_ens_generate(uint64_t seed, int nmem, int side_min, int side_max, double amp_scale,
+                      nemo_member* out);
+/* common supplies dx, dy, rdt, cbfr, visc, lat, stream and device. */
+int nemo_ens_create(const nemo_params* common, const nemo_member* members, int nmem,
+                    nemo_ens** out);
+int nemo_ens_destroy(nemo_ens* e);
+int nemo_ens_step_n(nemo_ens* e, int istp0, int n);
+/* out[3*m + k]: checksums of member m's sshn, un, vn (k = 0, 1, 2). */
+int nemo_ens_checksums(nemo_ens* e, double* out);
+int nemo_ens_retrieve(nemo_ens* e, int member, int field, double* host, long ld);
+int nemo_ens_set_state(nemo_ens* e, int member, const double* sshn, const double* un,
+                       const double* vn);
+int nemo_ens_set_schedule(nemo_ens* e, const nemo_ens_schedule* s);
+int nemo_ens_get_schedule(nemo_ens* e, nemo_ens_schedule* s);
+/* Graph capture of nemo_ens_step_n on (1, default) or off (0). */
+int nemo_ens_use_graph(nemo_ens* e, int on);
+int nemo_ens_info(nemo_ens* e, int* nmem, long long* cells);
+/* Times candidate schedules as nemo_autotune does, for the ensemble. */
+int nemo_ens_autotune(nemo_ens* e, int steps, nemo_ens_schedule* best, double* best_ms_per_step);
+
 /* ---- allocation-free checksums ----------------------------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc
  * (all device memory owned by their own pool, or a loop that must not pay a

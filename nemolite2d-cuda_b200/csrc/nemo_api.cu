@@ -6,7 +6,10 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <fstream>
 #include <new>
+#include <sstream>
+#include <string>
 #include <vector>
 
 #include "nemo_internal.h"
@@ -204,6 +207,53 @@ void depth_tables(const nemo_params& p, double* ax, double* gy) {
 
 }  // namespace nemo
 
+// ---- schedule cache (NEMO_TUNE_CACHE) ---------------------------------------
+// One line per (GPU, grid): "<gpu>:<jpi>x<jpj> warps occupancy rows ms".
+namespace {
+
+std::string tune_key(const nemo_ctx* c) {
+  cudaDeviceProp prop;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::string name = "gpu";
+  if (cudaGetDeviceProperties(&prop, dev) == cudaSuccess) name = prop.name;
+  for (auto& ch : name)
+    if (ch == ' ' || ch == ':') ch = '_';
+  std::ostringstream k;
+  k << name << ":" << c->L.jpi << "x" << c->L.jpj;
+  return k.str();
+}
+
+bool tune_lookup(const nemo_ctx* c, nemo_schedule* s) {
+  const char* path = getenv("NEMO_TUNE_CACHE");
+  if (!path || !*path) return false;
+  std::ifstream f(path);
+  if (!f) return false;
+  const std::string key = tune_key(c);
+  std::string line;
+  bool found = false;
+  while (std::getline(f, line)) {
+    std::istringstream ls(line);
+    std::string k;
+    nemo_schedule t;
+    double ms;
+    if (ls >> k >> t.warps >> t.occupancy >> t.rows >> ms && k == key && fused_variant_ok(t.warps, t.occupancy)) {
+      *s = t;
+      found = true;  // the last entry for a key wins
+    }
+  }
+  return found;
+}
+
+void tune_store(const nemo_ctx* c, const nemo_schedule& s, double ms) {
+  const char* path = getenv("NEMO_TUNE_CACHE");
+  if (!path || !*path) return;
+  std::ofstream f(path, std::ios::app);
+  if (f) f << tune_key(c) << " " << s.warps << " " << s.occupancy << " " << s.rows << " " << ms << "\n";
+}
+
+}  // namespace
+
 extern "C" {
 
 int nemo_default_params(nemo_params* p) {
@@ -322,6 +372,8 @@ int nemo_create(const nemo_params* p, nemo_ctx** out) {
     e = launch_init_sshn_uv(c->L, c->C, nset(c).ssh, c->sshn_u, c->sshn_v, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) { nemo_destroy(c); return status_from(e); }
+  nemo_schedule cached;
+  if (tune_lookup(c, &cached)) c->sched = cached;
   *out = c;
   return NEMO_OK;
 }
@@ -560,6 +612,73 @@ int nemo_set_schedule(nemo_ctx* c, const nemo_schedule* s) {
 int nemo_get_schedule(nemo_ctx* c, nemo_schedule* s) {
   if (!c || !s) return NEMO_ERR_INVALID;
   *s = c->sched;
+  return NEMO_OK;
+}
+
+int nemo_autotune(nemo_ctx* c, int steps, nemo_schedule* best, double* best_ms) {
+  if (!c || steps < 1) return NEMO_ERR_INVALID;
+  int st = set_device(c); if (st) return st;
+  // both state sets and the bookkeeping are restored afterwards
+  const size_t fe = (size_t)c->L.elems();
+  double* backup = nullptr;
+  CK(cudaMalloc(&backup, 6 * fe * sizeof(double)));
+  const int n_save = c->n_idx;
+  const bool a_save = c->a_mirrors_n, uv_save = c->uv_stale;
+  cudaError_t er = cudaSuccess;
+  for (int s = 0; s < 2 && er == cudaSuccess; ++s) {
+    double* f3[3] = {c->set[s].ssh, c->set[s].u, c->set[s].v};
+    for (int k = 0; k < 3 && er == cudaSuccess; ++k)
+      er = cudaMemcpyAsync(backup + (3 * s + k) * fe, f3[k], fe * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
+  }
+  const nemo_schedule keep = c->sched;
+  nemo_schedule bsched = keep;
+  double bms = 1e300;
+  const int wo[][2] = {{2, -24}, {2, -20}, {2, -16}, {2, 0}, {2, 16}, {2, 20}, {2, 24},
+                       {4, -20}, {4, 0}, {4, 16}, {4, 20}, {4, 24}, {8, 0}, {8, 16}, {8, 24}};
+  const int rows_c[] = {8, 16, 32, 0};
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  if (er == cudaSuccess) er = cudaEventCreate(&t0);
+  if (er == cudaSuccess) er = cudaEventCreate(&t1);
+  for (const auto& w : wo) {
+    for (int rows : rows_c) {
+      if (er != cudaSuccess || st) break;
+      nemo_schedule cand{w[0], w[1], rows};
+      c->sched = cand;
+      if ((st = nemo_step_n(c, 1, 1))) break;  // warm
+      er = cudaEventRecord(t0, c->stream);
+      if (er == cudaSuccess && (st = nemo_step_n(c, 2, steps))) break;
+      if (er == cudaSuccess) er = cudaEventRecord(t1, c->stream);
+      if (er == cudaSuccess) er = cudaEventSynchronize(t1);
+      float ms = 0.f;
+      if (er == cudaSuccess) er = cudaEventElapsedTime(&ms, t0, t1);
+      if (er == cudaSuccess && ms / steps < bms) {
+        bms = ms / steps;
+        bsched = cand;
+      }
+    }
+  }
+  if (t0) cudaEventDestroy(t0);
+  if (t1) cudaEventDestroy(t1);
+  for (int s = 0; s < 2; ++s) {
+    double* f3[3] = {c->set[s].ssh, c->set[s].u, c->set[s].v};
+    for (int k = 0; k < 3; ++k) {
+      cudaError_t e2 = cudaMemcpyAsync(f3[k], backup + (3 * s + k) * fe, fe * sizeof(double),
+                                       cudaMemcpyDeviceToDevice, c->stream);
+      if (er == cudaSuccess) er = e2;
+    }
+  }
+  cudaError_t e3 = cudaStreamSynchronize(c->stream);
+  if (er == cudaSuccess) er = e3;
+  cudaFree(backup);
+  c->n_idx = n_save;
+  c->a_mirrors_n = a_save;
+  c->uv_stale = uv_save;
+  c->sched = (bms < 1e300) ? bsched : keep;
+  if (er != cudaSuccess) return status_from(er);
+  if (st) return st;
+  if (bms < 1e300) tune_store(c, c->sched, bms);
+  if (best) *best = c->sched;
+  if (best_ms) *best_ms = bms;
   return NEMO_OK;
 }
 

@@ -1,0 +1,285 @@
+// Device code of the fused NEMOLite2D step shared by the single-grid kernel
+// (nemo_fused.cu) and the ensemble kernel (nemo_ensemble.cu): one warp
+// advances a strip of 30 T columns over a block of rows.  See nemo_fused.cu
+// for the design and the exactness argument.
+#pragma once
+
+#include "nemo_internal.h"
+
+namespace nemo {
+namespace stepdev {
+
+
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int COLS_PER_WARP = 30;
+
+struct Cell {
+  double s, u, v, ht, hu, hv;
+};
+
+__device__ __forceinline__ void load_cell(Cell& x, const FusedArgs& A, long o) {
+  x.s = __ldg(A.sshn + o);
+  x.u = __ldg(A.un + o);
+  x.v = __ldg(A.vn + o);
+  x.ht = __ldg(A.ht + o);
+  x.hu = __ldg(A.hu + o);
+  x.hv = __ldg(A.hv + o);
+}
+
+__device__ __forceinline__ double dn(double x) { return __shfl_down_sync(FULL, x, 1); }
+__device__ __forceinline__ double up(double x) { return __shfl_up_sync(FULL, x, 1); }
+
+// a/b given rb = RN(1/b): the corrected-reciprocal quotient (see div_const)
+// with its range check reduced to what finite states need: `bad` collects
+// nonzero quotients below 2^-959, where the row is redone with IEEE
+// division.  Exact zeros (most of a domain at rest) are exact here.  An
+// infinite or NaN operand gives a non-finite quotient on both paths.
+template <bool SAFE>
+__device__ __forceinline__ double qdiv(double a, double b, double rb, bool& bad) {
+  if (SAFE) return a / b;
+  double q = __dmul_rn(a, rb);
+  const unsigned hi2 = (unsigned)__double2hiint(q) << 1;
+  const unsigned lo = (unsigned)__double2loint(q);
+  bad |= (hi2 < (64u << 21)) & ((hi2 | lo) != 0u);
+  double r = fma(-q, b, a);
+  return -fma(-r, rb, -q);
+}
+
+__device__ __forceinline__ double interp_u(const Consts& C, int c, int jpi, double s0, double s1,
+                                          bool safe, bool& bad) {
+  if (c == 0) return s1;
+  if (c == jpi) return s0;
+  double a = 0.5 * (C.e12t * s0 + C.e12t * s1);
+  return safe ? qdiv<true>(a, C.e12u, C.r_e12u, bad) : qdiv<false>(a, C.e12u, C.r_e12u, bad);
+}
+
+__device__ __forceinline__ double interp_v(const Consts& C, int jj, int jpj, double s0, double s1,
+                                          bool safe, bool& bad) {
+  if (jj == jpj) return s0;
+  double a = 0.5 * (C.e12t * s0 + C.e12t * s1);
+  return safe ? qdiv<true>(a, C.e12v, C.r_e12v, bad) : qdiv<false>(a, C.e12v, C.r_e12v, bad);
+}
+
+// Values carried from row j-1 to row j for one column.
+struct Carry {
+  double su, Hu;       // sshn_u and hu+sshn_u at (c, j)
+  double s_e;          // sshn(c+1, j)
+  double Fuy_s;        // upwind flux through the south face of u(c,j)
+  double dudy_s;       // dudy_s of u(c,j)
+  double vnc_s;        // v_sc of u(c,j)
+  double Fvy_s;        // upwind flux through the south face of v(c,j)
+  double Dvy_s;        // dvdy_s of v(c,j)
+  double cf_s;         // (sshn_v + hv)*vn at (c, j-1)
+};
+
+struct RowOut {
+  double ssha, ua, va, sv;
+  Carry next;
+};
+
+// One row of the step for one lane: outputs at (c, j) and the carry to j+1.
+// EDGE = false is the interior form: the caller guarantees that no lane of
+// the warp sits on column 0, 1 or jpi and that j is neither 1 nor jpj, so
+// every mask of the reference geometry is inactive.
+template <bool SAFE, bool EDGE>
+__device__ __forceinline__ void row(const Consts& C, int c, int j, int jpi, int jpj, double tide,
+                                    const Cell& cur, const Cell& nx, const Carry& k, RowOut& o,
+                                    bool& bad) {
+  const bool south = EDGE && (j == 1), north = EDGE && (j == jpj);
+  const bool west0 = EDGE && (c == 0), west1 = EDGE && (c == 1), east = EDGE && (c == jpi);
+  // sshn_v at (c, j), sshn_u at (c, j+1)
+  const double sv = EDGE ? interp_v(C, j, jpj, cur.s, nx.s, SAFE, bad)
+                         : interp_v(C, 0, 1, cur.s, nx.s, SAFE, bad);
+  const double Hv = cur.hv + sv;
+  const double s_e_n = dn(nx.s);
+  const double su_n = EDGE ? interp_u(C, c, jpi, nx.s, s_e_n, SAFE, bad)
+                           : interp_u(C, 1, 0, nx.s, s_e_n, SAFE, bad);
+  const double Hu_n = nx.hu + su_n;
+
+  // x-face of the u equation at T(c,j), between u(c-1,j) and u(c,j)
+  const double u_w = up(cur.u);
+  const double uw = 0.5 * (cur.u + u_w) * C.e2t;
+  const double dep = cur.ht + cur.s;
+  const double Fx = upwind(uw, u_w, cur.u) * uw * dep;
+  const double Dx = qdiv<SAFE>(cur.u - u_w, C.e1t, C.r_e1t, bad) * dep;
+
+  // corner (c,j): east face of v(c,j), north face of u(c,j)
+  const double uec = 0.5 * (cur.u + nx.u);
+  const double ue = 0.5 * uec * C.two_dy;
+  const double Sn = (k.Hu + nx.hu) + su_n;
+  const double v_e = dn(cur.v);
+  const double uuv = west0 ? upwind_hi_only(ue, v_e)
+                          : east ? upwind_lo_only(ue, cur.v) : upwind(ue, cur.v, v_e);
+  const double Fvx = uuv * ue * (0.5 * Sn);
+  const double Gx = qdiv<SAFE>(v_e - cur.v, C.two_dx, C.r_2dx, bad);
+  const double vnc = 0.5 * (cur.v + v_e);
+  const double vn_ = 0.5 * vnc * C.two_dx;
+  const double Re = (Hv + dn(cur.hv)) + dn(sv);
+  const double uuu = north ? upwind_lo_only(vn_, cur.u) : upwind(vn_, cur.u, nx.u);
+  const double Fuy = uuu * vn_ * (0.5 * Re);
+  const double Gy = qdiv<SAFE>(nx.u - cur.u, C.two_dy, C.r_2dy, bad);
+
+  // y-face of the v equation at T(c,j+1), between v(c,j) and v(c,j+1)
+  const double vs = 0.5 * (nx.v + cur.v) * C.e1t;
+  const double depn = nx.ht + nx.s;
+  const double Fvy_n = upwind(vs, cur.v, nx.v) * vs * depn;
+  const double Dvy_n = qdiv<SAFE>(nx.v - cur.v, C.e2t, C.r_e2t, bad) * depn;
+
+  // continuity (:399-403), clamped SSH row (:631-644)
+  const double r1 = k.Hu * cur.u;
+  const double r2 = up(r1);
+  const double r3 = Hv * cur.v;
+  const double ssh = cur.s + qdiv<SAFE>((r2 - r1 + k.cf_s - r3) * C.rdt, C.e12t, C.r_e12t, bad);
+  o.ssha = south ? tide : ssh;
+
+  // u equation (:439-514); u(jpi,j) is the east wall (:650)
+  {
+    const double Fx_e = dn(Fx);
+    const double Dx_e = dn(Dx);
+    const double adv = Fx - Fx_e + k.Fuy_s - Fuy;
+    const double dudy_n = north ? 0.0 : Gy * Sn;
+    const double dudy_s = south ? 0.0 : k.dudy_s;
+    double vis = (Dx_e - Dx) * C.e2u + (dudy_n - dudy_s) * C.e1u * 0.5;
+    vis = C.visc * vis;
+    const double cor = 0.5 * (C.fcor * (k.vnc_s + vnc)) * C.e12u * k.Hu;
+    const double hpg = -(C.g * k.Hu * C.e2u * (k.s_e - cur.s));
+    const double num = cur.u * k.Hu + qdiv<SAFE>(C.rdt * (adv + vis + cor + hpg), C.e12u, C.r_e12u, bad);
+    const double q = num / (cur.hu + 0.0);
+    o.ua = east ? 0.0 : qdiv<SAFE>(q, C.cfric, C.r_cfric, bad);
+  }
+  // v equation (:527-606); v(c,jpj) is the north wall (:658)
+  {
+    const double Fvx_w = up(Fvx);
+    const double Gx_w = up(Gx);
+    const double hv_w = up(cur.hv);
+    const double sv_w = up(sv);
+    const double uec_w = up(uec);
+    const double adv = Fvx_w - Fvx + k.Fvy_s - Fvy_n;
+    const double dvdx_e = east ? 0.0 : Gx * Re;
+    const double dvdx_w = west1 ? 0.0 : Gx_w * ((Hv + hv_w) + sv_w);
+    double vis = (Dvy_n - k.Dvy_s) * C.e1v + (dvdx_e - dvdx_w) * C.e2v * 0.5;
+    vis = C.visc * vis;
+    const double cor = -(0.5 * (C.fcor * (uec + uec_w)) * C.e12v * Hv);
+    const double hpg = -(C.g * Hv * C.e1v * (nx.s - cur.s));
+    const double num = cur.v * Hv + qdiv<SAFE>(C.rdt * (adv + vis + cor + hpg), C.e12v, C.r_e12v, bad);
+    const double q = num / (cur.hv + 0.0);
+    o.va = north ? 0.0 : qdiv<SAFE>(q, C.cfric, C.r_cfric, bad);
+  }
+  o.sv = sv;
+  // carry to row j+1
+  o.next.su = su_n;
+  o.next.Hu = Hu_n;
+  o.next.s_e = s_e_n;
+  o.next.Fuy_s = Fuy;
+  o.next.dudy_s = Gy * ((Hu_n + cur.hu) + k.su);  // dudy_s of u(c,j+1)
+  o.next.vnc_s = vnc;
+  o.next.Fvy_s = Fvy_n;
+  o.next.Dvy_s = Dvy_n;
+  o.next.cf_s = r3;
+}
+
+// Carried values at row J0 from rows J0-1 (p) and J0 (q).
+template <bool SAFE>
+__device__ __forceinline__ void prologue(const Consts& C, int c, int J0, int jpi, int jpj,
+                                         double sv_p_stored, const Cell& p, const Cell& q,
+                                         Carry& k, double& sv_p, bool& bad) {
+  k.s_e = dn(q.s);
+  k.su = interp_u(C, c, jpi, q.s, k.s_e, SAFE, bad);
+  k.Hu = q.hu + k.su;
+  sv_p = (J0 == 1) ? sv_p_stored : interp_v(C, J0 - 1, jpj, p.s, q.s, SAFE, bad);
+  const double Hv_p = p.hv + sv_p;
+  // corner (c, J0-1): south face of u(c, J0)
+  const double vnc = 0.5 * (p.v + dn(p.v));
+  const double vn_ = 0.5 * vnc * C.two_dx;
+  const double dep = 0.5 * ((Hv_p + dn(p.hv)) + dn(sv_p));
+  const double uu = (J0 == 1) ? upwind_hi_only(vn_, q.u) : upwind(vn_, p.u, q.u);
+  k.Fuy_s = uu * vn_ * dep;
+  k.vnc_s = vnc;
+  const double s_e_p = dn(p.s);
+  if (J0 == 1) {
+    k.dudy_s = 0.0;
+  } else {
+    const double su_p = interp_u(C, c, jpi, p.s, s_e_p, SAFE, bad);
+    const double gy = qdiv<SAFE>(q.u - p.u, C.two_dy, C.r_2dy, bad);
+    k.dudy_s = gy * ((k.Hu + p.hu) + su_p);
+  }
+  // T(c, J0): south face of v(c, J0)
+  const double vs = 0.5 * (q.v + p.v) * C.e1t;
+  const double depc = q.ht + q.s;
+  k.Fvy_s = upwind(vs, p.v, q.v) * vs * depc;
+  k.Dvy_s = qdiv<SAFE>(q.v - p.v, C.e2t, C.r_e2t, bad) * depc;
+  k.cf_s = Hv_p * p.v;
+}
+
+// One warp's strip: columns c0 .. c0+29 (lanes 1..30), rows J0 .. J1 of the
+// grid described by L, inputs/outputs in A.  All 32 lanes of the warp must
+// call it together.  PF = 1 prefetches row j+2 into registers.
+template <int PF>
+__device__ __forceinline__ void run_strip(const Layout& L, const Consts& C, const FusedArgs& A,
+                                          int c0, int J0, int J1, int lane) {
+  const int jpi = L.jpi, jpj = L.jpj;
+  const int c = c0 + lane - 1;
+  const int cl = min(c, jpi + 1);  // lanes beyond the halo column read column jpi+1
+  const bool store = (lane >= 1) && (lane <= COLS_PER_WARP) && (c <= jpi);
+
+  // lanes span columns c0-1 .. c0+30; the interior row form applies when
+  // none of them is 0, 1 or jpi
+  const bool edge_warp = (c0 - 1 <= 1) || (c0 + COLS_PER_WARP >= jpi);
+
+  Cell p, cur, nx;
+  load_cell(p, A, L.idx(cl, J0 - 1));
+  load_cell(cur, A, L.idx(cl, J0));
+  const double sv_stored = (J0 == 1) ? __ldg(A.sshv0 + L.idx(cl, 0)) : 0.0;
+  Carry k;
+  double sv0;
+  {
+    bool bad = false;
+    prologue<false>(C, c, J0, jpi, jpj, sv_stored, p, cur, k, sv0, bad);
+    if (__any_sync(FULL, bad)) prologue<true>(C, c, J0, jpi, jpj, sv_stored, p, cur, k, sv0, bad);
+  }
+  const double hv0 = p.hv;
+  if (PF) load_cell(nx, A, L.idx(cl, J0 + 1));
+
+  const long pitch = L.pitch;
+  long o_ld = L.idx(cl, J0 + 1 + PF);  // next row to load
+  const long o_last = L.idx(cl, jpj + 1);
+  long o_st = L.idx(c, J0);
+#pragma unroll 1
+  for (int j = J0; j <= J1; ++j) {
+    Cell pf;
+    if (PF) {
+      load_cell(pf, A, o_ld < o_last ? o_ld : o_last);  // row j+2 (clamped to jpj+1)
+    } else {
+      load_cell(nx, A, o_ld);  // row j+1 <= jpj+1
+    }
+    o_ld += pitch;
+
+    RowOut o;
+    bool bad = false;
+    if (edge_warp || j == 1 || j == jpj)
+      row<false, true>(C, c, j, jpi, jpj, A.tide, cur, nx, k, o, bad);
+    else
+      row<false, false>(C, c, j, jpi, jpj, A.tide, cur, nx, k, o, bad);
+    if (__any_sync(FULL, bad)) {
+      bool b2 = false;
+      row<true, true>(C, c, j, jpi, jpj, A.tide, cur, nx, k, o, b2);
+    }
+    if (store) {
+      A.ssha[o_st] = o.ssha;
+      A.ua[o_st] = o.ua;
+      A.va[o_st] = o.va;
+      if (edge_warp && c == 1) A.ua[o_st - 1] = 0.0;  // u(0,j), west wall (:650)
+      if (j == 1) {
+        // Flather open boundary (:684-695): v(c,0) = v(c,1) + sqrt(g/hv(c,0))*(sshn_v(c,0) - sshn_v(c,1))
+        A.va[o_st - pitch] = o.va + sqrt(kG / hv0) * (sv0 - o.sv);
+      }
+    }
+    o_st += pitch;
+    k = o.next;
+    cur = nx;
+    if (PF) nx = pf;
+  }
+}
+
+}  // namespace stepdev
+}  // namespace nemo

@@ -35,7 +35,10 @@ EXPORTED = [
     "nemo_bc_solid_v", "nemo_bc_flather_u", "nemo_bc_flather_v", "nemo_next", "nemo_step",
     "nemo_step_n", "nemo_checksums", "nemo_checksum", "nemo_retrieve", "nemo_set_state",
     "nemo_sync", "nemo_get_dims", "nemo_device_field", "nemo_set_schedule", "nemo_get_schedule",
-    "nemo_status_string", "nemo_build_is_strict", "nemo_checksums_noalloc",
+    "nemo_status_string", "nemo_build_is_strict", "nemo_checksums_noalloc", "nemo_autotune",
+    "nemo_ens_generate", "nemo_ens_create", "nemo_ens_destroy", "nemo_ens_step_n",
+    "nemo_ens_checksums", "nemo_ens_retrieve", "nemo_ens_set_state", "nemo_ens_set_schedule",
+    "nemo_ens_get_schedule", "nemo_ens_use_graph", "nemo_ens_info", "nemo_ens_autotune",
     "cuda_setup_model_params_", "cuda_initialise_grid_", "cuda_continuity_", "cuda_momentum_",
     "cuda_boundary_conditions_", "cuda_next_", "cuda_retrieve_grid_constants_",
     "cuda_retrieve_results_", "cuda_finalise_", "nemo_compat_last_status", "nemo_compat_context",
@@ -64,6 +67,19 @@ class Params(ctypes.Structure):
 
 class Schedule(ctypes.Structure):
     _fields_ = [("warps", ctypes.c_int), ("occupancy", ctypes.c_int), ("rows", ctypes.c_int)]
+
+
+class Member(ctypes.Structure):
+    _fields_ = [("jpi", ctypes.c_int), ("jpj", ctypes.c_int),
+                ("amp_tide", ctypes.c_double), ("tide_phase", ctypes.c_double),
+                ("dep_const", ctypes.c_double), ("nbump", ctypes.c_int), ("seed", ctypes.c_uint64),
+                ("bump_amp", ctypes.c_double), ("bump_wmin", ctypes.c_double),
+                ("bump_wmax", ctypes.c_double), ("hmin", ctypes.c_double), ("hmax", ctypes.c_double)]
+
+
+class EnsSchedule(ctypes.Structure):
+    _fields_ = [("warps", ctypes.c_int), ("occupancy", ctypes.c_int), ("rows", ctypes.c_int),
+                ("order", ctypes.c_int), ("ctas", ctypes.c_int)]
 
 
 def lib_path(strict=False):
@@ -120,6 +136,19 @@ def load(strict=False):
     L.nemo_compat_context.restype = vp
     L.nemo_checksums_noalloc.argtypes = [P(ctypes.c_void_p), ip, ip, ip, ctypes.c_long,
                                          ctypes.c_void_p, ctypes.c_void_p]
+    L.nemo_autotune.argtypes = [vp, ip, P(Schedule), P(dp)]
+    L.nemo_ens_generate.argtypes = [ctypes.c_uint64, ip, ip, ip, dp, P(Member)]
+    L.nemo_ens_create.argtypes = [P(Params), P(Member), ip, P(vp)]
+    L.nemo_ens_destroy.argtypes = [vp]
+    L.nemo_ens_step_n.argtypes = [vp, ip, ip]
+    L.nemo_ens_checksums.argtypes = [vp, P(dp)]
+    L.nemo_ens_retrieve.argtypes = [vp, ip, ip, P(dp), ctypes.c_long]
+    L.nemo_ens_set_state.argtypes = [vp, ip, P(dp), P(dp), P(dp)]
+    L.nemo_ens_set_schedule.argtypes = [vp, P(EnsSchedule)]
+    L.nemo_ens_get_schedule.argtypes = [vp, P(EnsSchedule)]
+    L.nemo_ens_use_graph.argtypes = [vp, ip]
+    L.nemo_ens_info.argtypes = [vp, P(ip), P(ctypes.c_longlong)]
+    L.nemo_ens_autotune.argtypes = [vp, ip, P(EnsSchedule), P(dp)]
     _libs[strict] = L
     return L
 
@@ -260,6 +289,13 @@ class Model:
             assert x.shape == field_shape(f, self.jpi, self.jpj), (f, x.shape)
         check(self.lib.nemo_set_state(self.h, *[_dptr(x) for x in a]), "nemo_set_state")
 
+    def autotune(self, steps=5):
+        sch = Schedule()
+        ms = ctypes.c_double()
+        check(self.lib.nemo_autotune(self.h, steps, ctypes.byref(sch), ctypes.byref(ms)),
+              "nemo_autotune")
+        return (sch.warps, sch.occupancy, sch.rows), ms.value
+
     def device_field(self, f):
         ptr = ctypes.POINTER(ctypes.c_double)()
         pitch = ctypes.c_long()
@@ -270,3 +306,94 @@ class Model:
 
 def is_strict_build(strict):
     return bool(load(strict).nemo_build_is_strict())
+
+
+def generate_members(seed, n, side_min=64, side_max=1024, amp_scale=1.0, strict=False):
+    """Member recipe of the batched configuration (see nemo_ens_generate)."""
+    arr = (Member * n)()
+    check(load(strict).nemo_ens_generate(seed, n, side_min, side_max, amp_scale, arr),
+          "nemo_ens_generate")
+    return list(arr)
+
+
+def member_params(common, m):
+    """Single-grid parameters equal to ensemble member m (for comparisons)."""
+    p = Params()
+    ctypes.pointer(p)[0] = common
+    p.jpi, p.jpj = m.jpi, m.jpj
+    p.amp_tide, p.tide_phase = m.amp_tide, m.tide_phase
+    p.dep_const, p.nbump, p.seed = m.dep_const, m.nbump, m.seed
+    p.bump_amp, p.bump_wmin, p.bump_wmax = m.bump_amp, m.bump_wmin, m.bump_wmax
+    p.hmin, p.hmax = m.hmin, m.hmax
+    return p
+
+
+class Ensemble:
+    """Many members of uneven size advanced together (a nemo_ens)."""
+
+    def __init__(self, members, strict=False, common=None, **kw):
+        self.lib = load(strict)
+        self.common = common if common is not None else default_params(strict, **kw)
+        self.members = list(members)
+        arr = (Member * len(self.members))(*self.members)
+        h = ctypes.c_void_p()
+        check(self.lib.nemo_ens_create(ctypes.byref(self.common), arr, len(self.members),
+                                       ctypes.byref(h)), "nemo_ens_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.nemo_ens_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step_n(self, istp0, n):
+        check(self.lib.nemo_ens_step_n(self.h, istp0, n), "nemo_ens_step_n")
+
+    def checksums(self):
+        out = np.zeros(3 * len(self.members), dtype=np.float64)
+        check(self.lib.nemo_ens_checksums(self.h, _dptr(out)), "nemo_ens_checksums")
+        return out.reshape(-1, 3)
+
+    def field(self, member, f):
+        m = self.members[member]
+        shape = field_shape(f, m.jpi, m.jpj)
+        out = np.empty(shape, dtype=np.float64)
+        check(self.lib.nemo_ens_retrieve(self.h, member, f, _dptr(out), shape[1]),
+              "nemo_ens_retrieve")
+        return out
+
+    def set_state(self, member, sshn, un, vn):
+        a = [np.ascontiguousarray(x, dtype=np.float64) for x in (sshn, un, vn)]
+        check(self.lib.nemo_ens_set_state(self.h, member, *[_dptr(x) for x in a]),
+              "nemo_ens_set_state")
+
+    def set_schedule(self, warps=2, occupancy=-24, rows=16, order=1, ctas=0):
+        s = EnsSchedule(warps, occupancy, rows, order, ctas)
+        check(self.lib.nemo_ens_set_schedule(self.h, ctypes.byref(s)), "nemo_ens_set_schedule")
+
+    def get_schedule(self):
+        s = EnsSchedule()
+        check(self.lib.nemo_ens_get_schedule(self.h, ctypes.byref(s)), "nemo_ens_get_schedule")
+        return (s.warps, s.occupancy, s.rows, s.order, s.ctas)
+
+    def use_graph(self, on):
+        check(self.lib.nemo_ens_use_graph(self.h, 1 if on else 0), "nemo_ens_use_graph")
+
+    def info(self):
+        n = ctypes.c_int()
+        c = ctypes.c_longlong()
+        check(self.lib.nemo_ens_info(self.h, ctypes.byref(n), ctypes.byref(c)), "nemo_ens_info")
+        return n.value, c.value
+
+    def autotune(self, steps=5):
+        s = EnsSchedule()
+        ms = ctypes.c_double()
+        check(self.lib.nemo_ens_autotune(self.h, steps, ctypes.byref(s), ctypes.byref(ms)),
+              "nemo_ens_autotune")
+        return (s.warps, s.occupancy, s.rows, s.order, s.ctas), ms.value

@@ -16,7 +16,7 @@ HEADER = os.path.join(ROOT, "include", "nemo_b200.h")
 def header_symbols():
     text = open(HEADER).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"^\s*(?:int|void|nemo_ctx\*|const char\*)\s+\*?(\w+)\s*\(",
+    return sorted(set(re.findall(r"^\s*(?:int|void|nemo_ctx\*|const char\*|long long)\s+\*?(\w+)\s*\(",
                                  text, flags=re.M)))
 
 
@@ -84,3 +84,23 @@ def test_missing_library_fails_loudly(built, monkeypatch, tmp_path):
     monkeypatch.setattr(built, "_libs", {})
     with pytest.raises(ImportError):
         built.load(False)
+
+
+def test_member_recipe_is_seeded_and_bounded(built):
+    """nemo_ens_generate is host-only: sides log-uniform in [64, 1024], aspect
+    in [0.5, 2], tidal amplitude amp_scale*[0.5, 1.5], phase in [0, 2*pi)."""
+    a = built.generate_members(42, 256)
+    b = built.generate_members(42, 256)
+    c = built.generate_members(43, 256)
+    key = lambda ms: [(m.jpi, m.jpj, m.amp_tide, m.seed) for m in ms]
+    assert key(a) == key(b) and key(a) != key(c)
+    import math
+    for m in a:
+        assert 64 <= m.jpi <= 1024
+        assert 0.5 - 1e-2 <= m.jpj / m.jpi <= 2.0 + 1e-2
+        assert 0.5 <= m.amp_tide <= 1.5 and 0.0 <= m.tide_phase < 2 * math.pi
+        assert (m.dep_const, m.nbump, m.hmin, m.hmax) == (100.0, 8, 50.0, 150.0)
+    cells = sum(m.jpi * m.jpj for m in a)
+    assert 2e7 < cells < 1.2e8
+    s = built.generate_members(42, 8, amp_scale=0.2)
+    assert all(0.1 <= m.amp_tide <= 0.3 for m in s)

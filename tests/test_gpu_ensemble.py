@@ -1,0 +1,145 @@
+"""Batched ensemble and autotuners against single grids and the oracle.
+
+Every ensemble member must evolve exactly as a single grid with the member's
+parameters: bit-for-bit against the oracle in the -fmad=false build, within
+1e-12 relative max-norm in the default build, whatever the schedule, with or
+without graph capture.  The autotuners must leave the model state untouched.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12
+STATE = [("sshn", 0), ("un", 1), ("vn", 2)]
+COMMON = dict(dx=1000.0, dy=1000.0, rdt=20.0, cbfr=0.00015, visc=0.1)
+
+
+@pytest.fixture(scope="module")
+def nb():
+    import nemo_b200
+    return nemo_b200
+
+
+def bits(a):
+    return np.ascontiguousarray(a).view(np.int64)
+
+
+def relerr(a, b):
+    s = np.max(np.abs(b))
+    d = np.max(np.abs(a - b))
+    return d / s if s > 0 else d
+
+
+def oracle_member(oracle_mod, m):
+    return oracle_mod.Model(jpi=m.jpi, jpj=m.jpj, rdt=20.0, cbfr=0.00015, visc=0.1,
+                            amp_tide=m.amp_tide, tide_phase=m.tide_phase, dep_const=m.dep_const,
+                            nbump=m.nbump, seed=m.seed, bump_amp=m.bump_amp,
+                            bump_wmin=m.bump_wmin, bump_wmax=m.bump_wmax, hmin=m.hmin,
+                            hmax=m.hmax)
+
+
+@pytest.mark.parametrize("graph", [True, False])
+@pytest.mark.parametrize("sched", [(2, -24, 16, 1), (4, 20, 8, 0), (2, 24, 5, 0)])
+def test_strict_ensemble_members_match_oracle_bitwise(nb, oracle_mod, graph, sched):
+    members = nb.generate_members(7, 6, side_min=20, side_max=90, amp_scale=0.2)
+    e = nb.Ensemble(members, strict=True, **COMMON)
+    e.use_graph(graph)
+    e.set_schedule(*sched)
+    orc = [oracle_member(oracle_mod, m) for m in members]
+    istp = 1
+    for n in (7, 16):
+        e.step_n(istp, n)
+        for o in orc:
+            o.run(istp, n)
+        istp += n
+        ck = e.checksums()
+        for k, (m, o) in enumerate(zip(members, orc)):
+            for name, fid in STATE:
+                np.testing.assert_array_equal(bits(e.field(k, fid)), bits(o.field(fid)),
+                                              err_msg="member %d %s" % (k, name))
+            tree = [o.checksum(f, "tree") for f in (oracle_mod.SSHN, oracle_mod.UN, oracle_mod.VN)]
+            assert list(ck[k]) == tree
+
+
+def test_default_ensemble_matches_single_grids(nb):
+    members = nb.generate_members(11, 10, side_min=30, side_max=300, amp_scale=0.2)
+    common = nb.default_params(**COMMON)
+    e = nb.Ensemble(members, common=common)
+    e.step_n(1, 40)
+    ck = e.checksums()
+    for k, m in enumerate(members):
+        single = nb.Model(nb.member_params(common, m))
+        single.step_n(1, 40)
+        for name, fid in STATE:
+            assert relerr(e.field(k, fid), single.field(fid)) <= TOL, (k, name)
+        np.testing.assert_allclose(ck[k], single.checksums(), rtol=1e-13)
+
+
+def test_ensemble_set_state_and_graph_replay_agree(nb):
+    members = nb.generate_members(3, 4, side_min=25, side_max=70, amp_scale=0.2)
+    a = nb.Ensemble(members, **COMMON)
+    b = nb.Ensemble(members, **COMMON)
+    b.use_graph(False)
+    rng = np.random.default_rng(4)
+    for k, m in enumerate(members):
+        st = (rng.normal(0, 0.05, (m.jpj, m.jpi)), rng.normal(0, 0.1, (m.jpj, m.jpi + 1)),
+              rng.normal(0, 0.1, (m.jpj + 1, m.jpi)))
+        a.set_state(k, *st)
+        b.set_state(k, *st)
+    for _ in range(3):  # the same graph is replayed for equal (n, parity)
+        a.step_n(5, 6)
+        b.step_n(5, 6)
+    for k in range(len(members)):
+        for name, fid in STATE:
+            np.testing.assert_array_equal(bits(a.field(k, fid)), bits(b.field(k, fid)))
+
+
+def test_ensemble_autotune_keeps_state(nb):
+    members = nb.generate_members(5, 12, side_min=40, side_max=200, amp_scale=0.2)
+    e = nb.Ensemble(members, **COMMON)
+    ref = nb.Ensemble(members, **COMMON)
+    e.step_n(1, 10)
+    ref.step_n(1, 10)
+    sched, ms = e.autotune(steps=2)
+    assert ms > 0 and sched[0] in (2, 4)
+    e.set_schedule(2, -24, 16, 1)  # same arithmetic variant as ref for a bitwise check
+    e.step_n(11, 10)
+    ref.step_n(11, 10)
+    for k in range(len(members)):
+        for name, fid in STATE:
+            np.testing.assert_array_equal(bits(e.field(k, fid)), bits(ref.field(k, fid)))
+
+
+def test_single_grid_autotune_keeps_state(nb, tmp_path, monkeypatch):
+    monkeypatch.setenv("NEMO_TUNE_CACHE", str(tmp_path / "tune.txt"))
+    kw = dict(jpi=300, jpj=250, rdt=20.0, cbfr=0.00015, visc=0.1, nbump=4, seed=2,
+              bump_amp=20.0, bump_wmin=5e3, bump_wmax=40e3)
+    a = nb.Model(strict=True, **kw)
+    b = nb.Model(strict=True, **kw)
+    a.step_n(1, 15)
+    b.step_n(1, 15)
+    sched, ms = a.autotune(steps=2)
+    assert ms > 0
+    a.step_n(16, 10)
+    b.step_n(16, 10)
+    for name, fid in STATE + [("ua", 4), ("sshn_u", 6)]:
+        np.testing.assert_array_equal(bits(a.field(fid)), bits(b.field(fid)), err_msg=name)
+    text = (tmp_path / "tune.txt").read_text().split()
+    assert text[0].endswith(":300x250")
+    c = nb.Model(strict=True, **kw)  # picks the cached schedule
+    assert c.get_schedule() == sched
+
+
+def test_ensemble_rejects_bad_members(nb):
+    bad = nb.generate_members(1, 2, side_min=10, side_max=20)
+    bad[1].jpi = 1
+    with pytest.raises(nb.NemoError):
+        nb.Ensemble(bad, **COMMON)
+    e = nb.Ensemble(nb.generate_members(1, 2, side_min=10, side_max=20), **COMMON)
+    with pytest.raises(nb.NemoError):
+        e.set_schedule(8, 16, 16, 0)
+    out = np.zeros(16)
+    assert e.lib.nemo_ens_retrieve(e.h, 5, nb.SSHN, nb._dptr(out), 4) == 1  # no member 5
+    with pytest.raises(IndexError):
+        e.field(5, nb.SSHN)
