@@ -231,6 +231,95 @@ int nemo_ens_autotune(nemo_ens* e, int steps, nemo_ens_schedule* best, double* b
 int nemo_checksums_noalloc(const double* const* fields, int nfields, int nx, int ny,
                            long ld, double* out, void* stream);
 
+/* ---- BF16 convolutional surrogate and hybrid controller ----------------------
+ * No counterpart in the reference.  A residual CNN (nblocks blocks of two 3x3
+ * convolutions, 64 channels, plus input and output convolutions) maps the
+ * state of a grid at step s to its state at s + 10.  Tensors are NHWC with
+ * one pixel per T-cell (ji, jj) -> (x = ji-1, y = jj-1).  A snapshot is FP32
+ * [n][height][width][4]: ssh(ji,jj), u(ji-1,jj) (west face), v(ji,jj-1) (south
+ * face), ht(ji,jj).  width must be a multiple of 128.  Device pointers are
+ * the caller's; every call is ordered on the configured stream. */
+typedef struct nemo_sur nemo_sur;
+
+typedef struct nemo_sur_config {
+  int nblocks;          /* residual blocks (8) */
+  int batch;            /* images per call (64) */
+  int height, width;    /* grid (256 x 256) */
+  int train;            /* 1: keep activations, gradients and AdamW moments */
+  uint64_t seed;        /* weight initialisation */
+  void* stream;         /* cudaStream_t; NULL: the surrogate creates one */
+  int device;           /* -1: current device */
+} nemo_sur_config;
+
+typedef struct nemo_adamw {
+  float lr, beta1, beta2, eps, weight_decay;
+} nemo_adamw;
+
+int nemo_sur_default_config(nemo_sur_config* c);
+int nemo_sur_create(const nemo_sur_config* c, nemo_sur** out);
+int nemo_sur_destroy(nemo_sur* s);
+/* Parameter count (FP32: all layers' weights [9][64 out][64 in], then all
+ * biases [64]) and convolution FLOPs per pixel of one forward pass. */
+int nemo_sur_info(nemo_sur* s, long long* nparams, long long* flops_per_pixel);
+int nemo_sur_get_params(nemo_sur* s, float* host);
+int nemo_sur_set_params(nemo_sur* s, const float* host);
+int nemo_sur_get_grads(nemo_sur* s, float* host);
+/* norm[11]: input scale[4], input shift[4] (ssh, u, v, depth; the tide channel
+ * uses the ssh pair), output scale[3] (network output = delta * scale). */
+int nemo_sur_set_norm(nemo_sur* s, const float* norm);
+int nemo_sur_get_norm(nemo_sur* s, float* norm);
+/* out (device, [n][h][w][4] FP32): normalised deltas; tide[n] (device, FP32):
+ * boundary-row SSH at the target time. */
+int nemo_sur_predict(nemo_sur* s, const float* snap, const float* tide, int n, float* out);
+/* Forward + mean-squared-error loss against snap1 + backward; gradients are
+ * recomputed from zero.  loss: host double. */
+int nemo_sur_loss_grad(nemo_sur* s, const float* snap0, const float* snap1, const float* tide,
+                       int n, double* loss);
+int nemo_sur_adamw(nemo_sur* s, const nemo_adamw* hp);
+int nemo_sur_train_step(nemo_sur* s, const float* snap0, const float* snap1, const float* tide,
+                        int n, const nemo_adamw* hp, double* loss);
+/* Snapshot of every ensemble member (all must be height x width). */
+int nemo_sur_pack_ens(nemo_sur* s, nemo_ens* e, float* snap);
+/* One surrogate call: every member advances from its current state (after
+ * step istp_end - 10) to step istp_end; the boundary row takes the exact
+ * tidal SSH, the walls keep zero normal velocity. */
+int nemo_sur_advance_ens(nemo_sur* s, nemo_ens* e, int istp_end);
+/* out[3*m + f]: relative L2 difference of member m's ssh, u, v (f) in a
+ * against ref. */
+int nemo_ens_compare(nemo_ens* a, nemo_ens* ref, double* out);
+
+typedef struct nemo_hyb_config {
+  int k;        /* steps per surrogate call (10) */
+  int anchor;   /* FP64 re-anchor interval (100) */
+  double tol;   /* fallback threshold on relative SSH L2 error (0.01) */
+} nemo_hyb_config;
+
+typedef struct nemo_hyb_stats {
+  long long sur_calls, sur_steps, solver_steps, fallbacks;
+  double max_shadow_err, last_shadow_err, seconds;
+} nemo_hyb_stats;
+
+int nemo_hyb_default_config(nemo_hyb_config* c);
+/* Advances e by nsteps (a multiple of anchor) from the state after istp0.
+ * Each anchor window: the surrogate predicts the first k steps while the
+ * FP64 solver runs them (re-anchoring the state); if any member's relative
+ * SSH L2 error of that prediction exceeds tol the solver runs the rest of the
+ * window, otherwise the surrogate does, k steps per call. */
+int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, int nsteps,
+                 nemo_hyb_stats* stats);
+
+/* Single convolution kernels on caller-owned device buffers.  x, out,
+ * residual, mask, dz: BF16 NHWC, 64 channels; w: BF16 [9][64 out][64 in];
+ * bias, dw ([9][64][64]), db ([64]): FP32; out32: FP32 [n][h][w][4] (first
+ * four channels).  err: device int set non-zero if a device wait gave up.
+ * fwd: out = epilogue(conv(x, w)) with v = acc + bias, += residual,
+ * *= (mask > 0), relu.  wgrad: dw += x (*) dz, db += sum dz (accumulating). */
+int nemo_conv3x3_fwd(const void* x, const void* w, const float* bias, const void* residual,
+                     const void* mask, int relu, void* out, float* out32, int n, int h, int w_,
+                     int* err, void* stream);
+int nemo_conv3x3_wgrad(const void* x, const void* dz, float* dw, float* db, int n, int h, int w_,
+                       int ctas, int* err, void* stream);
+
 /* ---- drop-in symbols (cuda/cuda_nemolite2d.cu:234-270) --------------------
  * One default context.  Errors are printed to stderr and kept in a sticky
  * status readable with nemo_compat_last_status() (the reference threw a C++

@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "nemo_step_dev.cuh"
+#include "sur_internal.h"
 
 using namespace nemo;
 
@@ -652,3 +653,31 @@ int nemo_ens_autotune(nemo_ens* e, int steps, nemo_ens_schedule* best, double* b
 }
 
 }  // extern "C"
+
+// ---- accessors for the surrogate and hybrid controller (same library) ----
+namespace nemo {
+
+int ens_member_state(nemo_ens* e, int m, MemberState* out) {
+  if (!e || !out || m < 0 || m >= (int)e->mem.size()) return NEMO_ERR_INVALID;
+  const MemberDev& d = e->hmem[m];
+  out->sshn = d.st[e->parity][0];
+  out->un = d.st[e->parity][1];
+  out->vn = d.st[e->parity][2];
+  out->ht = d.ht;
+  out->jpi = d.L.jpi;
+  out->jpj = d.L.jpj;
+  out->pitch = d.L.pitch;
+  return NEMO_OK;
+}
+
+int ens_member_count(nemo_ens* e) { return e ? (int)e->mem.size() : 0; }
+cudaStream_t ens_stream(nemo_ens* e) { return e->stream; }
+int ens_device(nemo_ens* e) { return e->device; }
+
+double ens_tide(nemo_ens* e, int m, int istp) {
+  const double omega_tide = 2.0 * 3.14159 / (12.42 * 3600.0);
+  const double rtime = (double)istp * e->common.rdt;
+  return e->mem[m].amp_tide * sin(omega_tide * rtime + e->mem[m].tide_phase);
+}
+
+}  // namespace nemo

@@ -1,0 +1,571 @@
+// 3x3 convolutions of the BF16 surrogate on the 5th-generation tensor cores
+// (tcgen05 MMA, accumulators in tensor memory, operands staged by TMA).
+//
+// Activations are NHWC BF16 with 64 channels.  Weights are [tap][cout][cin]
+// BF16 (tap = 3*(dy+1) + (dx+1)); FP32 accumulation throughout.
+//
+// k_conv_fwd -- implicit GEMM out[p, co] = sum_{tap,ci} x[p+off(tap), ci] *
+//   w[tap, co, ci], M = 128 pixels of one image row, N = 64, K = 9 x 64.  For
+//   every tap a TMA load brings the shifted 128 x 64 window into shared memory
+//   (coordinates outside the image are zero-filled, which is the convolution's
+//   zero padding); both operands are K-major with the 128-byte swizzle.  Warp 0
+//   issues TMA, one thread of warp 1 issues the MMAs, warps 2-5 drain the
+//   double-buffered accumulator and apply the fused epilogue: + bias, ReLU,
+//   + residual, x (mask > 0).  The same kernel computes the data gradient of a
+//   convolution when given the tap-flipped, transposed weights.
+//
+// k_conv_wgrad -- dw[tap, co, ci] += sum_p dz[p, co] * x[p+off(tap), ci] as
+//   D[(tap pair, ci), co] with K = pixels: M = 128 rows (two taps x 64 input
+//   channels), N = 64.  Both operands come straight from the NHWC tensors by
+//   TMA and are read by the MMA as MN-major (channels contiguous); CTAs split
+//   the pixel range and add their partial D into an FP32 dw with atomics.
+//
+// Every wait on an mbarrier is bounded; on timeout the kernel records an
+// error code, lets in-flight copies and MMAs finish (also bounded), frees its
+// tensor memory and returns.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cudaTypedefs.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include "sur_internal.h"
+
+namespace sur {
+namespace {
+
+constexpr int CH = 64;
+constexpr int TM = 128;                    // pixels per forward tile
+constexpr int NST = 4;                     // forward A stages (one tap each)
+constexpr int A_BYTES = TM * CH * 2;       // 16 KiB
+constexpr int WT_BYTES = CH * CH * 2;      // 8 KiB per tap
+constexpr int W_BYTES = 9 * WT_BYTES;      // 72 KiB
+constexpr int THREADS = 192;               // 6 warps
+constexpr uint64_t WAIT_NS = 2000000000ull;  // 2 s per wait before giving up
+
+constexpr int WG_NST = 4;                  // wgrad stages
+constexpr int WG_PIX = 64;                 // pixels per wgrad K chunk
+constexpr int WG_TILE = WG_PIX * CH * 2;   // 8 KiB
+
+// ---- PTX wrappers ------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ uint64_t gtimer() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+// Bounded wait for the phase with the given parity; false after WAIT_NS of
+// wall time without completion.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity) {
+  if (mbar_try(b, parity)) return true;
+  const uint64_t t0 = gtimer();
+  for (uint32_t i = 1;; ++i) {
+    if (mbar_try(b, parity)) return true;
+    if ((i & 255u) == 0 && gtimer() - t0 > WAIT_NS) return false;
+  }
+}
+// The same, agreed across the warp (for .sync.aligned tcgen05 instructions).
+__device__ __forceinline__ bool mbar_wait_warp(uint64_t* b, uint32_t parity) {
+  return __all_sync(0xffffffffu, mbar_wait(b, parity)) != 0;
+}
+__device__ __forceinline__ void fence_barrier_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* tm, uint64_t* bar, int c0,
+                                            int c1) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          smem_u32(dst)),
+      "l"(tm), "r"(c0), "r"(c1), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* tm, uint64_t* bar, int c0,
+                                            int c1, int c2, int c3) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(
+          smem_u32(dst)),
+      "l"(tm), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tmem_alloc(uint32_t* dst, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst)),
+               "r"(ncols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void mma_bf16(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc,
+                                         uint32_t accum) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d),
+      "l"(a), "l"(b), "r"(idesc), "r"(accum)
+      : "memory");
+}
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   smem_u32(bar))
+               : "memory");
+}
+// 32 consecutive fp32 columns of this thread's TMEM lane
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+        "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+        "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+        "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Shared-memory matrix descriptor (tcgen05): start, leading and stride byte
+// offsets in 16-byte units, descriptor version 1, 128-byte swizzle.
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46) | (2ull << 61);
+}
+// Instruction descriptor, kind::f16: D f32, A and B bf16, M x N, operand
+// majorness (0 K-major, 1 MN-major).
+__host__ __device__ constexpr uint32_t idesc(int M, int N, int a_mn, int b_mn) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)a_mn << 15) | ((uint32_t)b_mn << 16) |
+         ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+struct FwdSmem {
+  uint8_t a[NST][A_BYTES];
+  uint8_t w[W_BYTES];
+  uint64_t full[NST], empty[NST];
+  uint64_t wbar, done;
+  uint64_t tfull[2], tempty[2];
+  uint32_t tmem_base;
+  float bias[CH];
+};
+
+__device__ __forceinline__ void fail(int* err, int code) { atomicCAS(err, 0, code); }
+
+__global__ void __launch_bounds__(THREADS, 1)
+k_conv_fwd(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmW,
+           ConvEpi E) {
+  extern __shared__ uint8_t smem_raw[];
+  FwdSmem& S = *reinterpret_cast<FwdSmem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int xtiles = E.W / TM;
+  const int ntile = E.N * E.H * xtiles;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < NST; ++s) {
+      mbar_init(&S.full[s], 1);
+      mbar_init(&S.empty[s], 1);
+    }
+    mbar_init(&S.wbar, 1);
+    mbar_init(&S.done, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&S.tfull[b], 1);
+      mbar_init(&S.tempty[b], 128);
+    }
+    fence_barrier_init();
+  }
+  if (threadIdx.x < CH) S.bias[threadIdx.x] = E.bias ? E.bias[threadIdx.x] : 0.0f;
+  if (warp == 1) tmem_alloc(&S.tmem_base, 128);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = S.tmem_base;
+
+  if (warp == 0 && lane == 0) {
+    // ---- TMA producer ----
+    mbar_expect_tx(&S.wbar, W_BYTES);
+    for (int tap = 0; tap < 9; ++tap) tma_load_2d(S.w + tap * WT_BYTES, &tmW, &S.wbar, 0, tap * CH);
+    int stage = 0;
+    uint32_t phase = 0;
+    bool ok = true;
+    for (int t = blockIdx.x; t < ntile && ok; t += gridDim.x) {
+      const int xt = t % xtiles, r = t / xtiles, y = r % E.H, n = r / E.H;
+      for (int tap = 0; tap < 9; ++tap) {
+        if (!mbar_wait(&S.empty[stage], phase ^ 1)) { fail(E.err, 1); ok = false; break; }
+        mbar_expect_tx(&S.full[stage], A_BYTES);
+        tma_load_4d(S.a[stage], &tmA, &S.full[stage], 0, xt * TM + (tap % 3) - 1, y + tap / 3 - 1, n);
+        if (++stage == NST) { stage = 0; phase ^= 1; }
+      }
+    }
+    // let every armed copy land before the CTA may exit
+    for (int s = 0; s < NST; ++s) {
+      // stages armed in the current phase round are s < stage; earlier ones completed
+      if (s < stage) mbar_wait(&S.full[s], phase);
+      else mbar_wait(&S.full[s], phase ^ 1);
+    }
+    mbar_wait(&S.wbar, 0);
+  } else if (warp == 1 && lane == 0) {
+    // ---- MMA issuer ----
+    const uint32_t ID = idesc(128, 64, 0, 0);
+    bool ok = mbar_wait(&S.wbar, 0);
+    if (!ok) fail(E.err, 2);
+    int stage = 0;
+    uint32_t phase = 0;
+    int it = 0;
+    const uint32_t wbase = smem_u32(S.w);
+    for (int t = blockIdx.x; t < ntile && ok; t += gridDim.x, ++it) {
+      const int b = it & 1;
+      const uint32_t tph = (it >> 1) & 1;
+      if (!mbar_wait(&S.tempty[b], tph ^ 1)) { fail(E.err, 3); ok = false; break; }
+      tc_fence_after();
+      const uint32_t d = tmem + (uint32_t)(b * 64);
+      for (int tap = 0; tap < 9; ++tap) {
+        if (!mbar_wait(&S.full[stage], phase)) { fail(E.err, 4); ok = false; break; }
+        tc_fence_after();
+        const uint32_t abase = smem_u32(S.a[stage]);
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+          mma_bf16(d, sdesc(abase + 32 * k, 16, 1024), sdesc(wbase + tap * WT_BYTES + 32 * k, 16, 1024), ID,
+                   (tap | k) != 0);
+        mma_commit(&S.empty[stage]);
+        if (++stage == NST) { stage = 0; phase ^= 1; }
+      }
+      if (ok) mma_commit(&S.tfull[b]);
+    }
+    mma_commit(&S.done);  // completes once every MMA issued above has finished
+    mbar_wait(&S.done, 0);
+  } else if (warp >= 2) {
+    // ---- epilogue: TMEM -> registers -> bias/ReLU/residual/mask -> BF16 ----
+    const int q = warp & 3;
+    const int row = 32 * q + lane;
+    int it = 0;
+    for (int t = blockIdx.x; t < ntile; t += gridDim.x, ++it) {
+      const int b = it & 1;
+      const uint32_t tph = (it >> 1) & 1;
+      if (!mbar_wait_warp(&S.tfull[b], tph)) { fail(E.err, 5); break; }
+      tc_fence_after();
+      float v[64];
+      const uint32_t ta = tmem + (uint32_t)(b * 64) + ((uint32_t)(32 * q) << 16);
+      tmem_ld32(ta, v);
+      tmem_ld32(ta + 32, v + 32);
+      tc_fence_before();
+      mbar_arrive(&S.tempty[b]);
+      const int xt = t % xtiles, r = t / xtiles, y = r % E.H, n = r / E.H;
+      const long p = ((long)(n * E.H + y) * E.W + xt * TM + row);
+#pragma unroll
+      for (int c = 0; c < 64; ++c) v[c] += S.bias[c];
+      if (E.residual) {
+        const uint4* rp = reinterpret_cast<const uint4*>(E.residual + p * CH);
+#pragma unroll
+        for (int g = 0; g < 8; ++g) {
+          uint4 u = rp[g];
+          const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&u);
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            float2 f = __bfloat1622float2(h[e]);
+            v[8 * g + 2 * e] += f.x;
+            v[8 * g + 2 * e + 1] += f.y;
+          }
+        }
+      }
+      if (E.mask) {
+        const uint4* mp = reinterpret_cast<const uint4*>(E.mask + p * CH);
+#pragma unroll
+        for (int g = 0; g < 8; ++g) {
+          uint4 u = mp[g];
+          const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&u);
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            float2 f = __bfloat1622float2(h[e]);
+            if (!(f.x > 0.0f)) v[8 * g + 2 * e] = 0.0f;
+            if (!(f.y > 0.0f)) v[8 * g + 2 * e + 1] = 0.0f;
+          }
+        }
+      }
+      if (E.relu) {
+#pragma unroll
+        for (int c = 0; c < 64; ++c) v[c] = fmaxf(v[c], 0.0f);
+      }
+      if (E.out32) {
+        float4* o32 = reinterpret_cast<float4*>(E.out32 + p * 4);
+        *o32 = make_float4(v[0], v[1], v[2], v[3]);
+      }
+      if (E.out) {
+        uint4* op = reinterpret_cast<uint4*>(E.out + p * CH);
+#pragma unroll
+        for (int g = 0; g < 8; ++g) {
+          uint4 u;
+          __nv_bfloat162* h = reinterpret_cast<__nv_bfloat162*>(&u);
+#pragma unroll
+          for (int e = 0; e < 4; ++e) h[e] = __floats2bfloat162_rn(v[8 * g + 2 * e], v[8 * g + 2 * e + 1]);
+          op[g] = u;
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    __syncwarp();
+    tc_fence_after();
+    tmem_dealloc(tmem, 128);
+  }
+}
+
+struct WgSmem {
+  // per stage: x window of tap a, x window of tap b (all ones for the last
+  // tap pair, which then yields the bias gradient), dz window
+  uint8_t st[WG_NST][3][WG_TILE];
+  uint64_t full[WG_NST], empty[WG_NST];
+  uint64_t done;
+  uint32_t tmem_base;
+  // Slack so that descriptor strides read no further than the allocation
+  // even if a stride were misinterpreted; never written.
+  uint8_t pad[8192];
+};
+
+// gridDim.y = 5 tap pairs: (0,1) (2,3) (4,5) (6,7) (8,bias).  gridDim.x CTAs
+// split the pixel chunks of each pair.
+__global__ void __launch_bounds__(THREADS, 1)
+k_conv_wgrad(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmZ,
+             WgradArgs G) {
+  extern __shared__ uint8_t smem_raw[];
+  WgSmem& S = *reinterpret_cast<WgSmem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int mt = blockIdx.y;
+  const bool bias_pair = (mt == 4);
+  const int ta = 2 * mt, tb = 2 * mt + 1;  // tb unused for the bias pair
+  const int xch = G.W / WG_PIX;
+  const long nchunk = (long)G.N * G.H * xch;
+  const long c_begin = nchunk * blockIdx.x / gridDim.x;
+  const long c_end = nchunk * (blockIdx.x + 1) / gridDim.x;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < WG_NST; ++s) {
+      mbar_init(&S.full[s], 1);
+      mbar_init(&S.empty[s], 1);
+    }
+    mbar_init(&S.done, 1);
+    fence_barrier_init();
+  }
+  if (bias_pair && warp >= 2) {
+    // BF16 1.0 everywhere in the second A half of every stage
+    const uint4 ones = make_uint4(0x3F803F80u, 0x3F803F80u, 0x3F803F80u, 0x3F803F80u);
+    for (int s = 0; s < WG_NST; ++s) {
+      uint4* d = reinterpret_cast<uint4*>(S.st[s][1]);
+      for (int i = threadIdx.x - 64; i < WG_TILE / 16; i += THREADS - 64) d[i] = ones;
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 1) tmem_alloc(&S.tmem_base, 64);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = S.tmem_base;
+  const bool have = c_end > c_begin;
+
+  if (warp == 0 && lane == 0) {
+    int stage = 0;
+    uint32_t phase = 0;
+    const uint32_t bytes = (bias_pair ? 2 : 3) * WG_TILE;
+    for (long c = c_begin; c < c_end; ++c) {
+      const int xc = (int)(c % xch);
+      const long r = c / xch;
+      const int y = (int)(r % G.H), n = (int)(r / G.H);
+      const int x0 = xc * WG_PIX;
+      if (!mbar_wait(&S.empty[stage], phase ^ 1)) { fail(G.err, 11); break; }
+      mbar_expect_tx(&S.full[stage], bytes);
+      tma_load_4d(S.st[stage][0], &tmX, &S.full[stage], 0, x0 + (ta % 3) - 1, y + ta / 3 - 1, n);
+      if (!bias_pair)
+        tma_load_4d(S.st[stage][1], &tmX, &S.full[stage], 0, x0 + (tb % 3) - 1, y + tb / 3 - 1, n);
+      tma_load_4d(S.st[stage][2], &tmZ, &S.full[stage], 0, x0, y, n);
+      if (++stage == WG_NST) { stage = 0; phase ^= 1; }
+    }
+    for (int s = 0; s < WG_NST; ++s) mbar_wait(&S.full[s], s < stage ? phase : phase ^ 1);
+  } else if (warp == 1 && lane == 0) {
+    // A: 128 rows (tap a ci 0-63, tap b ci 0-63) x K pixels with channels
+    // contiguous -> MN-major; the two 64-row halves are 8 KiB apart (leading
+    // byte offset), 8-pixel groups 1 KiB apart (stride byte offset).
+    // B: 64 co x K pixels, MN-major likewise.
+    const uint32_t ID = idesc(128, 64, 1, 1);
+    int stage = 0;
+    uint32_t phase = 0;
+    bool first = true;
+    for (long c = c_begin; c < c_end; ++c) {
+      if (!mbar_wait(&S.full[stage], phase)) { fail(G.err, 12); break; }
+      tc_fence_after();
+      const uint32_t a = smem_u32(S.st[stage][0]);
+      const uint32_t bz = smem_u32(S.st[stage][2]);
+#pragma unroll
+      for (int k = 0; k < WG_PIX / 16; ++k) {
+        mma_bf16(tmem, sdesc(a + 2048 * k, WG_TILE, 1024), sdesc(bz + 2048 * k, WG_TILE, 1024), ID,
+                 first ? 0u : 1u);
+        first = false;
+      }
+      mma_commit(&S.empty[stage]);
+      if (++stage == WG_NST) { stage = 0; phase ^= 1; }
+    }
+    mma_commit(&S.done);
+    if (!mbar_wait(&S.done, 0)) fail(G.err, 13);
+  }
+  if (warp >= 2 && have) {
+    const int q = warp & 3;
+    const int row = 32 * q + lane;  // (tap half, ci)
+    if (mbar_wait_warp(&S.done, 0)) {
+      tc_fence_after();
+      float v[64];
+      const uint32_t taddr = tmem + ((uint32_t)(32 * q) << 16);
+      tmem_ld32(taddr, v);
+      tmem_ld32(taddr + 32, v + 32);
+      if (row < 64 || !bias_pair) {
+        const int tap = row < 64 ? ta : tb;
+        float* dw = G.dw + (long)tap * CH * CH + (row & 63);
+#pragma unroll
+        for (int co = 0; co < 64; ++co) atomicAdd(dw + co * CH, v[co]);
+      } else if (row == 64 && G.db) {
+#pragma unroll
+        for (int co = 0; co < 64; ++co) atomicAdd(G.db + co, v[co]);
+      }
+    } else {
+      fail(G.err, 14);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    __syncwarp();
+    tc_fence_after();
+    tmem_dealloc(tmem, 64);
+  }
+}
+
+// ---- tensor maps ---------------------------------------------------------------
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+
+cudaError_t get_encoder() {
+  if (g_encode) return cudaSuccess;
+  cudaDriverEntryPointQueryResult q;
+  void* fn = nullptr;
+  cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+  if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn) return cudaErrorNotSupported;
+  g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  return cudaSuccess;
+}
+
+// NHWC activations (64 channels) as a 4-D map (C, W, H, N); box = 64 x box_w.
+cudaError_t act_map(CUtensorMap* m, const void* base, int N, int H, int W, int box_w) {
+  cuuint64_t dims[4] = {(cuuint64_t)CH, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)N};
+  cuuint64_t strides[3] = {(cuuint64_t)CH * 2, (cuuint64_t)W * CH * 2, (cuuint64_t)H * W * CH * 2};
+  cuuint32_t box[4] = {(cuuint32_t)CH, (cuuint32_t)box_w, 1, 1};
+  cuuint32_t es[4] = {1, 1, 1, 1};
+  CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(base), dims, strides, box,
+                        es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+// Weights [9*64 rows][64 cols] BF16; box 64 x 64 (one tap).
+cudaError_t w_map(CUtensorMap* m, const void* base) {
+  cuuint64_t dims[2] = {(cuuint64_t)CH, (cuuint64_t)9 * CH};
+  cuuint64_t strides[1] = {(cuuint64_t)CH * 2};
+  cuuint32_t box[2] = {(cuuint32_t)CH, (cuuint32_t)CH};
+  cuuint32_t es[2] = {1, 1};
+  CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, es,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+int g_sms[64];
+bool g_attr[64];
+
+// SM count of the current device; opts the kernels into their shared memory.
+cudaError_t prepare_device(int* sms) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  if (!g_attr[dev]) {
+    e = cudaDeviceGetAttribute(&g_sms[dev], cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_conv_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(sizeof(FwdSmem) + 1024));
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_conv_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(sizeof(WgSmem) + 1024));
+    if (e != cudaSuccess) return e;
+    g_attr[dev] = true;
+  }
+  *sms = g_sms[dev];
+  return cudaSuccess;
+}
+
+}  // namespace
+
+cudaError_t conv_fwd(const __nv_bfloat16* x, const __nv_bfloat16* w, const ConvEpi& epi, cudaStream_t s) {
+  if (epi.W % TM != 0 || epi.W < TM || epi.N < 1 || epi.H < 1 || !x || !w || !epi.err)
+    return cudaErrorInvalidValue;
+  if ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(w) | reinterpret_cast<uintptr_t>(epi.out) |
+       reinterpret_cast<uintptr_t>(epi.out32) | reinterpret_cast<uintptr_t>(epi.residual) |
+       reinterpret_cast<uintptr_t>(epi.mask)) & 15)
+    return cudaErrorInvalidValue;
+  cudaError_t e = get_encoder();
+  if (e != cudaSuccess) return e;
+  int sms = 0;
+  if ((e = prepare_device(&sms)) != cudaSuccess) return e;
+  CUtensorMap ta, tw;
+  if ((e = act_map(&ta, x, epi.N, epi.H, epi.W, TM)) != cudaSuccess) return e;
+  if ((e = w_map(&tw, w)) != cudaSuccess) return e;
+  const long ntile = (long)epi.N * epi.H * (epi.W / TM);
+  const int grid = (int)(ntile < sms ? ntile : sms);
+  k_conv_fwd<<<grid, THREADS, sizeof(FwdSmem) + 1024, s>>>(ta, tw, epi);
+  return cudaGetLastError();
+}
+
+cudaError_t conv_wgrad(const __nv_bfloat16* x, const __nv_bfloat16* dz, const WgradArgs& g, int ctas,
+                       cudaStream_t s) {
+  if (g.W % WG_PIX != 0 || g.W < WG_PIX || g.N < 1 || g.H < 1 || !x || !dz || !g.dw || !g.err)
+    return cudaErrorInvalidValue;
+  if ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(dz)) & 15) return cudaErrorInvalidValue;
+  cudaError_t e = get_encoder();
+  if (e != cudaSuccess) return e;
+  int sms = 0;
+  if ((e = prepare_device(&sms)) != cudaSuccess) return e;
+  CUtensorMap tx, tz;
+  if ((e = act_map(&tx, x, g.N, g.H, g.W, WG_PIX)) != cudaSuccess) return e;
+  if ((e = act_map(&tz, dz, g.N, g.H, g.W, WG_PIX)) != cudaSuccess) return e;
+  // two CTAs fit on an SM (shared memory and tensor memory): one wave of 5 pairs
+  int gx = ctas > 0 ? ctas : (2 * sms) / 5;
+  const long nchunk = (long)g.N * g.H * (g.W / WG_PIX);
+  if (gx > nchunk) gx = (int)nchunk;
+  if (gx < 1) gx = 1;
+  k_conv_wgrad<<<dim3((unsigned)gx, 5), THREADS, sizeof(WgSmem) + 1024, s>>>(tx, tz, g);
+  return cudaGetLastError();
+}
+
+}  // namespace sur

@@ -1,0 +1,57 @@
+// Internals of the BF16 convolutional surrogate shared between its
+// translation units.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include "nemo_b200.h"
+
+namespace sur {
+
+// Fused epilogue of a 3x3 convolution (64 -> 64 channels, NHWC BF16):
+//   v = acc + bias; v += residual; v *= (mask > 0); v = max(v, 0) if relu;
+//   out <- bf16(v) (64 channels), out32 <- v[0:4] (FP32, 4 per pixel).
+// Every pointer but err may be null.
+struct ConvEpi {
+  const float* bias;
+  const __nv_bfloat16* residual;
+  const __nv_bfloat16* mask;
+  __nv_bfloat16* out;
+  float* out32;
+  int relu;
+  int N, H, W;
+  int* err;  // device flag, first failing wait's code
+};
+
+// dw[tap][co][ci] += sum_p dz[p][co] x[p + off(tap)][ci]; db[co] += sum_p dz[p][co].
+struct WgradArgs {
+  float* dw;
+  float* db;
+  int N, H, W;
+  int* err;
+};
+
+// W % 128 == 0, x and w 16-byte aligned; w = [9][64 out][64 in] BF16.
+cudaError_t conv_fwd(const __nv_bfloat16* x, const __nv_bfloat16* w, const ConvEpi& epi, cudaStream_t s);
+// W % 64 == 0.  ctas <= 0 picks the count from the SM count.
+cudaError_t conv_wgrad(const __nv_bfloat16* x, const __nv_bfloat16* dz, const WgradArgs& g, int ctas,
+                       cudaStream_t s);
+
+}  // namespace sur
+
+namespace nemo {
+// Current-state view of one ensemble member (device pointers, pitched
+// single-grid layout: element (ji, jj) at (jj + 1) * pitch + ji + 2).
+struct MemberState {
+  double *sshn, *un, *vn;
+  const double* ht;
+  int jpi, jpj, pitch;
+};
+int ens_member_state(nemo_ens* e, int m, MemberState* out);
+int ens_member_count(nemo_ens* e);
+cudaStream_t ens_stream(nemo_ens* e);
+int ens_device(nemo_ens* e);
+// Tidal SSH a member's boundary row holds after step istp.
+double ens_tide(nemo_ens* e, int m, int istp);
+}  // namespace nemo

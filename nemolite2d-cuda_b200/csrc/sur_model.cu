@@ -1,0 +1,884 @@
+// BF16 residual CNN surrogate of the NEMOLite2D step (no reference
+// counterpart): training and inference on the tcgen05 convolution kernels,
+// data packing from ensemble members, and the hybrid controller that lets
+// the surrogate advance the ensemble k steps per call under FP64 re-anchoring.
+//
+// Network (all convolutions 3x3, 64 -> 64 channels, zero padding):
+//   h0 = relu(conv_0(x0) + b_0)
+//   t_i = relu(conv_{2i+1}(h_i) + b), h_{i+1} = h_i + conv_{2i+2}(t_i) + b   (i < nblocks)
+//   y = conv_{L-1}(h_nb) + b           (channels 0-2: normalised 10-step deltas)
+// Input channels of a T-cell (ji, jj) = pixel (ji-1, jj-1): 0 ssh, 1 u on the
+// cell's west face u(ji-1, jj), 2 v on its south face v(ji, jj-1), 3 depth,
+// 4 open-boundary row flag, 5 the boundary row's tidal SSH at the target
+// time; 6-63 zero.  Parameters are FP32 masters with BF16 copies (and the
+// tap-flipped transposes the data gradient needs) refreshed by AdamW.
+#include <math.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <chrono>
+#include <new>
+#include <vector>
+
+#include "sur_internal.h"
+
+using nemo::MemberState;
+
+namespace {
+
+constexpr int CH = 64;
+constexpr int WL = 9 * CH * CH;  // weights per layer
+
+struct Norm {
+  float in_scale[4], in_shift[4], out_scale[3];
+};
+
+int status_of(cudaError_t e) {
+  if (e == cudaSuccess) return NEMO_OK;
+  if (e == cudaErrorMemoryAllocation) return NEMO_ERR_ALLOC;
+  if (e == cudaErrorInvalidValue) return NEMO_ERR_INVALID;
+  return NEMO_ERR_CUDA;
+}
+#define ECK(call)                                \
+  do {                                           \
+    cudaError_t e_ = (call);                     \
+    if (e_ != cudaSuccess) return status_of(e_); \
+  } while (0)
+#define SCK(call)              \
+  do {                         \
+    int s_ = (call);           \
+    if (s_ != NEMO_OK) return s_; \
+  } while (0)
+
+__device__ __forceinline__ uint4 pack8(const float* f) {
+  uint4 u;
+  __nv_bfloat162* h = reinterpret_cast<__nv_bfloat162*>(&u);
+#pragma unroll
+  for (int e = 0; e < 4; ++e) h[e] = __floats2bfloat162_rn(f[2 * e], f[2 * e + 1]);
+  return u;
+}
+
+// x0 from FP32 snapshots (ssh, u_west, v_south, depth) and per-image tides.
+__global__ void k_make_input(const float4* __restrict__ snap, const float* __restrict__ tide, Norm nm,
+                             uint4* __restrict__ x0, long npix, int H, int W) {
+  for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < npix; p += (long)gridDim.x * blockDim.x) {
+    const float4 s = snap[p];
+    const long img = p / ((long)H * W);
+    const int y = (int)((p / W) % H);
+    float f[8];
+    f[0] = (s.x - nm.in_shift[0]) * nm.in_scale[0];
+    f[1] = (s.y - nm.in_shift[1]) * nm.in_scale[1];
+    f[2] = (s.z - nm.in_shift[2]) * nm.in_scale[2];
+    f[3] = (s.w - nm.in_shift[3]) * nm.in_scale[3];
+    f[4] = y == 0 ? 1.0f : 0.0f;
+    f[5] = y == 0 ? (tide[img] - nm.in_shift[0]) * nm.in_scale[0] : 0.0f;
+    f[6] = 0.0f;
+    f[7] = 0.0f;
+    uint4* o = x0 + p * 8;
+    o[0] = pack8(f);
+    const uint4 z = make_uint4(0, 0, 0, 0);
+#pragma unroll
+    for (int g = 1; g < 8; ++g) o[g] = z;
+  }
+}
+
+// Normalised 10-step deltas (channels 0-2; channel 3 zero).
+__global__ void k_make_target(const float4* __restrict__ s0, const float4* __restrict__ s1, Norm nm,
+                              float4* __restrict__ tgt, long npix) {
+  for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < npix; p += (long)gridDim.x * blockDim.x) {
+    const float4 a = s0[p], b = s1[p];
+    tgt[p] = make_float4((b.x - a.x) * nm.out_scale[0], (b.y - a.y) * nm.out_scale[1],
+                         (b.z - a.z) * nm.out_scale[2], 0.0f);
+  }
+}
+
+template <int BT>
+__device__ __forceinline__ double block_sum_d(double v, double* sh) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) sh[w] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0)
+    for (int i = 0; i < BT / 32; ++i) t += sh[i];
+  __syncthreads();
+  return t;
+}
+
+// Mean squared error over channels 0-2 and its gradient (BF16, 64 channels).
+__global__ void __launch_bounds__(256) k_loss(const float4* __restrict__ out, const float4* __restrict__ tgt,
+                                              uint4* __restrict__ dout, double* __restrict__ loss, long npix,
+                                              float gscale) {
+  __shared__ double sh[8];
+  double acc = 0.0;
+  for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < npix; p += (long)gridDim.x * blockDim.x) {
+    const float4 o = out[p], t = tgt[p];
+    const float d0 = o.x - t.x, d1 = o.y - t.y, d2 = o.z - t.z;
+    acc += (double)d0 * d0 + (double)d1 * d1 + (double)d2 * d2;
+    float f[8] = {2.0f * gscale * d0, 2.0f * gscale * d1, 2.0f * gscale * d2, 0, 0, 0, 0, 0};
+    uint4* g = dout + p * 8;
+    g[0] = pack8(f);
+    const uint4 z = make_uint4(0, 0, 0, 0);
+#pragma unroll
+    for (int k = 1; k < 8; ++k) g[k] = z;
+  }
+  const double s = block_sum_d<256>(acc, sh);
+  if (threadIdx.x == 0) atomicAdd(loss, s);
+}
+
+// BF16 copies of layer weights: w[l][tap][co][ci] and the data-gradient
+// weights wt[l][8 - tap][ci][co].
+__device__ __forceinline__ void put_weight(long i, float p, __nv_bfloat16* wbf, __nv_bfloat16* wt) {
+  const __nv_bfloat16 b = __float2bfloat16_rn(p);
+  wbf[i] = b;
+  const long l = i / WL;
+  const int r = (int)(i % WL);
+  const int tap = r / (CH * CH), co = (r / CH) % CH, ci = r % CH;
+  wt[l * WL + (long)(8 - tap) * CH * CH + ci * CH + co] = b;
+}
+
+__global__ void k_prep_weights(const float* __restrict__ p, long nw, __nv_bfloat16* wbf, __nv_bfloat16* wt) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < nw; i += (long)gridDim.x * blockDim.x)
+    put_weight(i, p[i], wbf, wt);
+}
+
+struct AdamArgs {
+  float lr, b1, b2, eps, wd, bc1, bc2;
+};
+
+// AdamW (decoupled weight decay on weights, not biases); refreshes the BF16
+// copies and clears the gradient for the next accumulation.
+__global__ void k_adamw(float* __restrict__ p, float* __restrict__ g, float* __restrict__ m, float* __restrict__ v,
+                        long np, long nw, AdamArgs a, __nv_bfloat16* wbf, __nv_bfloat16* wt) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < np; i += (long)gridDim.x * blockDim.x) {
+    const float gi = g[i];
+    const float mi = a.b1 * m[i] + (1.0f - a.b1) * gi;
+    const float vi = a.b2 * v[i] + (1.0f - a.b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    const float mh = mi / a.bc1, vh = vi / a.bc2;
+    float pi = p[i];
+    const float upd = mh / (sqrtf(vh) + a.eps) + (i < nw ? a.wd * pi : 0.0f);
+    pi -= a.lr * upd;
+    p[i] = pi;
+    g[i] = 0.0f;
+    if (i < nw) put_weight(i, pi, wbf, wt);
+  }
+}
+
+// ---- ensemble <-> network tensors -------------------------------------------
+__device__ __forceinline__ long gidx(int pitch, int ji, int jj) { return (long)(jj + 1) * pitch + ji + 2; }
+
+__global__ void k_pack(const MemberState* __restrict__ ms, int m0, int nm, int H, int W, float4* __restrict__ snap) {
+  const long npix = (long)nm * H * W;
+  for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < npix; p += (long)gridDim.x * blockDim.x) {
+    const int m = (int)(p / ((long)H * W));
+    const int y = (int)((p / W) % H), x = (int)(p % W);
+    const MemberState& M = ms[m0 + m];
+    const int ji = x + 1, jj = y + 1;
+    snap[p] = make_float4((float)M.sshn[gidx(M.pitch, ji, jj)], (float)M.un[gidx(M.pitch, ji - 1, jj)],
+                          (float)M.vn[gidx(M.pitch, ji, jj - 1)], (float)M.ht[gidx(M.pitch, ji, jj)]);
+  }
+}
+
+// state += delta / out_scale; the boundary row takes the exact tidal SSH;
+// u(0, :), u(jpi, :) and v(:, jpj) (walls) are left at zero.
+__global__ void k_apply(const MemberState* __restrict__ ms, int m0, int nm, int H, int W,
+                        const float4* __restrict__ out, Norm nm_, const double* __restrict__ tide) {
+  const long npix = (long)nm * H * W;
+  for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < npix; p += (long)gridDim.x * blockDim.x) {
+    const int m = (int)(p / ((long)H * W));
+    const int y = (int)((p / W) % H), x = (int)(p % W);
+    const MemberState& M = ms[m0 + m];
+    const int ji = x + 1, jj = y + 1;
+    const float4 d = out[p];
+    double* s = M.sshn + gidx(M.pitch, ji, jj);
+    *s = (jj == 1) ? tide[m0 + m] : *s + (double)(d.x / nm_.out_scale[0]);
+    if (ji >= 2) {
+      double* u = M.un + gidx(M.pitch, ji - 1, jj);
+      *u = *u + (double)(d.y / nm_.out_scale[1]);
+    }
+    double* v = M.vn + gidx(M.pitch, ji, jj - 1);
+    *v = *v + (double)(d.z / nm_.out_scale[2]);
+  }
+}
+
+// Per member: sum (pred - ref)^2 and sum ref^2 for ssh, u, v (acc[m][6]).
+// pred = snap + delta / out_scale when out != null, else the state of `pm`.
+__global__ void __launch_bounds__(256) k_err(const MemberState* __restrict__ ref, const float4* __restrict__ snap,
+                                             const float4* __restrict__ out, Norm nm_,
+                                             const MemberState* __restrict__ pm, int m0, int H, int W,
+                                             double* __restrict__ acc) {
+  __shared__ double sh[8];
+  const int m = blockIdx.y;
+  const MemberState& R = ref[m0 + m];
+  double a[6] = {0, 0, 0, 0, 0, 0};
+  const long np = (long)H * W;
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < np; q += (long)gridDim.x * blockDim.x) {
+    const int y = (int)(q / W), x = (int)(q % W);
+    const int ji = x + 1, jj = y + 1;
+    const double rs = R.sshn[gidx(R.pitch, ji, jj)];
+    const double ru = R.un[gidx(R.pitch, ji - 1, jj)];
+    const double rv = R.vn[gidx(R.pitch, ji, jj - 1)];
+    double ps, pu, pv;
+    if (out) {
+      const long p = (long)m * np + q;
+      const float4 s = snap[p], d = out[p];
+      ps = (jj == 1) ? rs : (double)s.x + (double)(d.x / nm_.out_scale[0]);
+      pu = (ji >= 2) ? (double)s.y + (double)(d.y / nm_.out_scale[1]) : 0.0;
+      pv = (double)s.z + (double)(d.z / nm_.out_scale[2]);
+    } else {
+      const MemberState& P = pm[m0 + m];
+      ps = P.sshn[gidx(P.pitch, ji, jj)];
+      pu = P.un[gidx(P.pitch, ji - 1, jj)];
+      pv = P.vn[gidx(P.pitch, ji, jj - 1)];
+    }
+    a[0] += (ps - rs) * (ps - rs);
+    a[1] += rs * rs;
+    a[2] += (pu - ru) * (pu - ru);
+    a[3] += ru * ru;
+    a[4] += (pv - rv) * (pv - rv);
+    a[5] += rv * rv;
+  }
+  for (int k = 0; k < 6; ++k) {
+    const double s = block_sum_d<256>(a[k], sh);
+    if (threadIdx.x == 0) atomicAdd(acc + (m0 + m) * 6 + k, s);
+  }
+}
+
+int grid_for(long n, int block) {
+  long g = (n + block - 1) / block;
+  if (g > 148 * 16) g = 148 * 16;
+  return (int)(g < 1 ? 1 : g);
+}
+
+uint64_t smix(uint64_t* s) {
+  uint64_t z = (*s += 0x9E3779B97F4A7C15ULL);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  return z ^ (z >> 31);
+}
+double unif(uint64_t* s) { return ((double)(smix(s) >> 11) + 0.5) * 0x1.0p-53; }
+double gauss(uint64_t* s) {
+  const double u = unif(s), v = unif(s);
+  return sqrt(-2.0 * log(u)) * cos(6.283185307179586 * v);
+}
+
+}  // namespace
+
+struct nemo_sur {
+  nemo_sur_config cfg{};
+  int L = 0;
+  long np = 0, nw = 0;          // parameters, of which weights
+  long npix = 0;                 // batch * H * W
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  Norm norm{};
+  float* p = nullptr;            // params (weights of all layers, then biases)
+  float* g = nullptr;
+  float* m = nullptr;
+  float* v = nullptr;
+  __nv_bfloat16* wbf = nullptr;
+  __nv_bfloat16* wt = nullptr;
+  std::vector<__nv_bfloat16*> act;  // activation tensors
+  __nv_bfloat16 *x0 = nullptr, *dout = nullptr, *g0 = nullptr, *g1 = nullptr, *dt = nullptr;
+  std::vector<__nv_bfloat16*> h, t;
+  float* out32 = nullptr;        // [batch][H][W][4]
+  float* tgt = nullptr;
+  float* snap = nullptr;         // [batch][H][W][4] (ensemble calls)
+  float* tide_f = nullptr;       // [batch]
+  double* tide_d = nullptr;      // [members]
+  double* loss = nullptr;
+  double* h_loss = nullptr;
+  int* err = nullptr;
+  MemberState* d_ms = nullptr;
+  MemberState* d_ms2 = nullptr;
+  int ms_cap = 0;
+  double* d_acc = nullptr;
+  int acc_cap = 0;
+  long adam_t = 0;
+};
+
+namespace {
+
+__nv_bfloat16* W_of(nemo_sur* s, int l) { return s->wbf + (long)l * WL; }
+__nv_bfloat16* WT_of(nemo_sur* s, int l) { return s->wt + (long)l * WL; }
+float* B_of(nemo_sur* s, int l) { return s->p + s->nw + (long)l * CH; }
+float* dW_of(nemo_sur* s, int l) { return s->g + (long)l * WL; }
+float* dB_of(nemo_sur* s, int l) { return s->g + s->nw + (long)l * CH; }
+
+int set_dev(nemo_sur* s) {
+  if (s->cfg.device >= 0) ECK(cudaSetDevice(s->cfg.device));
+  return NEMO_OK;
+}
+
+int conv(nemo_sur* s, const __nv_bfloat16* x, const __nv_bfloat16* w, const float* bias,
+         const __nv_bfloat16* res, const __nv_bfloat16* mask, int relu, __nv_bfloat16* out, float* out32, int n) {
+  sur::ConvEpi e{bias, res, mask, out, out32, relu, n, s->cfg.height, s->cfg.width, s->err};
+  ECK(sur::conv_fwd(x, w, e, s->stream));
+  return NEMO_OK;
+}
+
+int wgrad(nemo_sur* s, const __nv_bfloat16* x, const __nv_bfloat16* dz, int l, int n) {
+  sur::WgradArgs a{dW_of(s, l), dB_of(s, l), n, s->cfg.height, s->cfg.width, s->err};
+  ECK(sur::conv_wgrad(x, dz, a, 0, s->stream));
+  return NEMO_OK;
+}
+
+// Forward from x0 over n images; training keeps every activation.
+int forward(nemo_sur* s, int n, bool train, float* out32) {
+  const int nb = s->cfg.nblocks;
+  __nv_bfloat16* hcur = train ? s->h[0] : s->act[1];
+  SCK(conv(s, s->x0, W_of(s, 0), B_of(s, 0), nullptr, nullptr, 1, hcur, nullptr, n));
+  for (int i = 0; i < nb; ++i) {
+    __nv_bfloat16* ti = train ? s->t[i] : s->act[3];
+    __nv_bfloat16* hn = train ? s->h[i + 1] : (hcur == s->act[1] ? s->act[2] : s->act[1]);
+    SCK(conv(s, hcur, W_of(s, 1 + 2 * i), B_of(s, 1 + 2 * i), nullptr, nullptr, 1, ti, nullptr, n));
+    SCK(conv(s, ti, W_of(s, 2 + 2 * i), B_of(s, 2 + 2 * i), hcur, nullptr, 0, hn, nullptr, n));
+    hcur = hn;
+  }
+  SCK(conv(s, hcur, W_of(s, s->L - 1), B_of(s, s->L - 1), nullptr, nullptr, 0, nullptr, out32, n));
+  return NEMO_OK;
+}
+
+// Gradients of the loss held in dout (accumulated into g).
+int backward(nemo_sur* s, int n) {
+  const int nb = s->cfg.nblocks, L = s->L;
+  SCK(wgrad(s, s->h[nb], s->dout, L - 1, n));
+  __nv_bfloat16* gcur = s->g0;
+  __nv_bfloat16* gnext = s->g1;
+  SCK(conv(s, s->dout, WT_of(s, L - 1), nullptr, nullptr, nullptr, 0, gcur, nullptr, n));
+  for (int i = nb - 1; i >= 0; --i) {
+    const int la = 1 + 2 * i, lb = 2 + 2 * i;
+    SCK(wgrad(s, s->t[i], gcur, lb, n));
+    SCK(conv(s, gcur, WT_of(s, lb), nullptr, nullptr, s->t[i], 0, s->dt, nullptr, n));
+    SCK(wgrad(s, s->h[i], s->dt, la, n));
+    // d h_i = g + dgrad_a(dt), through the input ReLU for h_0
+    SCK(conv(s, s->dt, WT_of(s, la), nullptr, gcur, i == 0 ? s->h[0] : nullptr, 0, gnext, nullptr, n));
+    __nv_bfloat16* tmp = gcur;
+    gcur = gnext;
+    gnext = tmp;
+  }
+  if (nb == 0)  // no blocks: apply the input ReLU here
+    SCK(conv(s, s->dout, WT_of(s, L - 1), nullptr, nullptr, s->h[0], 0, gcur, nullptr, n));
+  SCK(wgrad(s, s->x0, gcur, 0, n));
+  return NEMO_OK;
+}
+
+int check_err(nemo_sur* s) {
+  int h = 0;
+  ECK(cudaMemcpyAsync(&h, s->err, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+  ECK(cudaStreamSynchronize(s->stream));
+  if (h != 0) {
+    fprintf(stderr, "nemo_sur: device wait gave up (code %d)\n", h);
+    cudaMemsetAsync(s->err, 0, sizeof(int), s->stream);
+    return NEMO_ERR_TIMEOUT;
+  }
+  return NEMO_OK;
+}
+
+int loss_grad(nemo_sur* s, const float* snap0, const float* snap1, const float* tide, int n, double* loss) {
+  if (n < 1 || n > s->cfg.batch || !snap0 || !snap1 || !tide || !s->cfg.train) return NEMO_ERR_INVALID;
+  const long npix = (long)n * s->cfg.height * s->cfg.width;
+  k_make_input<<<grid_for(npix, 256), 256, 0, s->stream>>>(reinterpret_cast<const float4*>(snap0), tide, s->norm,
+                                                         reinterpret_cast<uint4*>(s->x0), npix, s->cfg.height,
+                                                         s->cfg.width);
+  ECK(cudaGetLastError());
+  k_make_target<<<grid_for(npix, 256), 256, 0, s->stream>>>(reinterpret_cast<const float4*>(snap0),
+                                                          reinterpret_cast<const float4*>(snap1), s->norm,
+                                                          reinterpret_cast<float4*>(s->tgt), npix);
+  ECK(cudaGetLastError());
+  SCK(forward(s, n, true, s->out32));
+  ECK(cudaMemsetAsync(s->loss, 0, sizeof(double), s->stream));
+  k_loss<<<grid_for(npix, 256), 256, 0, s->stream>>>(reinterpret_cast<const float4*>(s->out32),
+                                                   reinterpret_cast<const float4*>(s->tgt),
+                                                   reinterpret_cast<uint4*>(s->dout), s->loss, npix,
+                                                   (float)(1.0 / (3.0 * (double)npix)));
+  ECK(cudaGetLastError());
+  SCK(backward(s, n));
+  ECK(cudaMemcpyAsync(s->h_loss, s->loss, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  SCK(check_err(s));
+  if (loss) *loss = *s->h_loss / (3.0 * (double)npix);
+  return NEMO_OK;
+}
+
+int ensure_members(nemo_sur* s, nemo_ens* e, std::vector<MemberState>& ms, MemberState** dst) {
+  const int nm = nemo::ens_member_count(e);
+  ms.resize(nm);
+  for (int i = 0; i < nm; ++i) {
+    SCK(nemo::ens_member_state(e, i, &ms[i]));
+    if (ms[i].jpi != s->cfg.width || ms[i].jpj != s->cfg.height) return NEMO_ERR_INVALID;
+  }
+  if (nm > s->ms_cap) {
+    cudaFree(s->d_ms);
+    cudaFree(s->d_ms2);
+    cudaFree(s->tide_d);
+    s->d_ms = s->d_ms2 = nullptr;
+    s->tide_d = nullptr;
+    s->ms_cap = 0;
+    ECK(cudaMalloc(&s->d_ms, nm * sizeof(MemberState)));
+    ECK(cudaMalloc(&s->d_ms2, nm * sizeof(MemberState)));
+    ECK(cudaMalloc(&s->tide_d, nm * sizeof(double)));
+    s->ms_cap = nm;
+  }
+  if (6 * nm > s->acc_cap) {
+    cudaFree(s->d_acc);
+    s->d_acc = nullptr;
+    s->acc_cap = 0;
+    ECK(cudaMalloc(&s->d_acc, 6 * nm * sizeof(double)));
+    s->acc_cap = 6 * nm;
+  }
+  MemberState* d = dst ? *dst : s->d_ms;
+  ECK(cudaMemcpyAsync(d, ms.data(), nm * sizeof(MemberState), cudaMemcpyHostToDevice, s->stream));
+  return NEMO_OK;
+}
+
+// Orders the surrogate's stream after the ensemble's work (and back).
+int join(cudaStream_t wait_on, cudaStream_t waiter) {
+  if (wait_on == waiter) return NEMO_OK;
+  cudaEvent_t ev;
+  ECK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  cudaError_t e = cudaEventRecord(ev, wait_on);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(waiter, ev, 0);
+  cudaEventDestroy(ev);
+  ECK(e);
+  return NEMO_OK;
+}
+
+// Surrogate forward for members [m0, m0+n) of e from their current state
+// (d_ms); tide_next[m] is the boundary SSH at the target time.  The chunk's
+// snapshot goes to snap_dst and the normalised deltas to out_dst.
+int predict_chunk(nemo_sur* s, int m0, int n, const std::vector<double>& tide_next, float* snap_dst,
+                  float* out_dst) {
+  const int H = s->cfg.height, W = s->cfg.width;
+  const long npix = (long)n * H * W;
+  std::vector<float> tf(n);
+  for (int i = 0; i < n; ++i) tf[i] = (float)tide_next[m0 + i];
+  // pageable source: the call returns once tf has been staged
+  ECK(cudaMemcpyAsync(s->tide_f, tf.data(), n * sizeof(float), cudaMemcpyHostToDevice, s->stream));
+  k_pack<<<grid_for(npix, 256), 256, 0, s->stream>>>(s->d_ms, m0, n, H, W, reinterpret_cast<float4*>(snap_dst));
+  ECK(cudaGetLastError());
+  k_make_input<<<grid_for(npix, 256), 256, 0, s->stream>>>(reinterpret_cast<const float4*>(snap_dst), s->tide_f,
+                                                         s->norm, reinterpret_cast<uint4*>(s->x0), npix, H, W);
+  ECK(cudaGetLastError());
+  return forward(s, n, false, out_dst);
+}
+
+}  // namespace
+
+extern "C" {
+
+int nemo_sur_default_config(nemo_sur_config* c) {
+  if (!c) return NEMO_ERR_INVALID;
+  memset(c, 0, sizeof(*c));
+  c->nblocks = 8;
+  c->batch = 64;
+  c->height = 256;
+  c->width = 256;
+  c->train = 1;
+  c->seed = 1234;
+  c->stream = nullptr;
+  c->device = -1;
+  return NEMO_OK;
+}
+
+int nemo_sur_destroy(nemo_sur* s) {
+  if (!s) return NEMO_ERR_INVALID;
+  if (s->cfg.device >= 0) cudaSetDevice(s->cfg.device);
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  for (auto* a : s->act) cudaFree(a);
+  cudaFree(s->p);
+  cudaFree(s->g);
+  cudaFree(s->m);
+  cudaFree(s->v);
+  cudaFree(s->wbf);
+  cudaFree(s->wt);
+  cudaFree(s->out32);
+  cudaFree(s->tgt);
+  cudaFree(s->snap);
+  cudaFree(s->tide_f);
+  cudaFree(s->tide_d);
+  cudaFree(s->loss);
+  cudaFree(s->err);
+  cudaFree(s->d_ms);
+  cudaFree(s->d_ms2);
+  cudaFree(s->d_acc);
+  if (s->h_loss) cudaFreeHost(s->h_loss);
+  if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+  return NEMO_OK;
+}
+
+int nemo_sur_create(const nemo_sur_config* c, nemo_sur** out) {
+  if (!c || !out) return NEMO_ERR_INVALID;
+  *out = nullptr;
+  if (c->nblocks < 0 || c->nblocks > 64 || c->batch < 1 || c->height < 1 || c->width < 128 ||
+      c->width % 128 != 0)
+    return NEMO_ERR_INVALID;
+  nemo_sur* s = new (std::nothrow) nemo_sur;
+  if (!s) return NEMO_ERR_ALLOC;
+  s->cfg = *c;
+  s->L = 2 * c->nblocks + 2;
+  s->nw = (long)s->L * WL;
+  s->np = s->nw + (long)s->L * CH;
+  s->npix = (long)c->batch * c->height * c->width;
+  for (int k = 0; k < 4; ++k) {
+    s->norm.in_scale[k] = 1.0f;
+    s->norm.in_shift[k] = 0.0f;
+  }
+  for (int k = 0; k < 3; ++k) s->norm.out_scale[k] = 1.0f;
+  auto fail = [&](int st) {
+    nemo_sur_destroy(s);
+    return st;
+  };
+  if (set_dev(s)) return fail(NEMO_ERR_CUDA);
+  if (c->stream) {
+    s->stream = (cudaStream_t)c->stream;
+  } else {
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(NEMO_ERR_CUDA);
+    s->own_stream = true;
+  }
+  const size_t pb = s->np * sizeof(float);
+  if (cudaMalloc(&s->p, pb) || cudaMalloc(&s->g, pb) || cudaMalloc(&s->wbf, s->nw * 2) ||
+      cudaMalloc(&s->wt, s->nw * 2) || cudaMalloc(&s->loss, sizeof(double)) || cudaMalloc(&s->err, sizeof(int)) ||
+      cudaMallocHost(&s->h_loss, sizeof(double)))
+    return fail(NEMO_ERR_ALLOC);
+  if (c->train && (cudaMalloc(&s->m, pb) || cudaMalloc(&s->v, pb))) return fail(NEMO_ERR_ALLOC);
+  const size_t ab = (size_t)s->npix * CH * 2;
+  const int nact = c->train ? 1 + (c->nblocks + 1) + c->nblocks + 4 : 4;
+  for (int i = 0; i < nact; ++i) {
+    __nv_bfloat16* a = nullptr;
+    if (cudaMalloc(&a, ab)) return fail(NEMO_ERR_ALLOC);
+    s->act.push_back(a);
+  }
+  s->x0 = s->act[0];
+  if (c->train) {
+    int k = 1;
+    for (int i = 0; i <= c->nblocks; ++i) s->h.push_back(s->act[k++]);
+    for (int i = 0; i < c->nblocks; ++i) s->t.push_back(s->act[k++]);
+    s->dout = s->act[k++];
+    s->g0 = s->act[k++];
+    s->g1 = s->act[k++];
+    s->dt = s->act[k++];
+  }
+  if (cudaMalloc(&s->out32, s->npix * 16) || cudaMalloc(&s->snap, s->npix * 16) ||
+      cudaMalloc(&s->tide_f, c->batch * sizeof(float)))
+    return fail(NEMO_ERR_ALLOC);
+  if (c->train && cudaMalloc(&s->tgt, s->npix * 16)) return fail(NEMO_ERR_ALLOC);
+  if (cudaMemsetAsync(s->err, 0, sizeof(int), s->stream) || cudaMemsetAsync(s->g, 0, pb, s->stream) ||
+      (c->train && (cudaMemsetAsync(s->m, 0, pb, s->stream) || cudaMemsetAsync(s->v, 0, pb, s->stream))))
+    return fail(NEMO_ERR_CUDA);
+  // seeded initialisation: He-normal convolutions; the residual branches'
+  // second convolutions and the output convolution start small
+  std::vector<float> hp(s->np, 0.0f);
+  uint64_t st = c->seed;
+  for (int l = 0; l < s->L; ++l) {
+    const bool first = l == 0, last = l == s->L - 1, branch_out = l > 0 && !last && (l % 2 == 0);
+    const int cin = first ? 6 : CH;
+    const int cout = last ? 3 : CH;
+    double sd = sqrt(2.0 / (9.0 * cin));
+    if (branch_out) sd *= 0.1;
+    if (last) sd = 0.1 * sqrt(1.0 / (9.0 * cin));
+    for (int tap = 0; tap < 9; ++tap)
+      for (int co = 0; co < cout; ++co)
+        for (int ci = 0; ci < cin; ++ci)
+          hp[(long)l * WL + tap * CH * CH + co * CH + ci] = (float)(sd * gauss(&st));
+  }
+  if (cudaMemcpyAsync(s->p, hp.data(), pb, cudaMemcpyHostToDevice, s->stream)) return fail(NEMO_ERR_CUDA);
+  k_prep_weights<<<grid_for(s->nw, 256), 256, 0, s->stream>>>(s->p, s->nw, s->wbf, s->wt);
+  if (cudaGetLastError() || cudaStreamSynchronize(s->stream)) return fail(NEMO_ERR_CUDA);
+  *out = s;
+  return NEMO_OK;
+}
+
+int nemo_sur_info(nemo_sur* s, long long* nparams, long long* flops_per_pixel) {
+  if (!s) return NEMO_ERR_STATE;
+  if (nparams) *nparams = s->np;
+  if (flops_per_pixel) *flops_per_pixel = (long long)s->L * 2 * WL;
+  return NEMO_OK;
+}
+
+int nemo_sur_get_params(nemo_sur* s, float* host) {
+  if (!s || !host) return NEMO_ERR_INVALID;
+  SCK(set_dev(s));
+  ECK(cudaMemcpyAsync(host, s->p, s->np * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+  ECK(cudaStreamSynchronize(s->stream));
+  return NEMO_OK;
+}
+
+int nemo_sur_set_params(nemo_sur* s, const float* host) {
+  if (!s || !host) return NEMO_ERR_INVALID;
+  SCK(set_dev(s));
+  ECK(cudaMemcpyAsync(s->p, host, s->np * sizeof(float), cudaMemcpyHostToDevice, s->stream));
+  k_prep_weights<<<grid_for(s->nw, 256), 256, 0, s->stream>>>(s->p, s->nw, s->wbf, s->wt);
+  ECK(cudaGetLastError());
+  ECK(cudaStreamSynchronize(s->stream));
+  return NEMO_OK;
+}
+
+int nemo_sur_get_grads(nemo_sur* s, float* host) {
+  if (!s || !host) return NEMO_ERR_INVALID;
+  SCK(set_dev(s));
+  ECK(cudaMemcpyAsync(host, s->g, s->np * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+  ECK(cudaStreamSynchronize(s->stream));
+  return NEMO_OK;
+}
+
+int nemo_sur_set_norm(nemo_sur* s, const float* norm11) {
+  if (!s || !norm11) return NEMO_ERR_INVALID;
+  Norm n;
+  memcpy(n.in_scale, norm11, 4 * sizeof(float));
+  memcpy(n.in_shift, norm11 + 4, 4 * sizeof(float));
+  memcpy(n.out_scale, norm11 + 8, 3 * sizeof(float));
+  for (int k = 0; k < 3; ++k)
+    if (!(n.out_scale[k] > 0.0f) || !isfinite(n.out_scale[k])) return NEMO_ERR_INVALID;
+  s->norm = n;
+  return NEMO_OK;
+}
+
+int nemo_sur_get_norm(nemo_sur* s, float* norm11) {
+  if (!s || !norm11) return NEMO_ERR_INVALID;
+  memcpy(norm11, s->norm.in_scale, 4 * sizeof(float));
+  memcpy(norm11 + 4, s->norm.in_shift, 4 * sizeof(float));
+  memcpy(norm11 + 8, s->norm.out_scale, 3 * sizeof(float));
+  return NEMO_OK;
+}
+
+int nemo_sur_predict(nemo_sur* s, const float* snap, const float* tide, int n, float* out) {
+  if (!s || !snap || !tide || n < 1 || n > s->cfg.batch) return NEMO_ERR_INVALID;
+  SCK(set_dev(s));
+  const long npix = (long)n * s->cfg.height * s->cfg.width;
+  k_make_input<<<grid_for(npix, 256), 256, 0, s->stream>>>(reinterpret_cast<const float4*>(snap), tide, s->norm,
+                                                         reinterpret_cast<uint4*>(s->x0), npix, s->cfg.height,
+                                                         s->cfg.width);
+  ECK(cudaGetLastError());
+  SCK(forward(s, n, false, out ? out : s->out32));
+  return check_err(s);
+}
+
+int nemo_sur_loss_grad(nemo_sur* s, const float* snap0, const float* snap1, const float* tide, int n,
+                       double* loss) {
+  if (!s) return NEMO_ERR_STATE;
+  SCK(set_dev(s));
+  ECK(cudaMemsetAsync(s->g, 0, s->np * sizeof(float), s->stream));
+  return loss_grad(s, snap0, snap1, tide, n, loss);
+}
+
+int nemo_sur_adamw(nemo_sur* s, const nemo_adamw* hp) {
+  if (!s || !hp || !s->cfg.train) return NEMO_ERR_INVALID;
+  SCK(set_dev(s));
+  s->adam_t += 1;
+  AdamArgs a{hp->lr, hp->beta1, hp->beta2, hp->eps, hp->weight_decay,
+             (float)(1.0 - pow((double)hp->beta1, (double)s->adam_t)),
+             (float)(1.0 - pow((double)hp->beta2, (double)s->adam_t))};
+  k_adamw<<<grid_for(s->np, 256), 256, 0, s->stream>>>(s->p, s->g, s->m, s->v, s->np, s->nw, a, s->wbf, s->wt);
+  ECK(cudaGetLastError());
+  return NEMO_OK;
+}
+
+int nemo_sur_train_step(nemo_sur* s, const float* snap0, const float* snap1, const float* tide, int n,
+                        const nemo_adamw* hp, double* loss) {
+  if (!s || !hp) return NEMO_ERR_INVALID;
+  SCK(set_dev(s));
+  SCK(loss_grad(s, snap0, snap1, tide, n, loss));  // g is clear after the last AdamW
+  return nemo_sur_adamw(s, hp);
+}
+
+int nemo_sur_pack_ens(nemo_sur* s, nemo_ens* e, float* snap) {
+  if (!s || !e || !snap) return NEMO_ERR_INVALID;
+  SCK(set_dev(s));
+  std::vector<MemberState> ms;
+  SCK(join(nemo::ens_stream(e), s->stream));
+  SCK(ensure_members(s, e, ms, nullptr));
+  const int nm = (int)ms.size();
+  const long npix = (long)nm * s->cfg.height * s->cfg.width;
+  k_pack<<<grid_for(npix, 256), 256, 0, s->stream>>>(s->d_ms, 0, nm, s->cfg.height, s->cfg.width,
+                                                   reinterpret_cast<float4*>(snap));
+  ECK(cudaGetLastError());
+  ECK(cudaStreamSynchronize(s->stream));  // ms (host) copied
+  return NEMO_OK;
+}
+
+int nemo_sur_advance_ens(nemo_sur* s, nemo_ens* e, int istp_end) {
+  if (!s || !e) return NEMO_ERR_INVALID;
+  SCK(set_dev(s));
+  std::vector<MemberState> ms;
+  SCK(join(nemo::ens_stream(e), s->stream));
+  SCK(ensure_members(s, e, ms, nullptr));
+  const int nm = (int)ms.size();
+  std::vector<double> tide(nm);
+  for (int i = 0; i < nm; ++i) tide[i] = nemo::ens_tide(e, i, istp_end);
+  ECK(cudaMemcpyAsync(s->tide_d, tide.data(), nm * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  for (int m0 = 0; m0 < nm; m0 += s->cfg.batch) {
+    const int n = nm - m0 < s->cfg.batch ? nm - m0 : s->cfg.batch;
+    SCK(predict_chunk(s, m0, n, tide, s->snap, s->out32));
+    const long npix = (long)n * s->cfg.height * s->cfg.width;
+    k_apply<<<grid_for(npix, 256), 256, 0, s->stream>>>(s->d_ms, m0, n, s->cfg.height, s->cfg.width,
+                                                      reinterpret_cast<const float4*>(s->out32), s->norm, s->tide_d);
+    ECK(cudaGetLastError());
+  }
+  SCK(check_err(s));
+  return join(s->stream, nemo::ens_stream(e));
+}
+
+int nemo_ens_compare(nemo_ens* a, nemo_ens* ref, double* out) {
+  if (!a || !ref || !out) return NEMO_ERR_INVALID;
+  const int nm = nemo::ens_member_count(a);
+  if (nm != nemo::ens_member_count(ref)) return NEMO_ERR_INVALID;
+  if (nemo::ens_device(a) >= 0) ECK(cudaSetDevice(nemo::ens_device(a)));
+  std::vector<MemberState> ma(nm), mr(nm);
+  for (int i = 0; i < nm; ++i) {
+    SCK(nemo::ens_member_state(a, i, &ma[i]));
+    SCK(nemo::ens_member_state(ref, i, &mr[i]));
+    if (ma[i].jpi != mr[i].jpi || ma[i].jpj != mr[i].jpj) return NEMO_ERR_INVALID;
+  }
+  cudaStream_t st = nemo::ens_stream(a);
+  SCK(join(nemo::ens_stream(ref), st));
+  MemberState *da = nullptr, *dr = nullptr;
+  double* acc = nullptr;
+  cudaError_t e = cudaMalloc(&da, nm * sizeof(MemberState));
+  if (e == cudaSuccess) e = cudaMalloc(&dr, nm * sizeof(MemberState));
+  if (e == cudaSuccess) e = cudaMalloc(&acc, 6 * nm * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemcpyAsync(da, ma.data(), nm * sizeof(MemberState), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dr, mr.data(), nm * sizeof(MemberState), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(acc, 0, 6 * nm * sizeof(double), st);
+  std::vector<double> h(6 * nm);
+  if (e == cudaSuccess) {
+    // one launch per member (sizes differ)
+    for (int m = 0; m < nm && e == cudaSuccess; ++m) {
+      Norm dummy{};
+      k_err<<<dim3((unsigned)grid_for((long)ma[m].jpi * ma[m].jpj, 256) / 16 + 1, 1), 256, 0, st>>>(
+          dr, nullptr, nullptr, dummy, da, m, ma[m].jpj, ma[m].jpi, acc);
+      e = cudaGetLastError();
+    }
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), acc, 6 * nm * sizeof(double), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFree(da);
+  cudaFree(dr);
+  cudaFree(acc);
+  ECK(e);
+  for (int m = 0; m < nm; ++m)
+    for (int f = 0; f < 3; ++f) {
+      const double num = h[6 * m + 2 * f], den = h[6 * m + 2 * f + 1];
+      out[3 * m + f] = den > 0 ? sqrt(num / den) : sqrt(num);
+    }
+  return NEMO_OK;
+}
+
+int nemo_hyb_default_config(nemo_hyb_config* c) {
+  if (!c) return NEMO_ERR_INVALID;
+  c->k = 10;
+  c->anchor = 100;
+  c->tol = 0.01;
+  return NEMO_OK;
+}
+
+// Advances e from the state after step istp0 by nsteps (a multiple of
+// anchor, anchor a multiple of k).  Each anchor window: the surrogate
+// predicts the first k steps, the FP64 solver runs them (the shadow step and
+// the re-anchored state), and if any member's relative SSH L2 error of the
+// prediction exceeds tol the solver runs the whole window; otherwise the
+// surrogate advances the remaining anchor - k steps, k per call.
+int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, int nsteps,
+                 nemo_hyb_stats* stats) {
+  if (!s || !e || !c || c->k != 10 || c->anchor < c->k || c->anchor % c->k || nsteps % c->anchor ||
+      !(c->tol > 0))
+    return NEMO_ERR_INVALID;
+  SCK(set_dev(s));
+  nemo_hyb_stats st{};
+  std::vector<MemberState> ms;
+  SCK(join(nemo::ens_stream(e), s->stream));
+  SCK(ensure_members(s, e, ms, nullptr));
+  const int nm = (int)ms.size();
+  const int H = s->cfg.height, W = s->cfg.width;
+  const long hw = (long)H * W;
+  // predictions of all members are kept for the shadow comparison
+  float *snap_all = s->snap, *out_all = s->out32;
+  float* own = nullptr;
+  if (nm > s->cfg.batch) {
+    ECK(cudaMalloc(&own, 2 * (size_t)nm * hw * 16));
+    snap_all = own;
+    out_all = own + (size_t)nm * hw * 4;
+  }
+  std::vector<double> tide(nm), acc(6 * nm);
+  const auto t_start = std::chrono::steady_clock::now();
+  int istp = istp0;
+  int rc = NEMO_OK;
+  for (int w = 0; w < nsteps / c->anchor && rc == NEMO_OK; ++w) {
+    for (int i = 0; i < nm; ++i) tide[i] = nemo::ens_tide(e, i, istp + c->k);
+    for (int m0 = 0; m0 < nm && rc == NEMO_OK; m0 += s->cfg.batch) {
+      const int n = nm - m0 < s->cfg.batch ? nm - m0 : s->cfg.batch;
+      rc = predict_chunk(s, m0, n, tide, snap_all + (size_t)m0 * hw * 4, out_all + (size_t)m0 * hw * 4);
+    }
+    // shadow / re-anchor: the FP64 solver runs the same k steps
+    if (rc == NEMO_OK) rc = join(s->stream, nemo::ens_stream(e));
+    if (rc == NEMO_OK) rc = nemo_ens_step_n(e, istp + 1, c->k);
+    if (rc == NEMO_OK) rc = join(nemo::ens_stream(e), s->stream);
+    if (rc == NEMO_OK) rc = ensure_members(s, e, ms, nullptr);  // buffers swapped
+    if (rc != NEMO_OK) break;
+    cudaError_t ce = cudaMemsetAsync(s->d_acc, 0, 6 * nm * sizeof(double), s->stream);
+    if (ce == cudaSuccess) {
+      k_err<<<dim3((unsigned)(grid_for(hw, 256) / 16 + 1), (unsigned)nm), 256, 0, s->stream>>>(
+          s->d_ms, reinterpret_cast<const float4*>(snap_all), reinterpret_cast<const float4*>(out_all), s->norm,
+          nullptr, 0, H, W, s->d_acc);
+      ce = cudaGetLastError();
+    }
+    if (ce == cudaSuccess)
+      ce = cudaMemcpyAsync(acc.data(), s->d_acc, 6 * nm * sizeof(double), cudaMemcpyDeviceToHost, s->stream);
+    if (ce != cudaSuccess) { rc = status_of(ce); break; }
+    if ((rc = check_err(s)) != NEMO_OK) break;
+    double worst = 0.0;
+    for (int m = 0; m < nm; ++m) {
+      const double r = acc[6 * m + 1] > 0 ? sqrt(acc[6 * m] / acc[6 * m + 1]) : sqrt(acc[6 * m]);
+      if (r > worst) worst = r;
+    }
+    st.last_shadow_err = worst;
+    if (worst > st.max_shadow_err) st.max_shadow_err = worst;
+    st.solver_steps += c->k;
+    st.sur_calls += 1;
+    istp += c->k;
+    if (worst > c->tol) {  // fallback: the solver runs the rest of the window
+      st.fallbacks += 1;
+      rc = nemo_ens_step_n(e, istp + 1, c->anchor - c->k);
+      st.solver_steps += c->anchor - c->k;
+      istp += c->anchor - c->k;
+      continue;
+    }
+    for (int j = c->k; j < c->anchor && rc == NEMO_OK; j += c->k) {
+      rc = nemo_sur_advance_ens(s, e, istp + c->k);
+      st.sur_calls += 1;
+      st.sur_steps += c->k;
+      istp += c->k;
+    }
+  }
+  cudaError_t ce = cudaStreamSynchronize(nemo::ens_stream(e));
+  if (ce == cudaSuccess) ce = cudaStreamSynchronize(s->stream);
+  if (own) cudaFree(own);
+  if (rc != NEMO_OK) return rc;
+  ECK(ce);
+  st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+  if (stats) *stats = st;
+  return NEMO_OK;
+}
+
+// ---- single kernels on caller-owned device buffers (for parity tests) -------
+int nemo_conv3x3_fwd(const void* x, const void* w, const float* bias, const void* residual, const void* mask,
+                     int relu, void* out, float* out32, int n, int h, int wd, int* err, void* stream) {
+  if (!x || !w || !err || (!out && !out32)) return NEMO_ERR_INVALID;
+  sur::ConvEpi e{bias, (const __nv_bfloat16*)residual, (const __nv_bfloat16*)mask, (__nv_bfloat16*)out, out32,
+                 relu, n, h, wd, err};
+  ECK(sur::conv_fwd((const __nv_bfloat16*)x, (const __nv_bfloat16*)w, e, (cudaStream_t)stream));
+  return NEMO_OK;
+}
+
+int nemo_conv3x3_wgrad(const void* x, const void* dz, float* dw, float* db, int n, int h, int wd, int ctas,
+                       int* err, void* stream) {
+  if (!x || !dz || !dw || !err) return NEMO_ERR_INVALID;
+  sur::WgradArgs a{dw, db, n, h, wd, err};
+  ECK(sur::conv_wgrad((const __nv_bfloat16*)x, (const __nv_bfloat16*)dz, a, ctas, (cudaStream_t)stream));
+  return NEMO_OK;
+}
+
+}  // extern "C"

@@ -39,6 +39,11 @@ EXPORTED = [
     "nemo_ens_generate", "nemo_ens_create", "nemo_ens_destroy", "nemo_ens_step_n",
     "nemo_ens_checksums", "nemo_ens_retrieve", "nemo_ens_set_state", "nemo_ens_set_schedule",
     "nemo_ens_get_schedule", "nemo_ens_use_graph", "nemo_ens_info", "nemo_ens_autotune",
+    "nemo_sur_default_config", "nemo_sur_create", "nemo_sur_destroy", "nemo_sur_info",
+    "nemo_sur_get_params", "nemo_sur_set_params", "nemo_sur_get_grads", "nemo_sur_set_norm",
+    "nemo_sur_get_norm", "nemo_sur_predict", "nemo_sur_loss_grad", "nemo_sur_adamw",
+    "nemo_sur_train_step", "nemo_sur_pack_ens", "nemo_sur_advance_ens", "nemo_ens_compare",
+    "nemo_hyb_default_config", "nemo_hyb_run", "nemo_conv3x3_fwd", "nemo_conv3x3_wgrad",
     "cuda_setup_model_params_", "cuda_initialise_grid_", "cuda_continuity_", "cuda_momentum_",
     "cuda_boundary_conditions_", "cuda_next_", "cuda_retrieve_grid_constants_",
     "cuda_retrieve_results_", "cuda_finalise_", "nemo_compat_last_status", "nemo_compat_context",
@@ -149,6 +154,8 @@ def load(strict=False):
     L.nemo_ens_use_graph.argtypes = [vp, ip]
     L.nemo_ens_info.argtypes = [vp, P(ip), P(ctypes.c_longlong)]
     L.nemo_ens_autotune.argtypes = [vp, ip, P(EnsSchedule), P(dp)]
+    from . import surrogate as _sur
+    _sur.declare(L)
     _libs[strict] = L
     return L
 

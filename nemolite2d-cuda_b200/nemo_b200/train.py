@@ -1,0 +1,149 @@
+"""Training data from the ensemble solver, normalisation, the AdamW training
+loop and evaluation of the surrogate against the FP64 solver.
+
+Snapshots are FP32 device tensors [members][H][W][4] (ssh, u west face,
+v south face, depth) taken every `every` steps from seeded ensembles of
+equal-size members (the batched configuration's recipe at a fixed side).
+torch only provides device memory and index gathers; every network kernel
+runs in the library.
+"""
+import math
+
+import numpy as np
+
+from . import Ensemble, default_params, generate_members
+from .surrogate import adamw, ens_compare
+
+COMMON = dict(dx=1000.0, dy=1000.0, rdt=20.0, cbfr=0.00015, visc=0.1)
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def square_members(seed, n, side, amp_scale):
+    ms = generate_members(seed, n, side_min=side, side_max=side, amp_scale=amp_scale)
+    for m in ms:
+        m.jpi = side
+        m.jpj = side
+    return ms
+
+
+def tide_of(member, istp, rdt=20.0):
+    """Boundary-row SSH after step istp (original/nemolite2d.f90:629-635)."""
+    omega = 2.0 * 3.14159 / (12.42 * 3600.0)
+    return member.amp_tide * math.sin(omega * (istp * rdt) + member.tide_phase)
+
+
+def generate_runs(sur, seed, nmem, side, steps, every=10, amp_scale=0.2, strict=False):
+    """Runs nmem members from rest for `steps` steps; returns (snaps, tides):
+    snaps [steps//every + 1][nmem][side][side][4] float32 on the device and
+    tides [same][nmem] float32 (the boundary SSH at each snapshot's step)."""
+    torch = _torch()
+    members = square_members(seed, nmem, side, amp_scale)
+    ens = Ensemble(members, strict=strict, **COMMON)
+    ns = steps // every + 1
+    snaps = torch.empty((ns, nmem, side, side, 4), dtype=torch.float32, device="cuda")
+    tides = torch.empty((ns, nmem), dtype=torch.float32)
+    istp = 0
+    for k in range(ns):
+        if k:
+            ens.step_n(istp + 1, every)
+            istp += every
+        torch.cuda.synchronize()
+        sur.pack_ens(ens, snaps[k].data_ptr())
+        tides[k] = torch.tensor([tide_of(m, istp) for m in members], dtype=torch.float32)
+    ens.close()
+    return snaps, tides.cuda()
+
+
+def compute_norm(snaps):
+    """Input scale/shift per channel and output scale per delta channel from
+    a snapshot tensor [S][N][H][W][4]."""
+    torch = _torch()
+    x = snaps.reshape(-1, 4).double()
+    mean = x.mean(0)
+    std = x.std(0)
+    d = (snaps[1:] - snaps[:-1]).reshape(-1, 4).double()
+    dstd = d.std(0)
+    in_shift = [0.0, 0.0, 0.0, float(mean[3])]
+    in_scale = [1.0 / max(float(std[c]), 1e-12) for c in range(4)]
+    out_scale = [1.0 / max(float(dstd[c]), 1e-12) for c in range(3)]
+    del torch
+    return in_scale, in_shift, out_scale
+
+
+class PairSampler:
+    """Random (snapshot k, snapshot k+1) pairs of a run set, gathered into
+    contiguous device batches."""
+
+    def __init__(self, snaps, tides, seed=0):
+        torch = _torch()
+        self.snaps, self.tides = snaps, tides
+        S, N = snaps.shape[0], snaps.shape[1]
+        self.pairs = [(k, m) for k in range(S - 1) for m in range(N)]
+        self.rng = np.random.default_rng(seed)
+        self.order = []
+        self.s0 = self.s1 = self.t1 = None
+        self._torch = torch
+
+    def batch(self, n):
+        torch = self._torch
+        if len(self.order) < n:
+            self.order = list(self.rng.permutation(len(self.pairs)))
+        idx = [self.pairs[self.order.pop()] for _ in range(n)]
+        k = torch.tensor([i[0] for i in idx], device="cuda")
+        m = torch.tensor([i[1] for i in idx], device="cuda")
+        s0 = self.snaps[k, m].contiguous()
+        s1 = self.snaps[k + 1, m].contiguous()
+        t1 = self.tides[k + 1, m].contiguous()
+        torch.cuda.synchronize()
+        self.s0, self.s1, self.t1 = s0, s1, t1  # keep alive while the library reads
+        return s0, s1, t1
+
+
+def train(sur, sampler, iters, batch, lr=1e-3, weight_decay=1e-4, lr_min=1e-5, log_every=0):
+    """AdamW with cosine learning-rate decay; returns the loss history."""
+    losses = []
+    for it in range(iters):
+        c = 0.5 * (1.0 + math.cos(math.pi * it / max(iters, 1)))
+        hp = adamw(lr=lr_min + (lr - lr_min) * c, weight_decay=weight_decay)
+        s0, s1, t1 = sampler.batch(batch)
+        losses.append(sur.train_step(s0.data_ptr(), s1.data_ptr(), t1.data_ptr(), batch, hp))
+        if log_every and (it % log_every == 0 or it == iters - 1):
+            print("iter %5d  loss %.5f  lr %.2e" % (it, losses[-1], hp.lr), flush=True)
+    return losses
+
+
+def rel_l2(a, b):
+    """sqrt(sum (a-b)^2 / sum b^2) per leading index (torch tensors)."""
+    d = ((a - b).double() ** 2).flatten(1).sum(1)
+    r = (b.double() ** 2).flatten(1).sum(1)
+    return (d / r.clamp_min(1e-300)).sqrt()
+
+
+def evaluate_one_call(sur, seed, nmem, side, spin_up, amp_scale=0.2):
+    """Relative SSH/u/v L2 errors after one 10-step surrogate call from the
+    FP64 state after spin_up steps, against the FP64 solver, for the
+    surrogate and for persistence (no change).  nmem <= the surrogate's
+    batch.  Returns dict of (nmem, 3) arrays."""
+    torch = _torch()
+    members = square_members(seed, nmem, side, amp_scale)
+    a = Ensemble(members, **COMMON)
+    b = Ensemble(members, **COMMON)
+    a.step_n(1, spin_up)
+    b.step_n(1, spin_up)
+    s0 = torch.empty((nmem, side, side, 4), dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    sur.pack_ens(a, s0.data_ptr())
+    sur.advance_ens(a, spin_up + 10)    # surrogate call
+    b.step_n(spin_up + 1, 10)           # FP64 solver
+    sur_err = ens_compare(a, b)
+    s1 = torch.empty_like(s0)
+    sur.pack_ens(b, s1.data_ptr())
+    torch.cuda.synchronize()
+    pers = torch.stack([rel_l2(s0[..., c], s1[..., c]) for c in range(3)], 1).cpu().numpy()
+    a.close()
+    b.close()
+    return {"surrogate": sur_err, "persistence": pers}

@@ -1,0 +1,313 @@
+"""tcgen05/TMA convolution kernels, the surrogate's training step and the
+hybrid controller against the CPU FP64 oracle (oracle/sur_oracle.py).
+
+Tolerances: BF16 outputs within 1 BF16 ulp of the oracle rounded to BF16
+(FP32 device accumulation vs FP64 can flip a rounding); FP32 outputs within
+1e-4 of the output's max-norm; whole-network gradients within 2e-2 normwise
+per layer (BF16 activations and gradients in both, FP32 vs FP64 sums).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+from oracle import sur_oracle as so
+
+
+@pytest.fixture(scope="module")
+def env():
+    import torch
+    import nemo_b200
+    from nemo_b200 import surrogate as sm
+    return torch, nemo_b200, sm
+
+
+def dev_bf16(torch, a):
+    bits = so.bf16_bits(a).view(np.int16)
+    return torch.from_numpy(bits.copy()).view(torch.bfloat16).cuda()
+
+
+def host_bf16(torch, t):
+    return so.from_bf16_bits(t.view(torch.int16).cpu().numpy().view(np.uint16))
+
+
+def ulp_close(got, ref):
+    """|got - ref| <= 1 BF16 ulp of ref (plus a tiny absolute floor)."""
+    tol = np.abs(ref) * 2.0 ** -7 + 1e-30
+    bad = np.abs(got - ref) > tol
+    return bad.mean(), np.abs(got - ref).max()
+
+
+def run_fwd(torch, sm, lib, x, w, bias=None, residual=None, mask=None, relu=False, out32=False):
+    N, H, W, _ = x.shape
+    xd, wd = dev_bf16(torch, x), dev_bf16(torch, w)
+    bd = torch.from_numpy(np.asarray(bias, np.float32)).cuda() if bias is not None else None
+    rd = dev_bf16(torch, residual) if residual is not None else None
+    md = dev_bf16(torch, mask) if mask is not None else None
+    out = torch.empty((N, H, W, 64), dtype=torch.bfloat16, device="cuda")
+    o32 = torch.empty((N, H, W, 4), dtype=torch.float32, device="cuda") if out32 else None
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    ptr = lambda t: t.data_ptr() if t is not None else None
+    sm.conv3x3_fwd(lib, xd.data_ptr(), wd.data_ptr(), N, H, W, err.data_ptr(), bias=ptr(bd),
+                   residual=ptr(rd), mask=ptr(md), relu=relu, out=out.data_ptr(), out32=ptr(o32),
+                   stream=torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    return host_bf16(torch, out), (o32.cpu().numpy().astype(np.float64) if out32 else None)
+
+
+@pytest.mark.parametrize("tap", range(9))
+def test_fwd_one_hot_tap_is_an_exact_shift(env, tap):
+    torch, nb, sm = env
+    rng = np.random.default_rng(tap)
+    x = so.bf16(rng.normal(size=(2, 5, 256, 64)))
+    w = np.zeros((9, 64, 64))
+    perm = rng.permutation(64)
+    w[tap][np.arange(64), perm] = 1.0  # out channel co reads input channel perm[co]
+    got, _ = run_fwd(torch, sm, nb.load(False), x, w)
+    ref = so.conv3x3(x, w)
+    np.testing.assert_array_equal(got, ref)
+
+
+@pytest.mark.parametrize("shape", [(2, 6, 128), (1, 3, 384), (3, 1, 256)])
+def test_fwd_random_matches_oracle(env, shape):
+    torch, nb, sm = env
+    N, H, W = shape
+    rng = np.random.default_rng(N * 100 + H)
+    x = so.bf16(rng.normal(size=(N, H, W, 64)))
+    w = so.bf16(rng.normal(0, 0.1, size=(9, 64, 64)))
+    b = rng.normal(size=64).astype(np.float32)
+    res = so.bf16(rng.normal(size=(N, H, W, 64)))
+    mask = so.bf16(rng.normal(size=(N, H, W, 64)))
+    lib = nb.load(False)
+    for kw in (dict(), dict(bias=b, relu=True), dict(bias=b, residual=res), dict(residual=res, mask=mask)):
+        got, o32 = run_fwd(torch, sm, lib, x, w, out32=True, **kw)
+        ref = so.epilogue(so.conv3x3(x, w), kw.get("bias"), kw.get("residual"), kw.get("mask"),
+                          kw.get("relu", False))
+        frac, _ = ulp_close(got, so.bf16(ref))
+        assert frac < 2e-3, (kw.keys(), frac)
+        assert np.abs(o32 - ref[..., :4]).max() <= 1e-4 * np.abs(ref[..., :4]).max()
+
+
+def test_dgrad_with_flipped_weights_matches_oracle(env):
+    torch, nb, sm = env
+    rng = np.random.default_rng(7)
+    dz = so.bf16(rng.normal(size=(2, 4, 128, 64)))
+    w = so.bf16(rng.normal(0, 0.1, size=(9, 64, 64)))
+    t = so.bf16(np.maximum(rng.normal(size=(2, 4, 128, 64)), 0))
+    got, o32 = run_fwd(torch, sm, nb.load(False), dz, so.flip_transpose(w), mask=t, out32=True)
+    ref = so.epilogue(so.conv3x3(dz, so.flip_transpose(w)), mask=t)
+    frac, _ = ulp_close(got, so.bf16(ref))
+    assert frac < 2e-3
+    assert np.abs(o32 - ref[..., :4]).max() <= 1e-4 * np.abs(ref[..., :4]).max()
+
+
+@pytest.mark.parametrize("shape,ctas", [((2, 5, 128), 0), ((1, 7, 192), 3), ((3, 2, 64), 1)])
+def test_wgrad_and_bias_grad_match_oracle(env, shape, ctas):
+    torch, nb, sm = env
+    N, H, W = shape
+    rng = np.random.default_rng(H * W)
+    x = so.bf16(rng.normal(size=(N, H, W, 64)))
+    dz = so.bf16(rng.normal(size=(N, H, W, 64)))
+    dw = torch.full((9, 64, 64), 0.5, dtype=torch.float32, device="cuda")  # accumulates
+    db = torch.full((64,), -1.0, dtype=torch.float32, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    xd, dzd = dev_bf16(torch, x), dev_bf16(torch, dz)  # referenced until the kernel is done
+    sm.conv3x3_wgrad(nb.load(False), xd.data_ptr(), dzd.data_ptr(), dw.data_ptr(), N, H, W,
+                     err.data_ptr(), db=db.data_ptr(), ctas=ctas,
+                     stream=torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    rw, rb = so.wgrad(x, dz)
+    gw = dw.cpu().numpy() - 0.5
+    gb = db.cpu().numpy() + 1.0
+    assert np.abs(gw - rw).max() <= 1e-4 * np.abs(rw).max()
+    assert np.abs(gb - rb).max() <= 1e-4 * np.abs(rb).max()
+
+
+def test_conv_rejects_unsupported_shapes(env):
+    """Widths the kernels do not tile are refused before any launch (the
+    buffers are sized for the request, so nothing could go out of bounds)."""
+    torch, nb, sm = env
+    lib = nb.load(False)
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    x = torch.zeros((1, 2, 96, 64), dtype=torch.bfloat16, device="cuda")
+    w = torch.zeros((9, 64, 64), dtype=torch.bfloat16, device="cuda")
+    out = torch.zeros_like(x)
+    dw = torch.zeros((9, 64, 64), dtype=torch.float32, device="cuda")
+    with pytest.raises(nb.NemoError):  # 96 is not a multiple of 128
+        sm.conv3x3_fwd(lib, x.data_ptr(), w.data_ptr(), 1, 2, 96, err.data_ptr(), out=out.data_ptr())
+    with pytest.raises(nb.NemoError):  # 96 is not a multiple of 64
+        sm.conv3x3_wgrad(lib, x.data_ptr(), x.data_ptr(), dw.data_ptr(), 1, 2, 96, err.data_ptr())
+    torch.cuda.synchronize()
+    assert not out.any() and not dw.any() and int(err.item()) == 0
+
+
+def random_setup(rng, torch, N, H, W):
+    snap0 = rng.normal(size=(N, H, W, 4)).astype(np.float32)
+    snap1 = (snap0 + rng.normal(0, 0.5, size=snap0.shape)).astype(np.float32)
+    tide = rng.normal(size=N).astype(np.float32)
+    norm = ([1.0, 2.0, 0.5, 1.5], [0.0, 0.1, 0.0, 0.2], [1.0, 0.8, 1.2])
+    d = [torch.from_numpy(a).cuda() for a in (snap0, snap1, tide)]
+    return snap0, snap1, tide, norm, d
+
+
+@pytest.mark.parametrize("nblocks", [1, 2])
+def test_network_loss_and_gradients_match_oracle(env, nblocks):
+    torch, nb, sm = env
+    N, H, W = 2, 6, 128
+    rng = np.random.default_rng(10 + nblocks)
+    s = sm.Surrogate(nblocks=nblocks, batch=N, height=H, width=W, seed=5)
+    p = s.params()
+    Wt, Bs = s.split(p)
+    Bs[:] = rng.normal(0, 0.05, size=Bs.shape)
+    Wt[-1, :, :3, :] = rng.normal(0, 0.05, size=Wt[-1, :, :3, :].shape)  # a larger output layer
+    s.set_params(p)
+    snap0, snap1, tide, norm, d = random_setup(rng, torch, N, H, W)
+    s.set_norm(*norm)
+    torch.cuda.synchronize()
+    loss = s.loss_grad(d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), N)
+    g = s.grads()
+    rloss, rg = so.loss_grad(p.astype(np.float64), nblocks, snap0, snap1, tide, norm, bf16_acts=True)
+    assert abs(loss - rloss) <= 1e-3 * rloss
+    gw, gb = s.split(g)
+    rw, rb = so.split_params(rg, nblocks)
+    for l in range(2 * nblocks + 2):
+        e_w = np.linalg.norm(gw[l] - rw[l]) / np.linalg.norm(rw[l])
+        e_b = np.linalg.norm(gb[l] - rb[l]) / np.linalg.norm(rb[l])
+        assert e_w < 2e-2 and e_b < 2e-2, (l, e_w, e_b)
+    # the padded input channels and unused output channels get no gradient
+    assert not gw[0][:, :, 6:].any()
+    assert not gw[-1][:, 3:, :].any()
+
+
+def test_adamw_matches_oracle(env):
+    torch, nb, sm = env
+    N, H, W = 1, 4, 128
+    rng = np.random.default_rng(3)
+    s = sm.Surrogate(nblocks=1, batch=N, height=H, width=W, seed=9)
+    snap0, snap1, tide, norm, d = random_setup(rng, torch, N, H, W)
+    s.set_norm(*norm)
+    p0 = s.params()
+    hp = sm.adamw(lr=3e-3, weight_decay=0.05)
+    s.loss_grad(d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), N)
+    g = s.grads()
+    s.adamw(hp)
+    p1 = s.params()
+    nw = s.nlayers * 9 * 64 * 64
+    z = np.zeros_like(p0)
+    rp, _, _ = so.adamw(p0, g, z, z, 1, 3e-3, 0.9, 0.999, 1e-8, 0.05, nw)
+    np.testing.assert_allclose(p1, rp, rtol=2e-6, atol=1e-8)
+    assert not s.grads().any()  # cleared for the next accumulation
+
+
+def test_predict_matches_oracle_forward(env):
+    torch, nb, sm = env
+    N, H, W = 2, 5, 128
+    rng = np.random.default_rng(4)
+    s = sm.Surrogate(nblocks=2, batch=N, height=H, width=W, train=False, seed=2)
+    p = s.params()
+    Wt, Bs = s.split(p)
+    Wt[-1, :, :3, :] = rng.normal(0, 0.05, size=Wt[-1, :, :3, :].shape)
+    s.set_params(p)
+    snap0, _, tide, norm, d = random_setup(rng, torch, N, H, W)
+    s.set_norm(*norm)
+    out = torch.empty((N, H, W, 4), dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    s.predict(d[0].data_ptr(), d[2].data_ptr(), N, out.data_ptr())
+    Wr, Br = so.split_params(p.astype(np.float64), 2)
+    x0 = so.make_input(snap0, tide, norm[0], norm[1]).astype(np.float64)
+    y, _ = so.forward(x0, Wr, Br, 2, bf16_acts=True)
+    got = out.cpu().numpy()
+    assert np.abs(got[..., :3] - y[..., :3]).max() <= 2e-2 * np.abs(y[..., :3]).max()
+
+
+def small_ensemble(nb, seed, n, side):
+    from nemo_b200 import train as tr
+    return nb.Ensemble(tr.square_members(seed, n, side, 0.2), **tr.COMMON)
+
+
+def test_pack_and_advance_follow_the_grid_layout(env):
+    torch, nb, sm = env
+    side, n = 128, 3
+    e = small_ensemble(nb, 21, n, side)
+    e.step_n(1, 60)
+    s = sm.Surrogate(nblocks=1, batch=n, height=side, width=side, train=False, seed=3)
+    snap = torch.empty((n, side, side, 4), dtype=torch.float32, device="cuda")
+    s.pack_ens(e, snap.data_ptr())
+    sn = snap.cpu().numpy()
+    before = [[e.field(m, f) for f in (nb.SSHN, nb.UN, nb.VN, nb.HT)] for m in range(n)]
+    for m in range(n):
+        ssh, u, v, ht = before[m]
+        np.testing.assert_array_equal(sn[m, ..., 0], ssh.astype(np.float32))
+        np.testing.assert_array_equal(sn[m, ..., 1], u[:, :side].astype(np.float32))
+        np.testing.assert_array_equal(sn[m, ..., 2], v[:side, :].astype(np.float32))
+        np.testing.assert_array_equal(sn[m, ..., 3], ht.astype(np.float32))
+    # one surrogate call: compare with predict's deltas
+    from nemo_b200 import train as tr
+    out = torch.empty_like(snap)
+    tide = torch.tensor([tr.tide_of(mb, 70) for mb in e.members], dtype=torch.float32).cuda()
+    torch.cuda.synchronize()
+    s.predict(snap.data_ptr(), tide.data_ptr(), n, out.data_ptr())
+    o = out.cpu().numpy()
+    s.advance_ens(e, 70)
+    _, _, osc = s.get_norm()
+    for m in range(n):
+        ssh0, u0, v0, _ = before[m]
+        ssh, u, v = (e.field(m, f) for f in (nb.SSHN, nb.UN, nb.VN))
+        exp = ssh0 + (o[m, ..., 0] / osc[0]).astype(np.float64)
+        exp[0, :] = tr.tide_of(e.members[m], 70)
+        np.testing.assert_allclose(ssh, exp, rtol=1e-12, atol=0)
+        assert not u[:, 0].any() and not u[:, side].any() and not v[side, :].any()
+        np.testing.assert_allclose(u[:, 1:side], u0[:, 1:side] + (o[m, :, 1:, 1] / osc[1]), rtol=1e-12)
+        np.testing.assert_allclose(v[:side, :], v0[:side, :] + (o[m, ..., 2] / osc[2]), rtol=1e-12)
+
+
+def test_hybrid_with_zero_tolerance_reproduces_the_solver_bitwise(env):
+    torch, nb, sm = env
+    side, n = 128, 2
+    a = small_ensemble(nb, 31, n, side)
+    b = small_ensemble(nb, 31, n, side)
+    s = sm.Surrogate(nblocks=1, batch=n, height=side, width=side, train=False, seed=4)
+    st = sm.hyb_run(s, a, 0, 300, tol=1e-300)  # every window falls back
+    b.step_n(1, 300)
+    assert st["fallbacks"] == 3 and st["solver_steps"] == 300 and st["sur_steps"] == 0
+    for m in range(n):
+        for f in (nb.SSHN, nb.UN, nb.VN):
+            np.testing.assert_array_equal(a.field(m, f), b.field(m, f))
+    assert np.all(sm.ens_compare(a, b) == 0.0)
+
+
+def test_hybrid_accepts_surrogate_windows_and_reports_errors(env):
+    torch, nb, sm = env
+    side, n = 128, 2
+    a = small_ensemble(nb, 41, n, side)
+    b = small_ensemble(nb, 41, n, side)
+    s = sm.Surrogate(nblocks=1, batch=1, height=side, width=side, train=False, seed=4)  # 2 chunks
+    st = sm.hyb_run(s, a, 0, 200, k=10, anchor=100, tol=1e300)  # never falls back
+    b.step_n(1, 200)
+    assert st["fallbacks"] == 0 and st["sur_steps"] == 180 and st["solver_steps"] == 20
+    assert st["sur_calls"] == 20 and st["max_shadow_err"] > 0
+    err = sm.ens_compare(a, b)
+    assert err.shape == (n, 3) and np.all(np.isfinite(err)) and np.all(err > 0)
+
+
+def test_training_beats_persistence_on_held_out_runs(env):
+    """The trained surrogate's one-call SSH error on unseen members is well
+    below the error of the method without it (no change over 10 steps)."""
+    torch, nb, sm = env
+    from nemo_b200 import train as tr
+    side = 128
+    s = sm.Surrogate(nblocks=2, batch=16, height=side, width=side, seed=11)
+    snaps, tides = tr.generate_runs(s, seed=100, nmem=16, side=side, steps=400)
+    s.set_norm(*tr.compute_norm(snaps))
+    before = tr.evaluate_one_call(s, seed=900, nmem=8, side=side, spin_up=250)
+    losses = tr.train(s, tr.PairSampler(snaps, tides, seed=1), iters=400, batch=16, lr=2e-3)
+    after = tr.evaluate_one_call(s, seed=900, nmem=8, side=side, spin_up=250)
+    assert np.mean(losses[-20:]) < 0.2 * np.mean(losses[:5])
+    pers = after["persistence"][:, 0].mean()
+    trained = after["surrogate"][:, 0].mean()
+    untrained = before["surrogate"][:, 0].mean()
+    print("ssh rel err: persistence %.4f untrained %.4f trained %.4f" % (pers, untrained, trained))
+    assert trained < 0.5 * pers
+    assert trained < untrained
