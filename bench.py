@@ -56,8 +56,10 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--schedule", type=str, default="",
                     help="warps,occupancy,rows of the fused kernel (default: tuned)")
-    ap.add_argument("--workload", choices=["grid", "ensemble"], default="grid",
+    ap.add_argument("--workload", choices=["grid", "ensemble", "surrogate", "hybrid"], default="grid",
                     help="grid: the 4096^2 line (default); ensemble: the 256-member batch")
+    ap.add_argument("--hyb-steps", type=int, default=5000)
+    ap.add_argument("--train-iters", type=int, default=600)
     ap.add_argument("--n", type=int, default=N,
                     help="grid side (profiling of smaller cases only; the bench line is 4096)")
     return ap.parse_args()
@@ -260,12 +262,216 @@ def run_ensemble(args):
     e.close()
 
 
+def conv_kernel_rates(sur_mod, lib, n, h, w, reps, stream):
+    """Device time of one 3x3 conv forward (bias+ReLU epilogue) and one weight
+    gradient over n x h x w pixels (64 -> 64 channels), inputs larger than L2."""
+    import torch
+    x = torch.randn((n, h, w, 64), device="cuda").to(torch.bfloat16)
+    y = torch.empty_like(x)
+    wt = (0.05 * torch.randn((9, 64, 64), device="cuda")).to(torch.bfloat16)
+    b = torch.zeros(64, device="cuda")
+    dw = torch.zeros((9, 64, 64), device="cuda")
+    db = torch.zeros(64, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    out = {}
+    for name in ("fwd", "wgrad"):
+        def launch():
+            if name == "fwd":
+                sur_mod.conv3x3_fwd(lib, x.data_ptr(), wt.data_ptr(), n, h, w, err.data_ptr(),
+                                    bias=b.data_ptr(), relu=True, out=y.data_ptr(), stream=stream)
+            else:
+                sur_mod.conv3x3_wgrad(lib, x.data_ptr(), y.data_ptr(), dw.data_ptr(), n, h, w,
+                                      err.data_ptr(), db=db.data_ptr(), stream=stream)
+        for _ in range(3):
+            launch()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        s = torch.cuda.ExternalStream(stream)
+        e0.record(s)
+        for _ in range(reps):
+            launch()
+        e1.record(s)
+        torch.cuda.synchronize()
+        out[name] = e0.elapsed_time(e1) / reps / 1e3
+    assert int(err.item()) == 0
+    return out
+
+
+def run_surrogate(args):
+    """Surrogate training on solver-generated data: 64 seeded 256x256 runs of
+    the batched recipe (500 steps from rest, FP32 snapshots every 10 steps),
+    the 8-block 64-channel residual CNN, batch 64, AdamW.  One bench step =
+    one training iteration (forward, loss, backward, AdamW).  Also times the
+    forward and weight-gradient conv kernels alone at the same batch."""
+    import numpy as np
+    import torch
+    import nemo_b200
+    from nemo_b200 import surrogate as sm
+    from nemo_b200 import train as tr
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    B, S = 64, 256
+    sur = sm.Surrogate(nblocks=8, batch=B, height=S, width=S, seed=1234, stream=stream.cuda_stream,
+                       device=0)
+    nparams, flops_px = sur.info()
+    with torch.cuda.stream(stream):
+        snaps, tides = tr.generate_runs(sur, seed=7000, nmem=B, side=S, steps=500)
+        sur.set_norm(*tr.compute_norm(snaps))
+        sampler = tr.PairSampler(snaps, tides, seed=3)
+        hp = sm.adamw(lr=1e-3, weight_decay=1e-4)
+        losses = []
+        for _ in range(args.warmup):
+            s0, s1, t1 = sampler.batch(B)
+            losses.append(sur.train_step(s0.data_ptr(), s1.data_ptr(), t1.data_ptr(), B, hp))
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        clocks = ClockSampler(0)
+        clocks.start()
+        e0.record(stream)
+        for _ in range(args.steps):
+            s0, s1, t1 = sampler.batch(B)
+            losses.append(sur.train_step(s0.data_ptr(), s1.data_ptr(), t1.data_ptr(), B, hp))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        clk = clocks.stop()
+        ms = e0.elapsed_time(e1) / args.steps
+        del snaps, tides, sampler
+        rates = conv_kernel_rates(sm, nemo_b200.load(False), B, S, S, 20, stream.cuda_stream)
+    npix = B * S * S
+    conv_flop = 2 * 9 * 64 * 64 * npix
+    L = 2 * 8 + 2
+    # forward L convs, data gradient L-1 (none for the input), weight gradient L
+    iter_flop = conv_flop * (L + (L - 1) + L)
+    peak = load_peaks_tensor()
+    fwd_tf = conv_flop / rates["fwd"] / 1e12
+    line = {"metric": "surrogate training samples/s (8-block 64-ch BF16 residual CNN, 256^2, batch 64)",
+            "value": B / (ms / 1e3), "unit": "samples/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "bf16", "data": "synthetic (solver-generated)",
+            "config": {"workload": "surrogate training: 64 seeded 256x256 runs, 500 steps, FP32 "
+                                   "snapshots every 10 steps; batch 64; AdamW",
+                       "params": nparams, "conv_flop_per_iter": iter_flop,
+                       "runs_dropped_unbounded": tr.generate_runs.dropped,
+                       "l2": "activations 512 MiB per tensor, larger than L2"},
+            "train_tflops": iter_flop / (ms / 1e3) / 1e12,
+            "roofline": {"bound": "tensor", "kernel": "k_conv_fwd", "achieved": fwd_tf,
+                         "peak": peak[0], "unit": "TFLOP/s", "frac": fwd_tf / peak[0],
+                         "peak_source": peak[1], "traffic": None,
+                         "wgrad_tflops": conv_flop / rates["wgrad"] / 1e12,
+                         "fwd_us": rates["fwd"] * 1e6, "wgrad_us": rates["wgrad"] * 1e6},
+            "loss_first": losses[0], "loss_last": losses[-1],
+            "gpu_launches": args.steps * (2 * L + L - 1 + 6), "clocks": clk}
+    print(json.dumps(line), flush=True)
+    sur.close()
+
+
+def load_peaks_tensor():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return float(json.load(fh)["bf16_tflops"]), "measured (burst)"
+    except (OSError, KeyError, ValueError):
+        return 1590.0, "fallback"
+
+
+def run_hybrid(args):
+    """Hybrid inference versus the plain solver: 32 members at 2048x2048
+    (seeded bathymetry and tides of the batched recipe), 5000 steps.  The
+    surrogate (trained first on 256x256 runs) advances 10 steps per call; the
+    FP64 solver re-anchors every 100 steps and takes the window over when the
+    shadow SSH error exceeds 1%.  Reports both rates and the hybrid's error
+    against the plain FP64 run (which matches the FP64 oracle to 1e-12)."""
+    import numpy as np
+    import torch
+    from nemo_b200 import surrogate as sm
+    from nemo_b200 import train as tr
+    import nemo_b200
+    torch.cuda.set_device(0)
+    nsteps = args.hyb_steps
+    side, nm = 2048, 32
+    # ---- train on the 256x256 recipe
+    trainer = sm.Surrogate(nblocks=8, batch=64, height=256, width=256, seed=1234, device=0)
+    snaps, tides = tr.generate_runs(trainer, seed=7000, nmem=64, side=256, steps=500)
+    norm = tr.compute_norm(snaps)
+    trainer.set_norm(*norm)
+    t_train = time.time()
+    losses = tr.train(trainer, tr.PairSampler(snaps, tides, seed=3), iters=args.train_iters,
+                      batch=64, lr=1e-3)
+    t_train = time.time() - t_train
+    params = trainer.params()
+    trainer.close()
+    del snaps, tides
+    torch.cuda.empty_cache()
+    # ---- members: 40 seeded candidates screened by the FP64 solver over the
+    # run (the reference scheme lets a tide that starts rising grow without
+    # bound at the east-wall/open-boundary corner); the first 32 that stay
+    # finite are the workload
+    stream = torch.cuda.Stream()
+    common = dict(tr.COMMON, stream=stream.cuda_stream, device=0)
+    cands = tr.square_members(4242, 40, side, 0.2)
+    scr = nemo_b200.Ensemble(cands, **common)
+    scr.step_n(1, nsteps)
+    ck = scr.checksums()
+    scr.close()
+    ok = [i for i in range(len(cands)) if np.isfinite(ck[i]).all()]
+    members = [cands[i] for i in ok[:nm]]
+    nm = len(members)
+    plain = nemo_b200.Ensemble(members, **common)
+    hyb = nemo_b200.Ensemble(members, **common)
+    inf = sm.Surrogate(nblocks=8, batch=16, height=side, width=side, train=False, seed=1,
+                       stream=stream.cuda_stream, device=0)
+    inf.set_params(params)
+    inf.set_norm(*norm)
+    cells = nm * side * side
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    torch.cuda.synchronize()
+    ev[0].record(stream)
+    plain.step_n(1, nsteps)
+    ev[1].record(stream)
+    plain.checksums()
+    torch.cuda.synchronize()
+    t_plain = ev[0].elapsed_time(ev[1]) / 1e3
+    clocks = ClockSampler(0)
+    clocks.start()
+    ev[2].record(stream)
+    st = sm.hyb_run(inf, hyb, 0, nsteps, k=10, anchor=100, tol=0.01)
+    ev[3].record(stream)
+    torch.cuda.synchronize()
+    t_hyb = ev[2].elapsed_time(ev[3]) / 1e3
+    clk = clocks.stop()
+    err = sm.ens_compare(hyb, plain)
+    v_plain = cells * nsteps / t_plain
+    v_hyb = cells * nsteps / t_hyb
+    line = {"metric": "hybrid vs plain ensemble cell-steps/s (32 x 2048^2, 5000 steps, <=1% SSH err)",
+            "value": v_hyb, "unit": "cell-steps/s", "n_gpus": 1, "steps": 1, "warmup": 0,
+            "ms_per_step": t_hyb * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "bf16+f64", "data": "synthetic",
+            "config": {"workload": "%d members 2048x2048, %d steps, surrogate k=10, re-anchor 100, "
+                                   "tol 1%% relative SSH L2 vs shadow FP64 step" % (nm, nsteps),
+                       "candidates": len(cands), "screened_out": len(cands) - len(ok),
+                       "train_iters": args.train_iters, "train_s": t_train,
+                       "train_runs_dropped": tr.generate_runs.dropped},
+            "plain_value": v_plain, "hybrid_over_plain": v_hyb / v_plain,
+            "hybrid_stats": st,
+            "err_vs_fp64": {"ssh_max": float(err[:, 0].max()), "ssh_mean": float(err[:, 0].mean()),
+                            "u_max": float(err[:, 1].max()), "v_max": float(err[:, 2].max()),
+                            "u_mean": float(err[:, 1].mean()), "v_mean": float(err[:, 2].mean())},
+            "loss_first": losses[0], "loss_last": losses[-1], "clocks": clk,
+            "gpu_launches": None}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.workload == "ensemble":
         import numpy as np  # noqa: F401
         globals()["np"] = np
         return run_ensemble(args)
+    if args.workload == "surrogate":
+        return run_surrogate(args)
+    if args.workload == "hybrid":
+        return run_hybrid(args)
     if args.n != N:
         WORKLOAD["jpi"] = WORKLOAD["jpj"] = args.n
         CONFIG["grid"] = [args.n, args.n]

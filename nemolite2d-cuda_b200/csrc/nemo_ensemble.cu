@@ -411,7 +411,10 @@ int nemo_ens_create(const nemo_params* common, const nemo_member* members, int n
         tab_cap = nax + ngy;
       }
       if (err == cudaSuccess)
-        err = cudaMemcpy(tab, h.data(), (nax + ngy) * sizeof(double), cudaMemcpyHostToDevice);
+        // stream-ordered: a pageable cudaMemcpy on the legacy stream may return
+        // before its DMA lands and is not ordered with a non-blocking stream
+        err = cudaMemcpyAsync(tab, h.data(), (nax + ngy) * sizeof(double), cudaMemcpyHostToDevice,
+                              e->stream);
       if (err == cudaSuccess)
         err = launch_depth(d.L, p.dep_const, p.nbump, tab, tab + nax, p.hmin, p.hmax, ht, hu, hv, e->stream);
       if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
@@ -438,13 +441,13 @@ int nemo_ens_create(const nemo_params* common, const nemo_member* members, int n
   if (err == cudaSuccess) err = cudaMallocHost(&e->h_ck, 3 * nm * sizeof(double));
   if (err == cudaSuccess) err = cudaEventCreateWithFlags(&e->tide_ev, cudaEventDisableTiming);
   if (err == cudaSuccess)
-    err = cudaMemcpy(e->d_mem, e->hmem.data(), nm * sizeof(MemberDev), cudaMemcpyHostToDevice);
+    err = cudaMemcpyAsync(e->d_mem, e->hmem.data(), nm * sizeof(MemberDev), cudaMemcpyHostToDevice, e->stream);
   if (err == cudaSuccess)
-    err = cudaMemcpy(e->d_rows, rows.data(), rows.size() * sizeof(int2), cudaMemcpyHostToDevice);
+    err = cudaMemcpyAsync(e->d_rows, rows.data(), rows.size() * sizeof(int2), cudaMemcpyHostToDevice, e->stream);
   if (err == cudaSuccess)
-    err = cudaMemcpy(e->d_row_off, row_off.data(), nm * sizeof(int), cudaMemcpyHostToDevice);
+    err = cudaMemcpyAsync(e->d_row_off, row_off.data(), nm * sizeof(int), cudaMemcpyHostToDevice, e->stream);
   if (err == cudaSuccess)
-    err = cudaMemcpy(e->d_row_cnt, row_cnt.data(), nm * sizeof(int), cudaMemcpyHostToDevice);
+    err = cudaMemcpyAsync(e->d_row_cnt, row_cnt.data(), nm * sizeof(int), cudaMemcpyHostToDevice, e->stream);
   if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
   if (err != cudaSuccess) { cudaGetLastError(); nemo_ens_destroy(e); return status_of(err); }
   st = build_work(e);

@@ -829,17 +829,20 @@ int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, 
       ce = cudaMemcpyAsync(acc.data(), s->d_acc, 6 * nm * sizeof(double), cudaMemcpyDeviceToHost, s->stream);
     if (ce != cudaSuccess) { rc = status_of(ce); break; }
     if ((rc = check_err(s)) != NEMO_OK) break;
+    // a non-finite error (a member whose state blew up) counts as a failure
     double worst = 0.0;
+    bool fail = false;
     for (int m = 0; m < nm; ++m) {
       const double r = acc[6 * m + 1] > 0 ? sqrt(acc[6 * m] / acc[6 * m + 1]) : sqrt(acc[6 * m]);
-      if (r > worst) worst = r;
+      if (!(r <= c->tol)) fail = true;
+      if (!(r <= worst)) worst = r;  // NaN propagates
     }
     st.last_shadow_err = worst;
-    if (worst > st.max_shadow_err) st.max_shadow_err = worst;
+    if (!(worst <= st.max_shadow_err)) st.max_shadow_err = worst;
     st.solver_steps += c->k;
     st.sur_calls += 1;
     istp += c->k;
-    if (worst > c->tol) {  // fallback: the solver runs the rest of the window
+    if (fail) {  // fallback: the solver runs the rest of the window
       st.fallbacks += 1;
       rc = nemo_ens_step_n(e, istp + 1, c->anchor - c->k);
       st.solver_steps += c->anchor - c->k;

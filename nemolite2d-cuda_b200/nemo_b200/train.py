@@ -36,10 +36,15 @@ def tide_of(member, istp, rdt=20.0):
     return member.amp_tide * math.sin(omega * (istp * rdt) + member.tide_phase)
 
 
-def generate_runs(sur, seed, nmem, side, steps, every=10, amp_scale=0.2, strict=False):
-    """Runs nmem members from rest for `steps` steps; returns (snaps, tides):
-    snaps [steps//every + 1][nmem][side][side][4] float32 on the device and
-    tides [same][nmem] float32 (the boundary SSH at each snapshot's step)."""
+def generate_runs(sur, seed, nmem, side, steps, every=10, amp_scale=0.2, strict=False,
+                  bound=2.5):
+    """Runs nmem members from rest for `steps` steps and returns (snaps, tides)
+    of the members whose run stays bounded (finite, max |ssh| <= bound x the
+    member's tidal amplitude; the reference scheme lets a tide that starts
+    rising grow at the corner of the east wall and the open boundary):
+    snaps [steps//every + 1][kept][side][side][4] float32 on the device,
+    tides [same][kept] float32 (the boundary SSH at each snapshot's step).
+    The number of members dropped is in generate_runs.dropped."""
     torch = _torch()
     members = square_members(seed, nmem, side, amp_scale)
     ens = Ensemble(members, strict=strict, **COMMON)
@@ -55,7 +60,19 @@ def generate_runs(sur, seed, nmem, side, steps, every=10, amp_scale=0.2, strict=
         sur.pack_ens(ens, snaps[k].data_ptr())
         tides[k] = torch.tensor([tide_of(m, istp) for m in members], dtype=torch.float32)
     ens.close()
-    return snaps, tides.cuda()
+    amp = torch.tensor([m.amp_tide for m in members], dtype=torch.float32, device="cuda")
+    ssh = snaps[..., 0]
+    finite = torch.isfinite(snaps).flatten(2).all(2).all(0)
+    peak = torch.nan_to_num(ssh.abs(), nan=float("inf")).flatten(2).amax(2).amax(0)
+    keep = (finite & (peak <= bound * amp)).nonzero().flatten()
+    generate_runs.dropped = nmem - int(keep.numel())
+    snaps = snaps.index_select(1, keep)
+    tides = tides.cuda().index_select(1, keep)
+    torch.cuda.synchronize()
+    return snaps, tides
+
+
+generate_runs.dropped = 0
 
 
 def compute_norm(snaps):

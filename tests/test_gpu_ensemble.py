@@ -143,3 +143,21 @@ def test_ensemble_rejects_bad_members(nb):
     assert e.lib.nemo_ens_retrieve(e.h, 5, nb.SSHN, nb._dptr(out), 4) == 1  # no member 5
     with pytest.raises(IndexError):
         e.field(5, nb.SSHN)
+
+
+def test_ensembles_sharing_an_external_stream_are_independent(nb):
+    """Creating and stepping several ensembles on one caller-owned stream
+    gives each the same fields as an ensemble on its own stream (creation
+    uploads are ordered on the ensemble's stream)."""
+    import torch
+    s = torch.cuda.Stream()
+    members = nb.generate_members(17, 3, side_min=300, side_max=520, amp_scale=0.2)
+    ref = nb.Ensemble(members, **COMMON)
+    ref.step_n(1, 30)
+    shared = [nb.Ensemble(members, stream=s.cuda_stream, device=0, **COMMON) for _ in range(3)]
+    for e in shared:
+        e.step_n(1, 30)  # queued back to back, no host sync in between
+    for e in shared:
+        for k in range(len(members)):
+            for fid in (nb.HT, nb.HU, nb.HV, nb.SSHN, nb.UN, nb.VN):
+                np.testing.assert_array_equal(bits(e.field(k, fid)), bits(ref.field(k, fid)))
