@@ -27,6 +27,7 @@ struct nemo_ctx {
   StateSet set[2];
   int n_idx;              // set[n_idx] holds sshn/un/vn, set[1-n_idx] ssha/ua/va
   double *sshn_u, *sshn_v, *ht, *hu, *hv;
+  double *rhu, *rhv;      // RN(1/hu), RN(1/hv) for the fused step
   double* ck_partials;    // 4*jpj
   double* ck_out;         // 4
   double* ck_host;        // pinned, 4
@@ -311,7 +312,7 @@ int nemo_create(const nemo_params* p, nemo_ctx** out) {
   c->L.rows = (long)p->jpj + 3;
   c->C = make_consts(*p);
   c->sched.warps = 2;
-  c->sched.occupancy = -24;
+  c->sched.occupancy = -20;
   c->sched.rows = 16;
   int st = set_device(c);
   if (st) { delete c; return st; }
@@ -326,7 +327,7 @@ int nemo_create(const nemo_params* p, nemo_ctx** out) {
   }
   const size_t fe = (size_t)c->L.elems();
   const size_t ck = 4 * (size_t)p->jpj + 4;
-  const size_t total = 11 * fe + ck;
+  const size_t total = 13 * fe + ck;
   e = cudaMalloc(&c->slab, total * sizeof(double));
   if (e != cudaSuccess) { c->slab = nullptr; nemo_destroy(c); cudaGetLastError(); return NEMO_ERR_ALLOC; }
   e = cudaMallocHost(&c->ck_host, 4 * sizeof(double));
@@ -342,6 +343,8 @@ int nemo_create(const nemo_params* p, nemo_ctx** out) {
   c->ht = q; q += fe;
   c->hu = q; q += fe;
   c->hv = q; q += fe;
+  c->rhu = q; q += fe;
+  c->rhv = q; q += fe;
   c->ck_partials = q; q += 4 * (size_t)p->jpj;
   c->ck_out = q;
   c->n_idx = 0;
@@ -367,6 +370,7 @@ int nemo_create(const nemo_params* p, nemo_ctx** out) {
   } else {
     e = launch_depth(c->L, p->dep_const, 0, nullptr, nullptr, p->hmin, p->hmax, c->ht, c->hu, c->hv, c->stream);
   }
+  if (e == cudaSuccess) e = launch_recip(c->L, c->hu, c->hv, c->rhu, c->rhv, c->stream);
   // initialisation (:331-365): sshn = un = vn = 0, sshn_u/sshn_v averaged
   if (e == cudaSuccess)
     e = launch_init_sshn_uv(c->L, c->C, nset(c).ssh, c->sshn_u, c->sshn_v, c->stream);
@@ -488,6 +492,8 @@ int nemo_step_n(nemo_ctx* c, int istp0, int n) {
     a.ht = c->ht;
     a.hu = c->hu;
     a.hv = c->hv;
+    a.rhu = c->rhu;
+    a.rhv = c->rhv;
     a.sshv0 = c->sshn_v;
     a.ssha = aset(c).ssh;
     a.ua = aset(c).u;

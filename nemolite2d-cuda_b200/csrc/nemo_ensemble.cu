@@ -33,6 +33,7 @@ struct MemberDev {
   Layout L;
   double* st[2][3];  // [set][sshn, un, vn]
   const double *ht, *hu, *hv, *sshv0;
+  const double *rhu, *rhv;
 };
 
 template <int NW, int MB, int PF>
@@ -54,6 +55,8 @@ k_ens_step(const MemberDev* __restrict__ mem, const int4* __restrict__ work, int
     A.ht = M->ht;
     A.hu = M->hu;
     A.hv = M->hv;
+    A.rhu = M->rhu;
+    A.rhv = M->rhv;
     A.sshv0 = M->sshv0;
     A.tide = tide[it.x];
     const Layout L = M->L;
@@ -355,7 +358,7 @@ int nemo_ens_create(const nemo_params* common, const nemo_member* members, int n
     if (err != cudaSuccess) { delete e; return status_of(err); }
     e->own_stream = true;
   }
-  // storage: 11 fields per member in one slab
+  // storage: 13 fields per member in one slab
   std::vector<size_t> off(nmem);
   size_t total = 0;
   e->hmem.resize(nmem);
@@ -367,7 +370,7 @@ int nemo_ens_create(const nemo_params* common, const nemo_member* members, int n
     L.rows = (long)L.jpj + 3;
     e->hmem[m].L = L;
     off[m] = total;
-    total += 11 * (size_t)L.elems();
+    total += 13 * (size_t)L.elems();
     e->cells += (long long)L.jpi * L.jpj;
     e->nrows += L.jpj;
   }
@@ -391,7 +394,10 @@ int nemo_ens_create(const nemo_params* common, const nemo_member* members, int n
     double* ht = q; q += fe;
     double* hu = q; q += fe;
     double* hv = q; q += fe;
+    double* rhu = q; q += fe;
+    double* rhv = q; q += fe;
     d.ht = ht; d.hu = hu; d.hv = hv; d.sshv0 = sshn_v;
+    d.rhu = rhu; d.rhv = rhv;
     // grid: seeded bathymetry of the member
     nemo_params p = *common;
     p.jpi = d.L.jpi; p.jpj = d.L.jpj;
@@ -421,6 +427,7 @@ int nemo_ens_create(const nemo_params* common, const nemo_member* members, int n
     } else {
       err = launch_depth(d.L, p.dep_const, 0, nullptr, nullptr, p.hmin, p.hmax, ht, hu, hv, e->stream);
     }
+    if (err == cudaSuccess) err = launch_recip(d.L, hu, hv, rhu, rhv, e->stream);
     if (err == cudaSuccess) {
       Consts C = make_consts(p);
       err = launch_init_sshn_uv(d.L, C, d.st[0][0], sshn_u, sshn_v, e->stream);

@@ -23,6 +23,9 @@ struct RoutinePtrs {
 cudaError_t launch_depth(const Layout& L, double dep_const, int nbump, const double* ax,
                          const double* gy, double hmin, double hmax, double* ht,
                          double* hu, double* hv, cudaStream_t s);
+// rhu = RN(1/hu), rhv = RN(1/hv) over the whole storage (0 where the depth is 0).
+cudaError_t launch_recip(const Layout& L, const double* hu, const double* hv, double* rhu, double* rhv,
+                         cudaStream_t s);
 cudaError_t launch_init_sshn_uv(const Layout& L, const Consts& C, const double* sshn,
                                 double* sshn_u, double* sshn_v, cudaStream_t s);
 cudaError_t launch_continuity(const Layout& L, const Consts& C, const RoutinePtrs& p,
@@ -42,6 +45,7 @@ cudaError_t launch_derive_sshn_uv(const Layout& L, const Consts& C, const double
 
 struct FusedArgs {
   const double *sshn, *un, *vn, *ht, *hu, *hv;
+  const double *rhu, *rhv;  // RN(1/hu), RN(1/hv): divisors of the u and v updates
   const double* sshv0;  // stored sshn_v array (only its row jj=0 is read)
   double *ssha, *ua, *va;
   double tide;          // clamped SSH value for this step

@@ -328,6 +328,24 @@ cudaError_t launch_depth(const Layout& L, double dep_const, int nbump, const dou
   return cudaGetLastError();
 }
 
+__global__ void k_recip(long n, const double* __restrict__ hu, const double* __restrict__ hv,
+                        double* __restrict__ rhu, double* __restrict__ rhv) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const double a = hu[i] + 0.0, b = hv[i] + 0.0;
+    rhu[i] = a != 0.0 ? 1.0 / a : 0.0;
+    rhv[i] = b != 0.0 ? 1.0 / b : 0.0;
+  }
+}
+
+cudaError_t launch_recip(const Layout& L, const double* hu, const double* hv, double* rhu, double* rhv,
+                         cudaStream_t s) {
+  const long n = L.elems();
+  long g = (n + 255) / 256;
+  if (g > 4096) g = 4096;
+  k_recip<<<(unsigned)g, 256, 0, s>>>(n, hu, hv, rhu, rhv);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_init_sshn_uv(const Layout& L, const Consts& C, const double* sshn,
                                 double* sshn_u, double* sshn_v, cudaStream_t s) {
   k_init_sshn_uv<<<grid_for(L.jpi + 1, L.jpj + 1), dim3(BX, BY), 0, s>>>(L, C, sshn, sshn_u, sshn_v);

@@ -81,10 +81,11 @@ struct RowOut {
 // EDGE = false is the interior form: the caller guarantees that no lane of
 // the warp sits on column 0, 1 or jpi and that j is neither 1 nor jpj, so
 // every mask of the reference geometry is inactive.
+// rhu, rhv: RN(1/hu), RN(1/hv) at (c, j).
 template <bool SAFE, bool EDGE>
 __device__ __forceinline__ void row(const Consts& C, int c, int j, int jpi, int jpj, double tide,
-                                    const Cell& cur, const Cell& nx, const Carry& k, RowOut& o,
-                                    bool& bad) {
+                                    const Cell& cur, const Cell& nx, const Carry& k, double rhu,
+                                    double rhv, RowOut& o, bool& bad) {
   const bool south = EDGE && (j == 1), north = EDGE && (j == jpj);
   const bool west0 = EDGE && (c == 0), west1 = EDGE && (c == 1), east = EDGE && (c == jpi);
   // sshn_v at (c, j), sshn_u at (c, j+1)
@@ -144,7 +145,7 @@ __device__ __forceinline__ void row(const Consts& C, int c, int j, int jpi, int 
     const double cor = 0.5 * (C.fcor * (k.vnc_s + vnc)) * C.e12u * k.Hu;
     const double hpg = -(C.g * k.Hu * C.e2u * (k.s_e - cur.s));
     const double num = cur.u * k.Hu + qdiv<SAFE>(C.rdt * (adv + vis + cor + hpg), C.e12u, C.r_e12u, bad);
-    const double q = num / (cur.hu + 0.0);
+    const double q = qdiv<SAFE>(num, cur.hu + 0.0, rhu, bad);
     o.ua = east ? 0.0 : qdiv<SAFE>(q, C.cfric, C.r_cfric, bad);
   }
   // v equation (:527-606); v(c,jpj) is the north wall (:658)
@@ -162,7 +163,7 @@ __device__ __forceinline__ void row(const Consts& C, int c, int j, int jpi, int 
     const double cor = -(0.5 * (C.fcor * (uec + uec_w)) * C.e12v * Hv);
     const double hpg = -(C.g * Hv * C.e1v * (nx.s - cur.s));
     const double num = cur.v * Hv + qdiv<SAFE>(C.rdt * (adv + vis + cor + hpg), C.e12v, C.r_e12v, bad);
-    const double q = num / (cur.hv + 0.0);
+    const double q = qdiv<SAFE>(num, cur.hv + 0.0, rhv, bad);
     o.va = north ? 0.0 : qdiv<SAFE>(q, C.cfric, C.r_cfric, bad);
   }
   o.sv = sv;
@@ -244,6 +245,7 @@ __device__ __forceinline__ void run_strip(const Layout& L, const Consts& C, cons
   long o_ld = L.idx(cl, J0 + 1 + PF);  // next row to load
   const long o_last = L.idx(cl, jpj + 1);
   long o_st = L.idx(c, J0);
+  long o_cur = L.idx(cl, J0);
 #pragma unroll 1
   for (int j = J0; j <= J1; ++j) {
     Cell pf;
@@ -253,16 +255,20 @@ __device__ __forceinline__ void run_strip(const Layout& L, const Consts& C, cons
       load_cell(nx, A, o_ld);  // row j+1 <= jpj+1
     }
     o_ld += pitch;
+    // reciprocal depths of this row, loaded where they are used
+    const double rhu = __ldg(A.rhu + o_cur);
+    const double rhv = __ldg(A.rhv + o_cur);
+    o_cur += pitch;
 
     RowOut o;
     bool bad = false;
     if (edge_warp || j == 1 || j == jpj)
-      row<false, true>(C, c, j, jpi, jpj, A.tide, cur, nx, k, o, bad);
+      row<false, true>(C, c, j, jpi, jpj, A.tide, cur, nx, k, rhu, rhv, o, bad);
     else
-      row<false, false>(C, c, j, jpi, jpj, A.tide, cur, nx, k, o, bad);
+      row<false, false>(C, c, j, jpi, jpj, A.tide, cur, nx, k, rhu, rhv, o, bad);
     if (__any_sync(FULL, bad)) {
       bool b2 = false;
-      row<true, true>(C, c, j, jpi, jpj, A.tide, cur, nx, k, o, b2);
+      row<true, true>(C, c, j, jpi, jpj, A.tide, cur, nx, k, rhu, rhv, o, b2);
     }
     if (store) {
       A.ssha[o_st] = o.ssha;
