@@ -56,9 +56,11 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--schedule", type=str, default="",
                     help="warps,occupancy,rows of the fused kernel (default: tuned)")
-    ap.add_argument("--workload", choices=["grid", "ensemble", "surrogate", "hybrid"], default="grid",
+    ap.add_argument("--workload", choices=["grid", "ensemble", "surrogate", "hybrid", "conv"],
+                    default="grid",
                     help="grid: the 4096^2 line (default); ensemble: the 256-member batch")
     ap.add_argument("--hyb-steps", type=int, default=5000)
+    ap.add_argument("--batch", type=int, default=64, help="images per conv call (conv workload)")
     ap.add_argument("--train-iters", type=int, default=600)
     ap.add_argument("--n", type=int, default=N,
                     help="grid side (profiling of smaller cases only; the bench line is 4096)")
@@ -262,7 +264,7 @@ def run_ensemble(args):
     e.close()
 
 
-def conv_kernel_rates(sur_mod, lib, n, h, w, reps, stream):
+def conv_kernel_rates(sur_mod, lib, n, h, w, reps, stream, warm=3):
     """Device time of one 3x3 conv forward (bias+ReLU epilogue) and one weight
     gradient over n x h x w pixels (64 -> 64 channels), inputs larger than L2."""
     import torch
@@ -283,7 +285,7 @@ def conv_kernel_rates(sur_mod, lib, n, h, w, reps, stream):
             else:
                 sur_mod.conv3x3_wgrad(lib, x.data_ptr(), y.data_ptr(), dw.data_ptr(), n, h, w,
                                       err.data_ptr(), db=db.data_ptr(), stream=stream)
-        for _ in range(3):
+        for _ in range(warm):
             launch()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
@@ -296,6 +298,40 @@ def conv_kernel_rates(sur_mod, lib, n, h, w, reps, stream):
         out[name] = e0.elapsed_time(e1) / reps / 1e3
     assert int(err.item()) == 0
     return out
+
+
+def run_conv(args):
+    """The surrogate's two convolution kernels alone: forward (bias + ReLU
+    epilogue) and weight gradient (+ bias gradient), 64 -> 64 channels, 3x3,
+    batch x 256 x 256 BF16 NHWC, FP32 accumulation; `steps` timed launches
+    of each after `warmup`."""
+    import torch
+    import nemo_b200
+    from nemo_b200 import surrogate as sm
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    B, S = args.batch, 256
+    clocks = ClockSampler(0)
+    clocks.start()
+    rates = conv_kernel_rates(sm, nemo_b200.load(False), B, S, S, max(args.steps, 1),
+                              stream.cuda_stream, warm=args.warmup)
+    clk = clocks.stop()
+    flop = 2 * 9 * 64 * 64 * B * S * S
+    peak = load_peaks_tensor()
+    tf = {k: flop / v / 1e12 for k, v in rates.items()}
+    line = {"metric": "3x3 conv TFLOP/s (64->64 ch, BF16 in, FP32 accumulate, %dx256x256)" % B,
+            "value": tf["fwd"], "unit": "TFLOP/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": rates["fwd"] * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "bf16", "data": "synthetic",
+            "config": {"workload": "conv kernels alone", "batch": B, "grid": [S, S],
+                       "l2": "%d MiB per activation tensor" % (B * S * S * 128 >> 20)},
+            "roofline": {"bound": "tensor", "kernel": "k_conv_fwd", "achieved": tf["fwd"],
+                         "peak": peak[0], "unit": "TFLOP/s", "frac": tf["fwd"] / peak[0],
+                         "peak_source": peak[1], "traffic": None},
+            "wgrad": {"kernel": "k_conv_wgrad", "achieved": tf["wgrad"], "frac": tf["wgrad"] / peak[0],
+                      "us": rates["wgrad"] * 1e6},
+            "gpu_launches": 2 * (args.steps + args.warmup), "clocks": clk}
+    print(json.dumps(line), flush=True)
 
 
 def run_surrogate(args):
@@ -472,6 +508,8 @@ def main():
         return run_surrogate(args)
     if args.workload == "hybrid":
         return run_hybrid(args)
+    if args.workload == "conv":
+        return run_conv(args)
     if args.n != N:
         WORKLOAD["jpi"] = WORKLOAD["jpj"] = args.n
         CONFIG["grid"] = [args.n, args.n]

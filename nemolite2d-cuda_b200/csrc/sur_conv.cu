@@ -160,6 +160,7 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t
   return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
          ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46) | (2ull << 61);
 }
+
 // Instruction descriptor, kind::f16: D f32, A and B bf16, M x N, operand
 // majorness (0 K-major, 1 MN-major).
 __host__ __device__ constexpr uint32_t idesc(int M, int N, int a_mn, int b_mn) {
@@ -178,6 +179,61 @@ struct FwdSmem {
 };
 
 __device__ __forceinline__ void fail(int* err, int code) { atomicCAS(err, 0, code); }
+
+// Epilogue of one 128-pixel output tile for this thread's pixel `row`:
+// v = acc (64 fp32 values) + bias, + residual, *(mask > 0), relu; stores.
+__device__ __forceinline__ void epilogue_store(const ConvEpi& E, const float* bias, float* v, long p) {
+#pragma unroll
+  for (int c = 0; c < 64; ++c) v[c] += bias[c];
+  if (E.residual) {
+    const uint4* rp = reinterpret_cast<const uint4*>(E.residual + p * CH);
+#pragma unroll
+    for (int g = 0; g < 8; ++g) {
+      uint4 u = rp[g];
+      const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&u);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        float2 f = __bfloat1622float2(h[e]);
+        v[8 * g + 2 * e] += f.x;
+        v[8 * g + 2 * e + 1] += f.y;
+      }
+    }
+  }
+  if (E.mask) {
+    const uint4* mp = reinterpret_cast<const uint4*>(E.mask + p * CH);
+#pragma unroll
+    for (int g = 0; g < 8; ++g) {
+      uint4 u = mp[g];
+      const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&u);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        float2 f = __bfloat1622float2(h[e]);
+        if (!(f.x > 0.0f)) v[8 * g + 2 * e] = 0.0f;
+        if (!(f.y > 0.0f)) v[8 * g + 2 * e + 1] = 0.0f;
+      }
+    }
+  }
+  if (E.relu) {
+#pragma unroll
+    for (int c = 0; c < 64; ++c) v[c] = fmaxf(v[c], 0.0f);
+  }
+  if (E.out32) {
+    float4* o32 = reinterpret_cast<float4*>(E.out32 + p * 4);
+    *o32 = make_float4(v[0], v[1], v[2], v[3]);
+  }
+  if (E.out) {
+    uint4* op = reinterpret_cast<uint4*>(E.out + p * CH);
+#pragma unroll
+    for (int g = 0; g < 8; ++g) {
+      uint4 u;
+      __nv_bfloat162* h = reinterpret_cast<__nv_bfloat162*>(&u);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) h[e] = __floats2bfloat162_rn(v[8 * g + 2 * e], v[8 * g + 2 * e + 1]);
+      op[g] = u;
+    }
+  }
+}
+
 
 __global__ void __launch_bounds__(THREADS, 1)
 k_conv_fwd(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmW,
@@ -279,54 +335,167 @@ k_conv_fwd(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUte
       mbar_arrive(&S.tempty[b]);
       const int xt = t % xtiles, r = t / xtiles, y = r % E.H, n = r / E.H;
       const long p = ((long)(n * E.H + y) * E.W + xt * TM + row);
+      epilogue_store(E, S.bias, v, p);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    __syncwarp();
+    tc_fence_after();
+    tmem_dealloc(tmem, 128);
+  }
+}
+
+// ---- forward over column strips with a ring of input rows ------------------
+// A CTA takes strips (image n, 128-column tile xt, rows y0 .. y0+R-1) and
+// marches down them.  Each input row r is loaded once (TMA, 144 pixels
+// x0-8 .. x0+135, zero-filled outside the image) into a ring slot and serves
+// the three output rows r-1, r, r+1; the three horizontal taps of a row read
+// the slot through descriptors starting at pixels 7, 8, 9.  The 128-byte
+// swizzle is a function of the absolute shared-memory address (the phase of
+// a row is address bits 7-9, as TMA wrote it), so a view may start on any
+// 128-byte row with the base-offset field left at zero; the exact-shift
+// tests check this on the device.  One 18 KiB load feeds 36 MMAs instead
+// of 4.
+constexpr int RW_PIX = 144;
+constexpr int RW_BYTES = RW_PIX * CH * 2;  // 18 KiB, a multiple of 1024
+constexpr int NSLOT = 8;
+
+struct RowSmem {
+  uint8_t slot[NSLOT][RW_BYTES];
+  uint8_t w[W_BYTES];
+  uint64_t full[NSLOT], empty[NSLOT];
+  uint64_t wbar, done;
+  uint64_t tfull[2], tempty[2];
+  uint32_t tmem_base;
+  float bias[CH];
+};
+
+__global__ void __launch_bounds__(THREADS, 1)
+k_conv_fwd_rows(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmW,
+                ConvEpi E, int R) {
+  extern __shared__ uint8_t smem_raw[];
+  RowSmem& S = *reinterpret_cast<RowSmem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int xtiles = E.W / TM;
+  const int ystrips = (E.H + R - 1) / R;
+  const int nstrip = E.N * xtiles * ystrips;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < NSLOT; ++s) {
+      mbar_init(&S.full[s], 1);
+      mbar_init(&S.empty[s], 1);
+    }
+    mbar_init(&S.wbar, 1);
+    mbar_init(&S.done, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&S.tfull[b], 1);
+      mbar_init(&S.tempty[b], 128);
+    }
+    fence_barrier_init();
+  }
+  if (threadIdx.x < CH) S.bias[threadIdx.x] = E.bias ? E.bias[threadIdx.x] : 0.0f;
+  if (warp == 1) tmem_alloc(&S.tmem_base, 128);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = S.tmem_base;
+
+  if (warp == 0 && lane == 0) {
+    // ---- TMA producer: rows y0-1 .. y1+1 of every strip, in order ----
+    mbar_expect_tx(&S.wbar, W_BYTES);
+    for (int tap = 0; tap < 9; ++tap) tma_load_2d(S.w + tap * WT_BYTES, &tmW, &S.wbar, 0, tap * CH);
+    uint32_t L = 0;  // loads issued
+    bool ok = true;
+    for (int st = blockIdx.x; st < nstrip && ok; st += gridDim.x) {
+      const int ys = st % ystrips, r0 = st / ystrips, xt = r0 % xtiles, n = r0 / xtiles;
+      const int y0 = ys * R, y1 = min(y0 + R, E.H) - 1;
+      for (int r = y0 - 1; r <= y1 + 1; ++r, ++L) {
+        const int slot = (int)(L % NSLOT);
+        const uint32_t ph = (L / NSLOT) & 1;
+        if (!mbar_wait(&S.empty[slot], ph ^ 1)) { fail(E.err, 21); ok = false; break; }
+        mbar_expect_tx(&S.full[slot], RW_BYTES);
+        tma_load_4d(S.slot[slot], &tmA, &S.full[slot], 0, xt * TM - 8, r, n);
+      }
+    }
+    // every armed load lands before the CTA may exit
+    for (int s = 0; s < NSLOT; ++s) {
+      const uint32_t armed = L / NSLOT + ((uint32_t)s < L % NSLOT ? 1u : 0u);
+      if (armed) mbar_wait(&S.full[s], (armed - 1) & 1);
+    }
+    mbar_wait(&S.wbar, 0);
+  } else if (warp == 1 && lane == 0) {
+    // ---- MMA issuer ----
+    const uint32_t ID = idesc(128, 64, 0, 0);
+    bool ok = mbar_wait(&S.wbar, 0);
+    if (!ok) fail(E.err, 22);
+    const uint32_t wbase = smem_u32(S.w);
+    uint32_t L = 0;       // loads consumed (index of the strip's first row)
+    uint32_t waited = 0;  // loads whose full barrier has been waited for
+    int it = 0;
+    for (int st = blockIdx.x; st < nstrip && ok; st += gridDim.x) {
+      const int ys = st % ystrips;
+      const int y0 = ys * R, y1 = min(y0 + R, E.H) - 1;
+      const int rows = y1 - y0 + 1;
+      for (int i = 0; i < rows && ok; ++i, ++it) {
+        // rows y0+i-1, y0+i, y0+i+1 are loads L+i, L+i+1, L+i+2
+        while (waited <= L + i + 2) {
+          if (!mbar_wait(&S.full[waited % NSLOT], (waited / NSLOT) & 1)) { fail(E.err, 23); ok = false; break; }
+          ++waited;
+        }
+        if (!ok) break;
+        const int b = it & 1;
+        const uint32_t tph = (it >> 1) & 1;
+        if (!mbar_wait(&S.tempty[b], tph ^ 1)) { fail(E.err, 24); ok = false; break; }
+        tc_fence_after();
+        const uint32_t d = tmem + (uint32_t)(b * 64);
 #pragma unroll
-      for (int c = 0; c < 64; ++c) v[c] += S.bias[c];
-      if (E.residual) {
-        const uint4* rp = reinterpret_cast<const uint4*>(E.residual + p * CH);
+        for (int dy = 0; dy < 3; ++dy) {
+          const uint32_t sbase = smem_u32(S.slot[(L + i + dy) % NSLOT]);
 #pragma unroll
-        for (int g = 0; g < 8; ++g) {
-          uint4 u = rp[g];
-          const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&u);
+          for (int dx = 0; dx < 3; ++dx) {
+            const uint32_t a0 = sbase + (uint32_t)(7 + dx) * 128u;
+            const uint32_t b0 = wbase + (uint32_t)(3 * dy + dx) * WT_BYTES;
 #pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            float2 f = __bfloat1622float2(h[e]);
-            v[8 * g + 2 * e] += f.x;
-            v[8 * g + 2 * e + 1] += f.y;
+            for (int k = 0; k < 4; ++k)
+              mma_bf16(d, sdesc(a0 + 32 * k, 16, 1024), sdesc(b0 + 32 * k, 16, 1024), ID,
+                       (dy | dx | k) != 0);
           }
         }
+        mma_commit(&S.tfull[b]);
+        mma_commit(&S.empty[(L + i) % NSLOT]);  // row y0+i-1 has had its last use
       }
-      if (E.mask) {
-        const uint4* mp = reinterpret_cast<const uint4*>(E.mask + p * CH);
-#pragma unroll
-        for (int g = 0; g < 8; ++g) {
-          uint4 u = mp[g];
-          const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&u);
-#pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            float2 f = __bfloat1622float2(h[e]);
-            if (!(f.x > 0.0f)) v[8 * g + 2 * e] = 0.0f;
-            if (!(f.y > 0.0f)) v[8 * g + 2 * e + 1] = 0.0f;
-          }
-        }
+      if (ok) {
+        mma_commit(&S.empty[(L + rows) % NSLOT]);
+        mma_commit(&S.empty[(L + rows + 1) % NSLOT]);
       }
-      if (E.relu) {
-#pragma unroll
-        for (int c = 0; c < 64; ++c) v[c] = fmaxf(v[c], 0.0f);
-      }
-      if (E.out32) {
-        float4* o32 = reinterpret_cast<float4*>(E.out32 + p * 4);
-        *o32 = make_float4(v[0], v[1], v[2], v[3]);
-      }
-      if (E.out) {
-        uint4* op = reinterpret_cast<uint4*>(E.out + p * CH);
-#pragma unroll
-        for (int g = 0; g < 8; ++g) {
-          uint4 u;
-          __nv_bfloat162* h = reinterpret_cast<__nv_bfloat162*>(&u);
-#pragma unroll
-          for (int e = 0; e < 4; ++e) h[e] = __floats2bfloat162_rn(v[8 * g + 2 * e], v[8 * g + 2 * e + 1]);
-          op[g] = u;
-        }
+      L += rows + 2;
+    }
+    mma_commit(&S.done);
+    mbar_wait(&S.done, 0);
+  } else if (warp >= 2) {
+    // ---- epilogue ----
+    const int q = warp & 3;
+    const int row = 32 * q + lane;
+    int it = 0;
+    bool ok = true;
+    for (int st = blockIdx.x; st < nstrip && ok; st += gridDim.x) {
+      const int ys = st % ystrips, r0 = st / ystrips, xt = r0 % xtiles, n = r0 / xtiles;
+      const int y0 = ys * R, y1 = min(y0 + R, E.H) - 1;
+      for (int y = y0; y <= y1; ++y, ++it) {
+        const int b = it & 1;
+        const uint32_t tph = (it >> 1) & 1;
+        if (!mbar_wait_warp(&S.tfull[b], tph)) { fail(E.err, 25); ok = false; break; }
+        tc_fence_after();
+        float v[64];
+        const uint32_t ta = tmem + (uint32_t)(b * 64) + ((uint32_t)(32 * q) << 16);
+        tmem_ld32(ta, v);
+        tmem_ld32(ta + 32, v + 32);
+        tc_fence_before();
+        mbar_arrive(&S.tempty[b]);
+        const long p = ((long)(n * E.H + y) * E.W + xt * TM + row);
+        epilogue_store(E, S.bias, v, p);
       }
     }
   }
@@ -505,6 +674,8 @@ cudaError_t w_map(CUtensorMap* m, const void* base) {
 
 int g_sms[64];
 bool g_attr[64];
+int g_fwd_variant = 1;  // 1: row ring (k_conv_fwd_rows), 0: a TMA window per tap (k_conv_fwd)
+int g_fwd_rows = 16;    // rows per strip of the row-ring kernel
 
 // SM count of the current device; opts the kernels into their shared memory.
 cudaError_t prepare_device(int* sms) {
@@ -518,6 +689,9 @@ cudaError_t prepare_device(int* sms) {
     e = cudaFuncSetAttribute(k_conv_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(sizeof(FwdSmem) + 1024));
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k_conv_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(sizeof(WgSmem) + 1024));
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_conv_fwd_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(sizeof(RowSmem) + 1024));
     if (e != cudaSuccess) return e;
     g_attr[dev] = true;
   }
@@ -539,12 +713,27 @@ cudaError_t conv_fwd(const __nv_bfloat16* x, const __nv_bfloat16* w, const ConvE
   int sms = 0;
   if ((e = prepare_device(&sms)) != cudaSuccess) return e;
   CUtensorMap ta, tw;
-  if ((e = act_map(&ta, x, epi.N, epi.H, epi.W, TM)) != cudaSuccess) return e;
   if ((e = w_map(&tw, w)) != cudaSuccess) return e;
+  if (g_fwd_variant == 1) {
+    if ((e = act_map(&ta, x, epi.N, epi.H, epi.W, RW_PIX)) != cudaSuccess) return e;
+    const int R = g_fwd_rows;
+    const long nstrip = (long)epi.N * (epi.W / TM) * ((epi.H + R - 1) / R);
+    const int grid = (int)(nstrip < sms ? nstrip : sms);
+    k_conv_fwd_rows<<<grid, THREADS, sizeof(RowSmem) + 1024, s>>>(ta, tw, epi, R);
+    return cudaGetLastError();
+  }
+  if ((e = act_map(&ta, x, epi.N, epi.H, epi.W, TM)) != cudaSuccess) return e;
   const long ntile = (long)epi.N * epi.H * (epi.W / TM);
   const int grid = (int)(ntile < sms ? ntile : sms);
   k_conv_fwd<<<grid, THREADS, sizeof(FwdSmem) + 1024, s>>>(ta, tw, epi);
   return cudaGetLastError();
+}
+
+int set_fwd_variant(int variant, int rows) {
+  const int prev = g_fwd_variant;
+  if (variant == 0 || variant == 1) g_fwd_variant = variant;
+  if (rows >= 1 && rows <= 4096) g_fwd_rows = rows;
+  return prev;
 }
 
 cudaError_t conv_wgrad(const __nv_bfloat16* x, const __nv_bfloat16* dz, const WgradArgs& g, int ctas,

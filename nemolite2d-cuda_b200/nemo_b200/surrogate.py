@@ -55,6 +55,7 @@ def declare(L):
     L.nemo_hyb_run.argtypes = [vp, vp, P(HybConfig), ip, ip, P(HybStats)]
     L.nemo_conv3x3_fwd.argtypes = [vp, vp, vp, vp, vp, ip, vp, vp, ip, ip, ip, vp, vp]
     L.nemo_conv3x3_wgrad.argtypes = [vp, vp, vp, vp, ip, ip, ip, ip, vp, vp]
+    L.nemo_conv3x3_fwd_variant.argtypes = [ip, ip]
 
 
 def _fptr(a):
@@ -187,6 +188,12 @@ def conv3x3_fwd(lib, x, w, n, h, wd, err, bias=None, residual=None, mask=None, r
                 out=None, out32=None, stream=None):
     check(lib.nemo_conv3x3_fwd(x, w, bias, residual, mask, int(bool(relu)), out, out32, n, h, wd,
                                err, stream), "nemo_conv3x3_fwd")
+
+
+def conv3x3_fwd_variant(lib, variant, rows=0):
+    """Select the forward kernel process-wide (1: row ring, 0: window per tap);
+    returns the previous variant."""
+    return lib.nemo_conv3x3_fwd_variant(variant, rows)
 
 
 def conv3x3_wgrad(lib, x, dz, dw, n, h, wd, err, db=None, ctas=0, stream=None):

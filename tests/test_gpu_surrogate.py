@@ -38,6 +38,17 @@ def ulp_close(got, ref):
     return bad.mean(), np.abs(got - ref).max()
 
 
+@pytest.fixture(params=[(1, 16), (1, 2), (0, 0)], ids=["rows16", "rows2", "per-tap"])
+def variant(request, env):
+    """Each forward kernel variant (row ring with 16 or 2 rows per strip,
+    window per tap), restored to the default afterwards."""
+    torch, nb, sm = env
+    lib = nb.load(False)
+    prev = sm.conv3x3_fwd_variant(lib, *request.param)
+    yield request.param
+    sm.conv3x3_fwd_variant(lib, prev, 16)
+
+
 def run_fwd(torch, sm, lib, x, w, bias=None, residual=None, mask=None, relu=False, out32=False):
     N, H, W, _ = x.shape
     xd, wd = dev_bf16(torch, x), dev_bf16(torch, w)
@@ -57,7 +68,7 @@ def run_fwd(torch, sm, lib, x, w, bias=None, residual=None, mask=None, relu=Fals
 
 
 @pytest.mark.parametrize("tap", range(9))
-def test_fwd_one_hot_tap_is_an_exact_shift(env, tap):
+def test_fwd_one_hot_tap_is_an_exact_shift(env, variant, tap):
     torch, nb, sm = env
     rng = np.random.default_rng(tap)
     x = so.bf16(rng.normal(size=(2, 5, 256, 64)))
@@ -69,8 +80,8 @@ def test_fwd_one_hot_tap_is_an_exact_shift(env, tap):
     np.testing.assert_array_equal(got, ref)
 
 
-@pytest.mark.parametrize("shape", [(2, 6, 128), (1, 3, 384), (3, 1, 256)])
-def test_fwd_random_matches_oracle(env, shape):
+@pytest.mark.parametrize("shape", [(2, 6, 128), (1, 3, 384), (3, 1, 256), (2, 37, 128)])
+def test_fwd_random_matches_oracle(env, variant, shape):
     torch, nb, sm = env
     N, H, W = shape
     rng = np.random.default_rng(N * 100 + H)
@@ -89,7 +100,7 @@ def test_fwd_random_matches_oracle(env, shape):
         assert np.abs(o32 - ref[..., :4]).max() <= 1e-4 * np.abs(ref[..., :4]).max()
 
 
-def test_dgrad_with_flipped_weights_matches_oracle(env):
+def test_dgrad_with_flipped_weights_matches_oracle(env, variant):
     torch, nb, sm = env
     rng = np.random.default_rng(7)
     dz = so.bf16(rng.normal(size=(2, 4, 128, 64)))
