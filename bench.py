@@ -60,8 +60,12 @@ def parse():
                     default="grid",
                     help="grid: the 4096^2 line (default); ensemble: the 256-member batch")
     ap.add_argument("--hyb-steps", type=int, default=5000)
+    ap.add_argument("--patch", type=int, default=4, help="surrogate patch of the hybrid")
+    ap.add_argument("--train-side", type=int, default=512, help="training run side (hybrid)")
+    ap.add_argument("--train-steps", type=int, default=2000, help="training run length (hybrid)")
+    ap.add_argument("--train-runs", type=int, default=96, help="training runs (hybrid)")
     ap.add_argument("--batch", type=int, default=64, help="images per conv call (conv workload)")
-    ap.add_argument("--train-iters", type=int, default=600)
+    ap.add_argument("--train-iters", type=int, default=3000)
     ap.add_argument("--n", type=int, default=N,
                     help="grid side (profiling of smaller cases only; the bench line is 4096)")
     return ap.parse_args()
@@ -414,10 +418,14 @@ def load_peaks_tensor():
 def run_hybrid(args):
     """Hybrid inference versus the plain solver: 32 members at 2048x2048
     (seeded bathymetry and tides of the batched recipe), 5000 steps.  The
-    surrogate (trained first on 256x256 runs) advances 10 steps per call; the
-    FP64 solver re-anchors every 100 steps and takes the window over when the
-    shadow SSH error exceeds 1%.  Reports both rates and the hybrid's error
-    against the plain FP64 run (which matches the FP64 oracle to 1e-12)."""
+    surrogate runs on 4x4 patches of T-cells (a call costs 1/16 of the
+    full-resolution network) and is trained first on solver runs of the same
+    recipe at 512x512 (pairs of snapshots 10 steps apart every 50 steps of
+    2000-step runs); it advances 10 steps per call, and the FP64 solver
+    re-anchors every 100 steps and takes the rest of the window over for each
+    member whose shadow SSH error exceeds 1%.  Reports both rates and the
+    hybrid's error against the plain FP64 run (which matches the FP64 oracle
+    to 1e-12)."""
     import numpy as np
     import torch
     from nemo_b200 import surrogate as sm
@@ -425,15 +433,18 @@ def run_hybrid(args):
     import nemo_b200
     torch.cuda.set_device(0)
     nsteps = args.hyb_steps
-    side, nm = 2048, 32
-    # ---- train on the 256x256 recipe
-    trainer = sm.Surrogate(nblocks=8, batch=64, height=256, width=256, seed=1234, device=0)
-    snaps, tides = tr.generate_runs(trainer, seed=7000, nmem=64, side=256, steps=500)
-    norm = tr.compute_norm(snaps)
+    side, nm, P, ts = 2048, 32, args.patch, args.train_side
+    # ---- train on solver runs of the recipe
+    trainer = sm.Surrogate(nblocks=8, batch=64, height=ts, width=ts, seed=1234, device=0, patch=P)
+    t_gen = time.time()
+    snaps, tides = tr.generate_runs(trainer, seed=7000, nmem=args.train_runs, side=ts,
+                                    steps=args.train_steps, pair_stride=50)
+    t_gen = time.time() - t_gen
+    norm = tr.compute_norm(snaps, paired=True)
     trainer.set_norm(*norm)
     t_train = time.time()
-    losses = tr.train(trainer, tr.PairSampler(snaps, tides, seed=3), iters=args.train_iters,
-                      batch=64, lr=1e-3)
+    losses = tr.train(trainer, tr.PairSampler(snaps, tides, seed=3, paired=True),
+                      iters=args.train_iters, batch=64, lr=1e-3)
     t_train = time.time() - t_train
     params = trainer.params()
     trainer.close()
@@ -445,7 +456,7 @@ def run_hybrid(args):
     # finite are the workload
     stream = torch.cuda.Stream()
     common = dict(tr.COMMON, stream=stream.cuda_stream, device=0)
-    cands = tr.square_members(4242, 40, side, 0.2)
+    cands = tr.square_members(4242, 48, side, 0.2)
     scr = nemo_b200.Ensemble(cands, **common)
     scr.step_n(1, nsteps)
     ck = scr.checksums()
@@ -455,8 +466,8 @@ def run_hybrid(args):
     nm = len(members)
     plain = nemo_b200.Ensemble(members, **common)
     hyb = nemo_b200.Ensemble(members, **common)
-    inf = sm.Surrogate(nblocks=8, batch=16, height=side, width=side, train=False, seed=1,
-                       stream=stream.cuda_stream, device=0)
+    inf = sm.Surrogate(nblocks=8, batch=nm, height=side, width=side, train=False, seed=1,
+                       stream=stream.cuda_stream, device=0, patch=P)
     inf.set_params(params)
     inf.set_norm(*norm)
     cells = nm * side * side
@@ -486,10 +497,13 @@ def run_hybrid(args):
             "config": {"workload": "%d members 2048x2048, %d steps, surrogate k=10, re-anchor 100, "
                                    "tol 1%% relative SSH L2 vs shadow FP64 step" % (nm, nsteps),
                        "candidates": len(cands), "screened_out": len(cands) - len(ok),
-                       "train_iters": args.train_iters, "train_s": t_train,
+                       "patch": P, "train_side": ts, "train_steps": args.train_steps,
+                       "train_runs": args.train_runs, "fallback": "per member",
+                       "train_iters": args.train_iters, "train_s": t_train, "datagen_s": t_gen,
                        "train_runs_dropped": tr.generate_runs.dropped},
             "plain_value": v_plain, "hybrid_over_plain": v_hyb / v_plain,
             "hybrid_stats": st,
+            "surrogate_share": st["sur_steps"] / max(1, st["sur_steps"] + st["solver_steps"]),
             "err_vs_fp64": {"ssh_max": float(err[:, 0].max()), "ssh_mean": float(err[:, 0].mean()),
                             "u_max": float(err[:, 1].max()), "v_max": float(err[:, 2].max()),
                             "u_mean": float(err[:, 1].mean()), "v_mean": float(err[:, 2].mean())},

@@ -136,12 +136,14 @@ int nemo_get_dims(nemo_ctx* ctx, int* jpi, int* jpj);
  * (ji,jj) lives at ptr[(jj+1)*pitch + (ji+2)].  For device-side consumers. */
 int nemo_device_field(nemo_ctx* ctx, int field, double** ptr, long* pitch);
 /* Launch schedule of the fused kernel: warps per CTA (2, 4, 8; a warp covers
- * 30 columns), register budget as resident warps per SM (0 = compiler's
- * choice, 16, 20, 24; 8-warp CTAs take 0, 16 or 24; a negative value, -16,
- * -20, -24 for 2-warp and -20 for 4-warp CTAs, selects the same budget
- * without the register prefetch of the next row) and rows marched per CTA
- * (0: one wave, row blocks sized so every CTA is resident at once).  In the
- * -fmad=false build every schedule gives bit-identical results. */
+ * 30 columns), register budget as resident warps per SM and row staging
+ * (occupancy), and rows marched per CTA (0: one wave, row blocks sized so
+ * every CTA is resident at once).  occupancy: 116 or 120 (2- and 4-warp
+ * CTAs) stage rows through shared memory with a budget of 16 or 20 warps
+ * (the default, 2 warps, 116, 16 rows); 0 (compiler's choice), 16, 20, 24
+ * prefetch the next row into registers (8-warp CTAs take 0, 16 or 24); -16,
+ * -20, -24 for 2-warp and -20 for 4-warp CTAs load each row one step ahead.
+ * In the -fmad=false build every schedule gives bit-identical results. */
 typedef struct nemo_schedule {
   int warps;
   int occupancy;
@@ -182,7 +184,8 @@ typedef struct nemo_ens nemo_ens;
 
 typedef struct nemo_ens_schedule {
   int warps;      /* warps per CTA: 2 or 4 */
-  int occupancy;  /* register budget, as nemo_schedule.occupancy */
+  int occupancy;  /* as nemo_schedule.occupancy: 116, 120 (2 warps), 116 (4
+                     warps), 20, 24, -20, -24 (2 warps), 20, 24, -20 (4) */
   int rows;       /* rows per work item */
   int order;      /* work-list order: 0 member by member, 1 largest member first */
   int ctas;       /* persistent grid size; 0: every resident CTA slot */
@@ -234,11 +237,12 @@ int nemo_checksums_noalloc(const double* const* fields, int nfields, int nx, int
 /* ---- BF16 convolutional surrogate and hybrid controller ----------------------
  * No counterpart in the reference.  A residual CNN (nblocks blocks of two 3x3
  * convolutions, 64 channels, plus input and output convolutions) maps the
- * state of a grid at step s to its state at s + 10.  Tensors are NHWC with
- * one pixel per T-cell (ji, jj) -> (x = ji-1, y = jj-1).  A snapshot is FP32
- * [n][height][width][4]: ssh(ji,jj), u(ji-1,jj) (west face), v(ji,jj-1) (south
- * face), ht(ji,jj).  width must be a multiple of 128.  Device pointers are
- * the caller's; every call is ordered on the configured stream. */
+ * state of a grid at step s to its state at s + 10.  A snapshot is FP32
+ * [n][height][width][4], one entry per T-cell (ji, jj) -> (x = ji-1,
+ * y = jj-1): ssh(ji,jj), u(ji-1,jj) (west face), v(ji,jj-1) (south face),
+ * ht(ji,jj).  The network's NHWC tensors hold one pixel per P x P patch of
+ * T-cells (the configuration's patch).  Device pointers are the caller's;
+ * every call is ordered on the configured stream. */
 typedef struct nemo_sur nemo_sur;
 
 typedef struct nemo_sur_config {
@@ -249,6 +253,9 @@ typedef struct nemo_sur_config {
   uint64_t seed;        /* weight initialisation */
   void* stream;         /* cudaStream_t; NULL: the surrogate creates one */
   int device;           /* -1: current device */
+  int patch;            /* P = 1, 2 or 4: the network runs on P x P patches of
+                           T-cells (height, width multiples of P; width / P a
+                           multiple of 128); 0 means 1 */
 } nemo_sur_config;
 
 typedef struct nemo_adamw {
@@ -259,7 +266,8 @@ int nemo_sur_default_config(nemo_sur_config* c);
 int nemo_sur_create(const nemo_sur_config* c, nemo_sur** out);
 int nemo_sur_destroy(nemo_sur* s);
 /* Parameter count (FP32: all layers' weights [9][64 out][64 in], then all
- * biases [64]) and convolution FLOPs per pixel of one forward pass. */
+ * biases [64]) and convolution FLOPs of one forward pass per T-cell (per
+ * network pixel / P^2). */
 int nemo_sur_info(nemo_sur* s, long long* nparams, long long* flops_per_pixel);
 int nemo_sur_get_params(nemo_sur* s, float* host);
 int nemo_sur_set_params(nemo_sur* s, const float* host);
@@ -268,8 +276,11 @@ int nemo_sur_get_grads(nemo_sur* s, float* host);
  * uses the ssh pair), output scale[3] (network output = delta * scale). */
 int nemo_sur_set_norm(nemo_sur* s, const float* norm);
 int nemo_sur_get_norm(nemo_sur* s, float* norm);
-/* out (device, [n][h][w][4] FP32): normalised deltas; tide[n] (device, FP32):
- * boundary-row SSH at the target time. */
+/* snap (device, [n][h][w][4] FP32 per T-cell: ssh, u west face, v south face,
+ * depth); out (device, FP32): normalised deltas, [n][h][w][4] (channels
+ * ssh, u, v, 0) for patch 1, else [n][h/P][w/P][3 P^2] with channel
+ * f P^2 + P sy + sx = field f of T-cell (P X + sx, P Y + sy); tide[n] (device,
+ * FP32): boundary-row SSH at the target time. */
 int nemo_sur_predict(nemo_sur* s, const float* snap, const float* tide, int n, float* out);
 /* Forward + mean-squared-error loss against snap1 + backward; gradients are
  * recomputed from zero.  loss: host double. */
@@ -289,22 +300,29 @@ int nemo_sur_advance_ens(nemo_sur* s, nemo_ens* e, int istp_end);
 int nemo_ens_compare(nemo_ens* a, nemo_ens* ref, double* out);
 
 typedef struct nemo_hyb_config {
-  int k;        /* steps per surrogate call (10) */
-  int anchor;   /* FP64 re-anchor interval (100) */
-  double tol;   /* fallback threshold on relative SSH L2 error (0.01) */
+  int k;          /* steps per surrogate call (10) */
+  int anchor;     /* FP64 re-anchor interval (100) */
+  double tol;     /* fallback threshold on relative SSH L2 error (0.01) */
+  int per_member; /* 1: each member falls back on its own (anchor - k even);
+                     0: any failing member sends the whole ensemble back (1) */
 } nemo_hyb_config;
 
 typedef struct nemo_hyb_stats {
-  long long sur_calls, sur_steps, solver_steps, fallbacks;
-  double max_shadow_err, last_shadow_err, seconds;
+  long long sur_calls;     /* surrogate calls (each advances its members k steps) */
+  long long sur_steps;     /* member-steps advanced by the surrogate */
+  long long solver_steps;  /* member-steps advanced by the FP64 solver */
+  long long fallbacks;     /* member-windows that fell back to the solver */
+  long long windows;       /* member-windows */
+  double max_shadow_err, last_shadow_err;  /* worst member's shadow error */
+  double seconds;
 } nemo_hyb_stats;
 
 int nemo_hyb_default_config(nemo_hyb_config* c);
 /* Advances e by nsteps (a multiple of anchor) from the state after istp0.
  * Each anchor window: the surrogate predicts the first k steps while the
- * FP64 solver runs them (re-anchoring the state); if any member's relative
- * SSH L2 error of that prediction exceeds tol the solver runs the rest of the
- * window, otherwise the surrogate does, k steps per call. */
+ * FP64 solver runs them (re-anchoring the state); each member whose relative
+ * SSH L2 error of that prediction exceeds tol is advanced through the rest of
+ * the window by the solver, the others by the surrogate, k steps per call. */
 int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, int nsteps,
                  nemo_hyb_stats* stats);
 

@@ -312,7 +312,7 @@ int nemo_create(const nemo_params* p, nemo_ctx** out) {
   c->L.rows = (long)p->jpj + 3;
   c->C = make_consts(*p);
   c->sched.warps = 2;
-  c->sched.occupancy = -20;
+  c->sched.occupancy = 116;
   c->sched.rows = 16;
   int st = set_device(c);
   if (st) { delete c; return st; }
@@ -639,8 +639,9 @@ int nemo_autotune(nemo_ctx* c, int steps, nemo_schedule* best, double* best_ms) 
   const nemo_schedule keep = c->sched;
   nemo_schedule bsched = keep;
   double bms = 1e300;
-  const int wo[][2] = {{2, -24}, {2, -20}, {2, -16}, {2, 0}, {2, 16}, {2, 20}, {2, 24},
-                       {4, -20}, {4, 0}, {4, 16}, {4, 20}, {4, 24}, {8, 0}, {8, 16}, {8, 24}};
+  const int wo[][2] = {{2, 116}, {2, 120}, {4, 116}, {4, 120}, {2, -24}, {2, -20}, {2, -16}, {2, 0},
+                       {2, 16}, {2, 20}, {2, 24}, {4, -20}, {4, 0}, {4, 16}, {4, 20}, {4, 24},
+                       {8, 0}, {8, 16}, {8, 24}};
   const int rows_c[] = {8, 16, 32, 0};
   cudaEvent_t t0 = nullptr, t1 = nullptr;
   if (er == cudaSuccess) er = cudaEventCreate(&t0);

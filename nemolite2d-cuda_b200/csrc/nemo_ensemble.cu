@@ -60,7 +60,12 @@ k_ens_step(const MemberDev* __restrict__ mem, const int4* __restrict__ work, int
     A.sshv0 = M->sshv0;
     A.tide = tide[it.x];
     const Layout L = M->L;
-    stepdev::run_strip<PF>(L, C, A, it.y, it.z, it.w, lane);
+    if constexpr (PF == 2) {
+      __shared__ double ring[NW * stepdev::RING_DOUBLES];
+      stepdev::run_strip_ring(L, C, A, it.y, it.z, it.w, lane, ring + (threadIdx.x >> 5) * stepdev::RING_DOUBLES);
+    } else {
+      stepdev::run_strip<PF>(L, C, A, it.y, it.z, it.w, lane);
+    }
   }
 }
 
@@ -138,6 +143,9 @@ cudaError_t launch_ens(int warps, int occ, const MemberDev* mem, const int4* wor
                        const Consts& C, const double* tide, int parity, int ctas,
                        cudaStream_t s) {
   switch (warps * 100 + occ) {
+    case 316: return launch_ens_variant<2, 8, 2>(mem, work, nwork, C, tide, parity, ctas, s);
+    case 320: return launch_ens_variant<2, 10, 2>(mem, work, nwork, C, tide, parity, ctas, s);
+    case 516: return launch_ens_variant<4, 4, 2>(mem, work, nwork, C, tide, parity, ctas, s);
     case 200 - 24: return launch_ens_variant<2, 12, 0>(mem, work, nwork, C, tide, parity, ctas, s);
     case 200 - 20: return launch_ens_variant<2, 10, 0>(mem, work, nwork, C, tide, parity, ctas, s);
     case 220: return launch_ens_variant<2, 10, 1>(mem, work, nwork, C, tide, parity, ctas, s);
@@ -150,8 +158,8 @@ cudaError_t launch_ens(int warps, int occ, const MemberDev* mem, const int4* wor
 }
 
 bool ens_variant_ok(int warps, int occ) {
-  if (warps == 2) return occ == -24 || occ == -20 || occ == 20 || occ == 24;
-  if (warps == 4) return occ == -20 || occ == 20 || occ == 24;
+  if (warps == 2) return occ == -24 || occ == -20 || occ == 20 || occ == 24 || occ == 116 || occ == 120;
+  if (warps == 4) return occ == -20 || occ == 20 || occ == 24 || occ == 116;
   return false;
 }
 
@@ -205,6 +213,8 @@ struct nemo_ens {
   bool use_graph = true;
   std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
   long long cells = 0;
+  int4* d_work_sub = nullptr;  // work list of a member subset (ens_step_subset)
+  int sub_cap = 0;
 };
 
 namespace {
@@ -219,10 +229,11 @@ void drop_graphs(nemo_ens* e) {
   e->graphs.clear();
 }
 
-// Work items of every member in the schedule's order: row blocks of
-// `rows` rows, each split into 30-column strips, neighbouring strips of one
-// row block consecutive so concurrently running warps share halo rows in L2.
-int build_work(nemo_ens* e) {
+// Work items of every member (or of the members with sel[m] != 0) in the
+// schedule's order: row blocks of `rows` rows, each split into 30-column
+// strips, neighbouring strips of one row block consecutive so concurrently
+// running warps share halo rows in L2.
+std::vector<int4> work_items(const nemo_ens* e, const char* sel) {
   const int R = e->sched.rows;
   std::vector<int> order(e->mem.size());
   for (size_t m = 0; m < order.size(); ++m) order[m] = (int)m;
@@ -232,10 +243,16 @@ int build_work(nemo_ens* e) {
     });
   std::vector<int4> w;
   for (int m : order) {
+    if (sel && !sel[m]) continue;
     const int jpi = e->mem[m].jpi, jpj = e->mem[m].jpj;
     for (int J0 = 1; J0 <= jpj; J0 += R)
       for (int c0 = 1; c0 <= jpi; c0 += 30) w.push_back(make_int4(m, c0, J0, std::min(J0 + R - 1, jpj)));
   }
+  return w;
+}
+
+int build_work(nemo_ens* e) {
+  const std::vector<int4> w = work_items(e, nullptr);
   if ((int)w.size() > e->work_cap) {
     if (e->d_work) cudaFree(e->d_work);
     e->d_work = nullptr;
@@ -261,6 +278,24 @@ int ensure_tide(nemo_ens* e, int n) {
   ECK(cudaMallocHost(&e->h_tide, cnt * sizeof(double)));
   e->tide_cap = n;
   drop_graphs(e);  // graphs hold the old table address
+  return NEMO_OK;
+}
+
+// Tidal SSH of every member for steps istp0 .. istp0+n-1 into d_tide,
+// amp*sin(omega_tide*rtime + phase) as original/nemolite2d.f90:629-635.
+int upload_tides(nemo_ens* e, int istp0, int n) {
+  int st = ensure_tide(e, n);
+  if (st) return st;
+  ECK(cudaEventSynchronize(e->tide_ev));  // previous upload has left the pinned buffer
+  const size_t nm = e->mem.size();
+  const double omega_tide = 2.0 * 3.14159 / (12.42 * 3600.0);
+  for (int k = 0; k < n; ++k) {
+    const double rtime = (double)(istp0 + k) * e->common.rdt;
+    for (size_t m = 0; m < nm; ++m)
+      e->h_tide[(size_t)k * nm + m] = e->mem[m].amp_tide * sin(omega_tide * rtime + e->mem[m].tide_phase);
+  }
+  ECK(cudaMemcpyAsync(e->d_tide, e->h_tide, (size_t)n * nm * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+  ECK(cudaEventRecord(e->tide_ev, e->stream));
   return NEMO_OK;
 }
 
@@ -311,6 +346,7 @@ int nemo_ens_destroy(nemo_ens* e) {
   cudaFree(e->slab);
   cudaFree(e->d_mem);
   cudaFree(e->d_work);
+  cudaFree(e->d_work_sub);
   cudaFree(e->d_rows);
   cudaFree(e->d_row_off);
   cudaFree(e->d_row_cnt);
@@ -344,7 +380,7 @@ int nemo_ens_create(const nemo_params* common, const nemo_member* members, int n
   e->C = make_consts(*common);
   e->mem.assign(members, members + nmem);
   e->sched.warps = 2;
-  e->sched.occupancy = -24;
+  e->sched.occupancy = 116;
   e->sched.rows = 16;
   e->sched.order = 1;
   e->sched.ctas = 0;
@@ -469,18 +505,7 @@ int nemo_ens_step_n(nemo_ens* e, int istp0, int n) {
   if (n < 0) return NEMO_ERR_INVALID;
   if (n == 0) return NEMO_OK;
   int st = set_dev(e); if (st) return st;
-  if ((st = ensure_tide(e, n))) return st;
-  // member tides, amp*sin(omega_tide*rtime + phase) as original/nemolite2d.f90:629-635
-  ECK(cudaEventSynchronize(e->tide_ev));  // previous upload has left the pinned buffer
-  const size_t nm = e->mem.size();
-  const double omega_tide = 2.0 * 3.14159 / (12.42 * 3600.0);
-  for (int k = 0; k < n; ++k) {
-    const double rtime = (double)(istp0 + k) * e->common.rdt;
-    for (size_t m = 0; m < nm; ++m)
-      e->h_tide[(size_t)k * nm + m] = e->mem[m].amp_tide * sin(omega_tide * rtime + e->mem[m].tide_phase);
-  }
-  ECK(cudaMemcpyAsync(e->d_tide, e->h_tide, (size_t)n * nm * sizeof(double), cudaMemcpyHostToDevice, e->stream));
-  ECK(cudaEventRecord(e->tide_ev, e->stream));
+  if ((st = upload_tides(e, istp0, n))) return st;
   const int p0 = e->parity;
   if (e->use_graph) {
     auto key = std::make_pair(n, p0);
@@ -620,7 +645,8 @@ int nemo_ens_autotune(nemo_ens* e, int steps, nemo_ens_schedule* best, double* b
   e->use_graph = false;
   nemo_ens_schedule bsched = keep;
   double bms = 1e300;
-  const int warps_occ[][2] = {{2, -24}, {2, -20}, {2, 20}, {2, 24}, {4, -20}, {4, 20}, {4, 24}};
+  const int warps_occ[][2] = {{2, 116}, {2, 120}, {4, 116}, {2, -24}, {2, -20}, {2, 20}, {2, 24},
+                              {4, -20}, {4, 20}, {4, 24}};
   const int rows_c[] = {8, 16, 32};
   cudaEvent_t t0 = nullptr, t1 = nullptr;
   if (er == cudaSuccess) er = cudaEventCreate(&t0);
@@ -681,6 +707,34 @@ int ens_member_state(nemo_ens* e, int m, MemberState* out) {
 }
 
 int ens_member_count(nemo_ens* e) { return e ? (int)e->mem.size() : 0; }
+
+// Advances the members with sel[m] != 0 by n steps (direct launches over a
+// work list of those members only); the others keep their state.  n must be
+// even: every member then still holds its current state in the buffer set
+// the ensemble's parity names.
+int ens_step_subset(nemo_ens* e, int istp0, int n, const char* sel) {
+  if (!e || !sel || n < 0 || (n & 1)) return NEMO_ERR_INVALID;
+  if (n == 0) return NEMO_OK;
+  int st = set_dev(e); if (st) return st;
+  const std::vector<int4> w = work_items(e, sel);
+  if (w.empty()) return NEMO_OK;
+  if ((int)w.size() > e->sub_cap) {
+    ECK(cudaStreamSynchronize(e->stream));
+    if (e->d_work_sub) cudaFree(e->d_work_sub);
+    e->d_work_sub = nullptr;
+    e->sub_cap = 0;
+    ECK(cudaMalloc(&e->d_work_sub, w.size() * sizeof(int4)));
+    e->sub_cap = (int)w.size();
+  }
+  // pageable source: the copy is staged before the call returns
+  ECK(cudaMemcpyAsync(e->d_work_sub, w.data(), w.size() * sizeof(int4), cudaMemcpyHostToDevice, e->stream));
+  if ((st = upload_tides(e, istp0, n))) return st;
+  const size_t nm = e->mem.size();
+  for (int k = 0; k < n; ++k)
+    ECK(launch_ens(e->sched.warps, e->sched.occupancy, e->d_mem, e->d_work_sub, (int)w.size(), e->C,
+                   e->d_tide + (size_t)k * nm, (e->parity + k) & 1, e->sched.ctas, e->stream));
+  return NEMO_OK;
+}
 cudaStream_t ens_stream(nemo_ens* e) { return e->stream; }
 int ens_device(nemo_ens* e) { return e->device; }
 

@@ -16,11 +16,16 @@
 // expression tree up to commutation of + and *, so with contraction off the
 // results are bit-identical to the reference.
 //
-// Divisions by grid constants use the corrected-reciprocal quotient; its
-// operand check is accumulated over a row, and a row in which any lane has a
-// quotient outside the safe exponent range is recomputed with IEEE division
-// (warp-uniform, so the common path stays branch-free).  Divisions by the
-// depth fields are IEEE divisions.
+// Divisions by grid constants and by the static depths use the
+// corrected-reciprocal quotient with host-formed RN(1/b) (RN(1/hu), RN(1/hv)
+// are stored fields).  A row whose three rows of state hold a nonzero value
+// below 2^-300 anywhere in the warp is computed with IEEE division instead
+// (warp-uniform, so the common path stays branch-free); see qdiv.
+//
+// Row staging: PF = 2 (the default schedule) copies every row two rows
+// ahead of its use into a per-warp ring in shared memory with cp.async, so
+// DRAM latency is hidden without registers held for the prefetch; PF = 1
+// prefetches into registers, PF = 0 loads each row one iteration ahead.
 //
 // Masks are those of the reference geometry (walls at ji=0, jpi+1 and
 // jj=jpj+1, open boundary at jj=0), evaluated from the indices.
@@ -44,7 +49,12 @@ k_fused_step(Layout L, Consts C, FusedArgs A, int tile_y) {
   const int J0 = 1 + (int)blockIdx.y * tile_y;
   if (J0 > L.jpj) return;
   const int J1 = min(J0 + tile_y - 1, L.jpj);
-  run_strip<PF>(L, C, A, c0, J0, J1, lane);
+  if constexpr (PF == 2) {
+    __shared__ double ring[NWARPS * RING_DOUBLES];
+    run_strip_ring(L, C, A, c0, J0, J1, lane, ring + (threadIdx.x >> 5) * RING_DOUBLES);
+  } else {
+    run_strip<PF>(L, C, A, c0, J0, J1, lane);
+  }
 }
 
 }  // namespace
@@ -74,11 +84,16 @@ static cudaError_t launch_variant(const Layout& L, const Consts& C, const FusedA
 }
 
 // warps: 2, 4 or 8 per CTA; occ: register budget as resident warps per SM
-// (0: compiler's choice, 16, 20, 24); a negative occ selects the variant
-// without the register prefetch of the next row.
+// (0: compiler's choice, 16, 20, 24) with the register prefetch of the next
+// row; a negative occ: the same budget without it; 100 + budget (116, 120):
+// rows staged through the shared-memory ring.
 cudaError_t launch_fused_step(const Layout& L, const Consts& C, const FusedArgs& a, int warps,
                               int occ, int tile_y, cudaStream_t s) {
   switch (warps * 100 + occ) {
+    case 316: return launch_variant<2, 8, 2>(L, C, a, tile_y, s);
+    case 320: return launch_variant<2, 10, 2>(L, C, a, tile_y, s);
+    case 516: return launch_variant<4, 4, 2>(L, C, a, tile_y, s);
+    case 520: return launch_variant<4, 5, 2>(L, C, a, tile_y, s);
     case 200: return launch_variant<2, 1, 1>(L, C, a, tile_y, s);
     case 216: return launch_variant<2, 8, 1>(L, C, a, tile_y, s);
     case 220: return launch_variant<2, 10, 1>(L, C, a, tile_y, s);
@@ -103,8 +118,9 @@ cudaError_t launch_fused_step(const Layout& L, const Consts& C, const FusedArgs&
 namespace nemo {
 bool fused_variant_ok(int warps, int occ) {
   if (warps == 2) return occ == 0 || occ == 16 || occ == 20 || occ == 24 || occ == -16 ||
-                         occ == -20 || occ == -24;
-  if (warps == 4) return occ == 0 || occ == 16 || occ == 20 || occ == 24 || occ == -20;
+                         occ == -20 || occ == -24 || occ == 116 || occ == 120;
+  if (warps == 4) return occ == 0 || occ == 16 || occ == 20 || occ == 24 || occ == -20 || occ == 116 ||
+                         occ == 120;
   if (warps == 8) return occ == 0 || occ == 16 || occ == 24;
   return false;
 }

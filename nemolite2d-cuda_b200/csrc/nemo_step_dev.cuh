@@ -29,21 +29,37 @@ __device__ __forceinline__ void load_cell(Cell& x, const FusedArgs& A, long o) {
 __device__ __forceinline__ double dn(double x) { return __shfl_down_sync(FULL, x, 1); }
 __device__ __forceinline__ double up(double x) { return __shfl_up_sync(FULL, x, 1); }
 
-// a/b given rb = RN(1/b): the corrected-reciprocal quotient (see div_const)
-// with its range check reduced to what finite states need: `bad` collects
-// nonzero quotients below 2^-959, where the row is redone with IEEE
-// division.  Exact zeros (most of a domain at rest) are exact here.  An
-// infinite or NaN operand gives a non-finite quotient on both paths.
+// a/b given rb = RN(1/b): the corrected-reciprocal quotient (see div_const),
+// exact whenever the quotient is zero or at least 2^-959 in magnitude.  The
+// range is guaranteed per row instead of per quotient (row_tiny): a row whose
+// three rows of state hold no nonzero value below 2^-300 in magnitude has no
+// nonzero quotient below 2^-959.  Every quotient of a row is a sum of terms
+// with at most two state factors (velocity x velocity in the advective
+// fluxes) times grid constants and depths (depth >= hmin > 0); a nonzero
+// difference of state values >= 2^-300 is >= 2^-352 (their ulp), a product
+// of two such >= 2^-704 with ulp >= 2^-756, and a nonzero sum of such terms
+// keeps that grain; the remaining factors are grid constants, rdt, visc,
+// the Coriolis parameter and depths (at 1 km spacing, rdt 20 s: together
+// within 2^-45 of 1), so every nonzero quotient is >= 2^-810, leaving over
+// 140 binades for other grids and coefficients.  Rows outside that
+// guarantee take the IEEE division (SAFE).  An infinite or NaN operand gives
+// a non-finite quotient on both paths.
 template <bool SAFE>
 __device__ __forceinline__ double qdiv(double a, double b, double rb, bool& bad) {
+  (void)bad;
   if (SAFE) return a / b;
   double q = __dmul_rn(a, rb);
-  const unsigned hi2 = (unsigned)__double2hiint(q) << 1;
-  const unsigned lo = (unsigned)__double2loint(q);
-  bad |= (hi2 < (64u << 21)) & ((hi2 | lo) != 0u);
   double r = fma(-q, b, a);
   return -fma(-r, rb, -q);
 }
+
+// Nonzero with |x| < 2^-300 (biased exponent below 723).
+__device__ __forceinline__ bool tiny(double x) {
+  const unsigned hi2 = (unsigned)__double2hiint(x) << 1;
+  const unsigned lo = (unsigned)__double2loint(x);
+  return (hi2 < (723u << 21)) & ((hi2 | lo) != 0u);
+}
+__device__ __forceinline__ bool row_tiny(const Cell& x) { return tiny(x.s) | tiny(x.u) | tiny(x.v); }
 
 __device__ __forceinline__ double interp_u(const Consts& C, int c, int jpi, double s0, double s1,
                                           bool safe, bool& bad) {
@@ -214,7 +230,8 @@ __device__ __forceinline__ void prologue(const Consts& C, int c, int J0, int jpi
 
 // One warp's strip: columns c0 .. c0+29 (lanes 1..30), rows J0 .. J1 of the
 // grid described by L, inputs/outputs in A.  All 32 lanes of the warp must
-// call it together.  PF = 1 prefetches row j+2 into registers.
+// call it together.  PF = 1 prefetches row j+2 into registers (run_strip_ring
+// below stages rows through shared memory instead).
 template <int PF>
 __device__ __forceinline__ void run_strip(const Layout& L, const Consts& C, const FusedArgs& A,
                                           int c0, int J0, int J1, int lane) {
@@ -233,12 +250,14 @@ __device__ __forceinline__ void run_strip(const Layout& L, const Consts& C, cons
   const double sv_stored = (J0 == 1) ? __ldg(A.sshv0 + L.idx(cl, 0)) : 0.0;
   Carry k;
   double sv0;
+  // warp-wide tiny-value flags: bit 0 row j+1 (set as it arrives), bit 1
+  // row j, bit 2 row j-1; row j takes the IEEE form while any is set
+  unsigned hist = (__any_sync(FULL, row_tiny(p)) ? 2u : 0u) | (__any_sync(FULL, row_tiny(cur)) ? 1u : 0u);
   {
     bool bad = false;
-    prologue<false>(C, c, J0, jpi, jpj, sv_stored, p, cur, k, sv0, bad);
-    if (__any_sync(FULL, bad)) prologue<true>(C, c, J0, jpi, jpj, sv_stored, p, cur, k, sv0, bad);
+    if (hist) prologue<true>(C, c, J0, jpi, jpj, sv_stored, p, cur, k, sv0, bad);
+    else prologue<false>(C, c, J0, jpi, jpj, sv_stored, p, cur, k, sv0, bad);
   }
-  const double hv0 = p.hv;
   if (PF) load_cell(nx, A, L.idx(cl, J0 + 1));
 
   const long pitch = L.pitch;
@@ -262,13 +281,13 @@ __device__ __forceinline__ void run_strip(const Layout& L, const Consts& C, cons
 
     RowOut o;
     bool bad = false;
-    if (edge_warp || j == 1 || j == jpj)
+    hist = ((hist << 1) | (__any_sync(FULL, row_tiny(nx)) ? 1u : 0u)) & 7u;
+    if (hist) {
+      row<true, true>(C, c, j, jpi, jpj, A.tide, cur, nx, k, rhu, rhv, o, bad);
+    } else if (edge_warp || j == 1 || j == jpj) {
       row<false, true>(C, c, j, jpi, jpj, A.tide, cur, nx, k, rhu, rhv, o, bad);
-    else
+    } else {
       row<false, false>(C, c, j, jpi, jpj, A.tide, cur, nx, k, rhu, rhv, o, bad);
-    if (__any_sync(FULL, bad)) {
-      bool b2 = false;
-      row<true, true>(C, c, j, jpi, jpj, A.tide, cur, nx, k, rhu, rhv, o, b2);
     }
     if (store) {
       A.ssha[o_st] = o.ssha;
@@ -277,7 +296,8 @@ __device__ __forceinline__ void run_strip(const Layout& L, const Consts& C, cons
       if (edge_warp && c == 1) A.ua[o_st - 1] = 0.0;  // u(0,j), west wall (:650)
       if (j == 1) {
         // Flather open boundary (:684-695): v(c,0) = v(c,1) + sqrt(g/hv(c,0))*(sshn_v(c,0) - sshn_v(c,1))
-        A.va[o_st - pitch] = o.va + sqrt(kG / hv0) * (sv0 - o.sv);
+        const double hv0 = __ldg(A.hv + o_st - pitch), sv0r = __ldg(A.sshv0 + o_st - pitch);
+        A.va[o_st - pitch] = o.va + sqrt(kG / hv0) * (sv0r - o.sv);
       }
     }
     o_st += pitch;
@@ -285,6 +305,113 @@ __device__ __forceinline__ void run_strip(const Layout& L, const Consts& C, cons
     cur = nx;
     if (PF) nx = pf;
   }
+}
+
+// ---- shared-memory ring variant -------------------------------------------
+// Rows are staged by cp.async into a per-warp ring of RING rows x 8 fields x
+// 32 lanes (each lane copies and reads only its own column), two rows ahead
+// of their use, so DRAM latency is hidden without holding prefetched rows in
+// registers.
+constexpr int RING = 3;
+constexpr int RING_DOUBLES = RING * 8 * 32;
+
+__device__ __forceinline__ void cp_async8(double* dst, const double* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+__device__ __forceinline__ void ring_issue(double* slot, const FusedArgs& A, long o) {
+  cp_async8(slot + 0 * 32, A.sshn + o);
+  cp_async8(slot + 1 * 32, A.un + o);
+  cp_async8(slot + 2 * 32, A.vn + o);
+  cp_async8(slot + 3 * 32, A.ht + o);
+  cp_async8(slot + 4 * 32, A.hu + o);
+  cp_async8(slot + 5 * 32, A.hv + o);
+  cp_async8(slot + 6 * 32, A.rhu + o);
+  cp_async8(slot + 7 * 32, A.rhv + o);
+  cp_commit();
+}
+
+__device__ __forceinline__ void ring_cell(Cell& x, const double* slot) {
+  x.s = slot[0 * 32];
+  x.u = slot[1 * 32];
+  x.v = slot[2 * 32];
+  x.ht = slot[3 * 32];
+  x.hu = slot[4 * 32];
+  x.hv = slot[5 * 32];
+}
+
+// run_strip with rows staged through `ring` (this warp's RING_DOUBLES, in
+// shared memory).
+__device__ __forceinline__ void run_strip_ring(const Layout& L, const Consts& C, const FusedArgs& A,
+                                               int c0, int J0, int J1, int lane, double* ring) {
+  const int jpi = L.jpi, jpj = L.jpj;
+  const int c = c0 + lane - 1;
+  const int cl = min(c, jpi + 1);
+  const bool store = (lane >= 1) && (lane <= COLS_PER_WARP) && (c <= jpi);
+  const bool edge_warp = (c0 - 1 <= 1) || (c0 + COLS_PER_WARP >= jpi);
+  double* my = ring + lane;  // this lane's column of every ring row
+
+  const long pitch = L.pitch;
+  const long o_last = L.idx(cl, jpj + 1);
+  // rows J0 and J0+1 into the ring (row r in slot r % RING)
+  ring_issue(my + (J0 % RING) * 256, A, L.idx(cl, J0));
+  ring_issue(my + ((J0 + 1) % RING) * 256, A, L.idx(cl, J0 + 1));
+
+  Cell p, cur, nx;
+  load_cell(p, A, L.idx(cl, J0 - 1));
+  load_cell(cur, A, L.idx(cl, J0));
+  const double sv_stored = (J0 == 1) ? __ldg(A.sshv0 + L.idx(cl, 0)) : 0.0;
+  Carry k;
+  double sv0;
+  unsigned hist = (__any_sync(FULL, row_tiny(p)) ? 2u : 0u) | (__any_sync(FULL, row_tiny(cur)) ? 1u : 0u);
+  {
+    bool bad = false;
+    if (hist) prologue<true>(C, c, J0, jpi, jpj, sv_stored, p, cur, k, sv0, bad);
+    else prologue<false>(C, c, J0, jpi, jpj, sv_stored, p, cur, k, sv0, bad);
+  }
+  long o_ld = L.idx(cl, J0 + 2);
+  long o_st = L.idx(c, J0);
+  int slot_j = J0 % RING;
+#pragma unroll 1
+  for (int j = J0; j <= J1; ++j) {
+    const int slot_n = slot_j == RING - 1 ? 0 : slot_j + 1;      // row j+1
+    const int slot_f = slot_n == RING - 1 ? 0 : slot_n + 1;      // row j+2 (was row j-1)
+    ring_issue(my + slot_f * 256, A, o_ld < o_last ? o_ld : o_last);
+    o_ld += pitch;
+    cp_wait1();  // rows <= j+1 have landed
+    ring_cell(nx, my + slot_n * 256);
+    const double rhu = my[slot_j * 256 + 6 * 32];
+    const double rhv = my[slot_j * 256 + 7 * 32];
+
+    RowOut o;
+    bool bad = false;
+    hist = ((hist << 1) | (__any_sync(FULL, row_tiny(nx)) ? 1u : 0u)) & 7u;
+    if (hist) {
+      row<true, true>(C, c, j, jpi, jpj, A.tide, cur, nx, k, rhu, rhv, o, bad);
+    } else if (edge_warp || j == 1 || j == jpj) {
+      row<false, true>(C, c, j, jpi, jpj, A.tide, cur, nx, k, rhu, rhv, o, bad);
+    } else {
+      row<false, false>(C, c, j, jpi, jpj, A.tide, cur, nx, k, rhu, rhv, o, bad);
+    }
+    if (store) {
+      A.ssha[o_st] = o.ssha;
+      A.ua[o_st] = o.ua;
+      A.va[o_st] = o.va;
+      if (edge_warp && c == 1) A.ua[o_st - 1] = 0.0;
+      if (j == 1) {  // Flather open boundary, as in run_strip
+        const double hv0 = __ldg(A.hv + o_st - pitch), sv0r = __ldg(A.sshv0 + o_st - pitch);
+        A.va[o_st - pitch] = o.va + sqrt(kG / hv0) * (sv0r - o.sv);
+      }
+    }
+    o_st += pitch;
+    k = o.next;
+    cur = nx;
+    slot_j = slot_n;
+  }
+  asm volatile("cp.async.wait_all;" ::: "memory");  // no copy may outlive the strip's ring use
 }
 
 }  // namespace stepdev

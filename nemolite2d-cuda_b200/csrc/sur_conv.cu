@@ -218,8 +218,11 @@ __device__ __forceinline__ void epilogue_store(const ConvEpi& E, const float* bi
     for (int c = 0; c < 64; ++c) v[c] = fmaxf(v[c], 0.0f);
   }
   if (E.out32) {
-    float4* o32 = reinterpret_cast<float4*>(E.out32 + p * 4);
-    *o32 = make_float4(v[0], v[1], v[2], v[3]);
+    const int nq = E.out32_ch > 0 ? E.out32_ch >> 2 : 1;
+    float4* o32 = reinterpret_cast<float4*>(E.out32 + p * (4 * nq));
+#pragma unroll
+    for (int g = 0; g < 16; ++g)
+      if (g < nq) o32[g] = make_float4(v[4 * g], v[4 * g + 1], v[4 * g + 2], v[4 * g + 3]);
   }
   if (E.out) {
     uint4* op = reinterpret_cast<uint4*>(E.out + p * CH);
@@ -702,7 +705,8 @@ cudaError_t prepare_device(int* sms) {
 }  // namespace
 
 cudaError_t conv_fwd(const __nv_bfloat16* x, const __nv_bfloat16* w, const ConvEpi& epi, cudaStream_t s) {
-  if (epi.W % TM != 0 || epi.W < TM || epi.N < 1 || epi.H < 1 || !x || !w || !epi.err)
+  if (epi.W % TM != 0 || epi.W < TM || epi.N < 1 || epi.H < 1 || !x || !w || !epi.err ||
+      epi.out32_ch < 0 || epi.out32_ch > 64 || epi.out32_ch % 4 != 0)
     return cudaErrorInvalidValue;
   if ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(w) | reinterpret_cast<uintptr_t>(epi.out) |
        reinterpret_cast<uintptr_t>(epi.out32) | reinterpret_cast<uintptr_t>(epi.residual) |

@@ -11,7 +11,8 @@ namespace sur {
 
 // Fused epilogue of a 3x3 convolution (64 -> 64 channels, NHWC BF16):
 //   v = acc + bias; v += residual; v *= (mask > 0); v = max(v, 0) if relu;
-//   out <- bf16(v) (64 channels), out32 <- v[0:4] (FP32, 4 per pixel).
+//   out <- bf16(v) (64 channels), out32 <- v[0:out32_ch] (FP32, out32_ch per
+//   pixel; out32_ch a multiple of 4 up to 64, 0 meaning 4).
 // Every pointer but err may be null.
 struct ConvEpi {
   const float* bias;
@@ -22,6 +23,7 @@ struct ConvEpi {
   int relu;
   int N, H, W;
   int* err;  // device flag, first failing wait's code
+  int out32_ch;
 };
 
 // dw[tap][co][ci] += sum_p dz[p][co] x[p + off(tap)][ci]; db[co] += sum_p dz[p][co].
@@ -54,6 +56,8 @@ struct MemberState {
 };
 int ens_member_state(nemo_ens* e, int m, MemberState* out);
 int ens_member_count(nemo_ens* e);
+// Advances only the members with sel[m] != 0 by an even number n of steps.
+int ens_step_subset(nemo_ens* e, int istp0, int n, const char* sel);
 cudaStream_t ens_stream(nemo_ens* e);
 int ens_device(nemo_ens* e);
 // Tidal SSH a member's boundary row holds after step istp.

@@ -7,11 +7,19 @@
 //   h0 = relu(conv_0(x0) + b_0)
 //   t_i = relu(conv_{2i+1}(h_i) + b), h_{i+1} = h_i + conv_{2i+2}(t_i) + b   (i < nblocks)
 //   y = conv_{L-1}(h_nb) + b           (channels 0-2: normalised 10-step deltas)
-// Input channels of a T-cell (ji, jj) = pixel (ji-1, jj-1): 0 ssh, 1 u on the
-// cell's west face u(ji-1, jj), 2 v on its south face v(ji, jj-1), 3 depth,
-// 4 open-boundary row flag, 5 the boundary row's tidal SSH at the target
-// time; 6-63 zero.  Parameters are FP32 masters with BF16 copies (and the
-// tap-flipped transposes the data gradient needs) refreshed by AdamW.
+// The network runs on a grid of P x P patches of T-cells (P = 1, 2 or 4, the
+// `patch` of the configuration): network pixel (X, Y) holds T-cells
+// (ji, jj) = (P*X + sx + 1, P*Y + sy + 1), sub-cell k = P*sy + sx.  Input
+// channels: ssh at k, u on the cell's west face u(ji-1, jj) at P^2 + k, v on
+// its south face v(ji, jj-1) at 2 P^2 + k; depth (P = 1: channel 3; else the
+// means over the four (P/2 x P/2) quadrants, channels 3 P^2 .. 3 P^2 + 3);
+// then the open-boundary row flag and the boundary row's tidal SSH at the
+// target time on network row 0; the rest zero.  Output channel f P^2 + k is
+// the normalised 10-step delta of field f (ssh, u, v) at sub-cell k; the FP32
+// output holds 4 channels per pixel for P = 1, 3 P^2 otherwise.  A patch of
+// 4 runs the same network on 1/16 of the pixels.  Parameters are FP32
+// masters with BF16 copies (and the tap-flipped transposes the data gradient
+// needs) refreshed by AdamW.
 #include <math.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -59,28 +67,55 @@ __device__ __forceinline__ uint4 pack8(const float* f) {
   return u;
 }
 
-// x0 from FP32 snapshots (ssh, u_west, v_south, depth) and per-image tides.
+// FP32 output channels per network pixel
+__host__ __device__ constexpr int out_channels(int P) { return P == 1 ? 4 : 3 * P * P; }
+// first channel after the depth channels: the boundary flag, then the tide
+__host__ __device__ constexpr int flag_channel(int P) { return P == 1 ? 4 : 3 * P * P + 4; }
+
+// x0 from FP32 snapshots (ssh, u_west, v_south, depth per T-cell, layout
+// [n][H][W]) and per-image tides, over nnet = n * (H/P) * (W/P) network pixels.
+template <int P>
 __global__ void k_make_input(const float4* __restrict__ snap, const float* __restrict__ tide, Norm nm,
-                             uint4* __restrict__ x0, long npix, int H, int W) {
-  for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < npix; p += (long)gridDim.x * blockDim.x) {
-    const float4 s = snap[p];
-    const long img = p / ((long)H * W);
-    const int y = (int)((p / W) % H);
-    float f[8];
-    f[0] = (s.x - nm.in_shift[0]) * nm.in_scale[0];
-    f[1] = (s.y - nm.in_shift[1]) * nm.in_scale[1];
-    f[2] = (s.z - nm.in_shift[2]) * nm.in_scale[2];
-    f[3] = (s.w - nm.in_shift[3]) * nm.in_scale[3];
-    f[4] = y == 0 ? 1.0f : 0.0f;
-    f[5] = y == 0 ? (tide[img] - nm.in_shift[0]) * nm.in_scale[0] : 0.0f;
-    f[6] = 0.0f;
-    f[7] = 0.0f;
-    uint4* o = x0 + p * 8;
-    o[0] = pack8(f);
-    const uint4 z = make_uint4(0, 0, 0, 0);
+                             uint4* __restrict__ x0, long nnet, int H, int W) {
+  const int Hn = H / P, Wn = W / P;
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < nnet; q += (long)gridDim.x * blockDim.x) {
+    const long img = q / ((long)Hn * Wn);
+    const int Y = (int)((q / Wn) % Hn), X = (int)(q % Wn);
+    float f[CH];
 #pragma unroll
-    for (int g = 1; g < 8; ++g) o[g] = z;
+    for (int c = 0; c < CH; ++c) f[c] = 0.0f;
+    float dq[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+    for (int sy = 0; sy < P; ++sy)
+#pragma unroll
+      for (int sx = 0; sx < P; ++sx) {
+        const float4 v = snap[(img * H + (long)(P * Y + sy)) * W + P * X + sx];
+        const int k = P * sy + sx;
+        f[k] = (v.x - nm.in_shift[0]) * nm.in_scale[0];
+        f[P * P + k] = (v.y - nm.in_shift[1]) * nm.in_scale[1];
+        f[2 * P * P + k] = (v.z - nm.in_shift[2]) * nm.in_scale[2];
+        dq[P == 1 ? 0 : 2 * (2 * sy / P) + (2 * sx / P)] += (v.w - nm.in_shift[3]) * nm.in_scale[3];
+      }
+    if (P == 1) {
+      f[3] = dq[0];
+    } else {
+#pragma unroll
+      for (int i = 0; i < 4; ++i) f[3 * P * P + i] = dq[i] * (4.0f / (float)(P * P));
+    }
+    f[flag_channel(P)] = Y == 0 ? 1.0f : 0.0f;
+    f[flag_channel(P) + 1] = Y == 0 ? (tide[img] - nm.in_shift[0]) * nm.in_scale[0] : 0.0f;
+    uint4* o = x0 + q * 8;
+#pragma unroll
+    for (int g = 0; g < 8; ++g) o[g] = pack8(f + 8 * g);
   }
+}
+
+// Index of output channel (field f, T-cell (x, y) of image img) in the FP32
+// network output.
+template <int P>
+__device__ __forceinline__ long out_index(long img, int y, int x, int Hn, int Wn, int f) {
+  const long q = (img * Hn + y / P) * Wn + x / P;
+  return q * out_channels(P) + f * P * P + (y % P) * P + (x % P);
 }
 
 // Normalised 10-step deltas (channels 0-2; channel 3 zero).
@@ -106,22 +141,38 @@ __device__ __forceinline__ double block_sum_d(double v, double* sh) {
   return t;
 }
 
-// Mean squared error over channels 0-2 and its gradient (BF16, 64 channels).
-__global__ void __launch_bounds__(256) k_loss(const float4* __restrict__ out, const float4* __restrict__ tgt,
-                                              uint4* __restrict__ dout, double* __restrict__ loss, long npix,
-                                              float gscale) {
+// Mean squared error of the deltas against targets tgt ([n][H][W] float4,
+// channels 0-2) and its gradient (BF16, 64 channels per network pixel).
+template <int P>
+__global__ void __launch_bounds__(256) k_loss(const float* __restrict__ out, const float4* __restrict__ tgt,
+                                              uint4* __restrict__ dout, double* __restrict__ loss, long nnet,
+                                              int H, int W, float gscale) {
   __shared__ double sh[8];
+  constexpr int NO = out_channels(P);
+  const int Hn = H / P, Wn = W / P;
   double acc = 0.0;
-  for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < npix; p += (long)gridDim.x * blockDim.x) {
-    const float4 o = out[p], t = tgt[p];
-    const float d0 = o.x - t.x, d1 = o.y - t.y, d2 = o.z - t.z;
-    acc += (double)d0 * d0 + (double)d1 * d1 + (double)d2 * d2;
-    float f[8] = {2.0f * gscale * d0, 2.0f * gscale * d1, 2.0f * gscale * d2, 0, 0, 0, 0, 0};
-    uint4* g = dout + p * 8;
-    g[0] = pack8(f);
-    const uint4 z = make_uint4(0, 0, 0, 0);
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < nnet; q += (long)gridDim.x * blockDim.x) {
+    const long img = q / ((long)Hn * Wn);
+    const int Y = (int)((q / Wn) % Hn), X = (int)(q % Wn);
+    float f[CH];
 #pragma unroll
-    for (int k = 1; k < 8; ++k) g[k] = z;
+    for (int c = 0; c < CH; ++c) f[c] = 0.0f;
+#pragma unroll
+    for (int sy = 0; sy < P; ++sy)
+#pragma unroll
+      for (int sx = 0; sx < P; ++sx) {
+        const int k = P * sy + sx;
+        const float4 t = tgt[(img * H + (long)(P * Y + sy)) * W + P * X + sx];
+        const float d0 = out[q * NO + k] - t.x, d1 = out[q * NO + P * P + k] - t.y,
+                    d2 = out[q * NO + 2 * P * P + k] - t.z;
+        acc += (double)d0 * d0 + (double)d1 * d1 + (double)d2 * d2;
+        f[k] = 2.0f * gscale * d0;
+        f[P * P + k] = 2.0f * gscale * d1;
+        f[2 * P * P + k] = 2.0f * gscale * d2;
+      }
+    uint4* g = dout + q * 8;
+#pragma unroll
+    for (int e = 0; e < 8; ++e) g[e] = pack8(f + 8 * e);
   }
   const double s = block_sum_d<256>(acc, sh);
   if (threadIdx.x == 0) atomicAdd(loss, s);
@@ -184,15 +235,18 @@ __global__ void k_pack(const MemberState* __restrict__ ms, int m0, int nm, int H
 
 // state += delta / out_scale; the boundary row takes the exact tidal SSH;
 // u(0, :), u(jpi, :) and v(:, jpj) (walls) are left at zero.
+template <int P>
 __global__ void k_apply(const MemberState* __restrict__ ms, int m0, int nm, int H, int W,
-                        const float4* __restrict__ out, Norm nm_, const double* __restrict__ tide) {
+                        const float* __restrict__ out, Norm nm_, const double* __restrict__ tide) {
   const long npix = (long)nm * H * W;
+  const int Hn = H / P, Wn = W / P;
   for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < npix; p += (long)gridDim.x * blockDim.x) {
     const int m = (int)(p / ((long)H * W));
     const int y = (int)((p / W) % H), x = (int)(p % W);
     const MemberState& M = ms[m0 + m];
     const int ji = x + 1, jj = y + 1;
-    const float4 d = out[p];
+    const float4 d = make_float4(out[out_index<P>(m, y, x, Hn, Wn, 0)], out[out_index<P>(m, y, x, Hn, Wn, 1)],
+                                 out[out_index<P>(m, y, x, Hn, Wn, 2)], 0.0f);
     double* s = M.sshn + gidx(M.pitch, ji, jj);
     *s = (jj == 1) ? tide[m0 + m] : *s + (double)(d.x / nm_.out_scale[0]);
     if (ji >= 2) {
@@ -206,8 +260,9 @@ __global__ void k_apply(const MemberState* __restrict__ ms, int m0, int nm, int 
 
 // Per member: sum (pred - ref)^2 and sum ref^2 for ssh, u, v (acc[m][6]).
 // pred = snap + delta / out_scale when out != null, else the state of `pm`.
+template <int P>
 __global__ void __launch_bounds__(256) k_err(const MemberState* __restrict__ ref, const float4* __restrict__ snap,
-                                             const float4* __restrict__ out, Norm nm_,
+                                             const float* __restrict__ out, Norm nm_,
                                              const MemberState* __restrict__ pm, int m0, int H, int W,
                                              double* __restrict__ acc) {
   __shared__ double sh[8];
@@ -224,15 +279,18 @@ __global__ void __launch_bounds__(256) k_err(const MemberState* __restrict__ ref
     double ps, pu, pv;
     if (out) {
       const long p = (long)m * np + q;
-      const float4 s = snap[p], d = out[p];
+      const int Hn = H / P, Wn = W / P;
+      const float4 s = snap[p];
+      const float4 d = make_float4(out[out_index<P>(m, y, x, Hn, Wn, 0)], out[out_index<P>(m, y, x, Hn, Wn, 1)],
+                                   out[out_index<P>(m, y, x, Hn, Wn, 2)], 0.0f);
       ps = (jj == 1) ? rs : (double)s.x + (double)(d.x / nm_.out_scale[0]);
       pu = (ji >= 2) ? (double)s.y + (double)(d.y / nm_.out_scale[1]) : 0.0;
       pv = (double)s.z + (double)(d.z / nm_.out_scale[2]);
     } else {
-      const MemberState& P = pm[m0 + m];
-      ps = P.sshn[gidx(P.pitch, ji, jj)];
-      pu = P.un[gidx(P.pitch, ji - 1, jj)];
-      pv = P.vn[gidx(P.pitch, ji, jj - 1)];
+      const MemberState& Q = pm[m0 + m];
+      ps = Q.sshn[gidx(Q.pitch, ji, jj)];
+      pu = Q.un[gidx(Q.pitch, ji - 1, jj)];
+      pv = Q.vn[gidx(Q.pitch, ji, jj - 1)];
     }
     a[0] += (ps - rs) * (ps - rs);
     a[1] += rs * rs;
@@ -271,7 +329,10 @@ struct nemo_sur {
   nemo_sur_config cfg{};
   int L = 0;
   long np = 0, nw = 0;          // parameters, of which weights
-  long npix = 0;                 // batch * H * W
+  long npix = 0;                 // batch * H * W (T-cells)
+  int P = 1, Hn = 0, Wn = 0;     // patch and network grid (H/P x W/P)
+  int NO = 4;                    // FP32 output channels per network pixel
+  long nnet = 0;                 // batch * Hn * Wn (network pixels)
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   Norm norm{};
@@ -284,7 +345,7 @@ struct nemo_sur {
   std::vector<__nv_bfloat16*> act;  // activation tensors
   __nv_bfloat16 *x0 = nullptr, *dout = nullptr, *g0 = nullptr, *g1 = nullptr, *dt = nullptr;
   std::vector<__nv_bfloat16*> h, t;
-  float* out32 = nullptr;        // [batch][H][W][4]
+  float* out32 = nullptr;        // [batch][Hn][Wn][NO]
   float* tgt = nullptr;
   float* snap = nullptr;         // [batch][H][W][4] (ensemble calls)
   float* tide_f = nullptr;       // [batch]
@@ -315,15 +376,65 @@ int set_dev(nemo_sur* s) {
 
 int conv(nemo_sur* s, const __nv_bfloat16* x, const __nv_bfloat16* w, const float* bias,
          const __nv_bfloat16* res, const __nv_bfloat16* mask, int relu, __nv_bfloat16* out, float* out32, int n) {
-  sur::ConvEpi e{bias, res, mask, out, out32, relu, n, s->cfg.height, s->cfg.width, s->err};
+  sur::ConvEpi e{bias, res, mask, out, out32, relu, n, s->Hn, s->Wn, s->err, out32 ? s->NO : 0};
   ECK(sur::conv_fwd(x, w, e, s->stream));
   return NEMO_OK;
 }
 
 int wgrad(nemo_sur* s, const __nv_bfloat16* x, const __nv_bfloat16* dz, int l, int n) {
-  sur::WgradArgs a{dW_of(s, l), dB_of(s, l), n, s->cfg.height, s->cfg.width, s->err};
+  sur::WgradArgs a{dW_of(s, l), dB_of(s, l), n, s->Hn, s->Wn, s->err};
   ECK(sur::conv_wgrad(x, dz, a, 0, s->stream));
   return NEMO_OK;
+}
+
+// Launches of the patch-templated kernels for the surrogate's patch.
+cudaError_t make_input(nemo_sur* s, const float* snap, const float* tide, int n) {
+  const long nn = (long)n * s->Hn * s->Wn;
+  const int H = s->cfg.height, W = s->cfg.width, g = grid_for(nn, 256);
+  const float4* sp = reinterpret_cast<const float4*>(snap);
+  uint4* x0 = reinterpret_cast<uint4*>(s->x0);
+  switch (s->P) {
+    case 1: k_make_input<1><<<g, 256, 0, s->stream>>>(sp, tide, s->norm, x0, nn, H, W); break;
+    case 2: k_make_input<2><<<g, 256, 0, s->stream>>>(sp, tide, s->norm, x0, nn, H, W); break;
+    default: k_make_input<4><<<g, 256, 0, s->stream>>>(sp, tide, s->norm, x0, nn, H, W); break;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_loss(nemo_sur* s, int n, long npix) {
+  const long nn = (long)n * s->Hn * s->Wn;
+  const int H = s->cfg.height, W = s->cfg.width, g = grid_for(nn, 256);
+  const float gs = (float)(1.0 / (3.0 * (double)npix));
+  const float4* t = reinterpret_cast<const float4*>(s->tgt);
+  uint4* d = reinterpret_cast<uint4*>(s->dout);
+  switch (s->P) {
+    case 1: k_loss<1><<<g, 256, 0, s->stream>>>(s->out32, t, d, s->loss, nn, H, W, gs); break;
+    case 2: k_loss<2><<<g, 256, 0, s->stream>>>(s->out32, t, d, s->loss, nn, H, W, gs); break;
+    default: k_loss<4><<<g, 256, 0, s->stream>>>(s->out32, t, d, s->loss, nn, H, W, gs); break;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_apply(nemo_sur* s, int m0, int n, const float* out) {
+  const int H = s->cfg.height, W = s->cfg.width, g = grid_for((long)n * H * W, 256);
+  switch (s->P) {
+    case 1: k_apply<1><<<g, 256, 0, s->stream>>>(s->d_ms, m0, n, H, W, out, s->norm, s->tide_d); break;
+    case 2: k_apply<2><<<g, 256, 0, s->stream>>>(s->d_ms, m0, n, H, W, out, s->norm, s->tide_d); break;
+    default: k_apply<4><<<g, 256, 0, s->stream>>>(s->d_ms, m0, n, H, W, out, s->norm, s->tide_d); break;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_err(nemo_sur* s, int nm, const float* snap, const float* out) {
+  const int H = s->cfg.height, W = s->cfg.width;
+  const dim3 g((unsigned)(grid_for((long)H * W, 256) / 16 + 1), (unsigned)nm);
+  const float4* sp = reinterpret_cast<const float4*>(snap);
+  switch (s->P) {
+    case 1: k_err<1><<<g, 256, 0, s->stream>>>(s->d_ms, sp, out, s->norm, nullptr, 0, H, W, s->d_acc); break;
+    case 2: k_err<2><<<g, 256, 0, s->stream>>>(s->d_ms, sp, out, s->norm, nullptr, 0, H, W, s->d_acc); break;
+    default: k_err<4><<<g, 256, 0, s->stream>>>(s->d_ms, sp, out, s->norm, nullptr, 0, H, W, s->d_acc); break;
+  }
+  return cudaGetLastError();
 }
 
 // Forward from x0 over n images; training keeps every activation.
@@ -381,21 +492,14 @@ int check_err(nemo_sur* s) {
 int loss_grad(nemo_sur* s, const float* snap0, const float* snap1, const float* tide, int n, double* loss) {
   if (n < 1 || n > s->cfg.batch || !snap0 || !snap1 || !tide || !s->cfg.train) return NEMO_ERR_INVALID;
   const long npix = (long)n * s->cfg.height * s->cfg.width;
-  k_make_input<<<grid_for(npix, 256), 256, 0, s->stream>>>(reinterpret_cast<const float4*>(snap0), tide, s->norm,
-                                                         reinterpret_cast<uint4*>(s->x0), npix, s->cfg.height,
-                                                         s->cfg.width);
-  ECK(cudaGetLastError());
+  ECK(make_input(s, snap0, tide, n));
   k_make_target<<<grid_for(npix, 256), 256, 0, s->stream>>>(reinterpret_cast<const float4*>(snap0),
                                                           reinterpret_cast<const float4*>(snap1), s->norm,
                                                           reinterpret_cast<float4*>(s->tgt), npix);
   ECK(cudaGetLastError());
   SCK(forward(s, n, true, s->out32));
   ECK(cudaMemsetAsync(s->loss, 0, sizeof(double), s->stream));
-  k_loss<<<grid_for(npix, 256), 256, 0, s->stream>>>(reinterpret_cast<const float4*>(s->out32),
-                                                   reinterpret_cast<const float4*>(s->tgt),
-                                                   reinterpret_cast<uint4*>(s->dout), s->loss, npix,
-                                                   (float)(1.0 / (3.0 * (double)npix)));
-  ECK(cudaGetLastError());
+  ECK(launch_loss(s, n, npix));
   SCK(backward(s, n));
   ECK(cudaMemcpyAsync(s->h_loss, s->loss, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
   SCK(check_err(s));
@@ -459,10 +563,33 @@ int predict_chunk(nemo_sur* s, int m0, int n, const std::vector<double>& tide_ne
   ECK(cudaMemcpyAsync(s->tide_f, tf.data(), n * sizeof(float), cudaMemcpyHostToDevice, s->stream));
   k_pack<<<grid_for(npix, 256), 256, 0, s->stream>>>(s->d_ms, m0, n, H, W, reinterpret_cast<float4*>(snap_dst));
   ECK(cudaGetLastError());
-  k_make_input<<<grid_for(npix, 256), 256, 0, s->stream>>>(reinterpret_cast<const float4*>(snap_dst), s->tide_f,
-                                                         s->norm, reinterpret_cast<uint4*>(s->x0), npix, H, W);
-  ECK(cudaGetLastError());
+  ECK(make_input(s, snap_dst, s->tide_f, n));
   return forward(s, n, false, out_dst);
+}
+
+// One surrogate call for the members of ms with sel[m] != 0 (all if sel is
+// null): each advances from its current state to step istp_end.  Leaves the
+// selected members' table in d_ms.
+int advance_members(nemo_sur* s, nemo_ens* e, const std::vector<MemberState>& ms, const char* sel,
+                    int istp_end) {
+  std::vector<MemberState> sub;
+  std::vector<double> tide;
+  for (int m = 0; m < (int)ms.size(); ++m)
+    if (!sel || sel[m]) {
+      sub.push_back(ms[m]);
+      tide.push_back(nemo::ens_tide(e, m, istp_end));
+    }
+  const int n_sel = (int)sub.size();
+  if (n_sel == 0) return NEMO_OK;
+  // pageable sources: staged before the calls return
+  ECK(cudaMemcpyAsync(s->d_ms, sub.data(), n_sel * sizeof(MemberState), cudaMemcpyHostToDevice, s->stream));
+  ECK(cudaMemcpyAsync(s->tide_d, tide.data(), n_sel * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  for (int m0 = 0; m0 < n_sel; m0 += s->cfg.batch) {
+    const int n = n_sel - m0 < s->cfg.batch ? n_sel - m0 : s->cfg.batch;
+    SCK(predict_chunk(s, m0, n, tide, s->snap, s->out32));
+    ECK(launch_apply(s, m0, n, s->out32));
+  }
+  return NEMO_OK;
 }
 
 }  // namespace
@@ -480,6 +607,7 @@ int nemo_sur_default_config(nemo_sur_config* c) {
   c->seed = 1234;
   c->stream = nullptr;
   c->device = -1;
+  c->patch = 1;
   return NEMO_OK;
 }
 
@@ -513,8 +641,9 @@ int nemo_sur_destroy(nemo_sur* s) {
 int nemo_sur_create(const nemo_sur_config* c, nemo_sur** out) {
   if (!c || !out) return NEMO_ERR_INVALID;
   *out = nullptr;
-  if (c->nblocks < 0 || c->nblocks > 64 || c->batch < 1 || c->height < 1 || c->width < 128 ||
-      c->width % 128 != 0)
+  const int P = c->patch == 0 ? 1 : c->patch;
+  if (c->nblocks < 0 || c->nblocks > 64 || c->batch < 1 || (P != 1 && P != 2 && P != 4) || c->height < P ||
+      c->height % P != 0 || c->width % P != 0 || c->width / P < 128 || (c->width / P) % 128 != 0)
     return NEMO_ERR_INVALID;
   nemo_sur* s = new (std::nothrow) nemo_sur;
   if (!s) return NEMO_ERR_ALLOC;
@@ -522,7 +651,13 @@ int nemo_sur_create(const nemo_sur_config* c, nemo_sur** out) {
   s->L = 2 * c->nblocks + 2;
   s->nw = (long)s->L * WL;
   s->np = s->nw + (long)s->L * CH;
+  s->cfg.patch = P;
   s->npix = (long)c->batch * c->height * c->width;
+  s->P = P;
+  s->Hn = c->height / P;
+  s->Wn = c->width / P;
+  s->NO = out_channels(P);
+  s->nnet = (long)c->batch * s->Hn * s->Wn;
   for (int k = 0; k < 4; ++k) {
     s->norm.in_scale[k] = 1.0f;
     s->norm.in_shift[k] = 0.0f;
@@ -545,7 +680,7 @@ int nemo_sur_create(const nemo_sur_config* c, nemo_sur** out) {
       cudaMallocHost(&s->h_loss, sizeof(double)))
     return fail(NEMO_ERR_ALLOC);
   if (c->train && (cudaMalloc(&s->m, pb) || cudaMalloc(&s->v, pb))) return fail(NEMO_ERR_ALLOC);
-  const size_t ab = (size_t)s->npix * CH * 2;
+  const size_t ab = (size_t)s->nnet * CH * 2;
   const int nact = c->train ? 1 + (c->nblocks + 1) + c->nblocks + 4 : 4;
   for (int i = 0; i < nact; ++i) {
     __nv_bfloat16* a = nullptr;
@@ -562,7 +697,7 @@ int nemo_sur_create(const nemo_sur_config* c, nemo_sur** out) {
     s->g1 = s->act[k++];
     s->dt = s->act[k++];
   }
-  if (cudaMalloc(&s->out32, s->npix * 16) || cudaMalloc(&s->snap, s->npix * 16) ||
+  if (cudaMalloc(&s->out32, s->nnet * s->NO * sizeof(float)) || cudaMalloc(&s->snap, s->npix * 16) ||
       cudaMalloc(&s->tide_f, c->batch * sizeof(float)))
     return fail(NEMO_ERR_ALLOC);
   if (c->train && cudaMalloc(&s->tgt, s->npix * 16)) return fail(NEMO_ERR_ALLOC);
@@ -595,7 +730,7 @@ int nemo_sur_create(const nemo_sur_config* c, nemo_sur** out) {
 int nemo_sur_info(nemo_sur* s, long long* nparams, long long* flops_per_pixel) {
   if (!s) return NEMO_ERR_STATE;
   if (nparams) *nparams = s->np;
-  if (flops_per_pixel) *flops_per_pixel = (long long)s->L * 2 * WL;
+  if (flops_per_pixel) *flops_per_pixel = (long long)s->L * 2 * WL / ((long long)s->P * s->P);
   return NEMO_OK;
 }
 
@@ -648,11 +783,7 @@ int nemo_sur_get_norm(nemo_sur* s, float* norm11) {
 int nemo_sur_predict(nemo_sur* s, const float* snap, const float* tide, int n, float* out) {
   if (!s || !snap || !tide || n < 1 || n > s->cfg.batch) return NEMO_ERR_INVALID;
   SCK(set_dev(s));
-  const long npix = (long)n * s->cfg.height * s->cfg.width;
-  k_make_input<<<grid_for(npix, 256), 256, 0, s->stream>>>(reinterpret_cast<const float4*>(snap), tide, s->norm,
-                                                         reinterpret_cast<uint4*>(s->x0), npix, s->cfg.height,
-                                                         s->cfg.width);
-  ECK(cudaGetLastError());
+  ECK(make_input(s, snap, tide, n));
   SCK(forward(s, n, false, out ? out : s->out32));
   return check_err(s);
 }
@@ -706,18 +837,7 @@ int nemo_sur_advance_ens(nemo_sur* s, nemo_ens* e, int istp_end) {
   std::vector<MemberState> ms;
   SCK(join(nemo::ens_stream(e), s->stream));
   SCK(ensure_members(s, e, ms, nullptr));
-  const int nm = (int)ms.size();
-  std::vector<double> tide(nm);
-  for (int i = 0; i < nm; ++i) tide[i] = nemo::ens_tide(e, i, istp_end);
-  ECK(cudaMemcpyAsync(s->tide_d, tide.data(), nm * sizeof(double), cudaMemcpyHostToDevice, s->stream));
-  for (int m0 = 0; m0 < nm; m0 += s->cfg.batch) {
-    const int n = nm - m0 < s->cfg.batch ? nm - m0 : s->cfg.batch;
-    SCK(predict_chunk(s, m0, n, tide, s->snap, s->out32));
-    const long npix = (long)n * s->cfg.height * s->cfg.width;
-    k_apply<<<grid_for(npix, 256), 256, 0, s->stream>>>(s->d_ms, m0, n, s->cfg.height, s->cfg.width,
-                                                      reinterpret_cast<const float4*>(s->out32), s->norm, s->tide_d);
-    ECK(cudaGetLastError());
-  }
+  SCK(advance_members(s, e, ms, nullptr, istp_end));
   SCK(check_err(s));
   return join(s->stream, nemo::ens_stream(e));
 }
@@ -748,7 +868,7 @@ int nemo_ens_compare(nemo_ens* a, nemo_ens* ref, double* out) {
     // one launch per member (sizes differ)
     for (int m = 0; m < nm && e == cudaSuccess; ++m) {
       Norm dummy{};
-      k_err<<<dim3((unsigned)grid_for((long)ma[m].jpi * ma[m].jpj, 256) / 16 + 1, 1), 256, 0, st>>>(
+      k_err<1><<<dim3((unsigned)grid_for((long)ma[m].jpi * ma[m].jpj, 256) / 16 + 1, 1), 256, 0, st>>>(
           dr, nullptr, nullptr, dummy, da, m, ma[m].jpj, ma[m].jpi, acc);
       e = cudaGetLastError();
     }
@@ -772,19 +892,23 @@ int nemo_hyb_default_config(nemo_hyb_config* c) {
   c->k = 10;
   c->anchor = 100;
   c->tol = 0.01;
+  c->per_member = 1;
   return NEMO_OK;
 }
 
 // Advances e from the state after step istp0 by nsteps (a multiple of
 // anchor, anchor a multiple of k).  Each anchor window: the surrogate
-// predicts the first k steps, the FP64 solver runs them (the shadow step and
-// the re-anchored state), and if any member's relative SSH L2 error of the
-// prediction exceeds tol the solver runs the whole window; otherwise the
-// surrogate advances the remaining anchor - k steps, k per call.
+// predicts the first k steps of every member, the FP64 solver runs them (the
+// shadow step, which also re-anchors the state), and each member whose
+// relative SSH L2 error of the prediction exceeds tol (or is not finite)
+// falls back: the solver runs the rest of its window.  The other members
+// advance by surrogate calls, k steps each.  With per_member = 0 one failing
+// member sends the whole ensemble to the solver for the window.  Statistics
+// count member-windows and member-steps.
 int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, int nsteps,
                  nemo_hyb_stats* stats) {
   if (!s || !e || !c || c->k != 10 || c->anchor < c->k || c->anchor % c->k || nsteps % c->anchor ||
-      !(c->tol > 0))
+      !(c->tol > 0) || (c->per_member && (c->anchor - c->k) % 2 != 0))
     return NEMO_ERR_INVALID;
   SCK(set_dev(s));
   nemo_hyb_stats st{};
@@ -797,20 +921,23 @@ int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, 
   // predictions of all members are kept for the shadow comparison
   float *snap_all = s->snap, *out_all = s->out32;
   float* own = nullptr;
+  const size_t out_per = (size_t)s->Hn * s->Wn * s->NO;  // FP32 outputs per member
   if (nm > s->cfg.batch) {
-    ECK(cudaMalloc(&own, 2 * (size_t)nm * hw * 16));
+    ECK(cudaMalloc(&own, (size_t)nm * (hw * 4 + out_per) * sizeof(float)));
     snap_all = own;
     out_all = own + (size_t)nm * hw * 4;
   }
   std::vector<double> tide(nm), acc(6 * nm);
+  std::vector<char> pass(nm), fail(nm);
   const auto t_start = std::chrono::steady_clock::now();
   int istp = istp0;
   int rc = NEMO_OK;
+  const int rest = c->anchor - c->k;
   for (int w = 0; w < nsteps / c->anchor && rc == NEMO_OK; ++w) {
     for (int i = 0; i < nm; ++i) tide[i] = nemo::ens_tide(e, i, istp + c->k);
     for (int m0 = 0; m0 < nm && rc == NEMO_OK; m0 += s->cfg.batch) {
       const int n = nm - m0 < s->cfg.batch ? nm - m0 : s->cfg.batch;
-      rc = predict_chunk(s, m0, n, tide, snap_all + (size_t)m0 * hw * 4, out_all + (size_t)m0 * hw * 4);
+      rc = predict_chunk(s, m0, n, tide, snap_all + (size_t)m0 * hw * 4, out_all + (size_t)m0 * out_per);
     }
     // shadow / re-anchor: the FP64 solver runs the same k steps
     if (rc == NEMO_OK) rc = join(s->stream, nemo::ens_stream(e));
@@ -819,42 +946,51 @@ int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, 
     if (rc == NEMO_OK) rc = ensure_members(s, e, ms, nullptr);  // buffers swapped
     if (rc != NEMO_OK) break;
     cudaError_t ce = cudaMemsetAsync(s->d_acc, 0, 6 * nm * sizeof(double), s->stream);
-    if (ce == cudaSuccess) {
-      k_err<<<dim3((unsigned)(grid_for(hw, 256) / 16 + 1), (unsigned)nm), 256, 0, s->stream>>>(
-          s->d_ms, reinterpret_cast<const float4*>(snap_all), reinterpret_cast<const float4*>(out_all), s->norm,
-          nullptr, 0, H, W, s->d_acc);
-      ce = cudaGetLastError();
-    }
+    if (ce == cudaSuccess) ce = launch_err(s, nm, snap_all, out_all);
     if (ce == cudaSuccess)
       ce = cudaMemcpyAsync(acc.data(), s->d_acc, 6 * nm * sizeof(double), cudaMemcpyDeviceToHost, s->stream);
     if (ce != cudaSuccess) { rc = status_of(ce); break; }
     if ((rc = check_err(s)) != NEMO_OK) break;
     // a non-finite error (a member whose state blew up) counts as a failure
     double worst = 0.0;
-    bool fail = false;
+    int nfail = 0;
     for (int m = 0; m < nm; ++m) {
       const double r = acc[6 * m + 1] > 0 ? sqrt(acc[6 * m] / acc[6 * m + 1]) : sqrt(acc[6 * m]);
-      if (!(r <= c->tol)) fail = true;
+      fail[m] = !(r <= c->tol);
+      nfail += fail[m];
       if (!(r <= worst)) worst = r;  // NaN propagates
     }
+    if (!c->per_member && nfail > 0) {
+      for (int m = 0; m < nm; ++m) fail[m] = 1;
+      nfail = nm;
+    }
+    for (int m = 0; m < nm; ++m) pass[m] = !fail[m];
     st.last_shadow_err = worst;
     if (!(worst <= st.max_shadow_err)) st.max_shadow_err = worst;
-    st.solver_steps += c->k;
+    st.windows += nm;
+    st.fallbacks += nfail;
+    st.solver_steps += (long long)c->k * nm;
     st.sur_calls += 1;
     istp += c->k;
-    if (fail) {  // fallback: the solver runs the rest of the window
-      st.fallbacks += 1;
-      rc = nemo_ens_step_n(e, istp + 1, c->anchor - c->k);
-      st.solver_steps += c->anchor - c->k;
-      istp += c->anchor - c->k;
-      continue;
+    if (nfail == nm) {  // the whole ensemble: the graph-captured path
+      rc = nemo_ens_step_n(e, istp + 1, rest);
+    } else if (nfail > 0) {
+      rc = nemo::ens_step_subset(e, istp + 1, rest, fail.data());
     }
-    for (int j = c->k; j < c->anchor && rc == NEMO_OK; j += c->k) {
-      rc = nemo_sur_advance_ens(s, e, istp + c->k);
-      st.sur_calls += 1;
-      st.sur_steps += c->k;
-      istp += c->k;
+    st.solver_steps += (long long)rest * nfail;
+    if (rc != NEMO_OK) break;
+    if (nfail < nm) {
+      rc = join(nemo::ens_stream(e), s->stream);
+      for (int j = c->k; j < c->anchor && rc == NEMO_OK; j += c->k) {
+        rc = advance_members(s, e, ms, pass.data(), istp + j);
+        st.sur_calls += 1;
+        st.sur_steps += (long long)c->k * (nm - nfail);
+      }
+      if (rc == NEMO_OK) rc = check_err(s);
+      if (rc == NEMO_OK) rc = join(s->stream, nemo::ens_stream(e));
+      if (rc == NEMO_OK) rc = ensure_members(s, e, ms, nullptr);  // all members' table again
     }
+    istp += rest;
   }
   cudaError_t ce = cudaStreamSynchronize(nemo::ens_stream(e));
   if (ce == cudaSuccess) ce = cudaStreamSynchronize(s->stream);

@@ -261,7 +261,7 @@ class Model:
     def step_n(self, istp0, n):
         check(self.lib.nemo_step_n(self.h, istp0, n), "nemo_step_n")
 
-    def set_schedule(self, warps=4, occupancy=0, rows=64):
+    def set_schedule(self, warps=2, occupancy=116, rows=16):
         s = Schedule(warps, occupancy, rows)
         check(self.lib.nemo_set_schedule(self.h, ctypes.byref(s)), "nemo_set_schedule")
 
@@ -381,7 +381,7 @@ class Ensemble:
         check(self.lib.nemo_ens_set_state(self.h, member, *[_dptr(x) for x in a]),
               "nemo_ens_set_state")
 
-    def set_schedule(self, warps=2, occupancy=-24, rows=16, order=1, ctas=0):
+    def set_schedule(self, warps=2, occupancy=116, rows=16, order=1, ctas=0):
         s = EnsSchedule(warps, occupancy, rows, order, ctas)
         check(self.lib.nemo_ens_set_schedule(self.h, ctypes.byref(s)), "nemo_ens_set_schedule")
 

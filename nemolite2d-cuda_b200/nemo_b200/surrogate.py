@@ -15,7 +15,7 @@ from . import check, load
 class SurConfig(ctypes.Structure):
     _fields_ = [("nblocks", ctypes.c_int), ("batch", ctypes.c_int), ("height", ctypes.c_int),
                 ("width", ctypes.c_int), ("train", ctypes.c_int), ("seed", ctypes.c_uint64),
-                ("stream", ctypes.c_void_p), ("device", ctypes.c_int)]
+                ("stream", ctypes.c_void_p), ("device", ctypes.c_int), ("patch", ctypes.c_int)]
 
 
 class AdamW(ctypes.Structure):
@@ -24,12 +24,14 @@ class AdamW(ctypes.Structure):
 
 
 class HybConfig(ctypes.Structure):
-    _fields_ = [("k", ctypes.c_int), ("anchor", ctypes.c_int), ("tol", ctypes.c_double)]
+    _fields_ = [("k", ctypes.c_int), ("anchor", ctypes.c_int), ("tol", ctypes.c_double),
+                ("per_member", ctypes.c_int)]
 
 
 class HybStats(ctypes.Structure):
     _fields_ = [("sur_calls", ctypes.c_longlong), ("sur_steps", ctypes.c_longlong),
                 ("solver_steps", ctypes.c_longlong), ("fallbacks", ctypes.c_longlong),
+                ("windows", ctypes.c_longlong),
                 ("max_shadow_err", ctypes.c_double), ("last_shadow_err", ctypes.c_double),
                 ("seconds", ctypes.c_double)]
 
@@ -70,12 +72,13 @@ class Surrogate:
     """A nemo_sur: the residual CNN with its FP32 master parameters."""
 
     def __init__(self, nblocks=8, batch=64, height=256, width=256, train=True, seed=1234,
-                 stream=None, device=-1, strict=False):
+                 stream=None, device=-1, strict=False, patch=1):
         self.lib = load(strict)
         c = SurConfig()
         check(self.lib.nemo_sur_default_config(ctypes.byref(c)), "nemo_sur_default_config")
         c.nblocks, c.batch, c.height, c.width = nblocks, batch, height, width
         c.train, c.seed, c.stream, c.device = int(bool(train)), seed, stream, device
+        c.patch = patch
         self.cfg = c
         h = ctypes.c_void_p()
         check(self.lib.nemo_sur_create(ctypes.byref(c), ctypes.byref(h)), "nemo_sur_create")
@@ -96,6 +99,17 @@ class Surrogate:
         n, f = ctypes.c_longlong(), ctypes.c_longlong()
         check(self.lib.nemo_sur_info(self.h, ctypes.byref(n), ctypes.byref(f)), "nemo_sur_info")
         return n.value, f.value
+
+    @property
+    def patch(self):
+        return self.cfg.patch
+
+    def out_shape(self, n):
+        """Shape of predict's FP32 output for n images."""
+        P = self.cfg.patch
+        if P == 1:
+            return (n, self.cfg.height, self.cfg.width, 4)
+        return (n, self.cfg.height // P, self.cfg.width // P, 3 * P * P)
 
     @property
     def nlayers(self):
@@ -159,11 +173,12 @@ class Surrogate:
     def save(self, path):
         sc, sh, osc = self.get_norm()
         np.savez(path, params=self.params(), in_scale=sc, in_shift=sh, out_scale=osc,
-                 nblocks=self.cfg.nblocks)
+                 nblocks=self.cfg.nblocks, patch=self.cfg.patch)
 
     def load_file(self, path):
         z = np.load(path)
         assert int(z["nblocks"]) == self.cfg.nblocks
+        assert int(z["patch"]) == self.cfg.patch if "patch" in z else self.cfg.patch == 1
         self.set_params(z["params"])
         self.set_norm(z["in_scale"], z["in_shift"], z["out_scale"])
 
@@ -176,8 +191,10 @@ def ens_compare(a, ref):
     return out.reshape(-1, 3)
 
 
-def hyb_run(sur, ens, istp0, nsteps, k=10, anchor=100, tol=0.01):
-    c = HybConfig(k, anchor, tol)
+def hyb_run(sur, ens, istp0, nsteps, k=10, anchor=100, tol=0.01, per_member=True):
+    """Hybrid run (nemo_hyb_run); returns the statistics as a dict (counts of
+    member-windows and member-steps)."""
+    c = HybConfig(k, anchor, tol, int(bool(per_member)))
     st = HybStats()
     check(sur.lib.nemo_hyb_run(sur.h, ens.h, ctypes.byref(c), istp0, nsteps, ctypes.byref(st)),
           "nemo_hyb_run")

@@ -36,26 +36,40 @@ def tide_of(member, istp, rdt=20.0):
     return member.amp_tide * math.sin(omega * (istp * rdt) + member.tide_phase)
 
 
+def snapshot_steps(steps, every=10, pair_stride=None):
+    """Steps at which generate_runs records snapshots: every `every` steps,
+    or with pair_stride the pairs (t, t + every) for t = 0, pair_stride, ...
+    (long runs with a bounded number of snapshots)."""
+    if not pair_stride:
+        return list(range(0, steps + 1, every))
+    out = []
+    for t in range(0, steps - every + 1, pair_stride):
+        out += [t, t + every]
+    return out
+
+
 def generate_runs(sur, seed, nmem, side, steps, every=10, amp_scale=0.2, strict=False,
-                  bound=2.5):
+                  bound=2.5, pair_stride=None):
     """Runs nmem members from rest for `steps` steps and returns (snaps, tides)
     of the members whose run stays bounded (finite, max |ssh| <= bound x the
     member's tidal amplitude; the reference scheme lets a tide that starts
     rising grow at the corner of the east wall and the open boundary):
-    snaps [steps//every + 1][kept][side][side][4] float32 on the device,
-    tides [same][kept] float32 (the boundary SSH at each snapshot's step).
-    The number of members dropped is in generate_runs.dropped."""
+    snaps [S][kept][side][side][4] float32 on the device at the steps of
+    snapshot_steps(steps, every, pair_stride), tides [S][kept] float32 (the
+    boundary SSH at each snapshot's step).  The number of members dropped is
+    in generate_runs.dropped."""
     torch = _torch()
     members = square_members(seed, nmem, side, amp_scale)
     ens = Ensemble(members, strict=strict, **COMMON)
-    ns = steps // every + 1
+    at = snapshot_steps(steps, every, pair_stride)
+    ns = len(at)
     snaps = torch.empty((ns, nmem, side, side, 4), dtype=torch.float32, device="cuda")
     tides = torch.empty((ns, nmem), dtype=torch.float32)
     istp = 0
     for k in range(ns):
-        if k:
-            ens.step_n(istp + 1, every)
-            istp += every
+        if at[k] > istp:
+            ens.step_n(istp + 1, at[k] - istp)
+            istp = at[k]
         torch.cuda.synchronize()
         sur.pack_ens(ens, snaps[k].data_ptr())
         tides[k] = torch.tensor([tide_of(m, istp) for m in members], dtype=torch.float32)
@@ -75,14 +89,18 @@ def generate_runs(sur, seed, nmem, side, steps, every=10, amp_scale=0.2, strict=
 generate_runs.dropped = 0
 
 
-def compute_norm(snaps):
+def compute_norm(snaps, paired=False):
     """Input scale/shift per channel and output scale per delta channel from
-    a snapshot tensor [S][N][H][W][4]."""
+    a snapshot tensor [S][N][H][W][4] (paired: deltas of the pairs (2i, 2i+1))."""
     torch = _torch()
-    x = snaps.reshape(-1, 4).double()
+    sub = snaps[:, ::max(1, snaps.shape[1] // 8)]  # statistics from up to 8 runs
+    x = sub.reshape(-1, 4).double()
     mean = x.mean(0)
     std = x.std(0)
-    d = (snaps[1:] - snaps[:-1]).reshape(-1, 4).double()
+    if paired:
+        d = (sub[1::2] - sub[0::2]).reshape(-1, 4).double()
+    else:
+        d = (sub[1:] - sub[:-1]).reshape(-1, 4).double()
     dstd = d.std(0)
     in_shift = [0.0, 0.0, 0.0, float(mean[3])]
     in_scale = [1.0 / max(float(std[c]), 1e-12) for c in range(4)]
@@ -93,13 +111,15 @@ def compute_norm(snaps):
 
 class PairSampler:
     """Random (snapshot k, snapshot k+1) pairs of a run set, gathered into
-    contiguous device batches."""
+    contiguous device batches; with paired=True only the pairs (2i, 2i+1)
+    (runs recorded with a pair_stride)."""
 
-    def __init__(self, snaps, tides, seed=0):
+    def __init__(self, snaps, tides, seed=0, paired=False):
         torch = _torch()
         self.snaps, self.tides = snaps, tides
         S, N = snaps.shape[0], snaps.shape[1]
-        self.pairs = [(k, m) for k in range(S - 1) for m in range(N)]
+        ks = range(0, S - 1, 2) if paired else range(S - 1)
+        self.pairs = [(k, m) for k in ks for m in range(N)]
         self.rng = np.random.default_rng(seed)
         self.order = []
         self.s0 = self.s1 = self.t1 = None

@@ -89,22 +89,61 @@ def split_params(flat, nblocks):
     return flat[:nw].reshape(L, 9, CH, CH), flat[nw:].reshape(L, CH)
 
 
-def make_input(snap, tide, in_scale, in_shift):
-    """x0 (N, H, W, 64) from snapshots (N, H, W, 4) and tides (N,), in float32
-    arithmetic as the device does it."""
+def out_channels(patch):
+    """FP32 output channels per network pixel."""
+    return 4 if patch == 1 else 3 * patch * patch
+
+
+def to_patches(f, patch):
+    """(N, H, W, F) per T-cell -> (N, H/P, W/P, F*P*P), channel f*P*P + P*sy + sx."""
+    N, H, W, F = f.shape
+    P = patch
+    g = f.reshape(N, H // P, P, W // P, P, F)            # n, Y, sy, X, sx, f
+    return g.transpose(0, 1, 3, 5, 2, 4).reshape(N, H // P, W // P, F * P * P)
+
+
+def from_patches(g, patch, nf):
+    """Inverse of to_patches for the first nf*P*P channels."""
+    N, Hn, Wn, _ = g.shape
+    P = patch
+    h = g[..., :nf * P * P].reshape(N, Hn, Wn, nf, P, P)  # n, Y, X, f, sy, sx
+    return h.transpose(0, 1, 4, 2, 5, 3).reshape(N, Hn * P, Wn * P, nf)
+
+
+def make_input(snap, tide, in_scale, in_shift, patch=1):
+    """x0 (N, H/P, W/P, 64) from snapshots (N, H, W, 4) and tides (N,), in
+    float32 arithmetic as the device does it.  Channels: ssh, u, v of the
+    patch's T-cells (P*P each), depth (one channel for P = 1, else the means
+    of the four P/2 x P/2 quadrants), the open-boundary row flag and the tide
+    on network row 0."""
     snap = np.asarray(snap, dtype=np.float32)
     N, H, W, _ = snap.shape
+    P = patch
     sc = np.asarray(in_scale, dtype=np.float32)
     sh = np.asarray(in_shift, dtype=np.float32)
-    x = np.zeros((N, H, W, CH), dtype=np.float32)
-    x[..., 0:4] = (snap - sh) * sc
-    x[:, 0, :, 4] = 1.0
+    f = (snap - sh) * sc
+    x = np.zeros((N, H // P, W // P, CH), dtype=np.float32)
+    x[..., :3 * P * P] = to_patches(f[..., :3], P)
+    if P == 1:
+        x[..., 3] = f[..., 3]
+        fc = 4
+    else:
+        d = f[..., 3].reshape(N, H // P, 2, P // 2, W // P, 2, P // 2)  # n Y qy sy X qx sx
+        acc = np.zeros((N, H // P, 2, W // P, 2), dtype=np.float32)
+        for sy in range(P // 2):                # the device's summation order
+            for sx in range(P // 2):
+                acc = acc + d[:, :, :, sy, :, :, sx]
+        q = acc * np.float32(4.0 / (P * P))
+        x[..., 3 * P * P:3 * P * P + 4] = q.transpose(0, 1, 3, 2, 4).reshape(N, H // P, W // P, 4)
+        fc = 3 * P * P + 4
+    x[:, 0, :, fc] = 1.0
     t = (np.asarray(tide, dtype=np.float32) - sh[0]) * sc[0]
-    x[:, 0, :, 5] = t[:, None]
+    x[:, 0, :, fc + 1] = t[:, None]
     return x
 
 
 def make_target(snap0, snap1, out_scale):
+    """Normalised deltas per T-cell (N, H, W, 4), channel 3 zero."""
     d = (np.asarray(snap1, np.float32) - np.asarray(snap0, np.float32))[..., :3]
     t = np.zeros(d.shape[:-1] + (4,), dtype=np.float32)
     t[..., :3] = d * np.asarray(out_scale, np.float32)
@@ -112,7 +151,7 @@ def make_target(snap0, snap1, out_scale):
 
 
 def forward(x0, W, B, nblocks, bf16_acts=True):
-    """Returns (y [N,H,W,4] FP64 deltas, cache of activations)."""
+    """Returns (y [N,Hn,Wn,64] FP64 network output, cache of activations)."""
     r = bf16 if bf16_acts else (lambda a: a)
     Wq = bf16(W) if bf16_acts else W
     x0 = r(x0)
@@ -122,22 +161,30 @@ def forward(x0, W, B, nblocks, bf16_acts=True):
         ti = r(epilogue(conv3x3(h[i], Wq[1 + 2 * i]), B[1 + 2 * i], relu=True))
         t.append(ti)
         h.append(r(epilogue(conv3x3(ti, Wq[2 + 2 * i]), B[2 + 2 * i], residual=h[i])))
-    y = epilogue(conv3x3(h[-1], Wq[-1]), B[-1])[..., :4]
+    y = epilogue(conv3x3(h[-1], Wq[-1]), B[-1])
     return y, dict(x0=x0, h=h, t=t, Wq=Wq)
 
 
-def loss_and_dout(y, target, bf16_acts=True):
-    d = y[..., :3] - np.asarray(target, dtype=np.float64)[..., :3]
+def deltas(y, patch=1):
+    """Per-T-cell deltas (N, H, W, 3) of a network output (N, Hn, Wn, 64)."""
+    return y[..., :3] if patch == 1 else from_patches(y, patch, 3)
+
+
+def loss_and_dout(y, target, bf16_acts=True, patch=1):
+    d = deltas(y, patch) - np.asarray(target, dtype=np.float64)[..., :3]
     npix = d.shape[0] * d.shape[1] * d.shape[2]
     loss = float((d * d).sum() / (3.0 * npix))
-    dout = np.zeros(y.shape[:3] + (CH,))
     g = 2.0 * d / (3.0 * npix)
     if bf16_acts:
         # the device forms 2 * gscale * d in float32 before rounding
         gs = np.float32(1.0 / (3.0 * npix))
         g = (np.float32(2.0) * gs * d.astype(np.float32)).astype(np.float64)
         g = bf16(g)
-    dout[..., :3] = g
+    dout = np.zeros(y.shape[:3] + (CH,))
+    if patch == 1:
+        dout[..., :3] = g
+    else:
+        dout[..., :3 * patch * patch] = to_patches(g, patch)
     return loss, dout
 
 
@@ -164,14 +211,14 @@ def backward(dout, cache, nblocks, bf16_acts=True):
     return dW, dB
 
 
-def loss_grad(flat_params, nblocks, snap0, snap1, tide, norm, bf16_acts=True):
+def loss_grad(flat_params, nblocks, snap0, snap1, tide, norm, bf16_acts=True, patch=1):
     """Loss and flat gradient (weights then biases) as nemo_sur_loss_grad."""
     in_scale, in_shift, out_scale = norm
     W, B = split_params(np.asarray(flat_params, dtype=np.float64), nblocks)
-    x0 = make_input(snap0, tide, in_scale, in_shift).astype(np.float64)
+    x0 = make_input(snap0, tide, in_scale, in_shift, patch).astype(np.float64)
     tgt = make_target(snap0, snap1, out_scale)
     y, cache = forward(x0, W, B, nblocks, bf16_acts)
-    loss, dout = loss_and_dout(y, tgt, bf16_acts)
+    loss, dout = loss_and_dout(y, tgt, bf16_acts, patch)
     dW, dB = backward(dout, cache, nblocks, bf16_acts)
     return loss, np.concatenate([dW.ravel(), dB.ravel()])
 

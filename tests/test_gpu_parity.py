@@ -66,6 +66,8 @@ def test_strict_build_matches_golden_bitwise(nb, case, path):
 
 
 @pytest.mark.parametrize("jpi,jpj,tile", [(257, 131, (4, 0, 64)), (130, 300, (2, 20, 7)),
+                                          (257, 131, (2, 116, 16)), (130, 300, (4, 116, 7)),
+                                          (61, 29, (2, 120, 3)), (3, 5, (2, 116, 1)),
                                           (2, 2, (2, 0, 1)), (3, 5, (4, 16, 2)), (96, 33, (8, 16, 16)),
                                           (61, 29, (4, 24, 3)), (125, 40, (2, -16, 0)),
                                           (62, 9, (2, 0, 0)), (63, 12, (8, 24, 5)),
@@ -120,20 +122,26 @@ def test_strict_routines_one_by_one_from_random_state(nb, oracle_mod):
 
 
 @pytest.mark.parametrize("strict", [True, False])
-def test_tiny_values_take_the_exact_division_path(nb, oracle_mod, strict):
-    """A state whose values reach the subnormal range: quotients below 2^-959
-    must be recomputed with IEEE division, so the strict build stays
-    bit-identical to the oracle there too."""
+@pytest.mark.parametrize("mags", [(-322, -280), (-322, 0), (-310, -290)])
+@pytest.mark.parametrize("sched", [(2, 116, 16), (2, -20, 16), (2, 20, 7)])
+def test_tiny_values_take_the_exact_division_path(nb, oracle_mod, strict, mags, sched):
+    """States whose values reach the subnormal range, alone or mixed with
+    ordinary values and whole rows of zeros: rows holding nonzero values
+    below 2^-300 (and their neighbours) are computed with IEEE division, so
+    the strict build stays bit-identical to the oracle there too, for every
+    way of staging rows."""
     jpi, jpj = 150, 90
-    kw = dict(jpi=jpi, jpj=jpj, rdt=20.0, cbfr=0.00015, visc=0.1, amp_tide=0.0)
+    kw = dict(jpi=jpi, jpj=jpj, rdt=20.0, cbfr=0.00015, visc=0.1, amp_tide=0.2)
     rng = np.random.default_rng(5)
     def tiny(shape):
-        mag = 10.0 ** rng.uniform(-322, -280, shape)
+        mag = 10.0 ** rng.uniform(mags[0], mags[1], shape)
         x = mag * rng.choice([-1.0, 1.0], shape)
         x[rng.random(shape) < 0.3] = 0.0
+        x[rng.random(shape[0]) < 0.3] = 0.0
         return x
     st = (tiny((jpj, jpi)), tiny((jpj, jpi + 1)), tiny((jpj + 1, jpi)))
     m = nb.Model(strict=strict, **kw)
+    m.set_schedule(*sched)
     o = oracle_mod.Model(**kw)
     m.set_state(*st)
     o.set_state(*st)
@@ -195,7 +203,8 @@ def test_strict_checksums_bitwise_tree_order(nb, oracle_mod):
 
 
 @pytest.mark.parametrize("sched", [(2, 0, 1), (2, 16, 16), (4, 0, 64), (4, 20, 5), (8, 16, 256),
-                                   (8, 0, 33), (2, 24, 0), (2, -24, 16)])
+                                   (8, 0, 33), (2, 24, 0), (2, -24, 16), (2, 116, 16), (2, 120, 1),
+                                   (4, 116, 0), (4, 120, 9)])
 def test_schedule_does_not_change_results(nb, sched):
     """Strict build: bit-identical for every schedule.  Default build: each
     register-budget variant is compiled separately and may contract multiply-

@@ -233,6 +233,63 @@ def test_predict_matches_oracle_forward(env):
     assert np.abs(got[..., :3] - y[..., :3]).max() <= 2e-2 * np.abs(y[..., :3]).max()
 
 
+@pytest.mark.parametrize("patch", [2, 4])
+def test_patch_predict_matches_oracle_forward(env, patch):
+    """The patch network: inputs gathered from P x P T-cells, FP32 outputs
+    in the [n][h/P][w/P][3 P^2] layout."""
+    torch, nb, sm = env
+    P = patch
+    N, H, W = 2, 3 * P, 128 * P
+    rng = np.random.default_rng(40 + P)
+    s = sm.Surrogate(nblocks=1, batch=N, height=H, width=W, train=False, seed=6, patch=P)
+    p = s.params()
+    Wt, Bs = s.split(p)
+    Wt[-1, :, :3 * P * P, :] = rng.normal(0, 0.05, size=Wt[-1, :, :3 * P * P, :].shape)
+    Bs[-1, :3 * P * P] = rng.normal(0, 0.05, size=3 * P * P)
+    s.set_params(p)
+    snap0, _, tide, norm, d = random_setup(rng, torch, N, H, W)
+    s.set_norm(*norm)
+    out = torch.empty(s.out_shape(N), dtype=torch.float32, device="cuda")
+    assert s.out_shape(N) == (N, H // P, W // P, 3 * P * P)
+    torch.cuda.synchronize()
+    s.predict(d[0].data_ptr(), d[2].data_ptr(), N, out.data_ptr())
+    Wr, Br = so.split_params(p.astype(np.float64), 1)
+    x0 = so.make_input(snap0, tide, norm[0], norm[1], patch=P).astype(np.float64)
+    y, _ = so.forward(x0, Wr, Br, 1, bf16_acts=True)
+    got = out.cpu().numpy()
+    ref = y[..., :3 * P * P]
+    assert np.abs(got - ref).max() <= 2e-2 * np.abs(ref).max()
+
+
+def test_patch_loss_and_gradients_match_oracle(env):
+    torch, nb, sm = env
+    P, N, H, W, nblocks = 2, 2, 6, 256, 1
+    rng = np.random.default_rng(77)
+    s = sm.Surrogate(nblocks=nblocks, batch=N, height=H, width=W, seed=8, patch=P)
+    p = s.params()
+    Wt, Bs = s.split(p)
+    Bs[:] = rng.normal(0, 0.05, size=Bs.shape)
+    Wt[-1, :, :12, :] = rng.normal(0, 0.05, size=Wt[-1, :, :12, :].shape)
+    s.set_params(p)
+    snap0, snap1, tide, norm, d = random_setup(rng, torch, N, H, W)
+    s.set_norm(*norm)
+    torch.cuda.synchronize()
+    loss = s.loss_grad(d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), N)
+    g = s.grads()
+    rloss, rg = so.loss_grad(p.astype(np.float64), nblocks, snap0, snap1, tide, norm,
+                             bf16_acts=True, patch=P)
+    assert abs(loss - rloss) <= 1e-3 * rloss
+    gw, gb = s.split(g)
+    rw, rb = so.split_params(rg, nblocks)
+    for l in range(2 * nblocks + 2):
+        e_w = np.linalg.norm(gw[l] - rw[l]) / np.linalg.norm(rw[l])
+        e_b = np.linalg.norm(gb[l] - rb[l]) / np.linalg.norm(rb[l])
+        assert e_w < 2e-2 and e_b < 2e-2, (l, e_w, e_b)
+    # input channels past the tide and output channels past 3 P^2 get no gradient
+    assert not gw[0][:, :, 3 * P * P + 6:].any()
+    assert not gw[-1][:, 3 * P * P:, :].any()
+
+
 def small_ensemble(nb, seed, n, side):
     from nemo_b200 import train as tr
     return nb.Ensemble(tr.square_members(seed, n, side, 0.2), **tr.COMMON)
@@ -274,6 +331,43 @@ def test_pack_and_advance_follow_the_grid_layout(env):
         np.testing.assert_allclose(v[:side, :], v0[:side, :] + (o[m, ..., 2] / osc[2]), rtol=1e-12)
 
 
+def test_patch_advance_applies_each_cells_delta(env):
+    """One patch-4 surrogate call moves every T-cell by its own channel of
+    the patch output."""
+    torch, nb, sm = env
+    from nemo_b200 import train as tr
+    P, side, n = 4, 512, 2
+    e = small_ensemble(nb, 23, n, side)
+    e.step_n(1, 40)
+    s = sm.Surrogate(nblocks=1, batch=n, height=side, width=side, train=False, seed=3, patch=P)
+    p = s.params()
+    Wt, Bs = s.split(p)
+    Bs[-1, :48] = np.random.default_rng(5).normal(0, 0.1, size=48)
+    s.set_params(p)
+    s.set_norm([1, 1, 1, 1], [0, 0, 0, 100], [1e3, 1e3, 1e3])
+    snap = torch.empty((n, side, side, 4), dtype=torch.float32, device="cuda")
+    s.pack_ens(e, snap.data_ptr())
+    out = torch.empty(s.out_shape(n), dtype=torch.float32, device="cuda")
+    tide = torch.tensor([tr.tide_of(mb, 50) for mb in e.members], dtype=torch.float32).cuda()
+    torch.cuda.synchronize()
+    s.predict(snap.data_ptr(), tide.data_ptr(), n, out.data_ptr())
+    o = so.from_patches(out.cpu().numpy().astype(np.float64), P, 3)
+    before = [[e.field(m, f) for f in (nb.SSHN, nb.UN, nb.VN)] for m in range(n)]
+    s.advance_ens(e, 50)
+    _, _, osc = s.get_norm()
+    for m in range(n):
+        ssh0, u0, v0 = before[m]
+        ssh, u, v = (e.field(m, f) for f in (nb.SSHN, nb.UN, nb.VN))
+        exp = ssh0 + (o[m, ..., 0].astype(np.float32) / osc[0]).astype(np.float64)
+        exp[0, :] = tr.tide_of(e.members[m], 50)
+        np.testing.assert_allclose(ssh, exp, rtol=1e-12, atol=0)
+        np.testing.assert_allclose(u[:, 1:side], u0[:, 1:side] + (o[m, :, 1:, 1].astype(np.float32) / osc[1]),
+                                   rtol=1e-12)
+        np.testing.assert_allclose(v[:side, :], v0[:side, :] + (o[m, ..., 2].astype(np.float32) / osc[2]),
+                                   rtol=1e-12)
+        assert not u[:, 0].any() and not u[:, side].any() and not v[side, :].any()
+
+
 def test_hybrid_with_zero_tolerance_reproduces_the_solver_bitwise(env):
     torch, nb, sm = env
     side, n = 128, 2
@@ -282,7 +376,8 @@ def test_hybrid_with_zero_tolerance_reproduces_the_solver_bitwise(env):
     s = sm.Surrogate(nblocks=1, batch=n, height=side, width=side, train=False, seed=4)
     st = sm.hyb_run(s, a, 0, 300, tol=1e-300)  # every window falls back
     b.step_n(1, 300)
-    assert st["fallbacks"] == 3 and st["solver_steps"] == 300 and st["sur_steps"] == 0
+    assert st["fallbacks"] == 3 * n and st["windows"] == 3 * n
+    assert st["solver_steps"] == 300 * n and st["sur_steps"] == 0
     for m in range(n):
         for f in (nb.SSHN, nb.UN, nb.VN):
             np.testing.assert_array_equal(a.field(m, f), b.field(m, f))
@@ -297,10 +392,49 @@ def test_hybrid_accepts_surrogate_windows_and_reports_errors(env):
     s = sm.Surrogate(nblocks=1, batch=1, height=side, width=side, train=False, seed=4)  # 2 chunks
     st = sm.hyb_run(s, a, 0, 200, k=10, anchor=100, tol=1e300)  # never falls back
     b.step_n(1, 200)
-    assert st["fallbacks"] == 0 and st["sur_steps"] == 180 and st["solver_steps"] == 20
+    assert st["fallbacks"] == 0 and st["sur_steps"] == 180 * n and st["solver_steps"] == 20 * n
     assert st["sur_calls"] == 20 and st["max_shadow_err"] > 0
     err = sm.ens_compare(a, b)
     assert err.shape == (n, 3) and np.all(np.isfinite(err)) and np.all(err > 0)
+
+
+def test_hybrid_members_fall_back_on_their_own(env):
+    """Per-member fallback: with a tolerance between two members' shadow
+    errors, the failing member follows the FP64 solver bit for bit while the
+    other advances by the surrogate; whole-ensemble fallback sends both back."""
+    torch, nb, sm = env
+    side, n = 128, 3
+    s = sm.Surrogate(nblocks=1, batch=n, height=side, width=side, train=False, seed=4)
+    # shadow errors of the first window, per member
+    probe = small_ensemble(nb, 51, n, side)
+    ref = small_ensemble(nb, 51, n, side)
+    snap = torch.empty((n, side, side, 4), dtype=torch.float32, device="cuda")
+    s.pack_ens(probe, snap.data_ptr())
+    s.advance_ens(probe, 10)
+    ref.step_n(1, 10)
+    e0 = sm.ens_compare(probe, ref)[:, 0]
+    order = np.argsort(e0)
+    assert e0[order[0]] < e0[order[-1]]
+    if e0[order[1]] - e0[order[0]] < 1e-3 * e0[order[1]]:
+        pytest.skip("members' shadow errors too close to separate")
+    tol = 0.5 * (e0[order[0]] + e0[order[1]])
+    a = small_ensemble(nb, 51, n, side)
+    b = small_ensemble(nb, 51, n, side)
+    st = sm.hyb_run(s, a, 0, 100, tol=tol)
+    b.step_n(1, 100)
+    assert st["windows"] == n and st["fallbacks"] == n - 1
+    assert st["solver_steps"] == 10 * n + 90 * (n - 1) and st["sur_steps"] == 90
+    err = sm.ens_compare(a, b)
+    for m in range(n):
+        if m == order[0]:
+            assert err[m, 0] > 0  # advanced by the surrogate
+        else:
+            for f in (nb.SSHN, nb.UN, nb.VN):
+                np.testing.assert_array_equal(a.field(m, f), b.field(m, f))
+    c = small_ensemble(nb, 51, n, side)
+    st = sm.hyb_run(s, c, 0, 100, tol=tol, per_member=False)
+    assert st["fallbacks"] == n and st["sur_steps"] == 0
+    assert np.all(sm.ens_compare(c, b) == 0.0)
 
 
 def test_training_beats_persistence_on_held_out_runs(env):
