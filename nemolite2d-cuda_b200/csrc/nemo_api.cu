@@ -33,6 +33,7 @@ struct nemo_ctx {
   double* ck_host;        // pinned, 4
   bool a_mirrors_n;       // after a fused step the reference's a-fields equal n
   bool uv_stale;          // stored sshn_u/sshn_v lag behind sshn
+  bool recip_nr_ok;       // in-kernel reciprocal depths equal the stored ones
   nemo_schedule sched;
 };
 
@@ -238,7 +239,8 @@ bool tune_lookup(const nemo_ctx* c, nemo_schedule* s) {
     std::string k;
     nemo_schedule t;
     double ms;
-    if (ls >> k >> t.warps >> t.occupancy >> t.rows >> ms && k == key && fused_variant_ok(t.warps, t.occupancy)) {
+    if (ls >> k >> t.warps >> t.occupancy >> t.rows >> ms && k == key &&
+        fused_variant_ok(t.warps, t.occupancy, c->recip_nr_ok)) {
       *s = t;
       found = true;  // the last entry for a key wins
     }
@@ -312,8 +314,9 @@ int nemo_create(const nemo_params* p, nemo_ctx** out) {
   c->L.rows = (long)p->jpj + 3;
   c->C = make_consts(*p);
   c->sched.warps = 2;
-  c->sched.occupancy = 116;
-  c->sched.rows = 16;
+  c->sched.occupancy = 216;  // 116 when the depths fail the reciprocal check below
+  c->sched.rows = 32;
+  c->recip_nr_ok = false;
   int st = set_device(c);
   if (st) { delete c; return st; }
   cudaError_t e;
@@ -370,7 +373,16 @@ int nemo_create(const nemo_params* p, nemo_ctx** out) {
   } else {
     e = launch_depth(c->L, p->dep_const, 0, nullptr, nullptr, p->hmin, p->hmax, c->ht, c->hu, c->hv, c->stream);
   }
-  if (e == cudaSuccess) e = launch_recip(c->L, c->hu, c->hv, c->rhu, c->rhv, c->stream);
+  // reciprocal depths, and whether recip_nr reproduces them on every cell
+  // (the checksum scratch holds the mismatch count; it is not in use yet)
+  int* d_bad = reinterpret_cast<int*>(c->ck_partials);
+  int h_bad = -1;
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_bad, 0, sizeof(int), c->stream);
+  if (e == cudaSuccess) e = launch_recip(c->L, c->hu, c->hv, c->rhu, c->rhv, d_bad, c->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&h_bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  c->recip_nr_ok = (e == cudaSuccess && h_bad == 0);
+  if (!c->recip_nr_ok) c->sched.occupancy = 116;
   // initialisation (:331-365): sshn = un = vn = 0, sshn_u/sshn_v averaged
   if (e == cudaSuccess)
     e = launch_init_sshn_uv(c->L, c->C, nset(c).ssh, c->sshn_u, c->sshn_v, c->stream);
@@ -609,7 +621,7 @@ int nemo_device_field(nemo_ctx* c, int field, double** ptr, long* pitch) {
 
 int nemo_set_schedule(nemo_ctx* c, const nemo_schedule* s) {
   if (!c) return NEMO_ERR_STATE;
-  if (!s || !fused_variant_ok(s->warps, s->occupancy) || s->rows < 0 || s->rows > 65536)
+  if (!s || !fused_variant_ok(s->warps, s->occupancy, c->recip_nr_ok) || s->rows < 0 || s->rows > 65536)
     return NEMO_ERR_INVALID;
   c->sched = *s;
   return NEMO_OK;
@@ -639,14 +651,15 @@ int nemo_autotune(nemo_ctx* c, int steps, nemo_schedule* best, double* best_ms) 
   const nemo_schedule keep = c->sched;
   nemo_schedule bsched = keep;
   double bms = 1e300;
-  const int wo[][2] = {{2, 116}, {2, 120}, {4, 116}, {4, 120}, {2, -24}, {2, -20}, {2, -16}, {2, 0},
-                       {2, 16}, {2, 20}, {2, 24}, {4, -20}, {4, 0}, {4, 16}, {4, 20}, {4, 24},
-                       {8, 0}, {8, 16}, {8, 24}};
+  const int wo[][2] = {{2, 216}, {2, 220}, {4, 216}, {4, 220}, {2, 116}, {2, 120}, {4, 116}, {4, 120},
+                       {2, -24}, {2, -20}, {2, -16}, {2, 0}, {2, 16}, {2, 20}, {2, 24}, {4, -20}, {4, 0},
+                       {4, 16}, {4, 20}, {4, 24}, {8, 0}, {8, 16}, {8, 24}};
   const int rows_c[] = {8, 16, 32, 0};
   cudaEvent_t t0 = nullptr, t1 = nullptr;
   if (er == cudaSuccess) er = cudaEventCreate(&t0);
   if (er == cudaSuccess) er = cudaEventCreate(&t1);
   for (const auto& w : wo) {
+    if (!fused_variant_ok(w[0], w[1], c->recip_nr_ok)) continue;
     for (int rows : rows_c) {
       if (er != cudaSuccess || st) break;
       nemo_schedule cand{w[0], w[1], rows};

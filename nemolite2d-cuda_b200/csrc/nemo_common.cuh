@@ -73,6 +73,23 @@ __device__ __forceinline__ double div_const(double a, double b, double rb) {
   return -fma(-r, rb, -q);
 }
 
+// 1/b by two Newton-Raphson steps, y <- y + y*(1 - b*y) with fused
+// multiply-adds, from a single-precision seed (relative error below 2^-22,
+// so the second step leaves an error near 2^-88 before the last rounding).
+// The result is RN(1/b) unless 1/b lies that close to a rounding boundary;
+// callers that need RN(1/b) verify it against an IEEE division once per
+// static divisor (launch_recip) and keep the stored quotient otherwise.
+// b must be a normal number within single-precision range.
+__device__ __forceinline__ double recip_nr(double b) {
+  float yf;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"(__double2float_rn(b)));
+  double y = (double)yf;
+  double e = fma(-b, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-b, y, 1.0);
+  return fma(y, e, y);
+}
+
 constexpr unsigned long long kSign = 0x8000000000000000ull;
 
 __device__ __forceinline__ bool sign_clear(double w) { return __double2hiint(w) >= 0; }

@@ -60,9 +60,10 @@ k_ens_step(const MemberDev* __restrict__ mem, const int4* __restrict__ work, int
     A.sshv0 = M->sshv0;
     A.tide = tide[it.x];
     const Layout L = M->L;
-    if constexpr (PF == 2) {
+    if constexpr (PF >= 2) {
       __shared__ double ring[NW * stepdev::RING_DOUBLES];
-      stepdev::run_strip_ring(L, C, A, it.y, it.z, it.w, lane, ring + (threadIdx.x >> 5) * stepdev::RING_DOUBLES);
+      stepdev::run_strip_ring<PF == 3>(L, C, A, it.y, it.z, it.w, lane,
+                                       ring + (threadIdx.x >> 5) * stepdev::RING_DOUBLES);
     } else {
       stepdev::run_strip<PF>(L, C, A, it.y, it.z, it.w, lane);
     }
@@ -142,22 +143,34 @@ cudaError_t launch_ens_variant(const MemberDev* mem, const int4* work, int nwork
 cudaError_t launch_ens(int warps, int occ, const MemberDev* mem, const int4* work, int nwork,
                        const Consts& C, const double* tide, int parity, int ctas,
                        cudaStream_t s) {
-  switch (warps * 100 + occ) {
-    case 316: return launch_ens_variant<2, 8, 2>(mem, work, nwork, C, tide, parity, ctas, s);
-    case 320: return launch_ens_variant<2, 10, 2>(mem, work, nwork, C, tide, parity, ctas, s);
-    case 516: return launch_ens_variant<4, 4, 2>(mem, work, nwork, C, tide, parity, ctas, s);
-    case 200 - 24: return launch_ens_variant<2, 12, 0>(mem, work, nwork, C, tide, parity, ctas, s);
-    case 200 - 20: return launch_ens_variant<2, 10, 0>(mem, work, nwork, C, tide, parity, ctas, s);
-    case 220: return launch_ens_variant<2, 10, 1>(mem, work, nwork, C, tide, parity, ctas, s);
-    case 224: return launch_ens_variant<2, 12, 1>(mem, work, nwork, C, tide, parity, ctas, s);
-    case 400 - 20: return launch_ens_variant<4, 5, 0>(mem, work, nwork, C, tide, parity, ctas, s);
-    case 420: return launch_ens_variant<4, 5, 1>(mem, work, nwork, C, tide, parity, ctas, s);
-    case 424: return launch_ens_variant<4, 6, 1>(mem, work, nwork, C, tide, parity, ctas, s);
-    default: return cudaErrorInvalidValue;
+#define ENS(NW, MB, PF) launch_ens_variant<NW, MB, PF>(mem, work, nwork, C, tide, parity, ctas, s)
+  if (warps == 2) {
+    switch (occ) {
+      case 216: return ENS(2, 8, 3);
+      case 220: return ENS(2, 10, 3);
+      case 116: return ENS(2, 8, 2);
+      case 120: return ENS(2, 10, 2);
+      case -24: return ENS(2, 12, 0);
+      case -20: return ENS(2, 10, 0);
+      case 20: return ENS(2, 10, 1);
+      case 24: return ENS(2, 12, 1);
+    }
+  } else if (warps == 4) {
+    switch (occ) {
+      case 216: return ENS(4, 4, 3);
+      case 116: return ENS(4, 4, 2);
+      case -20: return ENS(4, 5, 0);
+      case 20: return ENS(4, 5, 1);
+      case 24: return ENS(4, 6, 1);
+    }
   }
+#undef ENS
+  return cudaErrorInvalidValue;
 }
 
-bool ens_variant_ok(int warps, int occ) {
+bool ens_variant_ok(int warps, int occ, bool nr_ok) {
+  if (warps == 2 && (occ == 216 || occ == 220)) return nr_ok;
+  if (warps == 4 && occ == 216) return nr_ok;
   if (warps == 2) return occ == -24 || occ == -20 || occ == 20 || occ == 24 || occ == 116 || occ == 120;
   if (warps == 4) return occ == -20 || occ == 20 || occ == 24 || occ == 116;
   return false;
@@ -215,6 +228,7 @@ struct nemo_ens {
   long long cells = 0;
   int4* d_work_sub = nullptr;  // work list of a member subset (ens_step_subset)
   int sub_cap = 0;
+  bool recip_nr_ok = false;    // every member's depths pass launch_recip's check
 };
 
 namespace {
@@ -380,7 +394,7 @@ int nemo_ens_create(const nemo_params* common, const nemo_member* members, int n
   e->C = make_consts(*common);
   e->mem.assign(members, members + nmem);
   e->sched.warps = 2;
-  e->sched.occupancy = 116;
+  e->sched.occupancy = 216;  // 116 when a member's depths fail the reciprocal check
   e->sched.rows = 16;
   e->sched.order = 1;
   e->sched.ctas = 0;
@@ -419,6 +433,9 @@ int nemo_ens_create(const nemo_params* common, const nemo_member* members, int n
   rows.reserve(e->nrows);
   double* tab = nullptr;
   size_t tab_cap = 0;
+  int* d_bad = nullptr;  // depths whose in-kernel reciprocal differs from RN(1/h)
+  err = cudaMalloc(&d_bad, sizeof(int));
+  if (err == cudaSuccess) err = cudaMemsetAsync(d_bad, 0, sizeof(int), e->stream);
   for (int m = 0; m < nmem && err == cudaSuccess; ++m) {
     MemberDev& d = e->hmem[m];
     const size_t fe = (size_t)d.L.elems();
@@ -463,7 +480,7 @@ int nemo_ens_create(const nemo_params* common, const nemo_member* members, int n
     } else {
       err = launch_depth(d.L, p.dep_const, 0, nullptr, nullptr, p.hmin, p.hmax, ht, hu, hv, e->stream);
     }
-    if (err == cudaSuccess) err = launch_recip(d.L, hu, hv, rhu, rhv, e->stream);
+    if (err == cudaSuccess) err = launch_recip(d.L, hu, hv, rhu, rhv, d_bad, e->stream);
     if (err == cudaSuccess) {
       Consts C = make_consts(p);
       err = launch_init_sshn_uv(d.L, C, d.st[0][0], sshn_u, sshn_v, e->stream);
@@ -473,6 +490,12 @@ int nemo_ens_create(const nemo_params* common, const nemo_member* members, int n
     for (int jj = 1; jj <= d.L.jpj; ++jj) rows.push_back(make_int2(m, jj));
   }
   if (tab) { cudaStreamSynchronize(e->stream); cudaFree(tab); }
+  int h_bad = -1;
+  if (err == cudaSuccess) err = cudaMemcpyAsync(&h_bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, e->stream);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
+  if (d_bad) cudaFree(d_bad);
+  e->recip_nr_ok = (err == cudaSuccess && h_bad == 0);
+  if (!e->recip_nr_ok) e->sched.occupancy = 116;
   if (err != cudaSuccess) { nemo_ens_destroy(e); return status_of(err); }
   const size_t nm = (size_t)nmem;
   err = cudaMalloc(&e->d_mem, nm * sizeof(MemberDev));
@@ -587,7 +610,7 @@ int nemo_ens_set_state(nemo_ens* e, int member, const double* sshn, const double
 
 int nemo_ens_set_schedule(nemo_ens* e, const nemo_ens_schedule* s) {
   if (!e) return NEMO_ERR_STATE;
-  if (!s || !ens_variant_ok(s->warps, s->occupancy) || s->rows < 1 || s->rows > 65536 ||
+  if (!s || !ens_variant_ok(s->warps, s->occupancy, e->recip_nr_ok) || s->rows < 1 || s->rows > 65536 ||
       s->order < 0 || s->order > 1 || s->ctas < 0)
     return NEMO_ERR_INVALID;
   int st = set_dev(e); if (st) return st;
@@ -645,13 +668,14 @@ int nemo_ens_autotune(nemo_ens* e, int steps, nemo_ens_schedule* best, double* b
   e->use_graph = false;
   nemo_ens_schedule bsched = keep;
   double bms = 1e300;
-  const int warps_occ[][2] = {{2, 116}, {2, 120}, {4, 116}, {2, -24}, {2, -20}, {2, 20}, {2, 24},
-                              {4, -20}, {4, 20}, {4, 24}};
+  const int warps_occ[][2] = {{2, 216}, {2, 220}, {4, 216}, {2, 116}, {2, 120}, {4, 116}, {2, -24},
+                              {2, -20}, {2, 20}, {2, 24}, {4, -20}, {4, 20}, {4, 24}};
   const int rows_c[] = {8, 16, 32};
   cudaEvent_t t0 = nullptr, t1 = nullptr;
   if (er == cudaSuccess) er = cudaEventCreate(&t0);
   if (er == cudaSuccess) er = cudaEventCreate(&t1);
   for (const auto& wo : warps_occ) {
+    if (!ens_variant_ok(wo[0], wo[1], e->recip_nr_ok)) continue;
     for (int rows : rows_c) {
       for (int order = 0; order <= 1 && er == cudaSuccess; ++order) {
         nemo_ens_schedule c{wo[0], wo[1], rows, order, 0};
@@ -700,6 +724,8 @@ int ens_member_state(nemo_ens* e, int m, MemberState* out) {
   out->un = d.st[e->parity][1];
   out->vn = d.st[e->parity][2];
   out->ht = d.ht;
+  out->hv = d.hv;
+  out->sshv0 = d.sshv0;
   out->jpi = d.L.jpi;
   out->jpj = d.L.jpj;
   out->pitch = d.L.pitch;

@@ -49,9 +49,9 @@ k_fused_step(Layout L, Consts C, FusedArgs A, int tile_y) {
   const int J0 = 1 + (int)blockIdx.y * tile_y;
   if (J0 > L.jpj) return;
   const int J1 = min(J0 + tile_y - 1, L.jpj);
-  if constexpr (PF == 2) {
+  if constexpr (PF >= 2) {
     __shared__ double ring[NWARPS * RING_DOUBLES];
-    run_strip_ring(L, C, A, c0, J0, J1, lane, ring + (threadIdx.x >> 5) * RING_DOUBLES);
+    run_strip_ring<PF == 3>(L, C, A, c0, J0, J1, lane, ring + (threadIdx.x >> 5) * RING_DOUBLES);
   } else {
     run_strip<PF>(L, C, A, c0, J0, J1, lane);
   }
@@ -86,37 +86,51 @@ static cudaError_t launch_variant(const Layout& L, const Consts& C, const FusedA
 // warps: 2, 4 or 8 per CTA; occ: register budget as resident warps per SM
 // (0: compiler's choice, 16, 20, 24) with the register prefetch of the next
 // row; a negative occ: the same budget without it; 100 + budget (116, 120):
-// rows staged through the shared-memory ring.
+// rows staged through the shared-memory ring; 200 + budget (216, 220): the
+// ring with the reciprocal depths formed in the kernel.
 cudaError_t launch_fused_step(const Layout& L, const Consts& C, const FusedArgs& a, int warps,
                               int occ, int tile_y, cudaStream_t s) {
-  switch (warps * 100 + occ) {
-    case 316: return launch_variant<2, 8, 2>(L, C, a, tile_y, s);
-    case 320: return launch_variant<2, 10, 2>(L, C, a, tile_y, s);
-    case 516: return launch_variant<4, 4, 2>(L, C, a, tile_y, s);
-    case 520: return launch_variant<4, 5, 2>(L, C, a, tile_y, s);
-    case 200: return launch_variant<2, 1, 1>(L, C, a, tile_y, s);
-    case 216: return launch_variant<2, 8, 1>(L, C, a, tile_y, s);
-    case 220: return launch_variant<2, 10, 1>(L, C, a, tile_y, s);
-    case 224: return launch_variant<2, 12, 1>(L, C, a, tile_y, s);
-    case 200 - 16: return launch_variant<2, 8, 0>(L, C, a, tile_y, s);
-    case 200 - 20: return launch_variant<2, 10, 0>(L, C, a, tile_y, s);
-    case 200 - 24: return launch_variant<2, 12, 0>(L, C, a, tile_y, s);
-    case 400: return launch_variant<4, 1, 1>(L, C, a, tile_y, s);
-    case 416: return launch_variant<4, 4, 1>(L, C, a, tile_y, s);
-    case 420: return launch_variant<4, 5, 1>(L, C, a, tile_y, s);
-    case 424: return launch_variant<4, 6, 1>(L, C, a, tile_y, s);
-    case 400 - 20: return launch_variant<4, 5, 0>(L, C, a, tile_y, s);
-    case 800: return launch_variant<8, 1, 1>(L, C, a, tile_y, s);
-    case 816: return launch_variant<8, 2, 1>(L, C, a, tile_y, s);
-    case 824: return launch_variant<8, 3, 1>(L, C, a, tile_y, s);
-    default: return cudaErrorInvalidValue;
+  if (warps == 2) {
+    switch (occ) {
+      case 216: return launch_variant<2, 8, 3>(L, C, a, tile_y, s);
+      case 220: return launch_variant<2, 10, 3>(L, C, a, tile_y, s);
+      case 116: return launch_variant<2, 8, 2>(L, C, a, tile_y, s);
+      case 120: return launch_variant<2, 10, 2>(L, C, a, tile_y, s);
+      case 0: return launch_variant<2, 1, 1>(L, C, a, tile_y, s);
+      case 16: return launch_variant<2, 8, 1>(L, C, a, tile_y, s);
+      case 20: return launch_variant<2, 10, 1>(L, C, a, tile_y, s);
+      case 24: return launch_variant<2, 12, 1>(L, C, a, tile_y, s);
+      case -16: return launch_variant<2, 8, 0>(L, C, a, tile_y, s);
+      case -20: return launch_variant<2, 10, 0>(L, C, a, tile_y, s);
+      case -24: return launch_variant<2, 12, 0>(L, C, a, tile_y, s);
+    }
+  } else if (warps == 4) {
+    switch (occ) {
+      case 216: return launch_variant<4, 4, 3>(L, C, a, tile_y, s);
+      case 220: return launch_variant<4, 5, 3>(L, C, a, tile_y, s);
+      case 116: return launch_variant<4, 4, 2>(L, C, a, tile_y, s);
+      case 120: return launch_variant<4, 5, 2>(L, C, a, tile_y, s);
+      case 0: return launch_variant<4, 1, 1>(L, C, a, tile_y, s);
+      case 16: return launch_variant<4, 4, 1>(L, C, a, tile_y, s);
+      case 20: return launch_variant<4, 5, 1>(L, C, a, tile_y, s);
+      case 24: return launch_variant<4, 6, 1>(L, C, a, tile_y, s);
+      case -20: return launch_variant<4, 5, 0>(L, C, a, tile_y, s);
+    }
+  } else if (warps == 8) {
+    switch (occ) {
+      case 0: return launch_variant<8, 1, 1>(L, C, a, tile_y, s);
+      case 16: return launch_variant<8, 2, 1>(L, C, a, tile_y, s);
+      case 24: return launch_variant<8, 3, 1>(L, C, a, tile_y, s);
+    }
   }
+  return cudaErrorInvalidValue;
 }
 
 }  // namespace nemo
 
 namespace nemo {
-bool fused_variant_ok(int warps, int occ) {
+bool fused_variant_ok(int warps, int occ, bool nr_ok) {
+  if ((occ == 216 || occ == 220) && (warps == 2 || warps == 4)) return nr_ok;
   if (warps == 2) return occ == 0 || occ == 16 || occ == 20 || occ == 24 || occ == -16 ||
                          occ == -20 || occ == -24 || occ == 116 || occ == 120;
   if (warps == 4) return occ == 0 || occ == 16 || occ == 20 || occ == 24 || occ == -20 || occ == 116 ||

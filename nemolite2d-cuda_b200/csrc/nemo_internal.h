@@ -23,8 +23,10 @@ struct RoutinePtrs {
 cudaError_t launch_depth(const Layout& L, double dep_const, int nbump, const double* ax,
                          const double* gy, double hmin, double hmax, double* ht,
                          double* hu, double* hv, cudaStream_t s);
-// rhu = RN(1/hu), rhv = RN(1/hv) over the whole storage (0 where the depth is 0).
+// rhu = RN(1/hu), rhv = RN(1/hv) over the whole storage (0 where the depth is 0);
+// adds to *mismatch (device) the number of depths whose recip_nr is not RN(1/h).
 cudaError_t launch_recip(const Layout& L, const double* hu, const double* hv, double* rhu, double* rhv,
+                         int* mismatch,
                          cudaStream_t s);
 cudaError_t launch_init_sshn_uv(const Layout& L, const Consts& C, const double* sshn,
                                 double* sshn_u, double* sshn_v, cudaStream_t s);
@@ -55,7 +57,8 @@ struct FusedArgs {
 // per CTA (0: one wave).
 cudaError_t launch_fused_step(const Layout& L, const Consts& C, const FusedArgs& a, int warps,
                               int occ, int tile_y, cudaStream_t s);
-bool fused_variant_ok(int warps, int occ);
+// nr_ok: the grid's depths passed launch_recip's check (variants 216, 220).
+bool fused_variant_ok(int warps, int occ, bool nr_ok);
 
 // Sums |f(1:jpi,1:jpj)| of nf fields into out[0..nf-1] (device), fixed order.
 // row_partials: nf*jpj doubles of scratch.

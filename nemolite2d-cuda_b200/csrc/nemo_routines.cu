@@ -328,21 +328,28 @@ cudaError_t launch_depth(const Layout& L, double dep_const, int nbump, const dou
   return cudaGetLastError();
 }
 
+// RN(1/hu), RN(1/hv) by IEEE division (0 where the depth is 0); counts the
+// cells where recip_nr differs from it in `mismatch`.
 __global__ void k_recip(long n, const double* __restrict__ hu, const double* __restrict__ hv,
-                        double* __restrict__ rhu, double* __restrict__ rhv) {
+                        double* __restrict__ rhu, double* __restrict__ rhv, int* __restrict__ mismatch) {
+  int bad = 0;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
     const double a = hu[i] + 0.0, b = hv[i] + 0.0;
-    rhu[i] = a != 0.0 ? 1.0 / a : 0.0;
-    rhv[i] = b != 0.0 ? 1.0 / b : 0.0;
+    const double ra = a != 0.0 ? 1.0 / a : 0.0, rb = b != 0.0 ? 1.0 / b : 0.0;
+    rhu[i] = ra;
+    rhv[i] = rb;
+    if (a != 0.0 && __double_as_longlong(recip_nr(a)) != __double_as_longlong(ra)) ++bad;
+    if (b != 0.0 && __double_as_longlong(recip_nr(b)) != __double_as_longlong(rb)) ++bad;
   }
+  if (bad) atomicAdd(mismatch, bad);
 }
 
 cudaError_t launch_recip(const Layout& L, const double* hu, const double* hv, double* rhu, double* rhv,
-                         cudaStream_t s) {
+                         int* mismatch, cudaStream_t s) {
   const long n = L.elems();
   long g = (n + 255) / 256;
   if (g > 4096) g = 4096;
-  k_recip<<<(unsigned)g, 256, 0, s>>>(n, hu, hv, rhu, rhv);
+  k_recip<<<(unsigned)g, 256, 0, s>>>(n, hu, hv, rhu, rhv, mismatch);
   return cudaGetLastError();
 }
 

@@ -322,6 +322,8 @@ __device__ __forceinline__ void cp_async8(double* dst, const double* src) {
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
+// NR: the reciprocal depths are formed in the kernel (recip_nr), not staged.
+template <bool NR>
 __device__ __forceinline__ void ring_issue(double* slot, const FusedArgs& A, long o) {
   cp_async8(slot + 0 * 32, A.sshn + o);
   cp_async8(slot + 1 * 32, A.un + o);
@@ -329,8 +331,10 @@ __device__ __forceinline__ void ring_issue(double* slot, const FusedArgs& A, lon
   cp_async8(slot + 3 * 32, A.ht + o);
   cp_async8(slot + 4 * 32, A.hu + o);
   cp_async8(slot + 5 * 32, A.hv + o);
-  cp_async8(slot + 6 * 32, A.rhu + o);
-  cp_async8(slot + 7 * 32, A.rhv + o);
+  if (!NR) {
+    cp_async8(slot + 6 * 32, A.rhu + o);
+    cp_async8(slot + 7 * 32, A.rhv + o);
+  }
   cp_commit();
 }
 
@@ -344,7 +348,10 @@ __device__ __forceinline__ void ring_cell(Cell& x, const double* slot) {
 }
 
 // run_strip with rows staged through `ring` (this warp's RING_DOUBLES, in
-// shared memory).
+// shared memory).  NR = true forms RN(1/hu), RN(1/hv) with recip_nr instead
+// of reading the stored fields: valid only for depths that launch_recip
+// found to give exactly the stored values (16 fewer bytes per cell-step).
+template <bool NR>
 __device__ __forceinline__ void run_strip_ring(const Layout& L, const Consts& C, const FusedArgs& A,
                                                int c0, int J0, int J1, int lane, double* ring) {
   const int jpi = L.jpi, jpj = L.jpj;
@@ -357,8 +364,8 @@ __device__ __forceinline__ void run_strip_ring(const Layout& L, const Consts& C,
   const long pitch = L.pitch;
   const long o_last = L.idx(cl, jpj + 1);
   // rows J0 and J0+1 into the ring (row r in slot r % RING)
-  ring_issue(my + (J0 % RING) * 256, A, L.idx(cl, J0));
-  ring_issue(my + ((J0 + 1) % RING) * 256, A, L.idx(cl, J0 + 1));
+  ring_issue<NR>(my + (J0 % RING) * 256, A, L.idx(cl, J0));
+  ring_issue<NR>(my + ((J0 + 1) % RING) * 256, A, L.idx(cl, J0 + 1));
 
   Cell p, cur, nx;
   load_cell(p, A, L.idx(cl, J0 - 1));
@@ -379,12 +386,12 @@ __device__ __forceinline__ void run_strip_ring(const Layout& L, const Consts& C,
   for (int j = J0; j <= J1; ++j) {
     const int slot_n = slot_j == RING - 1 ? 0 : slot_j + 1;      // row j+1
     const int slot_f = slot_n == RING - 1 ? 0 : slot_n + 1;      // row j+2 (was row j-1)
-    ring_issue(my + slot_f * 256, A, o_ld < o_last ? o_ld : o_last);
+    ring_issue<NR>(my + slot_f * 256, A, o_ld < o_last ? o_ld : o_last);
     o_ld += pitch;
     cp_wait1();  // rows <= j+1 have landed
     ring_cell(nx, my + slot_n * 256);
-    const double rhu = my[slot_j * 256 + 6 * 32];
-    const double rhv = my[slot_j * 256 + 7 * 32];
+    const double rhu = NR ? recip_nr(cur.hu + 0.0) : my[slot_j * 256 + 6 * 32];
+    const double rhv = NR ? recip_nr(cur.hv + 0.0) : my[slot_j * 256 + 7 * 32];
 
     RowOut o;
     bool bad = false;

@@ -51,7 +51,8 @@ namespace nemo {
 // single-grid layout: element (ji, jj) at (jj + 1) * pitch + ji + 2).
 struct MemberState {
   double *sshn, *un, *vn;
-  const double* ht;
+  const double *ht, *hv;
+  const double* sshv0;  // stored sshn_v (row jj = 0: the open boundary's)
   int jpi, jpj, pitch;
 };
 int ens_member_state(nemo_ens* e, int m, MemberState* out);

@@ -258,6 +258,21 @@ __global__ void k_apply(const MemberState* __restrict__ ms, int m0, int nm, int 
   }
 }
 
+// The open boundary after a surrogate call, as the solver closes every step
+// (original/nemolite2d.f90:684-695): v(ji,0) = v(ji,1) + sqrt(g/hv(ji,0)) *
+// (sshn_v(ji,0) - sshn_v(ji,1)), with sshn_v(ji,1) the mean of sshn on rows 1
+// and 2 (uniform metrics) and sshn_v(ji,0) the stored boundary value.  The
+// network's own v(ji,0) is replaced: the boundary velocity is diagnostic.
+__global__ void k_flather(const MemberState* __restrict__ ms, int m0) {
+  const MemberState& M = ms[m0 + blockIdx.y];
+  for (int ji = 1 + blockIdx.x * blockDim.x + threadIdx.x; ji <= M.jpi; ji += gridDim.x * blockDim.x) {
+    const double s1 = M.sshn[gidx(M.pitch, ji, 1)];
+    const double sv1 = M.jpj >= 2 ? 0.5 * (s1 + M.sshn[gidx(M.pitch, ji, 2)]) : s1;
+    const double v1 = M.vn[gidx(M.pitch, ji, 1)];
+    M.vn[gidx(M.pitch, ji, 0)] = v1 + sqrt(9.80665 / M.hv[gidx(M.pitch, ji, 0)]) * (M.sshv0[gidx(M.pitch, ji, 0)] - sv1);
+  }
+}
+
 // Per member: sum (pred - ref)^2 and sum ref^2 for ssh, u, v (acc[m][6]).
 // pred = snap + delta / out_scale when out != null, else the state of `pm`.
 template <int P>
@@ -422,6 +437,9 @@ cudaError_t launch_apply(nemo_sur* s, int m0, int n, const float* out) {
     case 2: k_apply<2><<<g, 256, 0, s->stream>>>(s->d_ms, m0, n, H, W, out, s->norm, s->tide_d); break;
     default: k_apply<4><<<g, 256, 0, s->stream>>>(s->d_ms, m0, n, H, W, out, s->norm, s->tide_d); break;
   }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_flather<<<dim3((unsigned)((W + 255) / 256), (unsigned)n), 256, 0, s->stream>>>(s->d_ms, m0);
   return cudaGetLastError();
 }
 

@@ -261,7 +261,11 @@ class Model:
     def step_n(self, istp0, n):
         check(self.lib.nemo_step_n(self.h, istp0, n), "nemo_step_n")
 
-    def set_schedule(self, warps=2, occupancy=116, rows=16):
+    def set_schedule(self, warps=2, occupancy=None, rows=32):
+        """occupancy None: the context's default staging (216 when the in-kernel
+        reciprocal depths passed their check, else 116)."""
+        if occupancy is None:
+            occupancy = 216 if self.recip_in_kernel() else 116
         s = Schedule(warps, occupancy, rows)
         check(self.lib.nemo_set_schedule(self.h, ctypes.byref(s)), "nemo_set_schedule")
 
@@ -269,6 +273,16 @@ class Model:
         s = Schedule()
         check(self.lib.nemo_get_schedule(self.h, ctypes.byref(s)), "nemo_get_schedule")
         return (s.warps, s.occupancy, s.rows)
+
+    def recip_in_kernel(self):
+        """True when the schedules that form the reciprocal depths in the
+        kernel (occupancy 216, 220) are available for this grid."""
+        s = Schedule(2, 216, 32)
+        keep = Schedule()
+        check(self.lib.nemo_get_schedule(self.h, ctypes.byref(keep)), "nemo_get_schedule")
+        ok = self.lib.nemo_set_schedule(self.h, ctypes.byref(s)) == 0
+        check(self.lib.nemo_set_schedule(self.h, ctypes.byref(keep)), "nemo_set_schedule")
+        return ok
 
     def sync(self):
         check(self.lib.nemo_sync(self.h), "nemo_sync")
@@ -381,7 +395,12 @@ class Ensemble:
         check(self.lib.nemo_ens_set_state(self.h, member, *[_dptr(x) for x in a]),
               "nemo_ens_set_state")
 
-    def set_schedule(self, warps=2, occupancy=116, rows=16, order=1, ctas=0):
+    def set_schedule(self, warps=2, occupancy=None, rows=16, order=1, ctas=0):
+        """occupancy None: 216 when every member's in-kernel reciprocal depths
+        passed their check, else 116."""
+        if occupancy is None:
+            s = EnsSchedule(2, 216, rows, order, ctas)
+            occupancy = 216 if self.lib.nemo_ens_set_schedule(self.h, ctypes.byref(s)) == 0 else 116
         s = EnsSchedule(warps, occupancy, rows, order, ctas)
         check(self.lib.nemo_ens_set_schedule(self.h, ctypes.byref(s)), "nemo_ens_set_schedule")
 

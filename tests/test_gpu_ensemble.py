@@ -40,8 +40,9 @@ def oracle_member(oracle_mod, m):
 
 
 @pytest.mark.parametrize("graph", [True, False])
-@pytest.mark.parametrize("sched", [(2, 116, 16, 1), (4, 116, 7, 0), (2, 120, 3, 1), (2, -24, 16, 1),
-                                   (4, 20, 8, 0), (2, 24, 5, 0)])
+@pytest.mark.parametrize("sched", [(2, 216, 16, 1), (4, 216, 7, 0), (2, 220, 3, 0), (2, 116, 16, 1),
+                                   (4, 116, 7, 0), (2, 120, 3, 1), (2, -24, 16, 1), (4, 20, 8, 0),
+                                   (2, 24, 5, 0)])
 def test_strict_ensemble_members_match_oracle_bitwise(nb, oracle_mod, graph, sched):
     members = nb.generate_members(7, 6, side_min=20, side_max=90, amp_scale=0.2)
     e = nb.Ensemble(members, strict=True, **COMMON)
@@ -104,7 +105,7 @@ def test_ensemble_autotune_keeps_state(nb):
     ref.step_n(1, 10)
     sched, ms = e.autotune(steps=2)
     assert ms > 0 and sched[0] in (2, 4)
-    e.set_schedule(2, 116, 16, 1)  # same arithmetic variant as ref for a bitwise check
+    e.set_schedule(2, 216, 16, 1)  # same arithmetic variant as ref for a bitwise check
     e.step_n(11, 10)
     ref.step_n(11, 10)
     for k in range(len(members)):

@@ -68,6 +68,8 @@ def test_strict_build_matches_golden_bitwise(nb, case, path):
 @pytest.mark.parametrize("jpi,jpj,tile", [(257, 131, (4, 0, 64)), (130, 300, (2, 20, 7)),
                                           (257, 131, (2, 116, 16)), (130, 300, (4, 116, 7)),
                                           (61, 29, (2, 120, 3)), (3, 5, (2, 116, 1)),
+                                          (257, 131, (2, 216, 32)), (130, 300, (4, 220, 9)),
+                                          (3, 5, (2, 216, 1)), (96, 33, (4, 216, 0)),
                                           (2, 2, (2, 0, 1)), (3, 5, (4, 16, 2)), (96, 33, (8, 16, 16)),
                                           (61, 29, (4, 24, 3)), (125, 40, (2, -16, 0)),
                                           (62, 9, (2, 0, 0)), (63, 12, (8, 24, 5)),
@@ -123,7 +125,7 @@ def test_strict_routines_one_by_one_from_random_state(nb, oracle_mod):
 
 @pytest.mark.parametrize("strict", [True, False])
 @pytest.mark.parametrize("mags", [(-322, -280), (-322, 0), (-310, -290)])
-@pytest.mark.parametrize("sched", [(2, 116, 16), (2, -20, 16), (2, 20, 7)])
+@pytest.mark.parametrize("sched", [(2, 216, 32), (2, 116, 16), (2, -20, 16), (2, 20, 7)])
 def test_tiny_values_take_the_exact_division_path(nb, oracle_mod, strict, mags, sched):
     """States whose values reach the subnormal range, alone or mixed with
     ordinary values and whole rows of zeros: rows holding nonzero values
@@ -153,6 +155,23 @@ def test_tiny_values_take_the_exact_division_path(nb, oracle_mod, strict, mags, 
             np.testing.assert_array_equal(bits(a), bits(b), err_msg=name)
         else:
             assert relerr(a, b) <= TOL, name
+
+
+def test_in_kernel_reciprocals_are_checked_and_default(nb):
+    """The depths of a seeded grid pass the setup check of the in-kernel
+    reciprocal depths (Newton steps from a single-precision seed, compared
+    with RN(1/h) cell by cell), so the default schedule forms them in the
+    kernel; with the stored reciprocals the strict results are identical."""
+    kw = dict(jpi=300, jpj=200, rdt=20.0, cbfr=0.00015, visc=0.1, amp_tide=0.4, nbump=16,
+              seed=21, bump_amp=35.0, bump_wmin=4e3, bump_wmax=80e3, hmin=12.0)
+    a = nb.Model(strict=True, **kw)
+    b = nb.Model(strict=True, **kw)
+    assert a.recip_in_kernel() and a.get_schedule() == (2, 216, 32)
+    b.set_schedule(2, 116, 32)
+    a.step_n(1, 60)
+    b.step_n(1, 60)
+    for name, fid in STATE:
+        np.testing.assert_array_equal(bits(a.field(fid)), bits(b.field(fid)), err_msg=name)
 
 
 def test_strict_fused_equals_routine_path_from_random_state(nb):
@@ -204,7 +223,8 @@ def test_strict_checksums_bitwise_tree_order(nb, oracle_mod):
 
 @pytest.mark.parametrize("sched", [(2, 0, 1), (2, 16, 16), (4, 0, 64), (4, 20, 5), (8, 16, 256),
                                    (8, 0, 33), (2, 24, 0), (2, -24, 16), (2, 116, 16), (2, 120, 1),
-                                   (4, 116, 0), (4, 120, 9)])
+                                   (4, 116, 0), (4, 120, 9), (2, 216, 32), (2, 220, 5), (4, 216, 0),
+                                   (4, 220, 11)])
 def test_schedule_does_not_change_results(nb, sched):
     """Strict build: bit-identical for every schedule.  Default build: each
     register-budget variant is compiled separately and may contract multiply-

@@ -290,6 +290,15 @@ def test_patch_loss_and_gradients_match_oracle(env):
     assert not gw[-1][:, 3 * P * P:, :].any()
 
 
+def assert_flather_row(nb, e, m, ssh, v):
+    """v(ji, 0) after a surrogate call: the solver's open-boundary closure
+    v(ji,1) + sqrt(g/hv(ji,0)) * (sshn_v(ji,0) - sshn_v(ji,1)), with the stored
+    sshn_v(ji,0) zero for members started from rest."""
+    hv0 = e.field(m, nb.HV)[0]
+    sv1 = 0.5 * (ssh[0] + ssh[1])
+    np.testing.assert_allclose(v[0], v[1] + np.sqrt(9.80665 / hv0) * (0.0 - sv1), rtol=1e-13, atol=1e-300)
+
+
 def small_ensemble(nb, seed, n, side):
     from nemo_b200 import train as tr
     return nb.Ensemble(tr.square_members(seed, n, side, 0.2), **tr.COMMON)
@@ -328,7 +337,8 @@ def test_pack_and_advance_follow_the_grid_layout(env):
         np.testing.assert_allclose(ssh, exp, rtol=1e-12, atol=0)
         assert not u[:, 0].any() and not u[:, side].any() and not v[side, :].any()
         np.testing.assert_allclose(u[:, 1:side], u0[:, 1:side] + (o[m, :, 1:, 1] / osc[1]), rtol=1e-12)
-        np.testing.assert_allclose(v[:side, :], v0[:side, :] + (o[m, ..., 2] / osc[2]), rtol=1e-12)
+        np.testing.assert_allclose(v[1:side, :], v0[1:side, :] + (o[m, 1:, :, 2] / osc[2]), rtol=1e-12)
+        assert_flather_row(nb, e, m, ssh, v)
 
 
 def test_patch_advance_applies_each_cells_delta(env):
@@ -363,8 +373,9 @@ def test_patch_advance_applies_each_cells_delta(env):
         np.testing.assert_allclose(ssh, exp, rtol=1e-12, atol=0)
         np.testing.assert_allclose(u[:, 1:side], u0[:, 1:side] + (o[m, :, 1:, 1].astype(np.float32) / osc[1]),
                                    rtol=1e-12)
-        np.testing.assert_allclose(v[:side, :], v0[:side, :] + (o[m, ..., 2].astype(np.float32) / osc[2]),
+        np.testing.assert_allclose(v[1:side, :], v0[1:side, :] + (o[m, 1:, :, 2].astype(np.float32) / osc[2]),
                                    rtol=1e-12)
+        assert_flather_row(nb, e, m, ssh, v)
         assert not u[:, 0].any() and not u[:, side].any() and not v[side, :].any()
 
 
