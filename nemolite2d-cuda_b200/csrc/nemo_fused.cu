@@ -51,7 +51,7 @@ k_fused_step(Layout L, Consts C, FusedArgs A, int tile_y) {
   const int J1 = min(J0 + tile_y - 1, L.jpj);
   if constexpr (PF >= 2) {
     __shared__ double ring[NWARPS * RING_DOUBLES];
-    run_strip_ring<PF == 3>(L, C, A, c0, J0, J1, lane, ring + (threadIdx.x >> 5) * RING_DOUBLES);
+    run_strip_ring<PF == 3, 2>(L, C, A, c0, J0, J1, lane, ring + (threadIdx.x >> 5) * RING_DOUBLES);
   } else {
     run_strip<PF>(L, C, A, c0, J0, J1, lane);
   }

@@ -348,10 +348,10 @@ __device__ __forceinline__ void ring_cell(Cell& x, const double* slot) {
 }
 
 // run_strip with rows staged through `ring` (this warp's RING_DOUBLES, in
-// shared memory).  NR = true forms RN(1/hu), RN(1/hv) with recip_nr instead
+// shared memory), its row loop unrolled UNROLL times.  NR = true forms RN(1/hu), RN(1/hv) with recip_nr instead
 // of reading the stored fields: valid only for depths that launch_recip
 // found to give exactly the stored values (16 fewer bytes per cell-step).
-template <bool NR>
+template <bool NR, int UNROLL>
 __device__ __forceinline__ void run_strip_ring(const Layout& L, const Consts& C, const FusedArgs& A,
                                                int c0, int J0, int J1, int lane, double* ring) {
   const int jpi = L.jpi, jpj = L.jpj;
@@ -382,7 +382,9 @@ __device__ __forceinline__ void run_strip_ring(const Layout& L, const Consts& C,
   long o_ld = L.idx(cl, J0 + 2);
   long o_st = L.idx(c, J0);
   int slot_j = J0 % RING;
-#pragma unroll 1
+// UNROLL = 2 keeps two rows in flight (the second row's independent work
+// fills FP64 latency) where registers allow it without spills
+#pragma unroll UNROLL
   for (int j = J0; j <= J1; ++j) {
     const int slot_n = slot_j == RING - 1 ? 0 : slot_j + 1;      // row j+1
     const int slot_f = slot_n == RING - 1 ? 0 : slot_n + 1;      // row j+2 (was row j-1)

@@ -11,7 +11,7 @@ import math
 
 import numpy as np
 
-from . import Ensemble, default_params, generate_members
+from . import SSHN, Ensemble, default_params, generate_members
 from .surrogate import adamw, ens_compare
 
 COMMON = dict(dx=1000.0, dy=1000.0, rdt=20.0, cbfr=0.00015, visc=0.1)
@@ -87,6 +87,27 @@ def generate_runs(sur, seed, nmem, side, steps, every=10, amp_scale=0.2, strict=
 
 
 generate_runs.dropped = 0
+
+
+def bounded_members(members, steps, common, bound=2.5, checks=2):
+    """Indices of the members whose FP64 run from rest stays bounded: finite
+    and max |ssh| <= bound x the member's tidal amplitude at `checks` evenly
+    spaced points of the run (the last at `steps`)."""
+    ens = Ensemble(members, **common)
+    alive = list(range(len(members)))
+    done = 0
+    for k in range(1, checks + 1):
+        to = steps * k // checks
+        ens.step_n(done + 1, to - done)
+        done = to
+        keep = []
+        for i in alive:
+            ssh = ens.field(i, SSHN)
+            if np.isfinite(ssh).all() and np.abs(ssh).max() <= bound * members[i].amp_tide:
+                keep.append(i)
+        alive = keep
+    ens.close()
+    return alive
 
 
 def compute_norm(snaps, paired=False):
