@@ -64,8 +64,12 @@ def parse():
     ap.add_argument("--train-side", type=int, default=512, help="training run side (hybrid)")
     ap.add_argument("--train-steps", type=int, default=2000, help="training run length (hybrid)")
     ap.add_argument("--train-runs", type=int, default=96, help="training runs (hybrid)")
+    ap.add_argument("--rollout-runs", type=int, default=48, help="rollout fine-tuning runs (hybrid)")
+    ap.add_argument("--rollout-windows", type=int, default=20, help="windows per rollout run (hybrid)")
+    ap.add_argument("--finetune-iters", type=int, default=0,
+                    help="fine-tuning iterations on rollout pairs (hybrid; 0: none)")
     ap.add_argument("--batch", type=int, default=64, help="images per conv call (conv workload)")
-    ap.add_argument("--train-iters", type=int, default=3000)
+    ap.add_argument("--train-iters", type=int, default=6000)
     ap.add_argument("--n", type=int, default=N,
                     help="grid side (profiling of smaller cases only; the bench line is 4096)")
     return ap.parse_args()
@@ -421,7 +425,8 @@ def run_hybrid(args):
     surrogate runs on 4x4 patches of T-cells (a call costs 1/16 of the
     full-resolution network) and is trained first on solver runs of the same
     recipe at 512x512 (pairs of snapshots 10 steps apart every 50 steps of
-    2000-step runs); it advances 10 steps per call, and the FP64 solver
+    2000-step runs), then fine-tuned on pairs along trajectories it advances
+    itself between solver windows; it advances 10 steps per call, and the FP64 solver
     re-anchors every 100 steps and takes the rest of the window over for each
     member whose shadow SSH error exceeds 1%.  Reports both rates and the
     hybrid's error against the plain FP64 run (which matches the FP64 oracle
@@ -443,12 +448,20 @@ def run_hybrid(args):
     norm = tr.compute_norm(snaps, paired=True)
     trainer.set_norm(*norm)
     t_train = time.time()
-    losses = tr.train(trainer, tr.PairSampler(snaps, tides, seed=3, paired=True),
-                      iters=args.train_iters, batch=64, lr=1e-3)
+    clean = tr.PairSampler(snaps, tides, seed=3, paired=True)
+    losses = tr.train(trainer, clean, iters=args.train_iters, batch=64, lr=1e-3)
+    if args.finetune_iters > 0:
+        # optional fine-tuning on the states the hybrid meets: pairs along
+        # trajectories the surrogate itself advances between solver windows
+        rsnaps, rtides = tr.rollout_runs(trainer, seed=9000, nmem=args.rollout_runs, side=ts,
+                                         windows=args.rollout_windows)
+        mix = tr.MixSampler([clean, tr.PairSampler(rsnaps, rtides, seed=4, paired=True)], [1.0, 1.0])
+        losses += tr.train(trainer, mix, iters=args.finetune_iters, batch=64, lr=5e-4)
+        del rsnaps, rtides, mix
     t_train = time.time() - t_train
     params = trainer.params()
     trainer.close()
-    del snaps, tides
+    del snaps, tides, clean
     torch.cuda.empty_cache()
     # ---- members: seeded candidates screened by the FP64 solver over the run
     # (the reference scheme lets a tide that starts rising grow without bound
@@ -496,6 +509,9 @@ def run_hybrid(args):
                        "candidates": len(cands), "screened_out": len(cands) - len(ok),
                        "patch": P, "train_side": ts, "train_steps": args.train_steps,
                        "train_runs": args.train_runs, "fallback": "per member",
+                       "rollout_runs": args.rollout_runs, "rollout_windows": args.rollout_windows,
+                       "rollout_runs_dropped": tr.rollout_runs.dropped,
+                       "finetune_iters": args.finetune_iters,
                        "train_iters": args.train_iters, "train_s": t_train, "datagen_s": t_gen,
                        "train_runs_dropped": tr.generate_runs.dropped},
             "plain_value": v_plain, "hybrid_over_plain": v_hyb / v_plain,

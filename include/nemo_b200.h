@@ -337,9 +337,12 @@ int nemo_conv3x3_fwd(const void* x, const void* w, const float* bias, const void
                      int* err, void* stream);
 int nemo_conv3x3_wgrad(const void* x, const void* dz, float* dw, float* db, int n, int h, int w_,
                        int ctas, int* err, void* stream);
-/* Process-wide forward kernel: 1 (default) marches column strips of `rows`
- * output rows with each input row loaded once; 0 loads one TMA window per
- * tap.  Returns the previous variant; values out of range change nothing. */
+/* Process-wide forward kernel: 2 (default) marches column strips of `rows`
+ * output rows with each input row loaded once and multiplied once per
+ * horizontal tap into all three output rows it feeds (N = 192 MMAs); 1 marches
+ * the same strips with one N = 64 MMA per tap and output row; 0 loads one TMA
+ * window per tap.  Returns the previous variant; values out of range change
+ * nothing. */
 int nemo_conv3x3_fwd_variant(int variant, int rows);
 
 /* ---- drop-in symbols (cuda/cuda_nemolite2d.cu:234-270) --------------------

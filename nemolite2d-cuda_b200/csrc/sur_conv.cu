@@ -511,6 +511,194 @@ k_conv_fwd_rows(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
   }
 }
 
+// ---- forward with three output rows per MMA -----------------------------------
+// The row-ring kernel issues 36 MMAs of N = 64 (one output channel block) per
+// output row, and those narrow MMAs keep the tensor pipe about half busy.
+// Here the weights of the three vertical taps of one horizontal tap are laid
+// side by side as one 192-row B operand (dy = -1, 0, +1), so each input row
+// r, multiplied once per horizontal tap and K chunk, accumulates into the
+// three output rows it feeds (r+1, r, r-1) with one N = 192 MMA: 12 MMAs per
+// input row instead of 36.  The three accumulators must be adjacent in tensor
+// memory: output row g of the CTA (counted across its strips) owns TMEM block
+// (-g) mod 8 of 64 columns, so consecutive output rows sit in descending
+// blocks and the three blocks of one input row are ascending; where they
+// wrap past block 7 the MMA is split in two.  Every MMA accumulates: the
+// epilogue zeroes a block after draining it (and all blocks start zeroed), so
+// no MMA needs to know whether it is an accumulator's first.  Strip edges use
+// N = 64 or 128 (an edge input row feeds one or two output rows of the
+// strip).  An input row's ring slot is released as soon as its 12 MMAs are
+// issued.
+constexpr int NSLOT_T = 6;
+constexpr int TBLK = 8;  // accumulator blocks of 64 columns (512 TMEM columns)
+
+struct TriSmem {
+  uint8_t slot[NSLOT_T][RW_BYTES];
+  uint8_t w[W_BYTES];  // [dx][dy][64 co][64 ci]: per dx a 192 x 64 K-major B operand
+  uint64_t full[NSLOT_T], empty[NSLOT_T];
+  uint64_t wbar, done;
+  uint64_t tfull[TBLK], tempty[TBLK];
+  uint32_t tmem_base;
+  float bias[CH];
+};
+
+__device__ __forceinline__ uint32_t tblk(uint32_t g) { return (TBLK - (g & (TBLK - 1))) & (TBLK - 1); }
+
+__device__ __forceinline__ void tmem_zero32(uint32_t taddr) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,"
+      "%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1};" ::"r"(taddr),
+      "r"(0u)
+      : "memory");
+}
+__device__ __forceinline__ void tmem_st_wait() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
+__global__ void __launch_bounds__(THREADS, 1)
+k_conv_fwd_tri(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmW,
+               ConvEpi E, int R) {
+  extern __shared__ uint8_t smem_raw[];
+  TriSmem& S = *reinterpret_cast<TriSmem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int xtiles = E.W / TM;
+  const int ystrips = (E.H + R - 1) / R;
+  const int nstrip = E.N * xtiles * ystrips;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < NSLOT_T; ++s) {
+      mbar_init(&S.full[s], 1);
+      mbar_init(&S.empty[s], 1);
+    }
+    mbar_init(&S.wbar, 1);
+    mbar_init(&S.done, 1);
+    for (int b = 0; b < TBLK; ++b) {
+      mbar_init(&S.tfull[b], 1);
+      mbar_init(&S.tempty[b], 128);
+    }
+    fence_barrier_init();
+  }
+  if (threadIdx.x < CH) S.bias[threadIdx.x] = E.bias ? E.bias[threadIdx.x] : 0.0f;
+  if (warp == 1) tmem_alloc(&S.tmem_base, 64 * TBLK);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = S.tmem_base;
+  if (warp >= 2) {  // every accumulator block starts at zero
+    const uint32_t tl = tmem + ((uint32_t)(32 * (warp & 3)) << 16);
+    for (int c = 0; c < 64 * TBLK; c += 32) tmem_zero32(tl + (uint32_t)c);
+    tmem_st_wait();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+
+  if (warp == 0 && lane == 0) {
+    // ---- TMA producer: rows y0-1 .. y1+1 of every strip, in order ----
+    mbar_expect_tx(&S.wbar, W_BYTES);
+    for (int tap = 0; tap < 9; ++tap)  // tap = 3*(dy+1) + (dx+1) -> [dx][dy]
+      tma_load_2d(S.w + ((tap % 3) * 3 + tap / 3) * WT_BYTES, &tmW, &S.wbar, 0, tap * CH);
+    uint32_t L = 0;  // loads issued
+    bool ok = true;
+    for (int st = blockIdx.x; st < nstrip && ok; st += gridDim.x) {
+      const int ys = st % ystrips, r0 = st / ystrips, xt = r0 % xtiles, n = r0 / xtiles;
+      const int y0 = ys * R, y1 = min(y0 + R, E.H) - 1;
+      for (int r = y0 - 1; r <= y1 + 1; ++r, ++L) {
+        const int slot = (int)(L % NSLOT_T);
+        const uint32_t ph = (L / NSLOT_T) & 1;
+        if (!mbar_wait(&S.empty[slot], ph ^ 1)) { fail(E.err, 31); ok = false; break; }
+        mbar_expect_tx(&S.full[slot], RW_BYTES);
+        tma_load_4d(S.slot[slot], &tmA, &S.full[slot], 0, xt * TM - 8, r, n);
+      }
+    }
+    // every armed load lands before the CTA may exit
+    for (int s = 0; s < NSLOT_T; ++s) {
+      const uint32_t armed = L / NSLOT_T + ((uint32_t)s < L % NSLOT_T ? 1u : 0u);
+      if (armed) mbar_wait(&S.full[s], (armed - 1) & 1);
+    }
+    mbar_wait(&S.wbar, 0);
+  } else if (warp == 1 && lane == 0) {
+    // ---- MMA issuer ----
+    bool ok = mbar_wait(&S.wbar, 0);
+    if (!ok) fail(E.err, 32);
+    const uint32_t wbase = smem_u32(S.w);
+    uint32_t L = 0;  // loads consumed
+    uint32_t g0 = 0;  // CTA-wide index of the strip's first output row
+    for (int st = blockIdx.x; st < nstrip && ok; st += gridDim.x) {
+      const int ys = st % ystrips;
+      const int y0 = ys * R, y1 = min(y0 + R, E.H) - 1;
+      const int rows = y1 - y0 + 1;
+      for (int t = 0; t <= rows + 1 && ok; ++t) {
+        // input row y0-1+t feeds the strip's output rows o_lo .. o_hi
+        const int o_hi = min(t, rows - 1), o_lo = max(t - 2, 0);
+        const uint32_t ld = L + (uint32_t)t;
+        const int slot = (int)(ld % NSLOT_T);
+        if (t <= rows - 1) {  // output row t starts here: its block must be drained and zeroed
+          const uint32_t g = g0 + (uint32_t)t;
+          if (!mbar_wait(&S.tempty[tblk(g)], ((g / TBLK) & 1) ^ 1)) { fail(E.err, 33); ok = false; break; }
+        }
+        if (!mbar_wait(&S.full[slot], (ld / NSLOT_T) & 1)) { fail(E.err, 34); ok = false; break; }
+        tc_fence_after();
+        const int nout = o_hi - o_lo + 1;
+        const uint32_t dfirst = tblk(g0 + (uint32_t)o_hi);
+        const int n1 = min(nout, TBLK - (int)dfirst), n2 = nout - n1;
+        const int bfirst = t - o_hi;  // B block: 0 for dy = -1, 1 for 0, 2 for +1
+        const uint32_t id1 = idesc(128, 64 * n1, 0, 0);
+        const uint32_t id2 = idesc(128, 64 * (n2 > 0 ? n2 : 1), 0, 0);
+        const uint32_t sbase = smem_u32(S.slot[slot]);
+#pragma unroll
+        for (int dx = 0; dx < 3; ++dx) {
+          const uint32_t a0 = sbase + (uint32_t)(7 + dx) * 128u;
+          const uint32_t b0 = wbase + (uint32_t)(dx * 3 + bfirst) * WT_BYTES;
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            mma_bf16(tmem + dfirst * 64, sdesc(a0 + 32 * k, 16, 1024), sdesc(b0 + 32 * k, 16, 1024), id1, 1);
+            if (n2 > 0)
+              mma_bf16(tmem, sdesc(a0 + 32 * k, 16, 1024), sdesc(b0 + (uint32_t)n1 * WT_BYTES + 32 * k, 16, 1024),
+                       id2, 1);
+          }
+        }
+        mma_commit(&S.empty[slot]);                         // the input row has had its last use
+        if (t >= 2) mma_commit(&S.tfull[tblk(g0 + (uint32_t)(t - 2))]);  // output row t-2 is complete
+      }
+      L += (uint32_t)rows + 2;
+      g0 += (uint32_t)rows;
+    }
+    mma_commit(&S.done);  // completes once every MMA issued above has finished
+    mbar_wait(&S.done, 0);
+  } else if (warp >= 2) {
+    // ---- epilogue: drain, zero for the next use, then bias/ReLU/residual/mask -> BF16 ----
+    const int q = warp & 3;
+    const int row = 32 * q + lane;
+    uint32_t g = 0;
+    bool ok = true;
+    for (int st = blockIdx.x; st < nstrip && ok; st += gridDim.x) {
+      const int ys = st % ystrips, r0 = st / ystrips, xt = r0 % xtiles, n = r0 / xtiles;
+      const int y0 = ys * R, y1 = min(y0 + R, E.H) - 1;
+      for (int y = y0; y <= y1; ++y, ++g) {
+        const uint32_t b = tblk(g);
+        if (!mbar_wait_warp(&S.tfull[b], (g / TBLK) & 1)) { fail(E.err, 35); ok = false; break; }
+        tc_fence_after();
+        float v[64];
+        const uint32_t ta = tmem + b * 64 + ((uint32_t)(32 * q) << 16);
+        tmem_ld32(ta, v);
+        tmem_ld32(ta + 32, v + 32);
+        tmem_zero32(ta);
+        tmem_zero32(ta + 32);
+        tmem_st_wait();
+        tc_fence_before();
+        mbar_arrive(&S.tempty[b]);
+        const long p = ((long)(n * E.H + y) * E.W + xt * TM + row);
+        epilogue_store(E, S.bias, v, p);
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    __syncwarp();
+    tc_fence_after();
+    tmem_dealloc(tmem, 64 * TBLK);
+  }
+}
+
 struct WgSmem {
   // per stage: x window of tap a, x window of tap b (all ones for the last
   // tap pair, which then yields the bias gradient), dz window
@@ -677,7 +865,8 @@ cudaError_t w_map(CUtensorMap* m, const void* base) {
 
 int g_sms[64];
 bool g_attr[64];
-int g_fwd_variant = 1;  // 1: row ring (k_conv_fwd_rows), 0: a TMA window per tap (k_conv_fwd)
+int g_fwd_variant = 2;  // 2: three output rows per MMA (k_conv_fwd_tri), 1: row ring
+                        // (k_conv_fwd_rows), 0: a TMA window per tap (k_conv_fwd)
 int g_fwd_rows = 16;    // rows per strip of the row-ring kernel
 
 // SM count of the current device; opts the kernels into their shared memory.
@@ -695,6 +884,9 @@ cudaError_t prepare_device(int* sms) {
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k_conv_fwd_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)(sizeof(RowSmem) + 1024));
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_conv_fwd_tri, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(sizeof(TriSmem) + 1024));
     if (e != cudaSuccess) return e;
     g_attr[dev] = true;
   }
@@ -718,6 +910,14 @@ cudaError_t conv_fwd(const __nv_bfloat16* x, const __nv_bfloat16* w, const ConvE
   if ((e = prepare_device(&sms)) != cudaSuccess) return e;
   CUtensorMap ta, tw;
   if ((e = w_map(&tw, w)) != cudaSuccess) return e;
+  if (g_fwd_variant == 2) {
+    if ((e = act_map(&ta, x, epi.N, epi.H, epi.W, RW_PIX)) != cudaSuccess) return e;
+    const int R = g_fwd_rows;
+    const long nstrip = (long)epi.N * (epi.W / TM) * ((epi.H + R - 1) / R);
+    const int grid = (int)(nstrip < sms ? nstrip : sms);
+    k_conv_fwd_tri<<<grid, THREADS, sizeof(TriSmem) + 1024, s>>>(ta, tw, epi, R);
+    return cudaGetLastError();
+  }
   if (g_fwd_variant == 1) {
     if ((e = act_map(&ta, x, epi.N, epi.H, epi.W, RW_PIX)) != cudaSuccess) return e;
     const int R = g_fwd_rows;
@@ -735,7 +935,7 @@ cudaError_t conv_fwd(const __nv_bfloat16* x, const __nv_bfloat16* w, const ConvE
 
 int set_fwd_variant(int variant, int rows) {
   const int prev = g_fwd_variant;
-  if (variant == 0 || variant == 1) g_fwd_variant = variant;
+  if (variant >= 0 && variant <= 2) g_fwd_variant = variant;
   if (rows >= 1 && rows <= 4096) g_fwd_rows = rows;
   return prev;
 }

@@ -36,9 +36,10 @@ struct WgradArgs {
 
 // W % 128 == 0, x and w 16-byte aligned; w = [9][64 out][64 in] BF16.
 cudaError_t conv_fwd(const __nv_bfloat16* x, const __nv_bfloat16* w, const ConvEpi& epi, cudaStream_t s);
-// Process-wide choice of the forward kernel: 1 = row ring (default), 0 = a
-// TMA window per tap; rows per strip of the row ring.  Returns the previous
-// variant; out-of-range values leave the setting unchanged.
+// Process-wide choice of the forward kernel: 2 = three output rows per MMA
+// (default), 1 = row ring, 0 = a TMA window per tap; rows per strip of the
+// ring kernels.  Returns the previous variant; out-of-range values leave the
+// setting unchanged.
 int set_fwd_variant(int variant, int rows);
 // W % 64 == 0.  ctas <= 0 picks the count from the SM count.
 cudaError_t conv_wgrad(const __nv_bfloat16* x, const __nv_bfloat16* dz, const WgradArgs& g, int ctas,

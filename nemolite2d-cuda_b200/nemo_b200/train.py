@@ -161,6 +161,62 @@ class PairSampler:
         return s0, s1, t1
 
 
+class MixSampler:
+    """Batches drawn from several samplers in proportion to `weights`."""
+
+    def __init__(self, samplers, weights, seed=0):
+        self.samplers = list(samplers)
+        w = np.asarray(weights, dtype=np.float64)
+        self.p = w / w.sum()
+        self.rng = np.random.default_rng(seed)
+
+    def batch(self, n):
+        return self.samplers[int(self.rng.choice(len(self.samplers), p=self.p))].batch(n)
+
+
+def rollout_runs(sur, seed, nmem, side, windows, k=10, anchor=100, amp_scale=0.2, bound=2.5):
+    """Training pairs along hybrid trajectories: members run from rest through
+    one solver window, then each window advances by (anchor - k) / k calls of
+    the surrogate `sur` followed by k FP64 solver steps, and the pair is (the
+    state the surrogate left, the solver's state k steps later) -- the states
+    the hybrid controller meets, which carry the surrogate's own errors.
+    Returns (snaps, tides) in the paired layout [2*windows][kept][side][side][4]
+    of the members that stay bounded; the number dropped is in
+    rollout_runs.dropped."""
+    torch = _torch()
+    members = square_members(seed, nmem, side, amp_scale)
+    ens = Ensemble(members, **COMMON)
+    snaps = torch.empty((2 * windows, nmem, side, side, 4), dtype=torch.float32, device="cuda")
+    tides = torch.empty((2 * windows, nmem), dtype=torch.float32)
+    ens.step_n(1, anchor)
+    istp = anchor
+    for w in range(windows):
+        for _ in range((anchor - k) // k):
+            sur.advance_ens(ens, istp + k)
+            istp += k
+        torch.cuda.synchronize()
+        sur.pack_ens(ens, snaps[2 * w].data_ptr())
+        tides[2 * w] = torch.tensor([tide_of(m, istp) for m in members], dtype=torch.float32)
+        ens.step_n(istp + 1, k)
+        istp += k
+        torch.cuda.synchronize()
+        sur.pack_ens(ens, snaps[2 * w + 1].data_ptr())
+        tides[2 * w + 1] = torch.tensor([tide_of(m, istp) for m in members], dtype=torch.float32)
+    ens.close()
+    amp = torch.tensor([m.amp_tide for m in members], dtype=torch.float32, device="cuda")
+    finite = torch.isfinite(snaps).flatten(2).all(2).all(0)
+    peak = torch.nan_to_num(snaps[..., 0].abs(), nan=float("inf")).flatten(2).amax(2).amax(0)
+    keep = (finite & (peak <= bound * amp)).nonzero().flatten()
+    rollout_runs.dropped = nmem - int(keep.numel())
+    snaps = snaps.index_select(1, keep)
+    tides = tides.cuda().index_select(1, keep)
+    torch.cuda.synchronize()
+    return snaps, tides
+
+
+rollout_runs.dropped = 0
+
+
 def train(sur, sampler, iters, batch, lr=1e-3, weight_decay=1e-4, lr_min=1e-5, log_every=0):
     """AdamW with cosine learning-rate decay; returns the loss history."""
     losses = []
