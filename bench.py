@@ -66,6 +66,8 @@ def parse():
     ap.add_argument("--train-runs", type=int, default=96, help="training runs (hybrid)")
     ap.add_argument("--rollout-runs", type=int, default=48, help="rollout fine-tuning runs (hybrid)")
     ap.add_argument("--rollout-windows", type=int, default=20, help="windows per rollout run (hybrid)")
+    ap.add_argument("--noise", type=float, default=0.03,
+                    help="training input noise, in units of each field's spread (hybrid)")
     ap.add_argument("--finetune-iters", type=int, default=0,
                     help="fine-tuning iterations on rollout pairs (hybrid; 0: none)")
     ap.add_argument("--batch", type=int, default=64, help="images per conv call (conv workload)")
@@ -449,7 +451,10 @@ def run_hybrid(args):
     trainer.set_norm(*norm)
     t_train = time.time()
     clean = tr.PairSampler(snaps, tides, seed=3, paired=True)
-    losses = tr.train(trainer, clean, iters=args.train_iters, batch=64, lr=1e-3)
+    # inputs perturbed by noise, targets the true states: the network learns to
+    # advance slightly wrong states, as it meets them after its own calls
+    noisy = tr.NoisySampler(clean, args.noise, tr.field_std(snaps), seed=5)
+    losses = tr.train(trainer, noisy, iters=args.train_iters, batch=64, lr=1e-3)
     if args.finetune_iters > 0:
         # optional fine-tuning on the states the hybrid meets: pairs along
         # trajectories the surrogate itself advances between solver windows
@@ -461,7 +466,7 @@ def run_hybrid(args):
     t_train = time.time() - t_train
     params = trainer.params()
     trainer.close()
-    del snaps, tides, clean
+    del snaps, tides, clean, noisy
     torch.cuda.empty_cache()
     # ---- members: seeded candidates screened by the FP64 solver over the run
     # (the reference scheme lets a tide that starts rising grow without bound
@@ -509,6 +514,7 @@ def run_hybrid(args):
                        "candidates": len(cands), "screened_out": len(cands) - len(ok),
                        "patch": P, "train_side": ts, "train_steps": args.train_steps,
                        "train_runs": args.train_runs, "fallback": "per member",
+                       "train_input_noise": args.noise,
                        "rollout_runs": args.rollout_runs, "rollout_windows": args.rollout_windows,
                        "rollout_runs_dropped": tr.rollout_runs.dropped,
                        "finetune_iters": args.finetune_iters,

@@ -344,6 +344,10 @@ int nemo_conv3x3_wgrad(const void* x, const void* dz, float* dw, float* db, int 
  * window per tap.  Returns the previous variant; values out of range change
  * nothing. */
 int nemo_conv3x3_fwd_variant(int variant, int rows);
+/* Process-wide weight-gradient kernel: 1 (default) multiplies the x windows of
+ * two horizontal taps with the dz windows of three rows (six taps per N = 192
+ * MMA); 0 pairs taps with N = 64 MMAs.  Returns the previous variant. */
+int nemo_conv3x3_wgrad_variant(int variant);
 
 /* ---- drop-in symbols (cuda/cuda_nemolite2d.cu:234-270) --------------------
  * One default context.  Errors are printed to stderr and kept in a sticky

@@ -826,6 +826,137 @@ k_conv_wgrad(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CU
   }
 }
 
+// ---- weight gradient with three vertical taps per MMA ----------------------------
+// dw[dy,dx][co][ci] = sum_q x[q + (0,dx)][ci] dz[q - (dy,0)][co]: for one pixel
+// chunk q (64 pixels of an image row) the x windows of two horizontal taps
+// form A (M = 128: dx_a ci 0-63, dx_b ci 0-63) and the dz windows of rows
+// y+1, y, y-1 form B (N = 192: dy = -1, 0, +1), so one chunk's 4 MMAs of
+// 128 x 192 x 16 cover six taps.  gridDim.y = 2 tap groups: dx = (-1, 0) and
+// (+1, ones); the all-ones window of the second group gives the bias
+// gradient in its dy = 0 block (the other two blocks of those rows are not
+// used).  Operands are MN-major straight from the NHWC tensors: the A halves
+// and the B blocks sit WG_TILE bytes apart (leading byte offset).
+constexpr int WT_NST = 4;  // stages of 5 windows (40 KiB)
+
+struct WtSmem {
+  uint8_t st[WT_NST][5][WG_TILE];  // x_a, x_b, dz(y+1), dz(y), dz(y-1)
+  uint64_t full[WT_NST], empty[WT_NST];
+  uint64_t done;
+  uint32_t tmem_base;
+  uint8_t pad[8192];  // descriptor strides never reach past the allocation
+};
+
+__global__ void __launch_bounds__(THREADS, 1)
+k_conv_wgrad_tri(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmZ,
+                 WgradArgs G) {
+  extern __shared__ uint8_t smem_raw[];
+  WtSmem& S = *reinterpret_cast<WtSmem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const bool bias_group = (blockIdx.y == 1);
+  const int dxa = bias_group ? 1 : -1;  // second half: dx = 0, or the ones window
+  const int xch = G.W / WG_PIX;
+  const long nchunk = (long)G.N * G.H * xch;
+  const long c_begin = nchunk * blockIdx.x / gridDim.x;
+  const long c_end = nchunk * (blockIdx.x + 1) / gridDim.x;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < WT_NST; ++s) {
+      mbar_init(&S.full[s], 1);
+      mbar_init(&S.empty[s], 1);
+    }
+    mbar_init(&S.done, 1);
+    fence_barrier_init();
+  }
+  if (bias_group && warp >= 2) {
+    const uint4 ones = make_uint4(0x3F803F80u, 0x3F803F80u, 0x3F803F80u, 0x3F803F80u);
+    for (int s = 0; s < WT_NST; ++s) {
+      uint4* d = reinterpret_cast<uint4*>(S.st[s][1]);
+      for (int i = threadIdx.x - 64; i < WG_TILE / 16; i += THREADS - 64) d[i] = ones;
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 1) tmem_alloc(&S.tmem_base, 256);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = S.tmem_base;
+  const bool have = c_end > c_begin;
+
+  if (warp == 0 && lane == 0) {
+    int stage = 0;
+    uint32_t phase = 0;
+    const uint32_t bytes = (bias_group ? 4 : 5) * WG_TILE;
+    for (long c = c_begin; c < c_end; ++c) {
+      const int xc = (int)(c % xch);
+      const long r = c / xch;
+      const int y = (int)(r % G.H), n = (int)(r / G.H);
+      const int x0 = xc * WG_PIX;
+      if (!mbar_wait(&S.empty[stage], phase ^ 1)) { fail(G.err, 41); break; }
+      mbar_expect_tx(&S.full[stage], bytes);
+      tma_load_4d(S.st[stage][0], &tmX, &S.full[stage], 0, x0 + dxa, y, n);
+      if (!bias_group) tma_load_4d(S.st[stage][1], &tmX, &S.full[stage], 0, x0, y, n);
+      for (int j = 0; j < 3; ++j)  // dz rows y+1, y, y-1 (dy = -1, 0, +1)
+        tma_load_4d(S.st[stage][2 + j], &tmZ, &S.full[stage], 0, x0, y + 1 - j, n);
+      if (++stage == WT_NST) { stage = 0; phase ^= 1; }
+    }
+    for (int s = 0; s < WT_NST; ++s) mbar_wait(&S.full[s], s < stage ? phase : phase ^ 1);
+  } else if (warp == 1 && lane == 0) {
+    const uint32_t ID = idesc(128, 192, 1, 1);
+    int stage = 0;
+    uint32_t phase = 0;
+    bool first = true;
+    for (long c = c_begin; c < c_end; ++c) {
+      if (!mbar_wait(&S.full[stage], phase)) { fail(G.err, 42); break; }
+      tc_fence_after();
+      const uint32_t a = smem_u32(S.st[stage][0]);
+      const uint32_t bz = smem_u32(S.st[stage][2]);
+#pragma unroll
+      for (int k = 0; k < WG_PIX / 16; ++k) {
+        mma_bf16(tmem, sdesc(a + 2048 * k, WG_TILE, 1024), sdesc(bz + 2048 * k, WG_TILE, 1024), ID,
+                 first ? 0u : 1u);
+        first = false;
+      }
+      mma_commit(&S.empty[stage]);
+      if (++stage == WT_NST) { stage = 0; phase ^= 1; }
+    }
+    mma_commit(&S.done);
+    if (!mbar_wait(&S.done, 0)) fail(G.err, 43);
+  }
+  if (warp >= 2 && have) {
+    const int q = warp & 3;
+    const int row = 32 * q + lane;  // (half, ci)
+    if (mbar_wait_warp(&S.done, 0)) {
+      tc_fence_after();
+      const uint32_t taddr = tmem + ((uint32_t)(32 * q) << 16);
+      const int half = row >> 6, ci = row & 63;
+      for (int j = 0; j < 3; ++j) {  // dy = j - 1
+        float v[64];
+        tmem_ld32(taddr + 64 * j, v);
+        tmem_ld32(taddr + 64 * j + 32, v + 32);
+        if (half == 0 || !bias_group) {
+          const int dx = half == 0 ? dxa : 0;
+          const int tap = 3 * j + (dx + 1);
+          float* dw = G.dw + (long)tap * CH * CH + ci;
+#pragma unroll
+          for (int co = 0; co < 64; ++co) atomicAdd(dw + co * CH, v[co]);
+        } else if (j == 1 && ci == 0 && G.db) {
+#pragma unroll
+          for (int co = 0; co < 64; ++co) atomicAdd(G.db + co, v[co]);
+        }
+      }
+    } else {
+      fail(G.err, 44);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    __syncwarp();
+    tc_fence_after();
+    tmem_dealloc(tmem, 256);
+  }
+}
+
 // ---- tensor maps ---------------------------------------------------------------
 PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
 
@@ -868,6 +999,7 @@ bool g_attr[64];
 int g_fwd_variant = 2;  // 2: three output rows per MMA (k_conv_fwd_tri), 1: row ring
                         // (k_conv_fwd_rows), 0: a TMA window per tap (k_conv_fwd)
 int g_fwd_rows = 16;    // rows per strip of the row-ring kernel
+int g_wgrad_variant = 1;  // 1: three vertical taps per MMA (k_conv_wgrad_tri), 0: tap pairs
 
 // SM count of the current device; opts the kernels into their shared memory.
 cudaError_t prepare_device(int* sms) {
@@ -881,6 +1013,9 @@ cudaError_t prepare_device(int* sms) {
     e = cudaFuncSetAttribute(k_conv_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(sizeof(FwdSmem) + 1024));
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k_conv_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(sizeof(WgSmem) + 1024));
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_conv_wgrad_tri, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(sizeof(WtSmem) + 1024));
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k_conv_fwd_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)(sizeof(RowSmem) + 1024));
@@ -933,6 +1068,12 @@ cudaError_t conv_fwd(const __nv_bfloat16* x, const __nv_bfloat16* w, const ConvE
   return cudaGetLastError();
 }
 
+int set_wgrad_variant(int variant) {
+  const int prev = g_wgrad_variant;
+  if (variant == 0 || variant == 1) g_wgrad_variant = variant;
+  return prev;
+}
+
 int set_fwd_variant(int variant, int rows) {
   const int prev = g_fwd_variant;
   if (variant >= 0 && variant <= 2) g_fwd_variant = variant;
@@ -952,6 +1093,15 @@ cudaError_t conv_wgrad(const __nv_bfloat16* x, const __nv_bfloat16* dz, const Wg
   CUtensorMap tx, tz;
   if ((e = act_map(&tx, x, g.N, g.H, g.W, WG_PIX)) != cudaSuccess) return e;
   if ((e = act_map(&tz, dz, g.N, g.H, g.W, WG_PIX)) != cudaSuccess) return e;
+  if (g_wgrad_variant == 1) {
+    // one CTA per SM: one wave of the 2 tap groups
+    int gx = ctas > 0 ? ctas : sms / 2;
+    const long nchunk = (long)g.N * g.H * (g.W / WG_PIX);
+    if (gx > nchunk) gx = (int)nchunk;
+    if (gx < 1) gx = 1;
+    k_conv_wgrad_tri<<<dim3((unsigned)gx, 2), THREADS, sizeof(WtSmem) + 1024, s>>>(tx, tz, g);
+    return cudaGetLastError();
+  }
   // two CTAs fit on an SM (shared memory and tensor memory): one wave of 5 pairs
   int gx = ctas > 0 ? ctas : (2 * sms) / 5;
   const long nchunk = (long)g.N * g.H * (g.W / WG_PIX);

@@ -41,6 +41,9 @@ cudaError_t conv_fwd(const __nv_bfloat16* x, const __nv_bfloat16* w, const ConvE
 // ring kernels.  Returns the previous variant; out-of-range values leave the
 // setting unchanged.
 int set_fwd_variant(int variant, int rows);
+// Process-wide choice of the weight-gradient kernel: 1 = three vertical taps
+// per MMA (default), 0 = tap pairs.  Returns the previous variant.
+int set_wgrad_variant(int variant);
 // W % 64 == 0.  ctas <= 0 picks the count from the SM count.
 cudaError_t conv_wgrad(const __nv_bfloat16* x, const __nv_bfloat16* dz, const WgradArgs& g, int ctas,
                        cudaStream_t s);

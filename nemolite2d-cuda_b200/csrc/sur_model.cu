@@ -1032,6 +1032,8 @@ int nemo_conv3x3_fwd(const void* x, const void* w, const float* bias, const void
 
 int nemo_conv3x3_fwd_variant(int variant, int rows) { return sur::set_fwd_variant(variant, rows); }
 
+int nemo_conv3x3_wgrad_variant(int variant) { return sur::set_wgrad_variant(variant); }
+
 int nemo_conv3x3_wgrad(const void* x, const void* dz, float* dw, float* db, int n, int h, int wd, int ctas,
                        int* err, void* stream) {
   if (!x || !dz || !dw || !err) return NEMO_ERR_INVALID;

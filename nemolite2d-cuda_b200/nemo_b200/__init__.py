@@ -44,7 +44,7 @@ EXPORTED = [
     "nemo_sur_get_norm", "nemo_sur_predict", "nemo_sur_loss_grad", "nemo_sur_adamw",
     "nemo_sur_train_step", "nemo_sur_pack_ens", "nemo_sur_advance_ens", "nemo_ens_compare",
     "nemo_hyb_default_config", "nemo_hyb_run", "nemo_conv3x3_fwd", "nemo_conv3x3_wgrad",
-    "nemo_conv3x3_fwd_variant",
+    "nemo_conv3x3_fwd_variant", "nemo_conv3x3_wgrad_variant",
     "cuda_setup_model_params_", "cuda_initialise_grid_", "cuda_continuity_", "cuda_momentum_",
     "cuda_boundary_conditions_", "cuda_next_", "cuda_retrieve_grid_constants_",
     "cuda_retrieve_results_", "cuda_finalise_", "nemo_compat_last_status", "nemo_compat_context",

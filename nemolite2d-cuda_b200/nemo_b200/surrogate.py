@@ -58,6 +58,7 @@ def declare(L):
     L.nemo_conv3x3_fwd.argtypes = [vp, vp, vp, vp, vp, ip, vp, vp, ip, ip, ip, vp, vp]
     L.nemo_conv3x3_wgrad.argtypes = [vp, vp, vp, vp, ip, ip, ip, ip, vp, vp]
     L.nemo_conv3x3_fwd_variant.argtypes = [ip, ip]
+    L.nemo_conv3x3_wgrad_variant.argtypes = [ip]
 
 
 def _fptr(a):
@@ -212,6 +213,12 @@ def conv3x3_fwd_variant(lib, variant, rows=0):
     the default; 1: row ring; 0: window per tap) and the rows per strip of the
     ring kernels; returns the previous variant."""
     return lib.nemo_conv3x3_fwd_variant(variant, rows)
+
+
+def conv3x3_wgrad_variant(lib, variant):
+    """Select the weight-gradient kernel process-wide (1: three vertical taps
+    per MMA, the default; 0: tap pairs); returns the previous variant."""
+    return lib.nemo_conv3x3_wgrad_variant(variant)
 
 
 def conv3x3_wgrad(lib, x, dz, dw, n, h, wd, err, db=None, ctas=0, stream=None):

@@ -161,6 +161,38 @@ class PairSampler:
         return s0, s1, t1
 
 
+class NoisySampler:
+    """Pairs of `base` with Gaussian noise of `sigma` x each field's spread
+    added to the input state (ssh, u, v) and the target left the true state
+    10 steps on: the network learns to advance a slightly wrong state to the
+    right one, which is what it meets after its own earlier calls."""
+
+    def __init__(self, base, sigma, std, seed=0):
+        torch = _torch()
+        self.base, self.sigma = base, float(sigma)
+        self.scale = torch.tensor([float(std[0]), float(std[1]), float(std[2]), 0.0],
+                                  dtype=torch.float32, device="cuda") * self.sigma
+        self.gen = torch.Generator(device="cuda")
+        self.gen.manual_seed(seed)
+        self._torch = torch
+
+    def batch(self, n):
+        s0, s1, t1 = self.base.batch(n)
+        if self.sigma > 0:
+            noise = self._torch.randn(s0.shape, generator=self.gen, device="cuda", dtype=self._torch.float32)
+            s0 = (s0 + noise * self.scale).contiguous()
+            self._torch.cuda.synchronize()
+            self.s0 = s0  # keep alive while the library reads
+        return s0, s1, t1
+
+
+def field_std(snaps):
+    """Spread of ssh, u, v over a snapshot tensor [S][N][H][W][4] (up to 8 runs)."""
+    sub = snaps[:, ::max(1, snaps.shape[1] // 8)]
+    x = sub.reshape(-1, 4).double()
+    return [float(v) for v in x.std(0)[:3]]
+
+
 class MixSampler:
     """Batches drawn from several samplers in proportion to `weights`."""
 

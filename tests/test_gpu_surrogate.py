@@ -115,8 +115,19 @@ def test_dgrad_with_flipped_weights_matches_oracle(env, variant):
     assert np.abs(o32 - ref[..., :4]).max() <= 1e-4 * np.abs(ref[..., :4]).max()
 
 
-@pytest.mark.parametrize("shape,ctas", [((2, 5, 128), 0), ((1, 7, 192), 3), ((3, 2, 64), 1)])
-def test_wgrad_and_bias_grad_match_oracle(env, shape, ctas):
+@pytest.fixture(params=[1, 0], ids=["wg-tri", "wg-pairs"])
+def wvariant(request, env):
+    """Each weight-gradient kernel (six taps per MMA, tap pairs), restored to
+    the default afterwards."""
+    torch, nb, sm = env
+    lib = nb.load(False)
+    prev = sm.conv3x3_wgrad_variant(lib, request.param)
+    yield request.param
+    sm.conv3x3_wgrad_variant(lib, prev)
+
+
+@pytest.mark.parametrize("shape,ctas", [((2, 5, 128), 0), ((1, 7, 192), 3), ((3, 2, 64), 1), ((1, 1, 64), 0)])
+def test_wgrad_and_bias_grad_match_oracle(env, wvariant, shape, ctas):
     torch, nb, sm = env
     N, H, W = shape
     rng = np.random.default_rng(H * W)
