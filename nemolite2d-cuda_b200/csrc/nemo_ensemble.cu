@@ -36,15 +36,12 @@ struct MemberDev {
   const double *rhu, *rhv;
 };
 
-// FLAT = false: a persistent grid whose warps loop over the work list;
-// FLAT = true: one warp per work item (the grid covers the list), which
-// leaves registers for the twice-unrolled row loop.
-template <int NW, int MB, int PF, bool FLAT>
+template <int NW, int MB, int PF>
 __global__ void __launch_bounds__(32 * NW, MB)
 k_ens_step(const MemberDev* __restrict__ mem, const int4* __restrict__ work, int nwork, Consts C,
            const double* __restrict__ tide, int parity) {
   const int lane = threadIdx.x & 31;
-  const int nw = FLAT ? nwork : (int)gridDim.x * NW;
+  const int nw = (int)gridDim.x * NW;
   for (int w = (int)blockIdx.x * NW + (int)(threadIdx.x >> 5); w < nwork; w += nw) {
     const int4 it = work[w];  // member, c0, J0, J1
     const MemberDev* M = mem + it.x;
@@ -65,7 +62,7 @@ k_ens_step(const MemberDev* __restrict__ mem, const int4* __restrict__ work, int
     const Layout L = M->L;
     if constexpr (PF >= 2) {
       __shared__ double ring[NW * stepdev::RING_DOUBLES];
-      stepdev::run_strip_ring<PF == 3, FLAT ? 2 : 1>(L, C, A, it.y, it.z, it.w, lane,
+      stepdev::run_strip_ring<PF == 3, 1>(L, C, A, it.y, it.z, it.w, lane,
                                        ring + (threadIdx.x >> 5) * stepdev::RING_DOUBLES);
     } else {
       stepdev::run_strip<PF>(L, C, A, it.y, it.z, it.w, lane);
@@ -122,30 +119,24 @@ __global__ void __launch_bounds__(CT) k_ens_cols(const int* __restrict__ row_off
   if (threadIdx.x == 0) out[3 * m + f] = s;
 }
 
-// ctas < 0: one warp per work item (FLAT); 0: every resident CTA slot; > 0:
-// that many persistent CTAs.
 template <int NW, int MB, int PF>
 cudaError_t launch_ens_variant(const MemberDev* mem, const int4* work, int nwork, const Consts& C,
                                const double* tide, int parity, int ctas, cudaStream_t s) {
-  const int need = (nwork + NW - 1) / NW;
-  if (ctas < 0) {
-    k_ens_step<NW, MB, PF, true><<<need > 0 ? need : 1, 32 * NW, 0, s>>>(mem, work, nwork, C, tide, parity);
-    return cudaGetLastError();
-  }
-  if (ctas == 0) {
+  if (ctas <= 0) {
     static int slots = 0;
     if (slots == 0) {
       int dev = 0, sms = 0, per_sm = 0;
       cudaGetDevice(&dev);
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ens_step<NW, MB, PF, false>, 32 * NW, 0);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ens_step<NW, MB, PF>, 32 * NW, 0);
       slots = sms * (per_sm > 0 ? per_sm : 1);
     }
     ctas = slots;
   }
+  const int need = (nwork + NW - 1) / NW;
   if (ctas > need) ctas = need;
   if (ctas < 1) ctas = 1;
-  k_ens_step<NW, MB, PF, false><<<ctas, 32 * NW, 0, s>>>(mem, work, nwork, C, tide, parity);
+  k_ens_step<NW, MB, PF><<<ctas, 32 * NW, 0, s>>>(mem, work, nwork, C, tide, parity);
   return cudaGetLastError();
 }
 
@@ -620,7 +611,7 @@ int nemo_ens_set_state(nemo_ens* e, int member, const double* sshn, const double
 int nemo_ens_set_schedule(nemo_ens* e, const nemo_ens_schedule* s) {
   if (!e) return NEMO_ERR_STATE;
   if (!s || !ens_variant_ok(s->warps, s->occupancy, e->recip_nr_ok) || s->rows < 1 || s->rows > 65536 ||
-      s->order < 0 || s->order > 1 || s->ctas < -1)
+      s->order < 0 || s->order > 1 || s->ctas < 0)
     return NEMO_ERR_INVALID;
   int st = set_dev(e); if (st) return st;
   const bool rebuild = s->rows != e->sched.rows || s->order != e->sched.order;
