@@ -81,6 +81,22 @@ def cells():
     return WORKLOAD["jpi"] * WORKLOAD["jpj"]
 
 
+def max_over_ranks(ms, dist=None, device="cuda"):
+    """The largest of every rank's time (the job's time); ms itself on one rank."""
+    if dist is None:
+        return ms
+    import torch
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(cells_per_rank, steps, world, t_max_ms):
+    """Whole-job cell-steps/s: every rank's independent replica advanced
+    `steps` steps, over the slowest rank's time."""
+    return cells_per_rank * steps * world / (t_max_ms / 1e3)
+
+
 def host_cores():
     try:
         return len(os.sched_getaffinity(0))
@@ -603,13 +619,8 @@ def main():
     clk = clocks.stop()
     total_ms = t_start.elapsed_time(t_end)
     fused_ms = sum(a.elapsed_time(b) for a, b in ev)
-    t_max = total_ms
-    if dist is not None:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
-    total_cell_steps = cells() * STEPS_PER_ITER * args.steps * world
-    value = total_cell_steps / (t_max / 1e3)
+    t_max = max_over_ranks(total_ms, dist)
+    value = job_rate(cells(), STEPS_PER_ITER * args.steps, world, t_max)
     launch_s = fused_ms / 1e3 / (STEPS_PER_ITER * args.steps)
     peak, peak_kind = load_peaks()
     achieved = BYTES_PER_CELL_STEP * cells() / launch_s / 1e9
@@ -638,12 +649,8 @@ def main():
         e1.record(stream)
         torch.cuda.synchronize()
         barrier()
-        e_ms = e0.elapsed_time(e1)
-        if dist is not None:
-            t = torch.tensor([e_ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e_ms = float(t.item())
-        e2e = {"value": cells() * STEPS_PER_ITER * k_e2e * world / (e_ms / 1e3),
+        e_ms = max_over_ranks(e0.elapsed_time(e1), dist)
+        e2e = {"value": job_rate(cells(), STEPS_PER_ITER * k_e2e, world, e_ms),
                "unit": "cell-steps/s", "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo,
                "steps": k_e2e}
 
