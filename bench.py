@@ -519,6 +519,8 @@ def run_hybrid(args):
     t_hyb = ev[2].elapsed_time(ev[3]) / 1e3
     clk = clocks.stop()
     err = sm.ens_compare(hyb, plain)
+    finite = np.isfinite(err).all(axis=1)
+    ef = err[finite] if finite.any() else np.full((1, 3), np.nan)
     v_plain = cells * nsteps / t_plain
     v_hyb = cells * nsteps / t_hyb
     line = {"metric": "hybrid vs plain ensemble cell-steps/s (32 x 2048^2, 5000 steps, <=1% SSH err)",
@@ -539,11 +541,12 @@ def run_hybrid(args):
             "plain_value": v_plain, "hybrid_over_plain": v_hyb / v_plain,
             "hybrid_stats": st,
             "surrogate_share": st["sur_steps"] / max(1, st["sur_steps"] + st["solver_steps"]),
-            "err_vs_fp64": {"ssh_max": float(err[:, 0].max()), "ssh_mean": float(err[:, 0].mean()),
-                            "u_max": float(err[:, 1].max()), "v_max": float(err[:, 2].max()),
-                            "u_mean": float(err[:, 1].mean()), "v_mean": float(err[:, 2].mean())},
+            "err_vs_fp64": {"ssh_max": float(ef[:, 0].max()), "ssh_mean": float(ef[:, 0].mean()),
+                            "u_max": float(ef[:, 1].max()), "v_max": float(ef[:, 2].max()),
+                            "u_mean": float(ef[:, 1].mean()), "v_mean": float(ef[:, 2].mean()),
+                            "members_nonfinite": int((~finite).sum())},
             "loss_first": losses[0], "loss_last": losses[-1], "clocks": clk,
-            "gpu_launches": None}
+            "gpu_launches": st["launches"]}
     print(json.dumps(line), flush=True)
 
 

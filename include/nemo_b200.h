@@ -123,6 +123,22 @@ int nemo_checksum(nemo_ctx* ctx, int field, double* out);
  * cuda_retrieve_results_ / cuda_retrieve_grid_constants_ (cu:565-593).
  * These synchronise the context's stream. */
 int nemo_retrieve(nemo_ctx* ctx, int field, double* host, long ld);
+/* Output record of the current state for the model's go2d files
+ * (original/nemolite2d.f90:773-799, which writes sshn and the cell-centred
+ * velocities every irecord steps): a kernel stages sshn,
+ * 0.5*(un(ji-1,jj)+un(ji,jj)) and 0.5*(vn(ji,jj-1)+vn(ji,jj)) at every T-cell
+ * on the device, and one copy on a side stream moves them to `host`
+ * ([3][jpj][jpi] FP64; pinned memory lets the copy overlap).  Returns at
+ * once: later steps wait only for the staging kernel, so the stepper keeps
+ * running while the record travels.  nemo_record_wait blocks until the last
+ * record has landed in host memory.  Not a counterpart of a reference
+ * routine: the reference copies whole fields back at every record. */
+int nemo_record(nemo_ctx* ctx, double* host);
+int nemo_record_wait(nemo_ctx* ctx);
+/* Page-locked host memory for records and retrievals (callers that do not link
+ * the CUDA runtime, e.g. Fortran or the C++ driver). */
+int nemo_host_alloc(size_t bytes, void** ptr);
+int nemo_host_free(void* ptr);
 /* Overwrites sshn, un, vn (dense, Fortran extents) and re-derives
  * sshn_u/sshn_v with the post-`next` interpolation (:736-764); the
  * open-boundary row sshn_v(:,0), which the reference never updates after
@@ -305,6 +321,8 @@ typedef struct nemo_hyb_config {
   double tol;     /* fallback threshold on relative SSH L2 error (0.01) */
   int per_member; /* 1: each member falls back on its own (anchor - k even);
                      0: any failing member sends the whole ensemble back (1) */
+  double quarantine; /* shadow error beyond which a member stays on the FP64
+                        solver for the rest of the run; 0: never (0.05) */
 } nemo_hyb_config;
 
 typedef struct nemo_hyb_stats {
@@ -315,6 +333,8 @@ typedef struct nemo_hyb_stats {
   long long windows;       /* member-windows */
   double max_shadow_err, last_shadow_err;  /* worst member's shadow error */
   double seconds;
+  long long launches;      /* kernels launched (solver steps and surrogate work) */
+  long long quarantined;   /* members kept on the solver after a large shadow error */
 } nemo_hyb_stats;
 
 int nemo_hyb_default_config(nemo_hyb_config* c);

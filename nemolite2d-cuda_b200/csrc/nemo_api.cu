@@ -35,6 +35,10 @@ struct nemo_ctx {
   bool uv_stale;          // stored sshn_u/sshn_v lag behind sshn
   bool recip_nr_ok;       // in-kernel reciprocal depths equal the stored ones
   nemo_schedule sched;
+  // output records (nemo_record): staging buffer, side stream and events
+  double* rec_dev = nullptr;
+  cudaStream_t rec_stream = nullptr;
+  cudaEvent_t rec_state = nullptr, rec_staged = nullptr, rec_copied = nullptr;
 };
 
 namespace {
@@ -293,8 +297,14 @@ int nemo_destroy(nemo_ctx* c) {
   if (!c) return NEMO_ERR_INVALID;
   if (c->device >= 0) cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->rec_stream) cudaStreamSynchronize(c->rec_stream);
   if (c->slab) cudaFree(c->slab);
   if (c->ck_host) cudaFreeHost(c->ck_host);
+  if (c->rec_dev) cudaFree(c->rec_dev);
+  if (c->rec_state) cudaEventDestroy(c->rec_state);
+  if (c->rec_staged) cudaEventDestroy(c->rec_staged);
+  if (c->rec_copied) cudaEventDestroy(c->rec_copied);
+  if (c->rec_stream) cudaStreamDestroy(c->rec_stream);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return NEMO_OK;
@@ -542,6 +552,55 @@ int nemo_checksums(nemo_ctx* c, double out[3]) {
   CK(cudaMemcpyAsync(c->ck_host, c->ck_out, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   for (int k = 0; k < 3; ++k) out[k] = c->ck_host[k];
+  return NEMO_OK;
+}
+
+int nemo_record(nemo_ctx* c, double* host) {
+  if (!c || !host) return NEMO_ERR_INVALID;
+  int st = set_device(c); if (st) return st;
+  if (!c->rec_dev) {
+    CK(cudaMalloc(&c->rec_dev, 3 * (size_t)c->L.jpi * c->L.jpj * sizeof(double)));
+    CK(cudaStreamCreateWithFlags(&c->rec_stream, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&c->rec_state, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&c->rec_staged, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&c->rec_copied, cudaEventDisableTiming));
+  }
+  // the staging kernel reads the state after the steps queued so far; the
+  // context's stream waits only for that kernel, the copy overlaps later steps
+  // (in stream order after the previous record's copy, so the buffer is free)
+  CK(cudaEventRecord(c->rec_state, c->stream));
+  CK(cudaStreamWaitEvent(c->rec_stream, c->rec_state, 0));
+  CK(launch_record(c->L, nset(c).ssh, nset(c).u, nset(c).v, c->rec_dev, c->rec_stream));
+  CK(cudaEventRecord(c->rec_staged, c->rec_stream));
+  CK(cudaStreamWaitEvent(c->stream, c->rec_staged, 0));
+  CK(cudaMemcpyAsync(host, c->rec_dev, 3 * (size_t)c->L.jpi * c->L.jpj * sizeof(double), cudaMemcpyDeviceToHost,
+                     c->rec_stream));
+  CK(cudaEventRecord(c->rec_copied, c->rec_stream));
+  return NEMO_OK;
+}
+
+int nemo_host_alloc(size_t bytes, void** ptr) {
+  if (!ptr || bytes == 0) return NEMO_ERR_INVALID;
+  *ptr = nullptr;
+  cudaError_t e = cudaMallocHost(ptr, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *ptr = nullptr;
+    return e == cudaErrorMemoryAllocation ? NEMO_ERR_ALLOC : NEMO_ERR_CUDA;
+  }
+  return NEMO_OK;
+}
+
+int nemo_host_free(void* ptr) {
+  if (!ptr) return NEMO_OK;
+  return cudaFreeHost(ptr) == cudaSuccess ? NEMO_OK : NEMO_ERR_CUDA;
+}
+
+int nemo_record_wait(nemo_ctx* c) {
+  if (!c) return NEMO_ERR_INVALID;
+  if (!c->rec_copied) return NEMO_OK;
+  int st = set_device(c); if (st) return st;
+  CK(cudaEventSynchronize(c->rec_copied));
   return NEMO_OK;
 }
 

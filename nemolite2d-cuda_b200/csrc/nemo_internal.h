@@ -42,6 +42,9 @@ cudaError_t launch_bc_solid_v(const Layout& L, double* va, cudaStream_t s);
 cudaError_t launch_bc_flather_u(const Layout& L, const RoutinePtrs& p, cudaStream_t s);
 cudaError_t launch_bc_flather_v(const Layout& L, const RoutinePtrs& p, cudaStream_t s);
 cudaError_t launch_copy_next(const Layout& L, const RoutinePtrs& p, cudaStream_t s);
+// sshn and the cell-centred velocities as three dense [jpj][jpi] planes.
+cudaError_t launch_record(const Layout& L, const double* sshn, const double* un, const double* vn, double* out,
+                          cudaStream_t s);
 cudaError_t launch_derive_sshn_uv(const Layout& L, const Consts& C, const double* sshn,
                                   double* sshn_u, double* sshn_v, cudaStream_t s);
 

@@ -353,6 +353,26 @@ cudaError_t launch_recip(const Layout& L, const double* hu, const double* hv, do
   return cudaGetLastError();
 }
 
+// Output record (original/nemolite2d.f90:785-790): sshn, 0.5*(un(ji-1)+un(ji)),
+// 0.5*(vn(jj-1)+vn(jj)) at every T-cell, as three dense [jpj][jpi] planes.
+__global__ void k_record(Layout L, const double* __restrict__ sshn, const double* __restrict__ un,
+                         const double* __restrict__ vn, double* __restrict__ out) {
+  const int ji = 1 + blockIdx.x * BX + threadIdx.x;
+  const int jj = 1 + blockIdx.y * BY + threadIdx.y;
+  if (ji > L.jpi || jj > L.jpj) return;
+  const long plane = (long)L.jpi * L.jpj;
+  const long t = (long)(jj - 1) * L.jpi + (ji - 1);
+  out[t] = sshn[L.idx(ji, jj)];
+  out[plane + t] = 0.5 * (un[L.idx(ji - 1, jj)] + un[L.idx(ji, jj)]);
+  out[2 * plane + t] = 0.5 * (vn[L.idx(ji, jj - 1)] + vn[L.idx(ji, jj)]);
+}
+
+cudaError_t launch_record(const Layout& L, const double* sshn, const double* un, const double* vn, double* out,
+                          cudaStream_t s) {
+  k_record<<<grid_for(L.jpi, L.jpj), dim3(BX, BY), 0, s>>>(L, sshn, un, vn, out);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_init_sshn_uv(const Layout& L, const Consts& C, const double* sshn,
                                 double* sshn_u, double* sshn_v, cudaStream_t s) {
   k_init_sshn_uv<<<grid_for(L.jpi + 1, L.jpj + 1), dim3(BX, BY), 0, s>>>(L, C, sshn, sshn_u, sshn_v);

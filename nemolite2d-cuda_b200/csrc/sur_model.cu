@@ -374,6 +374,7 @@ struct nemo_sur {
   double* d_acc = nullptr;
   int acc_cap = 0;
   long adam_t = 0;
+  long long nlaunch = 0;  // kernels this surrogate has launched
 };
 
 namespace {
@@ -393,17 +394,20 @@ int conv(nemo_sur* s, const __nv_bfloat16* x, const __nv_bfloat16* w, const floa
          const __nv_bfloat16* res, const __nv_bfloat16* mask, int relu, __nv_bfloat16* out, float* out32, int n) {
   sur::ConvEpi e{bias, res, mask, out, out32, relu, n, s->Hn, s->Wn, s->err, out32 ? s->NO : 0};
   ECK(sur::conv_fwd(x, w, e, s->stream));
+  s->nlaunch += 1;
   return NEMO_OK;
 }
 
 int wgrad(nemo_sur* s, const __nv_bfloat16* x, const __nv_bfloat16* dz, int l, int n) {
   sur::WgradArgs a{dW_of(s, l), dB_of(s, l), n, s->Hn, s->Wn, s->err};
   ECK(sur::conv_wgrad(x, dz, a, 0, s->stream));
+  s->nlaunch += 1;
   return NEMO_OK;
 }
 
 // Launches of the patch-templated kernels for the surrogate's patch.
 cudaError_t make_input(nemo_sur* s, const float* snap, const float* tide, int n) {
+  s->nlaunch += 1;
   const long nn = (long)n * s->Hn * s->Wn;
   const int H = s->cfg.height, W = s->cfg.width, g = grid_for(nn, 256);
   const float4* sp = reinterpret_cast<const float4*>(snap);
@@ -417,6 +421,7 @@ cudaError_t make_input(nemo_sur* s, const float* snap, const float* tide, int n)
 }
 
 cudaError_t launch_loss(nemo_sur* s, int n, long npix) {
+  s->nlaunch += 1;
   const long nn = (long)n * s->Hn * s->Wn;
   const int H = s->cfg.height, W = s->cfg.width, g = grid_for(nn, 256);
   const float gs = (float)(1.0 / (3.0 * (double)npix));
@@ -431,6 +436,7 @@ cudaError_t launch_loss(nemo_sur* s, int n, long npix) {
 }
 
 cudaError_t launch_apply(nemo_sur* s, int m0, int n, const float* out) {
+  s->nlaunch += 2;  // apply, open-boundary closure
   const int H = s->cfg.height, W = s->cfg.width, g = grid_for((long)n * H * W, 256);
   switch (s->P) {
     case 1: k_apply<1><<<g, 256, 0, s->stream>>>(s->d_ms, m0, n, H, W, out, s->norm, s->tide_d); break;
@@ -444,6 +450,7 @@ cudaError_t launch_apply(nemo_sur* s, int m0, int n, const float* out) {
 }
 
 cudaError_t launch_err(nemo_sur* s, int nm, const float* snap, const float* out) {
+  s->nlaunch += 1;
   const int H = s->cfg.height, W = s->cfg.width;
   const dim3 g((unsigned)(grid_for((long)H * W, 256) / 16 + 1), (unsigned)nm);
   const float4* sp = reinterpret_cast<const float4*>(snap);
@@ -580,6 +587,7 @@ int predict_chunk(nemo_sur* s, int m0, int n, const std::vector<double>& tide_ne
   // pageable source: the call returns once tf has been staged
   ECK(cudaMemcpyAsync(s->tide_f, tf.data(), n * sizeof(float), cudaMemcpyHostToDevice, s->stream));
   k_pack<<<grid_for(npix, 256), 256, 0, s->stream>>>(s->d_ms, m0, n, H, W, reinterpret_cast<float4*>(snap_dst));
+  s->nlaunch += 1;
   ECK(cudaGetLastError());
   ECK(make_input(s, snap_dst, s->tide_f, n));
   return forward(s, n, false, out_dst);
@@ -911,6 +919,7 @@ int nemo_hyb_default_config(nemo_hyb_config* c) {
   c->anchor = 100;
   c->tol = 0.01;
   c->per_member = 1;
+  c->quarantine = 0.05;
   return NEMO_OK;
 }
 
@@ -920,9 +929,12 @@ int nemo_hyb_default_config(nemo_hyb_config* c) {
 // shadow step, which also re-anchors the state), and each member whose
 // relative SSH L2 error of the prediction exceeds tol (or is not finite)
 // falls back: the solver runs the rest of its window.  The other members
-// advance by surrogate calls, k steps each.  With per_member = 0 one failing
-// member sends the whole ensemble to the solver for the window.  Statistics
-// count member-windows and member-steps.
+// advance by surrogate calls, k steps each.  A member whose shadow error
+// exceeds `quarantine` stays on the solver for the rest of the run (errors
+// that large precede the corner instability the surrogate's perturbations
+// can excite).  With per_member = 0 one failing member sends the whole
+// ensemble to the solver for the window.  Statistics count member-windows
+// and member-steps.
 int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, int nsteps,
                  nemo_hyb_stats* stats) {
   if (!s || !e || !c || c->k != 10 || c->anchor < c->k || c->anchor % c->k || nsteps % c->anchor ||
@@ -946,7 +958,9 @@ int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, 
     out_all = own + (size_t)nm * hw * 4;
   }
   std::vector<double> tide(nm), acc(6 * nm);
-  std::vector<char> pass(nm), fail(nm);
+  std::vector<char> pass(nm), fail(nm), quar(nm, 0);
+  const long long launches0 = s->nlaunch;
+  long long solver_launches = 0;  // one persistent ensemble launch per solver step
   const auto t_start = std::chrono::steady_clock::now();
   int istp = istp0;
   int rc = NEMO_OK;
@@ -960,6 +974,7 @@ int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, 
     // shadow / re-anchor: the FP64 solver runs the same k steps
     if (rc == NEMO_OK) rc = join(s->stream, nemo::ens_stream(e));
     if (rc == NEMO_OK) rc = nemo_ens_step_n(e, istp + 1, c->k);
+    solver_launches += c->k;
     if (rc == NEMO_OK) rc = join(nemo::ens_stream(e), s->stream);
     if (rc == NEMO_OK) rc = ensure_members(s, e, ms, nullptr);  // buffers swapped
     if (rc != NEMO_OK) break;
@@ -974,7 +989,11 @@ int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, 
     int nfail = 0;
     for (int m = 0; m < nm; ++m) {
       const double r = acc[6 * m + 1] > 0 ? sqrt(acc[6 * m] / acc[6 * m + 1]) : sqrt(acc[6 * m]);
-      fail[m] = !(r <= c->tol);
+      if (c->quarantine > 0 && !quar[m] && !(r <= c->quarantine)) {
+        quar[m] = 1;  // far off: the solver keeps this member from now on
+        st.quarantined += 1;
+      }
+      fail[m] = quar[m] || !(r <= c->tol);
       nfail += fail[m];
       if (!(r <= worst)) worst = r;  // NaN propagates
     }
@@ -995,6 +1014,7 @@ int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, 
     } else if (nfail > 0) {
       rc = nemo::ens_step_subset(e, istp + 1, rest, fail.data());
     }
+    if (nfail > 0) solver_launches += rest;
     st.solver_steps += (long long)rest * nfail;
     if (rc != NEMO_OK) break;
     if (nfail < nm) {
@@ -1016,6 +1036,7 @@ int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, 
   if (rc != NEMO_OK) return rc;
   ECK(ce);
   st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+  st.launches = solver_launches + (s->nlaunch - launches0);
   if (stats) *stats = st;
   return NEMO_OK;
 }

@@ -6,6 +6,10 @@
 //                   jpi = jpiglo-2, jpj = jpjglo-2               (:96-141)
 //   grid/init       nemo_create                                  (:145-371)
 //   output(0)       go2d_00000.dat                                (:67-68)
+//                   (records are staged on the device and copied back on a
+//                   side stream, nemo_record; a writer thread formats the
+//                   files while the stepper continues; x, y and depth are
+//                   read back once)
 //   DO istp        step: continuity, momentum, bc(rtime), next;  (:74-77,
 //                   output and checksums every irecord steps       :375-386)
 //   end            'ua checksum = ' / 'va checksum = ' (E16.8)    (:82-85)
@@ -31,10 +35,14 @@
 #include <algorithm>
 #include <cctype>
 #include <chrono>
+#include <condition_variable>
+#include <deque>
 #include <fstream>
 #include <map>
+#include <mutex>
 #include <sstream>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "nemo_b200.h"
@@ -347,17 +355,10 @@ int check(int st, const char* where) {
 }
 
 // output, original/nemolite2d.f90:773-799: go2d_%05d.dat, 6E20.7E4 per row,
-// a blank line after each jj.
-void output(nemo_ctx* c, int istp, int jpi, int jpj, std::vector<double>& buf) {
-  std::vector<double> xt((size_t)jpi * jpj), yt((size_t)jpi * jpj), ht((size_t)jpi * jpj),
-      ssh((size_t)jpi * jpj), un((size_t)(jpi + 1) * jpj), vn((size_t)jpi * (jpj + 1));
-  check(nemo_retrieve(c, NEMO_XT, xt.data(), jpi), "retrieve xt");
-  check(nemo_retrieve(c, NEMO_YT, yt.data(), jpi), "retrieve yt");
-  check(nemo_retrieve(c, NEMO_HT, ht.data(), jpi), "retrieve ht");
-  check(nemo_retrieve(c, NEMO_SSHN, ssh.data(), jpi), "retrieve sshn");
-  check(nemo_retrieve(c, NEMO_UN, un.data(), jpi + 1), "retrieve un");
-  check(nemo_retrieve(c, NEMO_VN, vn.data(), jpi), "retrieve vn");
-  (void)buf;
+// a blank line after each jj.  rec holds sshn and the cell-centred u, v as
+// three [jpj][jpi] planes (nemo_record); xt, yt, ht are static.
+void write_dat(int istp, int jpi, int jpj, const std::vector<double>& xt, const std::vector<double>& yt,
+               const std::vector<double>& ht, const double* rec) {
   char name[32];
   snprintf(name, sizeof name, "go2d_%05d.dat", istp);
   FILE* f = fopen(name, "w");
@@ -365,14 +366,14 @@ void output(nemo_ctx* c, int istp, int jpi, int jpj, std::vector<double>& buf) {
     fprintf(stderr, "cannot write %s\n", name);
     return;
   }
+  const size_t plane = (size_t)jpi * jpj;
   std::string line;
   for (int jj = 1; jj <= jpj; ++jj) {
     for (int ji = 1; ji <= jpi; ++ji) {
-      size_t t = (size_t)(jj - 1) * jpi + (ji - 1);
-      double r1 = 0.5 * (un[(size_t)(jj - 1) * (jpi + 1) + (ji - 1)] + un[(size_t)(jj - 1) * (jpi + 1) + ji]);
-      double r2 = 0.5 * (vn[(size_t)(jj - 1) * jpi + (ji - 1)] + vn[(size_t)jj * jpi + (ji - 1)]);
+      const size_t t = (size_t)(jj - 1) * jpi + (ji - 1);
       line = fortran_E(xt[t], 20, 7, 4) + fortran_E(yt[t], 20, 7, 4) + fortran_E(ht[t], 20, 7, 4) +
-             fortran_E(ssh[t], 20, 7, 4) + fortran_E(r1, 20, 7, 4) + fortran_E(r2, 20, 7, 4);
+             fortran_E(rec[t], 20, 7, 4) + fortran_E(rec[plane + t], 20, 7, 4) +
+             fortran_E(rec[2 * plane + t], 20, 7, 4);
       fputs(line.c_str(), f);
       fputc('\n', f);
     }
@@ -380,6 +381,79 @@ void output(nemo_ctx* c, int istp, int jpi, int jpj, std::vector<double>& buf) {
   }
   fclose(f);
 }
+
+// Records in flight: two page-locked buffers; the main thread starts a
+// record into a free buffer and queues it, the writer thread waits for the
+// copy and writes the file, then frees the buffer.
+struct Writer {
+  nemo_ctx* c;
+  int jpi, jpj;
+  std::vector<double> xt, yt, ht;
+  double* buf[2] = {nullptr, nullptr};
+  bool busy[2] = {false, false};
+  int next = 0;
+  std::deque<std::pair<int, int>> jobs;  // (istp, buffer)
+  bool done = false;
+  std::mutex mu;
+  std::condition_variable cv;
+  std::thread th;
+
+  Writer(nemo_ctx* c_, int jpi_, int jpj_) : c(c_), jpi(jpi_), jpj(jpj_) {
+    const size_t n = (size_t)jpi * jpj;
+    xt.resize(n);
+    yt.resize(n);
+    ht.resize(n);
+    check(nemo_retrieve(c, NEMO_XT, xt.data(), jpi), "retrieve xt");
+    check(nemo_retrieve(c, NEMO_YT, yt.data(), jpi), "retrieve yt");
+    check(nemo_retrieve(c, NEMO_HT, ht.data(), jpi), "retrieve ht");
+    for (auto& b : buf) check(nemo_host_alloc(3 * n * sizeof(double), reinterpret_cast<void**>(&b)), "nemo_host_alloc");
+    th = std::thread([this] { run(); });
+  }
+  ~Writer() {
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      done = true;
+    }
+    cv.notify_all();
+    th.join();
+    for (auto* b : buf) nemo_host_free(b);
+  }
+  void record(int istp) {
+    int b;
+    {
+      std::unique_lock<std::mutex> lk(mu);
+      cv.wait(lk, [&] { return !busy[next]; });
+      b = next;
+      busy[b] = true;
+      next ^= 1;
+    }
+    check(nemo_record(c, buf[b]), "nemo_record");
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      jobs.emplace_back(istp, b);
+    }
+    cv.notify_all();
+  }
+  void run() {
+    for (;;) {
+      std::pair<int, int> job;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        cv.wait(lk, [&] { return done || !jobs.empty(); });
+        if (jobs.empty()) return;
+        job = jobs.front();
+        jobs.pop_front();
+      }
+      check(nemo_record_wait(c), "nemo_record_wait");  // copies land in order
+      write_dat(job.first, jpi, jpj, xt, yt, ht, buf[job.second]);
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        busy[job.second] = false;
+      }
+      cv.notify_all();
+    }
+  }
+};
 
 }  // namespace
 
@@ -409,8 +483,8 @@ int main(int argc, char** argv) {
   nemo_ctx* c = nullptr;
   check(nemo_create(&s.p, &c), "nemo_create");
   if (s.has_sched) check(nemo_set_schedule(c, &s.sched), "nemo_set_schedule");
-  std::vector<double> buf;
-  if (s.write_dat) output(c, 0, jpi, jpj, buf);
+  Writer* writer = s.write_dat ? new Writer(c, jpi, jpj) : nullptr;
+  if (writer) writer->record(0);
   FILE* csv = fopen(s.csv.c_str(), "w");
   if (csv) fprintf(csv, "istp,ssh_checksum,ua_checksum,va_checksum\n");
 
@@ -433,7 +507,7 @@ int main(int argc, char** argv) {
            fortran_E(ck[0], 16, 8).c_str(), fortran_E(ck[1], 16, 8).c_str(),
            fortran_E(ck[2], 16, 8).c_str());
     if (csv) fprintf(csv, "%ld,%.17e,%.17e,%.17e\n", istp, ck[0], ck[1], ck[2]);
-    if (s.write_dat) output(c, (int)istp, jpi, jpj, buf);
+    if (writer) writer->record((int)istp);
   };
 
   check(nemo_sync(c), "nemo_sync");
@@ -476,6 +550,7 @@ int main(int argc, char** argv) {
   }
   check(nemo_sync(c), "nemo_sync");
   T.r[it_step].samples.push_back(now_s() - t0);
+  delete writer;  // the last files are written before the report
   if (csv) fclose(csv);
 
   // :82-85, field_checksum(ua(1:jpiglo,1:jpjglo)) -- ua == un after next

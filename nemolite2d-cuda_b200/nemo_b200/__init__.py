@@ -33,7 +33,8 @@ EXPORTED = [
     "nemo_default_params", "nemo_create", "nemo_destroy", "nemo_continuity", "nemo_momentum",
     "nemo_momentum_u", "nemo_momentum_v", "nemo_bc", "nemo_bc_ssh", "nemo_bc_solid_u",
     "nemo_bc_solid_v", "nemo_bc_flather_u", "nemo_bc_flather_v", "nemo_next", "nemo_step",
-    "nemo_step_n", "nemo_checksums", "nemo_checksum", "nemo_retrieve", "nemo_set_state",
+    "nemo_step_n", "nemo_checksums", "nemo_checksum", "nemo_retrieve", "nemo_record",
+    "nemo_record_wait", "nemo_host_alloc", "nemo_host_free", "nemo_set_state",
     "nemo_sync", "nemo_get_dims", "nemo_device_field", "nemo_set_schedule", "nemo_get_schedule",
     "nemo_status_string", "nemo_build_is_strict", "nemo_checksums_noalloc", "nemo_autotune",
     "nemo_ens_generate", "nemo_ens_create", "nemo_ens_destroy", "nemo_ens_step_n",
@@ -119,6 +120,8 @@ def load(strict=False):
     L.nemo_checksums.argtypes = [vp, P(dp)]
     L.nemo_checksum.argtypes = [vp, ip, P(dp)]
     L.nemo_retrieve.argtypes = [vp, ip, P(dp), ctypes.c_long]
+    L.nemo_record.argtypes = [vp, P(dp)]
+    L.nemo_record_wait.argtypes = [vp]
     L.nemo_set_state.argtypes = [vp, P(dp), P(dp), P(dp)]
     L.nemo_get_dims.argtypes = [vp, P(ip), P(ip)]
     L.nemo_device_field.argtypes = [vp, ip, P(P(dp)), P(ctypes.c_long)]
@@ -304,6 +307,17 @@ class Model:
         assert out.shape == shape and out.dtype == np.float64 and out.flags.c_contiguous
         check(self.lib.nemo_retrieve(self.h, f, _dptr(out), shape[1]), "nemo_retrieve")
         return out
+
+    def record(self, out):
+        """Start an output record of the current state into `out` (float64
+        [3][jpj][jpi], C-contiguous; pinned memory lets the copy overlap later
+        steps): sshn and the cell-centred u, v.  record_wait() blocks until it
+        has landed."""
+        assert out.dtype == np.float64 and out.flags.c_contiguous and out.size == 3 * self.jpi * self.jpj
+        check(self.lib.nemo_record(self.h, _dptr(out)), "nemo_record")
+
+    def record_wait(self):
+        check(self.lib.nemo_record_wait(self.h), "nemo_record_wait")
 
     def set_state(self, sshn, un, vn):
         a = [np.ascontiguousarray(x, dtype=np.float64) for x in (sshn, un, vn)]

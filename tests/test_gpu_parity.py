@@ -174,6 +174,33 @@ def test_in_kernel_reciprocals_are_checked_and_default(nb):
         np.testing.assert_array_equal(bits(a.field(fid)), bits(b.field(fid)), err_msg=name)
 
 
+def test_record_stages_the_output_fields_without_disturbing_the_run(nb):
+    """nemo_record: sshn and the cell-centred u, v of the current state reach
+    host memory (the go2d columns 4-6), and the steps launched while the
+    record travels give the same state as a run that never recorded."""
+    import torch
+    kw = dict(jpi=150, jpj=97, rdt=20.0, cbfr=0.00015, visc=0.1, amp_tide=0.3, nbump=6,
+              seed=8, bump_amp=20.0, bump_wmin=5e3, bump_wmax=40e3)
+    a = nb.Model(strict=True, **kw)
+    b = nb.Model(strict=True, **kw)
+    a.step_n(1, 40)
+    b.step_n(1, 40)
+    rec = [torch.zeros(3 * 97 * 150, dtype=torch.float64, pin_memory=True).numpy() for _ in range(2)]
+    ssh, u, v = a.field(nb.SSHN), a.field(nb.UN), a.field(nb.VN)
+    a.record(rec[0])
+    a.step_n(41, 30)  # overlaps the copy
+    a.record(rec[1])
+    a.record_wait()
+    b.step_n(41, 30)
+    r0 = rec[0].reshape(3, 97, 150)
+    np.testing.assert_array_equal(r0[0], ssh)
+    np.testing.assert_array_equal(r0[1], 0.5 * (u[:, :-1] + u[:, 1:]))
+    np.testing.assert_array_equal(r0[2], 0.5 * (v[:-1, :] + v[1:, :]))
+    for name, fid in STATE:
+        np.testing.assert_array_equal(bits(a.field(fid)), bits(b.field(fid)), err_msg=name)
+    np.testing.assert_array_equal(rec[1].reshape(3, 97, 150)[0], b.field(nb.SSHN))
+
+
 def test_strict_fused_equals_routine_path_from_random_state(nb):
     jpi, jpj = 200, 150
     kw = dict(jpi=jpi, jpj=jpj, rdt=20.0, cbfr=0.00015, visc=0.1, amp_tide=1.0, nbump=8,

@@ -414,10 +414,15 @@ def test_hybrid_accepts_surrogate_windows_and_reports_errors(env):
     a = small_ensemble(nb, 41, n, side)
     b = small_ensemble(nb, 41, n, side)
     s = sm.Surrogate(nblocks=1, batch=1, height=side, width=side, train=False, seed=4)  # 2 chunks
-    st = sm.hyb_run(s, a, 0, 200, k=10, anchor=100, tol=1e300)  # never falls back
+    st = sm.hyb_run(s, a, 0, 200, k=10, anchor=100, tol=1e300, quarantine=0.0)  # never falls back
     b.step_n(1, 200)
     assert st["fallbacks"] == 0 and st["sur_steps"] == 180 * n and st["solver_steps"] == 20 * n
     assert st["sur_calls"] == 20 and st["max_shadow_err"] > 0
+    # 20 solver launches; a window's shadow prediction packs, builds the input
+    # and runs the 4 convolutions per chunk of one member, then the error
+    # kernel; each of the 9 calls per window adds apply and the boundary closure
+    per_predict = 1 + 1 + 4
+    assert st["launches"] == 20 + 2 * n * per_predict + 2 * 1 + 2 * 9 * n * (per_predict + 2)
     err = sm.ens_compare(a, b)
     assert err.shape == (n, 3) and np.all(np.isfinite(err)) and np.all(err > 0)
 
@@ -444,7 +449,7 @@ def test_hybrid_members_fall_back_on_their_own(env):
     tol = 0.5 * (e0[order[0]] + e0[order[1]])
     a = small_ensemble(nb, 51, n, side)
     b = small_ensemble(nb, 51, n, side)
-    st = sm.hyb_run(s, a, 0, 100, tol=tol)
+    st = sm.hyb_run(s, a, 0, 100, tol=tol, quarantine=0.0)
     b.step_n(1, 100)
     assert st["windows"] == n and st["fallbacks"] == n - 1
     assert st["solver_steps"] == 10 * n + 90 * (n - 1) and st["sur_steps"] == 90
@@ -456,9 +461,28 @@ def test_hybrid_members_fall_back_on_their_own(env):
             for f in (nb.SSHN, nb.UN, nb.VN):
                 np.testing.assert_array_equal(a.field(m, f), b.field(m, f))
     c = small_ensemble(nb, 51, n, side)
-    st = sm.hyb_run(s, c, 0, 100, tol=tol, per_member=False)
+    st = sm.hyb_run(s, c, 0, 100, tol=tol, per_member=False, quarantine=0.0)
     assert st["fallbacks"] == n and st["sur_steps"] == 0
     assert np.all(sm.ens_compare(c, b) == 0.0)
+
+
+def test_quarantined_members_stay_on_the_solver(env):
+    """A member whose shadow error passes the quarantine limit stays on the
+    FP64 solver for the rest of the run, even where later errors would pass."""
+    torch, nb, sm = env
+    side, n = 128, 2
+    a = small_ensemble(nb, 61, n, side)
+    b = small_ensemble(nb, 61, n, side)
+    s = sm.Surrogate(nblocks=1, batch=n, height=side, width=side, train=False, seed=4)
+    st = sm.hyb_run(s, a, 0, 300, tol=1e300, quarantine=1e-300)
+    b.step_n(1, 300)
+    assert st["quarantined"] == n and st["fallbacks"] == 3 * n and st["sur_steps"] == 0
+    for m in range(n):
+        for f in (nb.SSHN, nb.UN, nb.VN):
+            np.testing.assert_array_equal(a.field(m, f), b.field(m, f))
+    c = small_ensemble(nb, 61, n, side)
+    st = sm.hyb_run(s, c, 0, 100, tol=1e300, quarantine=0.0)  # never (one window: the
+    assert st["quarantined"] == 0 and st["fallbacks"] == 0    # untrained network stays finite)
 
 
 def test_training_beats_persistence_on_held_out_runs(env):
