@@ -164,6 +164,7 @@ Consts make_consts(const nemo_params& p) {
   C.r_2dx = 1.0 / C.two_dx;
   C.r_2dy = 1.0 / C.two_dy;
   C.r_cfric = 1.0 / C.cfric;
+  C.r_cfric_lo = fma(-C.cfric, C.r_cfric, 1.0) / C.cfric;  // the residual is exact
   return C;
 }
 

@@ -43,6 +43,8 @@ struct Consts {
   double cfric;              // 1 + cbfr*rdt, :514, :606
   // round-to-nearest reciprocals for the corrected constant divisions
   double r_e1t, r_e2t, r_e12t, r_e12u, r_e12v, r_2dx, r_2dy, r_cfric;
+  // RN((1 - cfric*r_cfric)/cfric): with r_cfric, 1/cfric to about 2^-106
+  double r_cfric_lo;
 };
 
 // Mask of original/nemolite2d.f90:184-202: 1 water, 0 land (west, east and

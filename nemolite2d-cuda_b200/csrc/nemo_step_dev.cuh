@@ -29,6 +29,22 @@ __device__ __forceinline__ void load_cell(Cell& x, const FusedArgs& A, long o) {
 __device__ __forceinline__ double dn(double x) { return __shfl_down_sync(FULL, x, 1); }
 __device__ __forceinline__ double up(double x) { return __shfl_up_sync(FULL, x, 1); }
 
+// Quotients of the fused step.  The strict (-fmad=false) build forms every
+// quotient correctly rounded, as the reference's division does.  The default
+// build, which the reference's tolerance (1e-12 relative max-norm) governs,
+// relaxes the quotients whose rounding errors average out over the steps:
+// qdiv_k forms a/b by a grid constant as a * RN(1/b) (one rounding more, two
+// FP64 operations fewer), and no state row needs the range check.  The
+// divisions that scale the new velocities every step (by the depth and by
+// the friction factor) stay rounded: a fixed divisor's RN(1/b) errs the same
+// way at every step, and that bias accumulated to 1.4e-12 over 2000 steps of
+// the 128^2 case when those too took the one-multiply form (1.3e-14 without).
+#ifdef NEMO_STRICT_BUILD
+constexpr bool kRoundedQuotients = true;
+#else
+constexpr bool kRoundedQuotients = false;
+#endif
+
 // a/b given rb = RN(1/b): the corrected-reciprocal quotient (see div_const),
 // exact whenever the quotient is zero or at least 2^-959 in magnitude.  The
 // range is guaranteed per row instead of per quotient (row_tiny): a row whose
@@ -53,27 +69,52 @@ __device__ __forceinline__ double qdiv(double a, double b, double rb, bool& bad)
   return -fma(-r, rb, -q);
 }
 
+// a/b for a grid-constant divisor b: rounded in the strict build, a * RN(1/b)
+// in the default build.
+template <bool SAFE>
+__device__ __forceinline__ double qdiv_k(double a, double b, double rb, bool& bad) {
+  if (!SAFE && !kRoundedQuotients) return a * rb;
+  return qdiv<SAFE>(a, b, rb, bad);
+}
+
+// a/cfric: rounded in the strict build; in the default build from the two-part
+// reciprocal, a * (r_cfric + r_cfric_lo) with one rounding, which is the
+// rounded quotient except within about 2^-50 ulp of a rounding boundary (two
+// FP64 operations instead of three).
+template <bool SAFE>
+__device__ __forceinline__ double qdiv_fric(double a, const Consts& C, bool& bad) {
+  if (!SAFE && !kRoundedQuotients) return fma(a, C.r_cfric, a * C.r_cfric_lo);
+  return qdiv<SAFE>(a, C.cfric, C.r_cfric, bad);
+}
+
 // Nonzero with |x| < 2^-300 (biased exponent below 723).
 __device__ __forceinline__ bool tiny(double x) {
   const unsigned hi2 = (unsigned)__double2hiint(x) << 1;
   const unsigned lo = (unsigned)__double2loint(x);
   return (hi2 < (723u << 21)) & ((hi2 | lo) != 0u);
 }
-__device__ __forceinline__ bool row_tiny(const Cell& x) { return tiny(x.s) | tiny(x.u) | tiny(x.v); }
+// Only the rounded quotients need the range guarantee.
+__device__ __forceinline__ bool row_tiny(const Cell& x) {
+  return kRoundedQuotients && (tiny(x.s) | tiny(x.u) | tiny(x.v));
+}
+// Warp-wide: does any lane's row need the IEEE division form?
+__device__ __forceinline__ unsigned any_tiny(const Cell& x) {
+  return kRoundedQuotients && __any_sync(FULL, row_tiny(x)) ? 1u : 0u;
+}
 
 __device__ __forceinline__ double interp_u(const Consts& C, int c, int jpi, double s0, double s1,
                                           bool safe, bool& bad) {
   if (c == 0) return s1;
   if (c == jpi) return s0;
   double a = 0.5 * (C.e12t * s0 + C.e12t * s1);
-  return safe ? qdiv<true>(a, C.e12u, C.r_e12u, bad) : qdiv<false>(a, C.e12u, C.r_e12u, bad);
+  return safe ? qdiv<true>(a, C.e12u, C.r_e12u, bad) : qdiv_k<false>(a, C.e12u, C.r_e12u, bad);
 }
 
 __device__ __forceinline__ double interp_v(const Consts& C, int jj, int jpj, double s0, double s1,
                                           bool safe, bool& bad) {
   if (jj == jpj) return s0;
   double a = 0.5 * (C.e12t * s0 + C.e12t * s1);
-  return safe ? qdiv<true>(a, C.e12v, C.r_e12v, bad) : qdiv<false>(a, C.e12v, C.r_e12v, bad);
+  return safe ? qdiv<true>(a, C.e12v, C.r_e12v, bad) : qdiv_k<false>(a, C.e12v, C.r_e12v, bad);
 }
 
 // Values carried from row j-1 to row j for one column.
@@ -118,7 +159,7 @@ __device__ __forceinline__ void row(const Consts& C, int c, int j, int jpi, int 
   const double uw = 0.5 * (cur.u + u_w) * C.e2t;
   const double dep = cur.ht + cur.s;
   const double Fx = upwind(uw, u_w, cur.u) * uw * dep;
-  const double Dx = qdiv<SAFE>(cur.u - u_w, C.e1t, C.r_e1t, bad) * dep;
+  const double Dx = qdiv_k<SAFE>(cur.u - u_w, C.e1t, C.r_e1t, bad) * dep;
 
   // corner (c,j): east face of v(c,j), north face of u(c,j)
   const double uec = 0.5 * (cur.u + nx.u);
@@ -128,25 +169,25 @@ __device__ __forceinline__ void row(const Consts& C, int c, int j, int jpi, int 
   const double uuv = west0 ? upwind_hi_only(ue, v_e)
                           : east ? upwind_lo_only(ue, cur.v) : upwind(ue, cur.v, v_e);
   const double Fvx = uuv * ue * (0.5 * Sn);
-  const double Gx = qdiv<SAFE>(v_e - cur.v, C.two_dx, C.r_2dx, bad);
+  const double Gx = qdiv_k<SAFE>(v_e - cur.v, C.two_dx, C.r_2dx, bad);
   const double vnc = 0.5 * (cur.v + v_e);
   const double vn_ = 0.5 * vnc * C.two_dx;
   const double Re = (Hv + dn(cur.hv)) + dn(sv);
   const double uuu = north ? upwind_lo_only(vn_, cur.u) : upwind(vn_, cur.u, nx.u);
   const double Fuy = uuu * vn_ * (0.5 * Re);
-  const double Gy = qdiv<SAFE>(nx.u - cur.u, C.two_dy, C.r_2dy, bad);
+  const double Gy = qdiv_k<SAFE>(nx.u - cur.u, C.two_dy, C.r_2dy, bad);
 
   // y-face of the v equation at T(c,j+1), between v(c,j) and v(c,j+1)
   const double vs = 0.5 * (nx.v + cur.v) * C.e1t;
   const double depn = nx.ht + nx.s;
   const double Fvy_n = upwind(vs, cur.v, nx.v) * vs * depn;
-  const double Dvy_n = qdiv<SAFE>(nx.v - cur.v, C.e2t, C.r_e2t, bad) * depn;
+  const double Dvy_n = qdiv_k<SAFE>(nx.v - cur.v, C.e2t, C.r_e2t, bad) * depn;
 
   // continuity (:399-403), clamped SSH row (:631-644)
   const double r1 = k.Hu * cur.u;
   const double r2 = up(r1);
   const double r3 = Hv * cur.v;
-  const double ssh = cur.s + qdiv<SAFE>((r2 - r1 + k.cf_s - r3) * C.rdt, C.e12t, C.r_e12t, bad);
+  const double ssh = cur.s + qdiv_k<SAFE>((r2 - r1 + k.cf_s - r3) * C.rdt, C.e12t, C.r_e12t, bad);
   o.ssha = south ? tide : ssh;
 
   // u equation (:439-514); u(jpi,j) is the east wall (:650)
@@ -160,9 +201,9 @@ __device__ __forceinline__ void row(const Consts& C, int c, int j, int jpi, int 
     vis = C.visc * vis;
     const double cor = 0.5 * (C.fcor * (k.vnc_s + vnc)) * C.e12u * k.Hu;
     const double hpg = -(C.g * k.Hu * C.e2u * (k.s_e - cur.s));
-    const double num = cur.u * k.Hu + qdiv<SAFE>(C.rdt * (adv + vis + cor + hpg), C.e12u, C.r_e12u, bad);
+    const double num = cur.u * k.Hu + qdiv_k<SAFE>(C.rdt * (adv + vis + cor + hpg), C.e12u, C.r_e12u, bad);
     const double q = qdiv<SAFE>(num, cur.hu + 0.0, rhu, bad);
-    o.ua = east ? 0.0 : qdiv<SAFE>(q, C.cfric, C.r_cfric, bad);
+    o.ua = east ? 0.0 : qdiv_fric<SAFE>(q, C, bad);
   }
   // v equation (:527-606); v(c,jpj) is the north wall (:658)
   {
@@ -178,9 +219,9 @@ __device__ __forceinline__ void row(const Consts& C, int c, int j, int jpi, int 
     vis = C.visc * vis;
     const double cor = -(0.5 * (C.fcor * (uec + uec_w)) * C.e12v * Hv);
     const double hpg = -(C.g * Hv * C.e1v * (nx.s - cur.s));
-    const double num = cur.v * Hv + qdiv<SAFE>(C.rdt * (adv + vis + cor + hpg), C.e12v, C.r_e12v, bad);
+    const double num = cur.v * Hv + qdiv_k<SAFE>(C.rdt * (adv + vis + cor + hpg), C.e12v, C.r_e12v, bad);
     const double q = qdiv<SAFE>(num, cur.hv + 0.0, rhv, bad);
-    o.va = north ? 0.0 : qdiv<SAFE>(q, C.cfric, C.r_cfric, bad);
+    o.va = north ? 0.0 : qdiv_fric<SAFE>(q, C, bad);
   }
   o.sv = sv;
   // carry to row j+1
@@ -217,14 +258,14 @@ __device__ __forceinline__ void prologue(const Consts& C, int c, int J0, int jpi
     k.dudy_s = 0.0;
   } else {
     const double su_p = interp_u(C, c, jpi, p.s, s_e_p, SAFE, bad);
-    const double gy = qdiv<SAFE>(q.u - p.u, C.two_dy, C.r_2dy, bad);
+    const double gy = qdiv_k<SAFE>(q.u - p.u, C.two_dy, C.r_2dy, bad);
     k.dudy_s = gy * ((k.Hu + p.hu) + su_p);
   }
   // T(c, J0): south face of v(c, J0)
   const double vs = 0.5 * (q.v + p.v) * C.e1t;
   const double depc = q.ht + q.s;
   k.Fvy_s = upwind(vs, p.v, q.v) * vs * depc;
-  k.Dvy_s = qdiv<SAFE>(q.v - p.v, C.e2t, C.r_e2t, bad) * depc;
+  k.Dvy_s = qdiv_k<SAFE>(q.v - p.v, C.e2t, C.r_e2t, bad) * depc;
   k.cf_s = Hv_p * p.v;
 }
 
@@ -252,7 +293,7 @@ __device__ __forceinline__ void run_strip(const Layout& L, const Consts& C, cons
   double sv0;
   // warp-wide tiny-value flags: bit 0 row j+1 (set as it arrives), bit 1
   // row j, bit 2 row j-1; row j takes the IEEE form while any is set
-  unsigned hist = (__any_sync(FULL, row_tiny(p)) ? 2u : 0u) | (__any_sync(FULL, row_tiny(cur)) ? 1u : 0u);
+  unsigned hist = (any_tiny(p) << 1) | any_tiny(cur);
   {
     bool bad = false;
     if (hist) prologue<true>(C, c, J0, jpi, jpj, sv_stored, p, cur, k, sv0, bad);
@@ -281,7 +322,7 @@ __device__ __forceinline__ void run_strip(const Layout& L, const Consts& C, cons
 
     RowOut o;
     bool bad = false;
-    hist = ((hist << 1) | (__any_sync(FULL, row_tiny(nx)) ? 1u : 0u)) & 7u;
+    hist = ((hist << 1) | any_tiny(nx)) & 7u;
     if (hist) {
       row<true, true>(C, c, j, jpi, jpj, A.tide, cur, nx, k, rhu, rhv, o, bad);
     } else if (edge_warp || j == 1 || j == jpj) {
@@ -373,7 +414,7 @@ __device__ __forceinline__ void run_strip_ring(const Layout& L, const Consts& C,
   const double sv_stored = (J0 == 1) ? __ldg(A.sshv0 + L.idx(cl, 0)) : 0.0;
   Carry k;
   double sv0;
-  unsigned hist = (__any_sync(FULL, row_tiny(p)) ? 2u : 0u) | (__any_sync(FULL, row_tiny(cur)) ? 1u : 0u);
+  unsigned hist = (any_tiny(p) << 1) | any_tiny(cur);
   {
     bool bad = false;
     if (hist) prologue<true>(C, c, J0, jpi, jpj, sv_stored, p, cur, k, sv0, bad);
@@ -397,7 +438,7 @@ __device__ __forceinline__ void run_strip_ring(const Layout& L, const Consts& C,
 
     RowOut o;
     bool bad = false;
-    hist = ((hist << 1) | (__any_sync(FULL, row_tiny(nx)) ? 1u : 0u)) & 7u;
+    hist = ((hist << 1) | any_tiny(nx)) & 7u;
     if (hist) {
       row<true, true>(C, c, j, jpi, jpj, A.tide, cur, nx, k, rhu, rhv, o, bad);
     } else if (edge_warp || j == 1 || j == jpj) {
