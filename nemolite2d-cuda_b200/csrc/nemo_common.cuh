@@ -45,6 +45,13 @@ struct Consts {
   double r_e1t, r_e2t, r_e12t, r_e12u, r_e12v, r_2dx, r_2dy, r_cfric;
   // RN((1 - cfric*r_cfric)/cfric): with r_cfric, 1/cfric to about 2^-106
   double r_cfric_lo;
+  // Products of constants for the default build's folded forms (each RN of
+  // the exact product or quotient except where the scaling by a power of two
+  // is exact): 0.5*e12t/e12u, 0.5*e12t/e12v, 0.5*e2t, 0.5*e1t, two_dy/4,
+  // two_dx/4, rdt/e12t, rdt/e12u, rdt/e12v, visc*e2u, visc*e1u/2, visc*e1v,
+  // visc*e2v/2, fcor*e12u/2, -fcor*e12v/2, -g*e2u, -g*e1v.
+  double k_su, k_sv, h_e2t, h_e1t, q_2dy, q_2dx, k_ssh, k_u, k_v;
+  double vis_u1, vis_u2, vis_v1, vis_v2, cor_u, cor_v, hpg_u, hpg_v;
 };
 
 // Mask of original/nemolite2d.f90:184-202: 1 water, 0 land (west, east and

@@ -39,11 +39,24 @@ __device__ __forceinline__ double up(double x) { return __shfl_up_sync(FULL, x, 
 // the friction factor) stay rounded: a fixed divisor's RN(1/b) errs the same
 // way at every step, and that bias accumulated to 1.4e-12 over 2000 steps of
 // the 128^2 case when those too took the one-multiply form (1.3e-14 without).
+// The same reasoning lets the default build fold products of grid constants
+// (0.5*x*e2t as x*(0.5*e2t), rdt*(...)/e12u as (...)*(rdt/e12u), and the
+// viscosity, Coriolis and pressure-gradient coefficients; kFold below) and
+// pick the upwind value with a plain select.
 #ifdef NEMO_STRICT_BUILD
 constexpr bool kRoundedQuotients = true;
 #else
 constexpr bool kRoundedQuotients = false;
 #endif
+constexpr bool kFold = !kRoundedQuotients;
+
+// upwind() of the strict build, a select in the default build (the two differ
+// only in the sign of a zero result and in propagating a NaN from the unused
+// side)
+__device__ __forceinline__ double upw(double w, double lo, double hi) {
+  if (kFold) return sign_clear(w) ? lo : hi;
+  return upwind(w, lo, hi);
+}
 
 // a/b given rb = RN(1/b): the corrected-reciprocal quotient (see div_const),
 // exact whenever the quotient is zero or at least 2^-959 in magnitude.  The
@@ -106,6 +119,7 @@ __device__ __forceinline__ double interp_u(const Consts& C, int c, int jpi, doub
                                           bool safe, bool& bad) {
   if (c == 0) return s1;
   if (c == jpi) return s0;
+  if (kFold && !safe) return (s0 + s1) * C.k_su;
   double a = 0.5 * (C.e12t * s0 + C.e12t * s1);
   return safe ? qdiv<true>(a, C.e12u, C.r_e12u, bad) : qdiv_k<false>(a, C.e12u, C.r_e12u, bad);
 }
@@ -113,6 +127,7 @@ __device__ __forceinline__ double interp_u(const Consts& C, int c, int jpi, doub
 __device__ __forceinline__ double interp_v(const Consts& C, int jj, int jpj, double s0, double s1,
                                           bool safe, bool& bad) {
   if (jj == jpj) return s0;
+  if (kFold && !safe) return (s0 + s1) * C.k_sv;
   double a = 0.5 * (C.e12t * s0 + C.e12t * s1);
   return safe ? qdiv<true>(a, C.e12v, C.r_e12v, bad) : qdiv_k<false>(a, C.e12v, C.r_e12v, bad);
 }
@@ -156,38 +171,39 @@ __device__ __forceinline__ void row(const Consts& C, int c, int j, int jpi, int 
 
   // x-face of the u equation at T(c,j), between u(c-1,j) and u(c,j)
   const double u_w = up(cur.u);
-  const double uw = 0.5 * (cur.u + u_w) * C.e2t;
+  const double uw = kFold ? (cur.u + u_w) * C.h_e2t : 0.5 * (cur.u + u_w) * C.e2t;
   const double dep = cur.ht + cur.s;
-  const double Fx = upwind(uw, u_w, cur.u) * uw * dep;
+  const double Fx = upw(uw, u_w, cur.u) * uw * dep;
   const double Dx = qdiv_k<SAFE>(cur.u - u_w, C.e1t, C.r_e1t, bad) * dep;
 
   // corner (c,j): east face of v(c,j), north face of u(c,j)
   const double uec = 0.5 * (cur.u + nx.u);
-  const double ue = 0.5 * uec * C.two_dy;
+  const double ue = kFold ? uec * C.q_2dy : 0.5 * uec * C.two_dy;  // folded: half the face velocity
   const double Sn = (k.Hu + nx.hu) + su_n;
   const double v_e = dn(cur.v);
   const double uuv = west0 ? upwind_hi_only(ue, v_e)
-                          : east ? upwind_lo_only(ue, cur.v) : upwind(ue, cur.v, v_e);
-  const double Fvx = uuv * ue * (0.5 * Sn);
+                          : east ? upwind_lo_only(ue, cur.v) : upw(ue, cur.v, v_e);
+  const double Fvx = kFold ? uuv * ue * Sn : uuv * ue * (0.5 * Sn);
   const double Gx = qdiv_k<SAFE>(v_e - cur.v, C.two_dx, C.r_2dx, bad);
   const double vnc = 0.5 * (cur.v + v_e);
-  const double vn_ = 0.5 * vnc * C.two_dx;
+  const double vn_ = kFold ? vnc * C.q_2dx : 0.5 * vnc * C.two_dx;  // folded: half
   const double Re = (Hv + dn(cur.hv)) + dn(sv);
-  const double uuu = north ? upwind_lo_only(vn_, cur.u) : upwind(vn_, cur.u, nx.u);
-  const double Fuy = uuu * vn_ * (0.5 * Re);
+  const double uuu = north ? upwind_lo_only(vn_, cur.u) : upw(vn_, cur.u, nx.u);
+  const double Fuy = kFold ? uuu * vn_ * Re : uuu * vn_ * (0.5 * Re);
   const double Gy = qdiv_k<SAFE>(nx.u - cur.u, C.two_dy, C.r_2dy, bad);
 
   // y-face of the v equation at T(c,j+1), between v(c,j) and v(c,j+1)
-  const double vs = 0.5 * (nx.v + cur.v) * C.e1t;
+  const double vs = kFold ? (nx.v + cur.v) * C.h_e1t : 0.5 * (nx.v + cur.v) * C.e1t;
   const double depn = nx.ht + nx.s;
-  const double Fvy_n = upwind(vs, cur.v, nx.v) * vs * depn;
+  const double Fvy_n = upw(vs, cur.v, nx.v) * vs * depn;
   const double Dvy_n = qdiv_k<SAFE>(nx.v - cur.v, C.e2t, C.r_e2t, bad) * depn;
 
   // continuity (:399-403), clamped SSH row (:631-644)
   const double r1 = k.Hu * cur.u;
   const double r2 = up(r1);
   const double r3 = Hv * cur.v;
-  const double ssh = cur.s + qdiv_k<SAFE>((r2 - r1 + k.cf_s - r3) * C.rdt, C.e12t, C.r_e12t, bad);
+  const double ssh = (kFold && !SAFE) ? cur.s + (r2 - r1 + k.cf_s - r3) * C.k_ssh
+                                      : cur.s + qdiv_k<SAFE>((r2 - r1 + k.cf_s - r3) * C.rdt, C.e12t, C.r_e12t, bad);
   o.ssha = south ? tide : ssh;
 
   // u equation (:439-514); u(jpi,j) is the east wall (:650)
@@ -197,11 +213,19 @@ __device__ __forceinline__ void row(const Consts& C, int c, int j, int jpi, int 
     const double adv = Fx - Fx_e + k.Fuy_s - Fuy;
     const double dudy_n = north ? 0.0 : Gy * Sn;
     const double dudy_s = south ? 0.0 : k.dudy_s;
-    double vis = (Dx_e - Dx) * C.e2u + (dudy_n - dudy_s) * C.e1u * 0.5;
-    vis = C.visc * vis;
-    const double cor = 0.5 * (C.fcor * (k.vnc_s + vnc)) * C.e12u * k.Hu;
-    const double hpg = -(C.g * k.Hu * C.e2u * (k.s_e - cur.s));
-    const double num = cur.u * k.Hu + qdiv_k<SAFE>(C.rdt * (adv + vis + cor + hpg), C.e12u, C.r_e12u, bad);
+    double num;
+    if (kFold && !SAFE) {
+      const double vis = (Dx_e - Dx) * C.vis_u1 + (dudy_n - dudy_s) * C.vis_u2;
+      const double cor = (k.vnc_s + vnc) * C.cor_u * k.Hu;
+      const double hpg = k.Hu * (k.s_e - cur.s) * C.hpg_u;
+      num = cur.u * k.Hu + (adv + vis + cor + hpg) * C.k_u;
+    } else {
+      double vis = (Dx_e - Dx) * C.e2u + (dudy_n - dudy_s) * C.e1u * 0.5;
+      vis = C.visc * vis;
+      const double cor = 0.5 * (C.fcor * (k.vnc_s + vnc)) * C.e12u * k.Hu;
+      const double hpg = -(C.g * k.Hu * C.e2u * (k.s_e - cur.s));
+      num = cur.u * k.Hu + qdiv_k<SAFE>(C.rdt * (adv + vis + cor + hpg), C.e12u, C.r_e12u, bad);
+    }
     const double q = qdiv<SAFE>(num, cur.hu + 0.0, rhu, bad);
     o.ua = east ? 0.0 : qdiv_fric<SAFE>(q, C, bad);
   }
@@ -215,11 +239,19 @@ __device__ __forceinline__ void row(const Consts& C, int c, int j, int jpi, int 
     const double adv = Fvx_w - Fvx + k.Fvy_s - Fvy_n;
     const double dvdx_e = east ? 0.0 : Gx * Re;
     const double dvdx_w = west1 ? 0.0 : Gx_w * ((Hv + hv_w) + sv_w);
-    double vis = (Dvy_n - k.Dvy_s) * C.e1v + (dvdx_e - dvdx_w) * C.e2v * 0.5;
-    vis = C.visc * vis;
-    const double cor = -(0.5 * (C.fcor * (uec + uec_w)) * C.e12v * Hv);
-    const double hpg = -(C.g * Hv * C.e1v * (nx.s - cur.s));
-    const double num = cur.v * Hv + qdiv_k<SAFE>(C.rdt * (adv + vis + cor + hpg), C.e12v, C.r_e12v, bad);
+    double num;
+    if (kFold && !SAFE) {
+      const double vis = (Dvy_n - k.Dvy_s) * C.vis_v1 + (dvdx_e - dvdx_w) * C.vis_v2;
+      const double cor = (uec + uec_w) * C.cor_v * Hv;
+      const double hpg = Hv * (nx.s - cur.s) * C.hpg_v;
+      num = cur.v * Hv + (adv + vis + cor + hpg) * C.k_v;
+    } else {
+      double vis = (Dvy_n - k.Dvy_s) * C.e1v + (dvdx_e - dvdx_w) * C.e2v * 0.5;
+      vis = C.visc * vis;
+      const double cor = -(0.5 * (C.fcor * (uec + uec_w)) * C.e12v * Hv);
+      const double hpg = -(C.g * Hv * C.e1v * (nx.s - cur.s));
+      num = cur.v * Hv + qdiv_k<SAFE>(C.rdt * (adv + vis + cor + hpg), C.e12v, C.r_e12v, bad);
+    }
     const double q = qdiv<SAFE>(num, cur.hv + 0.0, rhv, bad);
     o.va = north ? 0.0 : qdiv_fric<SAFE>(q, C, bad);
   }
@@ -248,9 +280,9 @@ __device__ __forceinline__ void prologue(const Consts& C, int c, int J0, int jpi
   const double Hv_p = p.hv + sv_p;
   // corner (c, J0-1): south face of u(c, J0)
   const double vnc = 0.5 * (p.v + dn(p.v));
-  const double vn_ = 0.5 * vnc * C.two_dx;
-  const double dep = 0.5 * ((Hv_p + dn(p.hv)) + dn(sv_p));
-  const double uu = (J0 == 1) ? upwind_hi_only(vn_, q.u) : upwind(vn_, p.u, q.u);
+  const double vn_ = kFold ? vnc * C.q_2dx : 0.5 * vnc * C.two_dx;
+  const double dep = kFold ? (Hv_p + dn(p.hv)) + dn(sv_p) : 0.5 * ((Hv_p + dn(p.hv)) + dn(sv_p));
+  const double uu = (J0 == 1) ? upwind_hi_only(vn_, q.u) : upw(vn_, p.u, q.u);
   k.Fuy_s = uu * vn_ * dep;
   k.vnc_s = vnc;
   const double s_e_p = dn(p.s);
@@ -262,9 +294,9 @@ __device__ __forceinline__ void prologue(const Consts& C, int c, int J0, int jpi
     k.dudy_s = gy * ((k.Hu + p.hu) + su_p);
   }
   // T(c, J0): south face of v(c, J0)
-  const double vs = 0.5 * (q.v + p.v) * C.e1t;
+  const double vs = kFold ? (q.v + p.v) * C.h_e1t : 0.5 * (q.v + p.v) * C.e1t;
   const double depc = q.ht + q.s;
-  k.Fvy_s = upwind(vs, p.v, q.v) * vs * depc;
+  k.Fvy_s = upw(vs, p.v, q.v) * vs * depc;
   k.Dvy_s = qdiv_k<SAFE>(q.v - p.v, C.e2t, C.r_e2t, bad) * depc;
   k.cf_s = Hv_p * p.v;
 }
