@@ -169,17 +169,17 @@ Consts make_consts(const nemo_params& p) {
   C.k_sv = (0.5 * C.e12t) / C.e12v;
   C.h_e2t = 0.5 * C.e2t;
   C.h_e1t = 0.5 * C.e1t;
-  C.q_2dy = 0.25 * C.two_dy;
-  C.q_2dx = 0.25 * C.two_dx;
+  C.e_2dy = 0.125 * C.two_dy;
+  C.e_2dx = 0.125 * C.two_dx;
   C.k_ssh = C.rdt / C.e12t;
   C.k_u = C.rdt / C.e12u;
   C.k_v = C.rdt / C.e12v;
-  C.vis_u1 = C.visc * C.e2u;
-  C.vis_u2 = C.visc * (0.5 * C.e1u);
-  C.vis_v1 = C.visc * C.e1v;
-  C.vis_v2 = C.visc * (0.5 * C.e2v);
-  C.cor_u = (0.5 * C.fcor) * C.e12u;
-  C.cor_v = -((0.5 * C.fcor) * C.e12v);
+  C.vis_u1 = C.visc * C.e2u / C.e1t;
+  C.vis_u2 = C.visc * (0.5 * C.e1u) / C.two_dy;
+  C.vis_v1 = C.visc * C.e1v / C.e2t;
+  C.vis_v2 = C.visc * (0.5 * C.e2v) / C.two_dx;
+  C.cor_u = (0.25 * C.fcor) * C.e12u;
+  C.cor_v = -((0.25 * C.fcor) * C.e12v);
   C.hpg_u = -(C.g * C.e2u);
   C.hpg_v = -(C.g * C.e1v);
   return C;

@@ -45,12 +45,12 @@ struct Consts {
   double r_e1t, r_e2t, r_e12t, r_e12u, r_e12v, r_2dx, r_2dy, r_cfric;
   // RN((1 - cfric*r_cfric)/cfric): with r_cfric, 1/cfric to about 2^-106
   double r_cfric_lo;
-  // Products of constants for the default build's folded forms (each RN of
-  // the exact product or quotient except where the scaling by a power of two
-  // is exact): 0.5*e12t/e12u, 0.5*e12t/e12v, 0.5*e2t, 0.5*e1t, two_dy/4,
-  // two_dx/4, rdt/e12t, rdt/e12u, rdt/e12v, visc*e2u, visc*e1u/2, visc*e1v,
-  // visc*e2v/2, fcor*e12u/2, -fcor*e12v/2, -g*e2u, -g*e1v.
-  double k_su, k_sv, h_e2t, h_e1t, q_2dy, q_2dx, k_ssh, k_u, k_v;
+  // Products of constants for the default build's folded forms (formed on
+  // the host): 0.5*e12t/e12u, 0.5*e12t/e12v, 0.5*e2t, 0.5*e1t, two_dy/8,
+  // two_dx/8, rdt/e12t, rdt/e12u, rdt/e12v, visc*e2u/e1t, visc*e1u/2/two_dy,
+  // visc*e1v/e2t, visc*e2v/2/two_dx, fcor*e12u/4, -fcor*e12v/4, -g*e2u,
+  // -g*e1v.
+  double k_su, k_sv, h_e2t, h_e1t, e_2dy, e_2dx, k_ssh, k_u, k_v;
   double vis_u1, vis_u2, vis_v1, vis_v2, cor_u, cor_v, hpg_u, hpg_v;
 };
 
@@ -89,14 +89,19 @@ __device__ __forceinline__ double div_const(double a, double b, double rb) {
 // callers that need RN(1/b) verify it against an IEEE division once per
 // static divisor (launch_recip) and keep the stored quotient otherwise.
 // b must be a normal number within single-precision range.
-__device__ __forceinline__ double recip_nr(double b) {
+__device__ __forceinline__ double recip_seed(double b) {
   float yf;
   asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"(__double2float_rn(b)));
-  double y = (double)yf;
-  double e = fma(-b, y, 1.0);
-  y = fma(y, e, y);
-  e = fma(-b, y, 1.0);
-  return fma(y, e, y);
+  return (double)yf;
+}
+// One Newton step: relative error about 2^-46.
+__device__ __forceinline__ double recip_nr1(double b) {
+  const double y = recip_seed(b);
+  return fma(y, fma(-b, y, 1.0), y);
+}
+__device__ __forceinline__ double recip_nr(double b) {
+  const double y = recip_nr1(b);
+  return fma(y, fma(-b, y, 1.0), y);
 }
 
 constexpr unsigned long long kSign = 0x8000000000000000ull;

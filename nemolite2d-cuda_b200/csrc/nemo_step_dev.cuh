@@ -40,9 +40,12 @@ __device__ __forceinline__ double up(double x) { return __shfl_up_sync(FULL, x, 
 // way at every step, and that bias accumulated to 1.4e-12 over 2000 steps of
 // the 128^2 case when those too took the one-multiply form (1.3e-14 without).
 // The same reasoning lets the default build fold products of grid constants
-// (0.5*x*e2t as x*(0.5*e2t), rdt*(...)/e12u as (...)*(rdt/e12u), and the
-// viscosity, Coriolis and pressure-gradient coefficients; kFold below) and
-// pick the upwind value with a plain select.
+// (0.5*x*e2t as x*(0.5*e2t), rdt*(...)/e12u as (...)*(rdt/e12u), the grid
+// spacings of the viscous gradients into the viscosity coefficients, and
+// the Coriolis and pressure-gradient coefficients; kFold below) and pick the
+// upwind value with a plain select.  Carried face values then hold the
+// folded (scaled) forms, so the IEEE-division rows (SAFE) exist only in the
+// strict build.
 #ifdef NEMO_STRICT_BUILD
 constexpr bool kRoundedQuotients = true;
 #else
@@ -99,6 +102,13 @@ __device__ __forceinline__ double qdiv_fric(double a, const Consts& C, bool& bad
   if (!SAFE && !kRoundedQuotients) return fma(a, C.r_cfric, a * C.r_cfric_lo);
   return qdiv<SAFE>(a, C.cfric, C.r_cfric, bad);
 }
+
+// Reciprocal depth for the corrected depth quotients of the ring strips:
+// RN(1/b) (recip_nr, checked cell by cell at setup) in the strict build; one
+// Newton step in the default build, where the quotient's residual step turns
+// its 2^-46 error into a quotient that is still the rounded one except within
+// about 2^-39 ulp of a rounding boundary.
+__device__ __forceinline__ double recip_depth(double b) { return kFold ? recip_nr1(b) : recip_nr(b); }
 
 // Nonzero with |x| < 2^-300 (biased exponent below 723).
 __device__ __forceinline__ bool tiny(double x) {
@@ -174,35 +184,35 @@ __device__ __forceinline__ void row(const Consts& C, int c, int j, int jpi, int 
   const double uw = kFold ? (cur.u + u_w) * C.h_e2t : 0.5 * (cur.u + u_w) * C.e2t;
   const double dep = cur.ht + cur.s;
   const double Fx = upw(uw, u_w, cur.u) * uw * dep;
-  const double Dx = qdiv_k<SAFE>(cur.u - u_w, C.e1t, C.r_e1t, bad) * dep;
+  const double Dx = kFold ? (cur.u - u_w) * dep : qdiv_k<SAFE>(cur.u - u_w, C.e1t, C.r_e1t, bad) * dep;
 
   // corner (c,j): east face of v(c,j), north face of u(c,j)
-  const double uec = 0.5 * (cur.u + nx.u);
-  const double ue = kFold ? uec * C.q_2dy : 0.5 * uec * C.two_dy;  // folded: half the face velocity
+  const double uec = kFold ? cur.u + nx.u : 0.5 * (cur.u + nx.u);  // folded: twice
+  const double ue = kFold ? uec * C.e_2dy : 0.5 * uec * C.two_dy;    // folded: half
   const double Sn = (k.Hu + nx.hu) + su_n;
   const double v_e = dn(cur.v);
   const double uuv = west0 ? upwind_hi_only(ue, v_e)
                           : east ? upwind_lo_only(ue, cur.v) : upw(ue, cur.v, v_e);
   const double Fvx = kFold ? uuv * ue * Sn : uuv * ue * (0.5 * Sn);
-  const double Gx = qdiv_k<SAFE>(v_e - cur.v, C.two_dx, C.r_2dx, bad);
-  const double vnc = 0.5 * (cur.v + v_e);
-  const double vn_ = kFold ? vnc * C.q_2dx : 0.5 * vnc * C.two_dx;  // folded: half
+  const double Gx = kFold ? v_e - cur.v : qdiv_k<SAFE>(v_e - cur.v, C.two_dx, C.r_2dx, bad);
+  const double vnc = kFold ? cur.v + v_e : 0.5 * (cur.v + v_e);  // folded: twice
+  const double vn_ = kFold ? vnc * C.e_2dx : 0.5 * vnc * C.two_dx;  // folded: half
   const double Re = (Hv + dn(cur.hv)) + dn(sv);
   const double uuu = north ? upwind_lo_only(vn_, cur.u) : upw(vn_, cur.u, nx.u);
   const double Fuy = kFold ? uuu * vn_ * Re : uuu * vn_ * (0.5 * Re);
-  const double Gy = qdiv_k<SAFE>(nx.u - cur.u, C.two_dy, C.r_2dy, bad);
+  const double Gy = kFold ? nx.u - cur.u : qdiv_k<SAFE>(nx.u - cur.u, C.two_dy, C.r_2dy, bad);
 
   // y-face of the v equation at T(c,j+1), between v(c,j) and v(c,j+1)
   const double vs = kFold ? (nx.v + cur.v) * C.h_e1t : 0.5 * (nx.v + cur.v) * C.e1t;
   const double depn = nx.ht + nx.s;
   const double Fvy_n = upw(vs, cur.v, nx.v) * vs * depn;
-  const double Dvy_n = qdiv_k<SAFE>(nx.v - cur.v, C.e2t, C.r_e2t, bad) * depn;
+  const double Dvy_n = kFold ? (nx.v - cur.v) * depn : qdiv_k<SAFE>(nx.v - cur.v, C.e2t, C.r_e2t, bad) * depn;
 
   // continuity (:399-403), clamped SSH row (:631-644)
   const double r1 = k.Hu * cur.u;
   const double r2 = up(r1);
   const double r3 = Hv * cur.v;
-  const double ssh = (kFold && !SAFE) ? cur.s + (r2 - r1 + k.cf_s - r3) * C.k_ssh
+  const double ssh = kFold ? cur.s + (r2 - r1 + k.cf_s - r3) * C.k_ssh
                                       : cur.s + qdiv_k<SAFE>((r2 - r1 + k.cf_s - r3) * C.rdt, C.e12t, C.r_e12t, bad);
   o.ssha = south ? tide : ssh;
 
@@ -214,11 +224,10 @@ __device__ __forceinline__ void row(const Consts& C, int c, int j, int jpi, int 
     const double dudy_n = north ? 0.0 : Gy * Sn;
     const double dudy_s = south ? 0.0 : k.dudy_s;
     double num;
-    if (kFold && !SAFE) {
+    if (kFold) {
       const double vis = (Dx_e - Dx) * C.vis_u1 + (dudy_n - dudy_s) * C.vis_u2;
-      const double cor = (k.vnc_s + vnc) * C.cor_u * k.Hu;
-      const double hpg = k.Hu * (k.s_e - cur.s) * C.hpg_u;
-      num = cur.u * k.Hu + (adv + vis + cor + hpg) * C.k_u;
+      const double corhpg = k.Hu * ((k.vnc_s + vnc) * C.cor_u + (k.s_e - cur.s) * C.hpg_u);
+      num = cur.u * k.Hu + (adv + vis + corhpg) * C.k_u;
     } else {
       double vis = (Dx_e - Dx) * C.e2u + (dudy_n - dudy_s) * C.e1u * 0.5;
       vis = C.visc * vis;
@@ -226,7 +235,7 @@ __device__ __forceinline__ void row(const Consts& C, int c, int j, int jpi, int 
       const double hpg = -(C.g * k.Hu * C.e2u * (k.s_e - cur.s));
       num = cur.u * k.Hu + qdiv_k<SAFE>(C.rdt * (adv + vis + cor + hpg), C.e12u, C.r_e12u, bad);
     }
-    const double q = qdiv<SAFE>(num, cur.hu + 0.0, rhu, bad);
+    const double q = qdiv<SAFE>(num, kFold ? cur.hu : cur.hu + 0.0, rhu, bad);
     o.ua = east ? 0.0 : qdiv_fric<SAFE>(q, C, bad);
   }
   // v equation (:527-606); v(c,jpj) is the north wall (:658)
@@ -240,11 +249,10 @@ __device__ __forceinline__ void row(const Consts& C, int c, int j, int jpi, int 
     const double dvdx_e = east ? 0.0 : Gx * Re;
     const double dvdx_w = west1 ? 0.0 : Gx_w * ((Hv + hv_w) + sv_w);
     double num;
-    if (kFold && !SAFE) {
+    if (kFold) {
       const double vis = (Dvy_n - k.Dvy_s) * C.vis_v1 + (dvdx_e - dvdx_w) * C.vis_v2;
-      const double cor = (uec + uec_w) * C.cor_v * Hv;
-      const double hpg = Hv * (nx.s - cur.s) * C.hpg_v;
-      num = cur.v * Hv + (adv + vis + cor + hpg) * C.k_v;
+      const double corhpg = Hv * ((uec + uec_w) * C.cor_v + (nx.s - cur.s) * C.hpg_v);
+      num = cur.v * Hv + (adv + vis + corhpg) * C.k_v;
     } else {
       double vis = (Dvy_n - k.Dvy_s) * C.e1v + (dvdx_e - dvdx_w) * C.e2v * 0.5;
       vis = C.visc * vis;
@@ -252,7 +260,7 @@ __device__ __forceinline__ void row(const Consts& C, int c, int j, int jpi, int 
       const double hpg = -(C.g * Hv * C.e1v * (nx.s - cur.s));
       num = cur.v * Hv + qdiv_k<SAFE>(C.rdt * (adv + vis + cor + hpg), C.e12v, C.r_e12v, bad);
     }
-    const double q = qdiv<SAFE>(num, cur.hv + 0.0, rhv, bad);
+    const double q = qdiv<SAFE>(num, kFold ? cur.hv : cur.hv + 0.0, rhv, bad);
     o.va = north ? 0.0 : qdiv_fric<SAFE>(q, C, bad);
   }
   o.sv = sv;
@@ -279,8 +287,8 @@ __device__ __forceinline__ void prologue(const Consts& C, int c, int J0, int jpi
   sv_p = (J0 == 1) ? sv_p_stored : interp_v(C, J0 - 1, jpj, p.s, q.s, SAFE, bad);
   const double Hv_p = p.hv + sv_p;
   // corner (c, J0-1): south face of u(c, J0)
-  const double vnc = 0.5 * (p.v + dn(p.v));
-  const double vn_ = kFold ? vnc * C.q_2dx : 0.5 * vnc * C.two_dx;
+  const double vnc = kFold ? p.v + dn(p.v) : 0.5 * (p.v + dn(p.v));
+  const double vn_ = kFold ? vnc * C.e_2dx : 0.5 * vnc * C.two_dx;
   const double dep = kFold ? (Hv_p + dn(p.hv)) + dn(sv_p) : 0.5 * ((Hv_p + dn(p.hv)) + dn(sv_p));
   const double uu = (J0 == 1) ? upwind_hi_only(vn_, q.u) : upw(vn_, p.u, q.u);
   k.Fuy_s = uu * vn_ * dep;
@@ -290,14 +298,14 @@ __device__ __forceinline__ void prologue(const Consts& C, int c, int J0, int jpi
     k.dudy_s = 0.0;
   } else {
     const double su_p = interp_u(C, c, jpi, p.s, s_e_p, SAFE, bad);
-    const double gy = qdiv_k<SAFE>(q.u - p.u, C.two_dy, C.r_2dy, bad);
+    const double gy = kFold ? q.u - p.u : qdiv_k<SAFE>(q.u - p.u, C.two_dy, C.r_2dy, bad);
     k.dudy_s = gy * ((k.Hu + p.hu) + su_p);
   }
   // T(c, J0): south face of v(c, J0)
   const double vs = kFold ? (q.v + p.v) * C.h_e1t : 0.5 * (q.v + p.v) * C.e1t;
   const double depc = q.ht + q.s;
   k.Fvy_s = upw(vs, p.v, q.v) * vs * depc;
-  k.Dvy_s = qdiv_k<SAFE>(q.v - p.v, C.e2t, C.r_e2t, bad) * depc;
+  k.Dvy_s = (kFold ? q.v - p.v : qdiv_k<SAFE>(q.v - p.v, C.e2t, C.r_e2t, bad)) * depc;
   k.cf_s = Hv_p * p.v;
 }
 
@@ -328,7 +336,7 @@ __device__ __forceinline__ void run_strip(const Layout& L, const Consts& C, cons
   unsigned hist = (any_tiny(p) << 1) | any_tiny(cur);
   {
     bool bad = false;
-    if (hist) prologue<true>(C, c, J0, jpi, jpj, sv_stored, p, cur, k, sv0, bad);
+    if (kRoundedQuotients && hist) prologue<true>(C, c, J0, jpi, jpj, sv_stored, p, cur, k, sv0, bad);
     else prologue<false>(C, c, J0, jpi, jpj, sv_stored, p, cur, k, sv0, bad);
   }
   if (PF) load_cell(nx, A, L.idx(cl, J0 + 1));
@@ -355,7 +363,7 @@ __device__ __forceinline__ void run_strip(const Layout& L, const Consts& C, cons
     RowOut o;
     bool bad = false;
     hist = ((hist << 1) | any_tiny(nx)) & 7u;
-    if (hist) {
+    if (kRoundedQuotients && hist) {
       row<true, true>(C, c, j, jpi, jpj, A.tide, cur, nx, k, rhu, rhv, o, bad);
     } else if (edge_warp || j == 1 || j == jpj) {
       row<false, true>(C, c, j, jpi, jpj, A.tide, cur, nx, k, rhu, rhv, o, bad);
@@ -449,7 +457,7 @@ __device__ __forceinline__ void run_strip_ring(const Layout& L, const Consts& C,
   unsigned hist = (any_tiny(p) << 1) | any_tiny(cur);
   {
     bool bad = false;
-    if (hist) prologue<true>(C, c, J0, jpi, jpj, sv_stored, p, cur, k, sv0, bad);
+    if (kRoundedQuotients && hist) prologue<true>(C, c, J0, jpi, jpj, sv_stored, p, cur, k, sv0, bad);
     else prologue<false>(C, c, J0, jpi, jpj, sv_stored, p, cur, k, sv0, bad);
   }
   long o_ld = L.idx(cl, J0 + 2);
@@ -465,13 +473,13 @@ __device__ __forceinline__ void run_strip_ring(const Layout& L, const Consts& C,
     o_ld += pitch;
     cp_wait1();  // rows <= j+1 have landed
     ring_cell(nx, my + slot_n * 256);
-    const double rhu = NR ? recip_nr(cur.hu + 0.0) : my[slot_j * 256 + 6 * 32];
-    const double rhv = NR ? recip_nr(cur.hv + 0.0) : my[slot_j * 256 + 7 * 32];
+    const double rhu = NR ? recip_depth(cur.hu + 0.0) : my[slot_j * 256 + 6 * 32];
+    const double rhv = NR ? recip_depth(cur.hv + 0.0) : my[slot_j * 256 + 7 * 32];
 
     RowOut o;
     bool bad = false;
     hist = ((hist << 1) | any_tiny(nx)) & 7u;
-    if (hist) {
+    if (kRoundedQuotients && hist) {
       row<true, true>(C, c, j, jpi, jpj, A.tide, cur, nx, k, rhu, rhv, o, bad);
     } else if (edge_warp || j == 1 || j == jpj) {
       row<false, true>(C, c, j, jpi, jpj, A.tide, cur, nx, k, rhu, rhv, o, bad);
