@@ -390,10 +390,12 @@ __device__ __forceinline__ void run_strip(const Layout& L, const Consts& C, cons
 
 // ---- shared-memory ring variant -------------------------------------------
 // Rows are staged by cp.async into a per-warp ring of RING rows x 8 fields x
-// 32 lanes (each lane copies and reads only its own column), two rows ahead
+// 32 lanes (each lane copies and reads only its own column), AHEAD rows ahead
 // of their use, so DRAM latency is hidden without holding prefetched rows in
-// registers.
-constexpr int RING = 3;
+// registers.  Row r sits in slot r % RING; the copy of row j+AHEAD reuses
+// the slot of row j-1, read into registers two iterations earlier.
+constexpr int RING = 4;
+constexpr int AHEAD = RING - 1;
 constexpr int RING_DOUBLES = RING * 8 * 32;
 
 __device__ __forceinline__ void cp_async8(double* dst, const double* src) {
@@ -401,7 +403,9 @@ __device__ __forceinline__ void cp_async8(double* dst, const double* src) {
                : "memory");
 }
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+// Wait until at most N of this thread's copy groups are pending.
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 // NR: the reciprocal depths are formed in the kernel (recip_nr), not staged.
 template <bool NR>
@@ -444,9 +448,14 @@ __device__ __forceinline__ void run_strip_ring(const Layout& L, const Consts& C,
 
   const long pitch = L.pitch;
   const long o_last = L.idx(cl, jpj + 1);
-  // rows J0 and J0+1 into the ring (row r in slot r % RING)
-  ring_issue<NR>(my + (J0 % RING) * 256, A, L.idx(cl, J0));
-  ring_issue<NR>(my + ((J0 + 1) % RING) * 256, A, L.idx(cl, J0 + 1));
+  // rows J0+1 .. J0+AHEAD-1 into the ring, and row J0 when its stored
+  // reciprocal depths are read from there (rows J0-1 and J0 are loaded
+  // directly below; rows past jpj+1 read row jpj+1 again)
+#pragma unroll
+  for (int r = NR ? 1 : 0; r < AHEAD; ++r) {
+    const long o = L.idx(cl, J0 + r);
+    ring_issue<NR>(my + ((J0 + r) % RING) * 256, A, o < o_last ? o : o_last);
+  }
 
   Cell p, cur, nx;
   load_cell(p, A, L.idx(cl, J0 - 1));
@@ -460,18 +469,18 @@ __device__ __forceinline__ void run_strip_ring(const Layout& L, const Consts& C,
     if (kRoundedQuotients && hist) prologue<true>(C, c, J0, jpi, jpj, sv_stored, p, cur, k, sv0, bad);
     else prologue<false>(C, c, J0, jpi, jpj, sv_stored, p, cur, k, sv0, bad);
   }
-  long o_ld = L.idx(cl, J0 + 2);
+  long o_ld = L.idx(cl, J0 + AHEAD);
   long o_st = L.idx(c, J0);
   int slot_j = J0 % RING;
 // UNROLL = 2 keeps two rows in flight (the second row's independent work
 // fills FP64 latency) where registers allow it without spills
 #pragma unroll UNROLL
   for (int j = J0; j <= J1; ++j) {
-    const int slot_n = slot_j == RING - 1 ? 0 : slot_j + 1;      // row j+1
-    const int slot_f = slot_n == RING - 1 ? 0 : slot_n + 1;      // row j+2 (was row j-1)
+    const int slot_n = slot_j == RING - 1 ? 0 : slot_j + 1;  // row j+1
+    const int slot_f = slot_j == 0 ? RING - 1 : slot_j - 1;  // row j+AHEAD (was row j-1)
     ring_issue<NR>(my + slot_f * 256, A, o_ld < o_last ? o_ld : o_last);
     o_ld += pitch;
-    cp_wait1();  // rows <= j+1 have landed
+    cp_wait<AHEAD - 1>();  // rows <= j+1 have landed
     ring_cell(nx, my + slot_n * 256);
     const double rhu = NR ? recip_depth(cur.hu + 0.0) : my[slot_j * 256 + 6 * 32];
     const double rhv = NR ? recip_depth(cur.hv + 0.0) : my[slot_j * 256 + 7 * 32];
