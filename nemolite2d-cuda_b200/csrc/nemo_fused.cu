@@ -50,8 +50,9 @@ k_fused_step(Layout L, Consts C, FusedArgs A, int tile_y) {
   if (J0 > L.jpj) return;
   const int J1 = min(J0 + tile_y - 1, L.jpj);
   if constexpr (PF >= 2) {
-    __shared__ double ring[NWARPS * RING_DOUBLES];
-    run_strip_ring<PF == 3, 2>(L, C, A, c0, J0, J1, lane, ring + (threadIdx.x >> 5) * RING_DOUBLES);
+    constexpr int RD = ring_doubles<PF == 3>();
+    __shared__ double ring[NWARPS * RD];
+    run_strip_ring<PF == 3, 2>(L, C, A, c0, J0, J1, lane, ring + (threadIdx.x >> 5) * RD);
   } else {
     run_strip<PF>(L, C, A, c0, J0, J1, lane);
   }

@@ -389,14 +389,22 @@ __device__ __forceinline__ void run_strip(const Layout& L, const Consts& C, cons
 }
 
 // ---- shared-memory ring variant -------------------------------------------
-// Rows are staged by cp.async into a per-warp ring of RING rows x 8 fields x
-// 32 lanes (each lane copies and reads only its own column), AHEAD rows ahead
-// of their use, so DRAM latency is hidden without holding prefetched rows in
-// registers.  Row r sits in slot r % RING; the copy of row j+AHEAD reuses
-// the slot of row j-1, read into registers two iterations earlier.
-constexpr int RING = 4;
-constexpr int AHEAD = RING - 1;
-constexpr int RING_DOUBLES = RING * 8 * 32;
+// Rows are staged by cp.async into a per-warp ring of ring_slots<NR>() rows
+// x 6 or 8 fields x 32 lanes (each lane copies and reads only its own
+// column), ring_slots<NR>() - 1 rows ahead of their use, so DRAM latency is
+// hidden without holding prefetched rows in registers.  Row r sits in slot
+// r % slots; the copy of row j+ahead reuses the slot of row j-1, read into
+// registers two iterations earlier.  NR: the reciprocal depths are formed in
+// the kernel, so a row holds 6 fields instead of 8.
+#ifndef NEMO_RING_NR
+#define NEMO_RING_NR 4
+#endif
+template <bool NR>
+__host__ __device__ constexpr int ring_slots() { return NR ? NEMO_RING_NR : 4; }
+template <bool NR>
+__host__ __device__ constexpr int ring_row() { return (NR ? 6 : 8) * 32; }  // doubles per staged row
+template <bool NR>
+__host__ __device__ constexpr int ring_doubles() { return ring_slots<NR>() * ring_row<NR>(); }
 
 __device__ __forceinline__ void cp_async8(double* dst, const double* src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
@@ -432,7 +440,7 @@ __device__ __forceinline__ void ring_cell(Cell& x, const double* slot) {
   x.hv = slot[5 * 32];
 }
 
-// run_strip with rows staged through `ring` (this warp's RING_DOUBLES, in
+// run_strip with rows staged through `ring` (this warp's ring_doubles<NR>(), in
 // shared memory), its row loop unrolled UNROLL times.  NR = true forms RN(1/hu), RN(1/hv) with recip_nr instead
 // of reading the stored fields: valid only for depths that launch_recip
 // found to give exactly the stored values (16 fewer bytes per cell-step).
@@ -445,6 +453,7 @@ __device__ __forceinline__ void run_strip_ring(const Layout& L, const Consts& C,
   const bool store = (lane >= 1) && (lane <= COLS_PER_WARP) && (c <= jpi);
   const bool edge_warp = (c0 - 1 <= 1) || (c0 + COLS_PER_WARP >= jpi);
   double* my = ring + lane;  // this lane's column of every ring row
+  constexpr int RING = ring_slots<NR>(), AHEAD = RING - 1, RS = ring_row<NR>();
 
   const long pitch = L.pitch;
   const long o_last = L.idx(cl, jpj + 1);
@@ -454,7 +463,7 @@ __device__ __forceinline__ void run_strip_ring(const Layout& L, const Consts& C,
 #pragma unroll
   for (int r = NR ? 1 : 0; r < AHEAD; ++r) {
     const long o = L.idx(cl, J0 + r);
-    ring_issue<NR>(my + ((J0 + r) % RING) * 256, A, o < o_last ? o : o_last);
+    ring_issue<NR>(my + ((J0 + r) % RING) * RS, A, o < o_last ? o : o_last);
   }
 
   Cell p, cur, nx;
@@ -478,12 +487,12 @@ __device__ __forceinline__ void run_strip_ring(const Layout& L, const Consts& C,
   for (int j = J0; j <= J1; ++j) {
     const int slot_n = slot_j == RING - 1 ? 0 : slot_j + 1;  // row j+1
     const int slot_f = slot_j == 0 ? RING - 1 : slot_j - 1;  // row j+AHEAD (was row j-1)
-    ring_issue<NR>(my + slot_f * 256, A, o_ld < o_last ? o_ld : o_last);
+    ring_issue<NR>(my + slot_f * RS, A, o_ld < o_last ? o_ld : o_last);
     o_ld += pitch;
     cp_wait<AHEAD - 1>();  // rows <= j+1 have landed
-    ring_cell(nx, my + slot_n * 256);
-    const double rhu = NR ? recip_depth(cur.hu + 0.0) : my[slot_j * 256 + 6 * 32];
-    const double rhv = NR ? recip_depth(cur.hv + 0.0) : my[slot_j * 256 + 7 * 32];
+    ring_cell(nx, my + slot_n * RS);
+    const double rhu = NR ? recip_depth(cur.hu + 0.0) : my[slot_j * RS + 6 * 32];
+    const double rhv = NR ? recip_depth(cur.hv + 0.0) : my[slot_j * RS + 7 * 32];
 
     RowOut o;
     bool bad = false;
