@@ -72,6 +72,7 @@ def parse():
                     help="fine-tuning iterations on rollout pairs (hybrid; 0: none)")
     ap.add_argument("--batch", type=int, default=64, help="images per conv call (conv workload)")
     ap.add_argument("--train-iters", type=int, default=6000)
+    ap.add_argument("--nblocks", type=int, default=4, help="residual blocks of the hybrid's network")
     ap.add_argument("--n", type=int, default=N,
                     help="grid side (profiling of smaller cases only; the bench line is 4096)")
     return ap.parse_args()
@@ -458,7 +459,7 @@ def run_hybrid(args):
     nsteps = args.hyb_steps
     side, nm, P, ts = 2048, 32, args.patch, args.train_side
     # ---- train on solver runs of the recipe
-    trainer = sm.Surrogate(nblocks=8, batch=64, height=ts, width=ts, seed=1234, device=0, patch=P)
+    trainer = sm.Surrogate(nblocks=args.nblocks, batch=64, height=ts, width=ts, seed=1234, device=0, patch=P)
     t_gen = time.time()
     snaps, tides = tr.generate_runs(trainer, seed=7000, nmem=args.train_runs, side=ts,
                                     steps=args.train_steps, pair_stride=50)
@@ -497,7 +498,7 @@ def run_hybrid(args):
     nm = len(members)
     plain = nemo_b200.Ensemble(members, **common)
     hyb = nemo_b200.Ensemble(members, **common)
-    inf = sm.Surrogate(nblocks=8, batch=nm, height=side, width=side, train=False, seed=1,
+    inf = sm.Surrogate(nblocks=args.nblocks, batch=nm, height=side, width=side, train=False, seed=1,
                        stream=stream.cuda_stream, device=0, patch=P)
     inf.set_params(params)
     inf.set_norm(*norm)
@@ -530,7 +531,7 @@ def run_hybrid(args):
             "config": {"workload": "%d members 2048x2048, %d steps, surrogate k=10, re-anchor 100, "
                                    "tol 1%% relative SSH L2 vs shadow FP64 step" % (nm, nsteps),
                        "candidates": len(cands), "screened_out": len(cands) - len(ok),
-                       "patch": P, "train_side": ts, "train_steps": args.train_steps,
+                       "patch": P, "nblocks": args.nblocks, "train_side": ts, "train_steps": args.train_steps,
                        "train_runs": args.train_runs, "fallback": "per member",
                        "train_input_noise": args.noise,
                        "rollout_runs": args.rollout_runs, "rollout_windows": args.rollout_windows,

@@ -323,6 +323,11 @@ typedef struct nemo_hyb_config {
                      0: any failing member sends the whole ensemble back (1) */
   double quarantine; /* shadow error beyond which a member stays on the FP64
                         solver for the rest of the run; 0: never (0.05) */
+  int rewind;        /* 1: a member quarantined right after a window the
+                        surrogate advanced restarts from its FP64 state at
+                        that window's start, the solver re-running the
+                        window (keeps one saved state per member and window
+                        parity: 2 x 3 fields per member) (1) */
 } nemo_hyb_config;
 
 typedef struct nemo_hyb_stats {
@@ -335,6 +340,7 @@ typedef struct nemo_hyb_stats {
   double seconds;
   long long launches;      /* kernels launched (solver steps and surrogate work) */
   long long quarantined;   /* members kept on the solver after a large shadow error */
+  long long rewound;       /* quarantined members restarted from their previous anchor */
 } nemo_hyb_stats;
 
 int nemo_hyb_default_config(nemo_hyb_config* c);

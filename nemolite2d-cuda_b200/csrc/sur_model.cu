@@ -920,6 +920,7 @@ int nemo_hyb_default_config(nemo_hyb_config* c) {
   c->tol = 0.01;
   c->per_member = 1;
   c->quarantine = 0.05;
+  c->rewind = 1;
   return NEMO_OK;
 }
 
@@ -932,9 +933,12 @@ int nemo_hyb_default_config(nemo_hyb_config* c) {
 // advance by surrogate calls, k steps each.  A member whose shadow error
 // exceeds `quarantine` stays on the solver for the rest of the run (errors
 // that large precede the corner instability the surrogate's perturbations
-// can excite).  With per_member = 0 one failing member sends the whole
-// ensemble to the solver for the window.  Statistics count member-windows
-// and member-steps.
+// can excite).  With `rewind`, such a member whose current state came from
+// the previous window's surrogate calls is first restored to its FP64 state
+// at that window's start (saved at every window start) and the solver re-runs
+// the window, anchor + k steps, so the unchecked calls leave no trace.  With
+// per_member = 0 one failing member sends the whole ensemble to the solver
+// for the window.  Statistics count member-windows and member-steps.
 int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, int nsteps,
                  nemo_hyb_stats* stats) {
   if (!s || !e || !c || c->k != 10 || c->anchor < c->k || c->anchor % c->k || nsteps % c->anchor ||
@@ -958,7 +962,22 @@ int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, 
     out_all = own + (size_t)nm * hw * 4;
   }
   std::vector<double> tide(nm), acc(6 * nm);
-  std::vector<char> pass(nm), fail(nm), quar(nm, 0);
+  std::vector<char> pass(nm), fail(nm), quar(nm, 0), prev_pass(nm, 0), rew(nm);
+  // saved FP64 states (sshn, un, vn) of every member at the last two window
+  // starts, for rewinding
+  const size_t field_elems = (size_t)(ms.empty() ? 0 : (long)(ms[0].jpj + 3) * ms[0].pitch);
+  double* saved = nullptr;
+  const bool rewind = c->rewind && c->quarantine > 0 && c->per_member;
+  if (rewind && nm > 0) {
+    cudaError_t ae = cudaMalloc(&saved, 2 * (size_t)nm * 3 * field_elems * sizeof(double));
+    if (ae != cudaSuccess) {
+      if (own) cudaFree(own);
+      return status_of(ae);
+    }
+  }
+  auto saved_field = [&](int parity, int m, int f) {
+    return saved + (((size_t)parity * nm + m) * 3 + f) * field_elems;
+  };
   const long long launches0 = s->nlaunch;
   long long solver_launches = 0;  // one persistent ensemble launch per solver step
   const auto t_start = std::chrono::steady_clock::now();
@@ -966,6 +985,16 @@ int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, 
   int rc = NEMO_OK;
   const int rest = c->anchor - c->k;
   for (int w = 0; w < nsteps / c->anchor && rc == NEMO_OK; ++w) {
+    if (saved) {  // the window's starting states, while the members are still in them
+      for (int m = 0; m < nm && rc == NEMO_OK; ++m) {
+        if (quar[m]) continue;
+        double* src[3] = {ms[m].sshn, ms[m].un, ms[m].vn};
+        for (int f = 0; f < 3 && rc == NEMO_OK; ++f)
+          rc = status_of(cudaMemcpyAsync(saved_field(w & 1, m, f), src[f], field_elems * sizeof(double),
+                                         cudaMemcpyDeviceToDevice, s->stream));
+      }
+      if (rc != NEMO_OK) break;
+    }
     for (int i = 0; i < nm; ++i) tide[i] = nemo::ens_tide(e, i, istp + c->k);
     for (int m0 = 0; m0 < nm && rc == NEMO_OK; m0 += s->cfg.batch) {
       const int n = nm - m0 < s->cfg.batch ? nm - m0 : s->cfg.batch;
@@ -986,22 +1015,43 @@ int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, 
     if ((rc = check_err(s)) != NEMO_OK) break;
     // a non-finite error (a member whose state blew up) counts as a failure
     double worst = 0.0;
-    int nfail = 0;
+    int nfail = 0, nrew = 0;
     for (int m = 0; m < nm; ++m) {
       const double r = acc[6 * m + 1] > 0 ? sqrt(acc[6 * m] / acc[6 * m + 1]) : sqrt(acc[6 * m]);
+      rew[m] = 0;
       if (c->quarantine > 0 && !quar[m] && !(r <= c->quarantine)) {
         quar[m] = 1;  // far off: the solver keeps this member from now on
         st.quarantined += 1;
+        rew[m] = saved && w > 0 && prev_pass[m];  // its state came from surrogate calls
+        nrew += rew[m];
       }
       fail[m] = quar[m] || !(r <= c->tol);
       nfail += fail[m];
       if (!(r <= worst)) worst = r;  // NaN propagates
     }
+    if (nrew > 0) {
+      // back to the previous window's start (istp - anchor), then the solver
+      // re-runs that window and this window's first k steps (an even count,
+      // so the member's state buffers keep their parity)
+      for (int m = 0; m < nm && rc == NEMO_OK; ++m) {
+        if (!rew[m]) continue;
+        double* dst[3] = {ms[m].sshn, ms[m].un, ms[m].vn};
+        for (int f = 0; f < 3 && rc == NEMO_OK; ++f)
+          rc = status_of(cudaMemcpyAsync(dst[f], saved_field((w - 1) & 1, m, f), field_elems * sizeof(double),
+                                         cudaMemcpyDeviceToDevice, s->stream));
+      }
+      if (rc == NEMO_OK) rc = join(s->stream, nemo::ens_stream(e));
+      if (rc == NEMO_OK) rc = nemo::ens_step_subset(e, istp - c->anchor + 1, c->anchor + c->k, rew.data());
+      if (rc != NEMO_OK) break;
+      solver_launches += c->anchor + c->k;
+      st.solver_steps += (long long)(c->anchor + c->k) * nrew;
+      st.rewound += nrew;
+    }
     if (!c->per_member && nfail > 0) {
       for (int m = 0; m < nm; ++m) fail[m] = 1;
       nfail = nm;
     }
-    for (int m = 0; m < nm; ++m) pass[m] = !fail[m];
+    for (int m = 0; m < nm; ++m) pass[m] = prev_pass[m] = !fail[m];
     st.last_shadow_err = worst;
     if (!(worst <= st.max_shadow_err)) st.max_shadow_err = worst;
     st.windows += nm;
@@ -1033,6 +1083,7 @@ int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, 
   cudaError_t ce = cudaStreamSynchronize(nemo::ens_stream(e));
   if (ce == cudaSuccess) ce = cudaStreamSynchronize(s->stream);
   if (own) cudaFree(own);
+  if (saved) cudaFree(saved);
   if (rc != NEMO_OK) return rc;
   ECK(ce);
   st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();

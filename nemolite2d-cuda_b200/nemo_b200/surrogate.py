@@ -25,7 +25,7 @@ class AdamW(ctypes.Structure):
 
 class HybConfig(ctypes.Structure):
     _fields_ = [("k", ctypes.c_int), ("anchor", ctypes.c_int), ("tol", ctypes.c_double),
-                ("per_member", ctypes.c_int), ("quarantine", ctypes.c_double)]
+                ("per_member", ctypes.c_int), ("quarantine", ctypes.c_double), ("rewind", ctypes.c_int)]
 
 
 class HybStats(ctypes.Structure):
@@ -34,7 +34,7 @@ class HybStats(ctypes.Structure):
                 ("windows", ctypes.c_longlong),
                 ("max_shadow_err", ctypes.c_double), ("last_shadow_err", ctypes.c_double),
                 ("seconds", ctypes.c_double), ("launches", ctypes.c_longlong),
-                ("quarantined", ctypes.c_longlong)]
+                ("quarantined", ctypes.c_longlong), ("rewound", ctypes.c_longlong)]
 
 
 def declare(L):
@@ -193,11 +193,14 @@ def ens_compare(a, ref):
     return out.reshape(-1, 3)
 
 
-def hyb_run(sur, ens, istp0, nsteps, k=10, anchor=100, tol=0.01, per_member=True, quarantine=0.05):
+def hyb_run(sur, ens, istp0, nsteps, k=10, anchor=100, tol=0.01, per_member=True, quarantine=0.05,
+            rewind=True):
     """Hybrid run (nemo_hyb_run); returns the statistics as a dict (counts of
     member-windows and member-steps).  quarantine: shadow error beyond which a
-    member stays on the FP64 solver (0: never)."""
-    c = HybConfig(k, anchor, tol, int(bool(per_member)), quarantine)
+    member stays on the FP64 solver (0: never); rewind: such a member whose
+    state came from the previous window's surrogate calls restarts from that
+    window's FP64 starting state."""
+    c = HybConfig(k, anchor, tol, int(bool(per_member)), quarantine, int(bool(rewind)))
     st = HybStats()
     check(sur.lib.nemo_hyb_run(sur.h, ens.h, ctypes.byref(c), istp0, nsteps, ctypes.byref(st)),
           "nemo_hyb_run")

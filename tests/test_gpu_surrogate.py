@@ -485,6 +485,46 @@ def test_quarantined_members_stay_on_the_solver(env):
     assert st["quarantined"] == 0 and st["fallbacks"] == 0    # untrained network stays finite)
 
 
+def test_rewound_member_follows_the_solver_exactly(env):
+    """A member accepted in one window and quarantined in the next restarts
+    from its FP64 state at the accepted window's start: the solver re-runs
+    that window, so its trajectory is the plain solver's bit for bit.
+    Without rewinding the surrogate's window stays in it.  The network adds
+    1e38 to the SSH at every call: the first shadow error is large but
+    finite (accepted under a limit of 1e100); from the state nine calls
+    leave, the solver's shadow steps overflow (CFL number ~1e18), so the
+    second window's error is not finite and the member is quarantined."""
+    torch, nb, sm = env
+    side, n = 128, 1
+    s = sm.Surrogate(nblocks=1, batch=n, height=side, width=side, train=False, seed=4)
+    p = np.zeros_like(s.params())
+    p[-64:] = 1.0  # the output layer's biases (the parameters end with the layers' biases)
+    s.set_params(p)
+    s.set_norm([1.0] * 4, [0.0] * 4, [1e38, 1e-30, 1e-30])
+
+    def developed():  # 300 solver steps from rest
+        e = small_ensemble(nb, 61, n, side)
+        e.step_n(1, 300)
+        return e
+
+    r0 = sm.hyb_run(s, developed(), 300, 100, tol=1e300, quarantine=0.0)["last_shadow_err"]
+    assert np.isfinite(r0) and r0 < 1e100, r0
+    plain = developed()
+    plain.step_n(301, 300)
+    a = developed()
+    st = sm.hyb_run(s, a, 300, 300, tol=1e300, quarantine=1e100)
+    assert st["quarantined"] == 1 and st["rewound"] == 1 and st["fallbacks"] == 2
+    # three shadow steps, the rewound window re-run with the next shadow step,
+    # two fallen-back windows
+    assert st["sur_steps"] == 90 and st["solver_steps"] == 3 * 10 + 110 + 2 * 90
+    for f in (nb.SSHN, nb.UN, nb.VN):
+        np.testing.assert_array_equal(a.field(0, f), plain.field(0, f))
+    b = developed()
+    st = sm.hyb_run(s, b, 300, 300, tol=1e300, quarantine=1e100, rewind=False)
+    assert st["quarantined"] == 1 and st["rewound"] == 0
+    assert not np.array_equal(b.field(0, nb.SSHN), plain.field(0, nb.SSHN))
+
+
 def test_training_beats_persistence_on_held_out_runs(env):
     """The trained surrogate's one-call SSH error on unseen members is well
     below the error of the method without it (no change over 10 steps)."""
