@@ -985,6 +985,9 @@ int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, 
   int rc = NEMO_OK;
   const int rest = c->anchor - c->k;
   for (int w = 0; w < nsteps / c->anchor && rc == NEMO_OK; ++w) {
+    // every member's state is final once the solver work queued so far is done
+    rc = join(nemo::ens_stream(e), s->stream);
+    if (rc != NEMO_OK) break;
     if (saved) {  // the window's starting states, while the members are still in them
       for (int m = 0; m < nm && rc == NEMO_OK; ++m) {
         if (quar[m]) continue;
@@ -1068,7 +1071,8 @@ int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, 
     st.solver_steps += (long long)rest * nfail;
     if (rc != NEMO_OK) break;
     if (nfail < nm) {
-      rc = join(nemo::ens_stream(e), s->stream);
+      // the accepted members' surrogate calls overlap the fallen-back
+      // members' solver steps (disjoint states; the next window starts after both)
       for (int j = c->k; j < c->anchor && rc == NEMO_OK; j += c->k) {
         rc = advance_members(s, e, ms, pass.data(), istp + j);
         st.sur_calls += 1;
