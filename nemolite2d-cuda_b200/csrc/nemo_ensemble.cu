@@ -63,7 +63,7 @@ k_ens_step(const MemberDev* __restrict__ mem, const int4* __restrict__ work, int
     if constexpr (PF >= 2) {
       constexpr int RD = stepdev::ring_doubles<PF == 3>();
       __shared__ double ring[NW * RD];
-      stepdev::run_strip_ring<PF == 3, 1>(L, C, A, it.y, it.z, it.w, lane, ring + (threadIdx.x >> 5) * RD);
+      stepdev::run_strip_ring<PF == 3, 2>(L, C, A, it.y, it.z, it.w, lane, ring + (threadIdx.x >> 5) * RD);
     } else {
       stepdev::run_strip<PF>(L, C, A, it.y, it.z, it.w, lane);
     }
