@@ -72,7 +72,7 @@ def parse():
                     help="fine-tuning iterations on rollout pairs (hybrid; 0: none)")
     ap.add_argument("--batch", type=int, default=64, help="images per conv call (conv workload)")
     ap.add_argument("--train-iters", type=int, default=6000)
-    ap.add_argument("--nblocks", type=int, default=4, help="residual blocks of the hybrid's network")
+    ap.add_argument("--nblocks", type=int, default=2, help="residual blocks of the hybrid's network")
     ap.add_argument("--n", type=int, default=N,
                     help="grid side (profiling of smaller cases only; the bench line is 4096)")
     return ap.parse_args()

@@ -326,8 +326,9 @@ typedef struct nemo_hyb_config {
   int rewind;        /* 1: a member quarantined right after a window the
                         surrogate advanced restarts from its FP64 state at
                         that window's start, the solver re-running the
-                        window (keeps one saved state per member and window
-                        parity: 2 x 3 fields per member) (1) */
+                        window; so does a member the last window's calls
+                        left non-finite (keeps one saved state per member
+                        and window parity: 2 x 3 fields per member) (1) */
 } nemo_hyb_config;
 
 typedef struct nemo_hyb_stats {

@@ -449,6 +449,20 @@ cudaError_t launch_apply(nemo_sur* s, int m0, int n, const float* out) {
   return cudaGetLastError();
 }
 
+// flag[m] = 1 when member m (of those with sel[m] != 0) holds a non-finite
+// sshn, un or vn value anywhere in its storage (grid x: chunks of the
+// storage, grid y: members).
+__global__ void k_nonfinite(const MemberState* __restrict__ ms, const char* __restrict__ sel, int* flag) {
+  const int m = blockIdx.y;
+  if (!sel[m]) return;
+  const MemberState M = ms[m];
+  const long n = (long)(M.jpj + 3) * M.pitch;
+  bool bad = false;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    bad |= !isfinite(M.sshn[i]) | !isfinite(M.un[i]) | !isfinite(M.vn[i]);
+  if (__syncthreads_or(bad) && threadIdx.x == 0) flag[m] = 1;
+}
+
 cudaError_t launch_err(nemo_sur* s, int nm, const float* snap, const float* out) {
   s->nlaunch += 1;
   const int H = s->cfg.height, W = s->cfg.width;
@@ -1083,6 +1097,50 @@ int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, 
       if (rc == NEMO_OK) rc = ensure_members(s, e, ms, nullptr);  // all members' table again
     }
     istp += rest;
+  }
+  // The last window's surrogate calls meet no later shadow check: a member
+  // they left non-finite goes back to that window's start and the solver
+  // runs the window.
+  if (rc == NEMO_OK && saved && nsteps > 0) {
+    const int wl = nsteps / c->anchor - 1;
+    int* d_flag = nullptr;
+    char* d_sel = nullptr;
+    std::vector<int> flag(nm, 0);
+    cudaError_t fe = cudaMalloc(&d_flag, nm * sizeof(int) + nm);
+    if (fe == cudaSuccess) {
+      d_sel = reinterpret_cast<char*>(d_flag + nm);
+      fe = join(nemo::ens_stream(e), s->stream) == NEMO_OK ? cudaSuccess : cudaErrorUnknown;
+    }
+    if (fe == cudaSuccess) fe = cudaMemsetAsync(d_flag, 0, nm * sizeof(int), s->stream);
+    if (fe == cudaSuccess)
+      fe = cudaMemcpyAsync(d_sel, pass.data(), nm, cudaMemcpyHostToDevice, s->stream);
+    if (fe == cudaSuccess) {
+      k_nonfinite<<<dim3(64, (unsigned)nm), 256, 0, s->stream>>>(s->d_ms, d_sel, d_flag);
+      s->nlaunch += 1;
+      fe = cudaGetLastError();
+    }
+    if (fe == cudaSuccess) fe = cudaMemcpyAsync(flag.data(), d_flag, nm * sizeof(int), cudaMemcpyDeviceToHost, s->stream);
+    if (fe == cudaSuccess) fe = cudaStreamSynchronize(s->stream);
+    if (d_flag) cudaFree(d_flag);
+    if (fe != cudaSuccess) rc = status_of(fe);
+    int nbad = 0;
+    for (int m = 0; m < nm && rc == NEMO_OK; ++m) {
+      rew[m] = pass[m] && flag[m];
+      if (!rew[m]) continue;
+      ++nbad;
+      double* dst[3] = {ms[m].sshn, ms[m].un, ms[m].vn};
+      for (int f = 0; f < 3 && rc == NEMO_OK; ++f)
+        rc = status_of(cudaMemcpyAsync(dst[f], saved_field(wl & 1, m, f), field_elems * sizeof(double),
+                                       cudaMemcpyDeviceToDevice, s->stream));
+    }
+    if (rc == NEMO_OK && nbad > 0) {
+      rc = join(s->stream, nemo::ens_stream(e));
+      if (rc == NEMO_OK) rc = nemo::ens_step_subset(e, istp - c->anchor + 1, c->anchor, rew.data());
+      solver_launches += c->anchor;
+      st.solver_steps += (long long)c->anchor * nbad;
+      st.sur_steps -= (long long)(c->anchor - c->k) * nbad;
+      st.rewound += nbad;
+    }
   }
   cudaError_t ce = cudaStreamSynchronize(nemo::ens_stream(e));
   if (ce == cudaSuccess) ce = cudaStreamSynchronize(s->stream);

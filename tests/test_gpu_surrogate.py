@@ -490,10 +490,11 @@ def test_rewound_member_follows_the_solver_exactly(env):
     from its FP64 state at the accepted window's start: the solver re-runs
     that window, so its trajectory is the plain solver's bit for bit.
     Without rewinding the surrogate's window stays in it.  The network adds
-    1e38 to the SSH at every call: the first shadow error is large but
-    finite (accepted under a limit of 1e100); from the state nine calls
-    leave, the solver's shadow steps overflow (CFL number ~1e18), so the
-    second window's error is not finite and the member is quarantined."""
+    1e30 to u and v at every call (a call adds its output divided by the
+    output scale): the first shadow error is large but finite (accepted
+    under a limit of 1e100); from the state nine calls leave, the solver's
+    shadow steps overflow, so the second window's error is not finite and
+    the member is quarantined."""
     torch, nb, sm = env
     side, n = 128, 1
     s = sm.Surrogate(nblocks=1, batch=n, height=side, width=side, train=False, seed=4)
@@ -523,6 +524,43 @@ def test_rewound_member_follows_the_solver_exactly(env):
     st = sm.hyb_run(s, b, 300, 300, tol=1e300, quarantine=1e100, rewind=False)
     assert st["quarantined"] == 1 and st["rewound"] == 0
     assert not np.array_equal(b.field(0, nb.SSHN), plain.field(0, nb.SSHN))
+
+
+def test_last_window_left_non_finite_is_rerun_by_the_solver(env):
+    """The last window's surrogate calls meet no later shadow check: a member
+    they leave non-finite goes back to that window's start and the solver
+    runs the window.  The network (no residual blocks) maps the SSH's 3x3
+    sums through a ReLU and a second 3x3 sum, and a call adds that over an
+    output scale of 1e-30: from a normal state (|ssh| < 1) the addition is
+    finite (an accepted, finite shadow prediction), from the state one call
+    leaves the FP32 division overflows to inf."""
+    torch, nb, sm = env
+    side, n = 128, 1
+    s = sm.Surrogate(nblocks=0, batch=n, height=side, width=side, train=False, seed=4)
+    p = np.zeros_like(s.params())
+    wl = 9 * 64 * 64  # weights per layer, [tap][out channel][in channel]
+    for layer in (0, 1):
+        for tap in range(9):
+            p[layer * wl + tap * 64 * 64] = 1.0  # in channel 0 (ssh) -> out channel 0
+    s.set_params(p)
+    s.set_norm([1.0] * 4, [0.0] * 4, [1e-30, 1.0, 1.0])
+
+    def developed():
+        e = small_ensemble(nb, 61, n, side)
+        e.step_n(1, 300)
+        return e
+
+    plain = developed()
+    plain.step_n(301, 100)
+    a = developed()
+    st = sm.hyb_run(s, a, 300, 100, tol=1e300, quarantine=1e100)
+    assert st["fallbacks"] == 0 and st["rewound"] == 1
+    assert st["sur_steps"] == 0 and st["solver_steps"] == 10 + 100
+    for f in (nb.SSHN, nb.UN, nb.VN):
+        np.testing.assert_array_equal(a.field(0, f), plain.field(0, f))
+    b = developed()
+    st = sm.hyb_run(s, b, 300, 100, tol=1e300, quarantine=1e100, rewind=False)
+    assert st["rewound"] == 0 and not np.all(np.isfinite(b.field(0, nb.SSHN)))
 
 
 def test_training_beats_persistence_on_held_out_runs(env):
