@@ -146,6 +146,30 @@ int nemo_host_free(void* ptr);
 int nemo_set_state(nemo_ctx* ctx, const double* sshn, const double* un,
                    const double* vn);
 
+/* A general grid in place of `grid`'s uniform one (original/nemolite2d.f90
+ * :145-281): every array covers (0:jpi+1, 0:jpj+1), column-major (ji
+ * fastest, leading dimension jpi+2), as the reference allocates its grid
+ * arrays.  pt: 1 water, 0 land, -1 open water outside the domain (any cell of
+ * the border ring may be open, so the Flather conditions on u and v can both
+ * act, :669-695); e1t..e2v: scale factors (m); gphiu, gphiv: latitudes of
+ * the u and v points (degrees); ht, hu, hv: depths, NULL keeps the
+ * context's.  The reference fills each metric only over its own point set
+ * and leaves the rest zero, which callers reproduce by passing zeros there.
+ * Cell areas are formed over the ranges :263-279 fills, the Coriolis
+ * parameter per point as the momentum loops form it, and sshn_u/sshn_v are
+ * re-initialised from the current sshn (:337-353).  A context with a general
+ * grid runs every step through the per-routine kernels (nemo_step_n
+ * included; nemo_autotune answers NEMO_ERR_STATE): the fused kernel holds the
+ * uniform grid's constants and analytic mask.  No counterpart in the
+ * reference's CUDA library, whose grid is fixed. */
+typedef struct nemo_grid {
+  const int* pt;
+  const double *e1t, *e2t, *e1u, *e2u, *e1v, *e2v;
+  const double *gphiu, *gphiv;
+  const double *ht, *hu, *hv;
+} nemo_grid;
+int nemo_set_grid(nemo_ctx* ctx, const nemo_grid* grid);
+
 int nemo_sync(nemo_ctx* ctx);
 int nemo_get_dims(nemo_ctx* ctx, int* jpi, int* jpj);
 /* Device address and pitch (in doubles) of a field's storage; element

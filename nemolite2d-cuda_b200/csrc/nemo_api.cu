@@ -6,6 +6,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <cmath>
 #include <fstream>
 #include <new>
 #include <sstream>
@@ -35,6 +36,11 @@ struct nemo_ctx {
   bool uv_stale;          // stored sshn_u/sshn_v lag behind sshn
   bool recip_nr_ok;       // in-kernel reciprocal depths equal the stored ones
   nemo_schedule sched;
+  // general grid (nemo_set_grid): mask and metrics on the device; the
+  // routine kernels read them and steps run the routine sequence
+  bool general = false;
+  void* gslab = nullptr;
+  GridDev grid{};
   // output records (nemo_record): staging buffer, side stream and events
   double* rec_dev = nullptr;
   cudaStream_t rec_stream = nullptr;
@@ -59,6 +65,8 @@ int set_device(nemo_ctx* c) {
   if (c->device >= 0) CK(cudaSetDevice(c->device));
   return NEMO_OK;
 }
+
+const GridDev* gridp(const nemo_ctx* c) { return c->general ? &c->grid : nullptr; }
 
 StateSet& nset(nemo_ctx* c) { return c->set[c->n_idx]; }
 StateSet& aset(nemo_ctx* c) { return c->set[1 - c->n_idx]; }
@@ -85,7 +93,7 @@ size_t field_bytes(const Layout& L) { return (size_t)L.elems() * sizeof(double);
 // materialise the a-fields if the last step was fused.
 int prepare_routine(nemo_ctx* c, bool writes_a) {
   if (c->uv_stale) {
-    CK(launch_derive_sshn_uv(c->L, c->C, nset(c).ssh, c->sshn_u, c->sshn_v, c->stream));
+    CK(launch_derive_sshn_uv(c->L, c->C, nset(c).ssh, c->sshn_u, c->sshn_v, c->stream, gridp(c)));
     c->uv_stale = false;
   }
   if (writes_a && c->a_mirrors_n) {
@@ -323,6 +331,7 @@ int nemo_destroy(nemo_ctx* c) {
   if (c->rec_staged) cudaEventDestroy(c->rec_staged);
   if (c->rec_copied) cudaEventDestroy(c->rec_copied);
   if (c->rec_stream) cudaStreamDestroy(c->rec_stream);
+  if (c->gslab) cudaFree(c->gslab);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return NEMO_OK;
@@ -426,7 +435,7 @@ int nemo_continuity(nemo_ctx* c) {
   if (!c) return NEMO_ERR_STATE;
   int st = set_device(c); if (st) return st;
   st = prepare_routine(c, true); if (st) return st;
-  CK(launch_continuity(c->L, c->C, rptrs(c), c->stream));
+  CK(launch_continuity(c->L, c->C, rptrs(c), c->stream, gridp(c)));
   return NEMO_OK;
 }
 
@@ -434,7 +443,7 @@ int nemo_momentum_u(nemo_ctx* c) {
   if (!c) return NEMO_ERR_STATE;
   int st = set_device(c); if (st) return st;
   st = prepare_routine(c, true); if (st) return st;
-  CK(launch_momentum_u(c->L, c->C, rptrs(c), c->stream));
+  CK(launch_momentum_u(c->L, c->C, rptrs(c), c->stream, gridp(c)));
   return NEMO_OK;
 }
 
@@ -442,7 +451,7 @@ int nemo_momentum_v(nemo_ctx* c) {
   if (!c) return NEMO_ERR_STATE;
   int st = set_device(c); if (st) return st;
   st = prepare_routine(c, true); if (st) return st;
-  CK(launch_momentum_v(c->L, c->C, rptrs(c), c->stream));
+  CK(launch_momentum_v(c->L, c->C, rptrs(c), c->stream, gridp(c)));
   return NEMO_OK;
 }
 
@@ -455,7 +464,7 @@ int nemo_bc_ssh(nemo_ctx* c, double rtime) {
   if (!c) return NEMO_ERR_STATE;
   int st = set_device(c); if (st) return st;
   st = prepare_routine(c, true); if (st) return st;
-  CK(launch_bc_ssh(c->L, tide_at_time(c->p, rtime), aset(c).ssh, c->stream));
+  CK(launch_bc_ssh(c->L, tide_at_time(c->p, rtime), aset(c).ssh, c->stream, gridp(c)));
   return NEMO_OK;
 }
 
@@ -463,7 +472,7 @@ int nemo_bc_solid_u(nemo_ctx* c) {
   if (!c) return NEMO_ERR_STATE;
   int st = set_device(c); if (st) return st;
   st = prepare_routine(c, true); if (st) return st;
-  CK(launch_bc_solid_u(c->L, aset(c).u, c->stream));
+  CK(launch_bc_solid_u(c->L, aset(c).u, c->stream, gridp(c)));
   return NEMO_OK;
 }
 
@@ -471,7 +480,7 @@ int nemo_bc_solid_v(nemo_ctx* c) {
   if (!c) return NEMO_ERR_STATE;
   int st = set_device(c); if (st) return st;
   st = prepare_routine(c, true); if (st) return st;
-  CK(launch_bc_solid_v(c->L, aset(c).v, c->stream));
+  CK(launch_bc_solid_v(c->L, aset(c).v, c->stream, gridp(c)));
   return NEMO_OK;
 }
 
@@ -479,7 +488,7 @@ int nemo_bc_flather_u(nemo_ctx* c) {
   if (!c) return NEMO_ERR_STATE;
   int st = set_device(c); if (st) return st;
   st = prepare_routine(c, true); if (st) return st;
-  CK(launch_bc_flather_u(c->L, rptrs(c), c->stream));
+  CK(launch_bc_flather_u(c->L, rptrs(c), c->stream, gridp(c)));
   return NEMO_OK;
 }
 
@@ -487,7 +496,7 @@ int nemo_bc_flather_v(nemo_ctx* c) {
   if (!c) return NEMO_ERR_STATE;
   int st = set_device(c); if (st) return st;
   st = prepare_routine(c, true); if (st) return st;
-  CK(launch_bc_flather_v(c->L, rptrs(c), c->stream));
+  CK(launch_bc_flather_v(c->L, rptrs(c), c->stream, gridp(c)));
   return NEMO_OK;
 }
 
@@ -505,7 +514,7 @@ int nemo_next(nemo_ctx* c) {
   int st = set_device(c); if (st) return st;
   st = prepare_routine(c, true); if (st) return st;
   CK(launch_copy_next(c->L, rptrs(c), c->stream));
-  CK(launch_derive_sshn_uv(c->L, c->C, nset(c).ssh, c->sshn_u, c->sshn_v, c->stream));
+  CK(launch_derive_sshn_uv(c->L, c->C, nset(c).ssh, c->sshn_u, c->sshn_v, c->stream, gridp(c)));
   return NEMO_OK;
 }
 
@@ -524,6 +533,11 @@ int nemo_step_n(nemo_ctx* c, int istp0, int n) {
   if (n < 0) return NEMO_ERR_INVALID;
   if (n == 0) return NEMO_OK;
   int st = set_device(c); if (st) return st;
+  if (c->general) {  // the fused kernel holds the reference's grid: the routine sequence
+    for (int k = 0; k < n; ++k)
+      if ((st = nemo_step(c, istp0 + k))) return st;
+    return NEMO_OK;
+  }
   for (int k = 0; k < n; ++k) {
     FusedArgs a;
     a.sshn = nset(c).ssh;
@@ -663,7 +677,91 @@ int nemo_set_state(nemo_ctx* c, const double* sshn, const double* un, const doub
                        (size_t)(L.jpi + 1) * sizeof(double), (size_t)L.jpj, cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpy2DAsync(nset(c).v + L.idx(1, 0), P, vn, (size_t)L.jpi * sizeof(double),
                        (size_t)L.jpi * sizeof(double), (size_t)(L.jpj + 1), cudaMemcpyHostToDevice, c->stream));
-  CK(launch_derive_sshn_uv(L, c->C, nset(c).ssh, c->sshn_u, c->sshn_v, c->stream));
+  CK(launch_derive_sshn_uv(L, c->C, nset(c).ssh, c->sshn_u, c->sshn_v, c->stream, gridp(c)));
+  CK(cudaStreamSynchronize(c->stream));
+  c->uv_stale = false;
+  return NEMO_OK;
+}
+
+int nemo_set_grid(nemo_ctx* c, const nemo_grid* g) {
+  if (!c || !g || !g->pt || !g->e1t || !g->e2t || !g->e1u || !g->e2u || !g->e1v || !g->e2v || !g->gphiu ||
+      !g->gphiv)
+    return NEMO_ERR_INVALID;
+  const int jpi = c->L.jpi, jpj = c->L.jpj;
+  const long ld = jpi + 2;
+  const long nh = ld * (jpj + 2);
+  for (long k = 0; k < nh; ++k)
+    if (g->pt[k] < -1 || g->pt[k] > 1) return NEMO_ERR_INVALID;
+  const double* in[] = {g->e1t, g->e2t, g->e1u, g->e2u, g->e1v, g->e2v, g->gphiu, g->gphiv, g->ht, g->hu, g->hv};
+  for (const double* a : in)
+    if (a)
+      for (long k = 0; k < nh; ++k)
+        if (!std::isfinite(a[k])) return NEMO_ERR_INVALID;
+  int st = set_device(c); if (st) return st;
+  CK(cudaStreamSynchronize(c->stream));  // queued steps may still read the depths
+  const size_t fe = (size_t)c->L.elems();
+  // host images in the fields' layout: (ji, jj) of the reference's
+  // (0:jpi+1, 0:jpj+1) arrays at L.idx(ji, jj); everything else zero
+  auto put = [&](const double* src, std::vector<double>& dst) {
+    for (int jj = 0; jj <= jpj + 1; ++jj)
+      for (int ji = 0; ji <= jpi + 1; ++ji) dst[c->L.idx(ji, jj)] = src[jj * ld + ji];
+  };
+  enum { E1T, E2T, E1U, E2U, E1V, E2V, E12T, E12U, E12V, FCU, FCV, NA };
+  std::vector<std::vector<double>> h(NA, std::vector<double>(fe, 0.0));
+  for (int k = 0; k < 6; ++k) put(in[k], h[k]);
+  // cell areas over the ranges original/nemolite2d.f90:263-279 fills
+  for (int jj = 1; jj <= jpj; ++jj)
+    for (int ji = 1; ji <= jpi; ++ji) {
+      const long q = c->L.idx(ji, jj);
+      h[E12T][q] = h[E1T][q] * h[E2T][q];
+    }
+  for (int jj = 1; jj <= jpj; ++jj)
+    for (int ji = 0; ji <= jpi; ++ji) {
+      const long q = c->L.idx(ji, jj);
+      h[E12U][q] = h[E1U][q] * h[E2U][q];
+    }
+  for (int jj = 0; jj <= jpj; ++jj)
+    for (int ji = 1; ji <= jpi; ++ji) {
+      const long q = c->L.idx(ji, jj);
+      h[E12V][q] = h[E1V][q] * h[E2V][q];
+    }
+  // Coriolis parameters, as the momentum loops form them (:503, :594)
+  const double d2r = kPi / 180.0;
+  for (int jj = 0; jj <= jpj + 1; ++jj)
+    for (int ji = 0; ji <= jpi + 1; ++ji) {
+      const long q = c->L.idx(ji, jj);
+      h[FCU][q] = 2.0 * kOmega * sin(g->gphiu[jj * ld + ji] * d2r);
+      h[FCV][q] = 2.0 * kOmega * sin(g->gphiv[jj * ld + ji] * d2r);
+    }
+  std::vector<signed char> hp(fe, 0);
+  for (int jj = 0; jj <= jpj + 1; ++jj)
+    for (int ji = 0; ji <= jpi + 1; ++ji) hp[c->L.idx(ji, jj)] = (signed char)g->pt[jj * ld + ji];
+  if (!c->gslab) {
+    cudaError_t e = cudaMalloc(&c->gslab, NA * fe * sizeof(double) + fe);
+    if (e != cudaSuccess) { c->gslab = nullptr; cudaGetLastError(); return NEMO_ERR_ALLOC; }
+  }
+  double* base = static_cast<double*>(c->gslab);
+  for (int k = 0; k < NA; ++k)
+    CK(cudaMemcpy(base + k * fe, h[k].data(), fe * sizeof(double), cudaMemcpyHostToDevice));
+  signed char* pt = reinterpret_cast<signed char*>(base + NA * fe);
+  CK(cudaMemcpy(pt, hp.data(), fe, cudaMemcpyHostToDevice));
+  c->grid = GridDev{pt, base + E1T * fe, base + E2T * fe, base + E1U * fe, base + E2U * fe, base + E1V * fe,
+                    base + E2V * fe, base + E12T * fe, base + E12U * fe, base + E12V * fe, base + FCU * fe,
+                    base + FCV * fe};
+  // depths, when given
+  double* hd[3] = {c->ht, c->hu, c->hv};
+  std::vector<double> tmp(fe);
+  for (int k = 0; k < 3; ++k) {
+    if (!in[8 + k]) continue;
+    CK(cudaMemcpy(tmp.data(), hd[k], fe * sizeof(double), cudaMemcpyDeviceToHost));
+    put(in[8 + k], tmp);
+    CK(cudaMemcpy(hd[k], tmp.data(), fe * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  c->general = true;
+  // the a-fields stay as they are; sshn_u/sshn_v restart from the current
+  // sshn with the initialisation's averages (:337-353)
+  if ((st = prepare_routine(c, true))) return st;
+  CK(launch_init_sshn_uv(c->L, c->C, nset(c).ssh, c->sshn_u, c->sshn_v, c->stream, gridp(c)));
   CK(cudaStreamSynchronize(c->stream));
   c->uv_stale = false;
   return NEMO_OK;
@@ -712,6 +810,7 @@ int nemo_get_schedule(nemo_ctx* c, nemo_schedule* s) {
 
 int nemo_autotune(nemo_ctx* c, int steps, nemo_schedule* best, double* best_ms) {
   if (!c || steps < 1) return NEMO_ERR_INVALID;
+  if (c->general) return NEMO_ERR_STATE;  // no fused schedules on a general grid
   int st = set_device(c); if (st) return st;
   // both state sets and the bookkeeping are restored afterwards
   const size_t fe = (size_t)c->L.elems();

@@ -19,6 +19,15 @@ struct RoutinePtrs {
   double *sshn, *un, *vn, *ssha, *ua, *va, *sshn_u, *sshn_v, *ht, *hu, *hv;
 };
 
+// A general grid (nemo_set_grid): the mask pt (1 water, 0 land, -1 open) and
+// the metrics as arrays in the fields' layout; fcu, fcv = 2*omega*sin(gphi*d2r)
+// at u and v points.  The per-routine launchers take a GridDev pointer, null
+// for the reference's uniform grid (constants and the analytic mask).
+struct GridDev {
+  const signed char* pt;
+  const double *e1t, *e2t, *e1u, *e2u, *e1v, *e2v, *e12t, *e12u, *e12v, *fcu, *fcv;
+};
+
 // ---- launchers (asynchronous on `s`) -------------------------------------
 cudaError_t launch_depth(const Layout& L, double dep_const, int nbump, const double* ax,
                          const double* gy, double hmin, double hmax, double* ht,
@@ -29,24 +38,29 @@ cudaError_t launch_recip(const Layout& L, const double* hu, const double* hv, do
                          int* mismatch,
                          cudaStream_t s);
 cudaError_t launch_init_sshn_uv(const Layout& L, const Consts& C, const double* sshn,
-                                double* sshn_u, double* sshn_v, cudaStream_t s);
+                                double* sshn_u, double* sshn_v, cudaStream_t s,
+                                const GridDev* g = nullptr);
 cudaError_t launch_continuity(const Layout& L, const Consts& C, const RoutinePtrs& p,
-                              cudaStream_t s);
+                              cudaStream_t s, const GridDev* g = nullptr);
 cudaError_t launch_momentum_u(const Layout& L, const Consts& C, const RoutinePtrs& p,
-                              cudaStream_t s);
+                              cudaStream_t s, const GridDev* g = nullptr);
 cudaError_t launch_momentum_v(const Layout& L, const Consts& C, const RoutinePtrs& p,
-                              cudaStream_t s);
-cudaError_t launch_bc_ssh(const Layout& L, double value, double* ssha, cudaStream_t s);
-cudaError_t launch_bc_solid_u(const Layout& L, double* ua, cudaStream_t s);
-cudaError_t launch_bc_solid_v(const Layout& L, double* va, cudaStream_t s);
-cudaError_t launch_bc_flather_u(const Layout& L, const RoutinePtrs& p, cudaStream_t s);
-cudaError_t launch_bc_flather_v(const Layout& L, const RoutinePtrs& p, cudaStream_t s);
+                              cudaStream_t s, const GridDev* g = nullptr);
+cudaError_t launch_bc_ssh(const Layout& L, double value, double* ssha, cudaStream_t s,
+                          const GridDev* g = nullptr);
+cudaError_t launch_bc_solid_u(const Layout& L, double* ua, cudaStream_t s, const GridDev* g = nullptr);
+cudaError_t launch_bc_solid_v(const Layout& L, double* va, cudaStream_t s, const GridDev* g = nullptr);
+cudaError_t launch_bc_flather_u(const Layout& L, const RoutinePtrs& p, cudaStream_t s,
+                                const GridDev* g = nullptr);
+cudaError_t launch_bc_flather_v(const Layout& L, const RoutinePtrs& p, cudaStream_t s,
+                                const GridDev* g = nullptr);
 cudaError_t launch_copy_next(const Layout& L, const RoutinePtrs& p, cudaStream_t s);
 // sshn and the cell-centred velocities as three dense [jpj][jpi] planes.
 cudaError_t launch_record(const Layout& L, const double* sshn, const double* un, const double* vn, double* out,
                           cudaStream_t s);
 cudaError_t launch_derive_sshn_uv(const Layout& L, const Consts& C, const double* sshn,
-                                  double* sshn_u, double* sshn_v, cudaStream_t s);
+                                  double* sshn_u, double* sshn_v, cudaStream_t s,
+                                  const GridDev* g = nullptr);
 
 struct FusedArgs {
   const double *sshn, *un, *vn, *ht, *hu, *hv;

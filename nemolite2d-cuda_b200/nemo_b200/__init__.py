@@ -34,7 +34,7 @@ EXPORTED = [
     "nemo_momentum_u", "nemo_momentum_v", "nemo_bc", "nemo_bc_ssh", "nemo_bc_solid_u",
     "nemo_bc_solid_v", "nemo_bc_flather_u", "nemo_bc_flather_v", "nemo_next", "nemo_step",
     "nemo_step_n", "nemo_checksums", "nemo_checksum", "nemo_retrieve", "nemo_record",
-    "nemo_record_wait", "nemo_host_alloc", "nemo_host_free", "nemo_set_state",
+    "nemo_record_wait", "nemo_host_alloc", "nemo_host_free", "nemo_set_state", "nemo_set_grid",
     "nemo_sync", "nemo_get_dims", "nemo_device_field", "nemo_set_schedule", "nemo_get_schedule",
     "nemo_status_string", "nemo_build_is_strict", "nemo_checksums_noalloc", "nemo_autotune",
     "nemo_ens_generate", "nemo_ens_create", "nemo_ens_destroy", "nemo_ens_step_n",
@@ -123,6 +123,7 @@ def load(strict=False):
     L.nemo_record.argtypes = [vp, P(dp)]
     L.nemo_record_wait.argtypes = [vp]
     L.nemo_set_state.argtypes = [vp, P(dp), P(dp), P(dp)]
+    L.nemo_set_grid.argtypes = [vp, P(Grid)]
     L.nemo_get_dims.argtypes = [vp, P(ip), P(ip)]
     L.nemo_device_field.argtypes = [vp, ip, P(P(dp)), P(ctypes.c_long)]
     L.nemo_set_schedule.argtypes = [vp, P(Schedule)]
@@ -192,6 +193,13 @@ def field_shape(field, jpi, jpj):
     if field in V_FIELDS:
         return (jpj + 1, jpi)
     raise ValueError("unknown field %r" % field)
+
+
+class Grid(ctypes.Structure):
+    """nemo_grid: host arrays over (0:jpi+1, 0:jpj+1), column-major."""
+    _fields_ = [("pt", ctypes.POINTER(ctypes.c_int))] + [
+        (n, ctypes.POINTER(ctypes.c_double))
+        for n in ("e1t", "e2t", "e1u", "e2u", "e1v", "e2v", "gphiu", "gphiv", "ht", "hu", "hv")]
 
 
 class Model:
@@ -324,6 +332,20 @@ class Model:
         for f, x in zip((SSHN, UN, VN), a):
             assert x.shape == field_shape(f, self.jpi, self.jpj), (f, x.shape)
         check(self.lib.nemo_set_state(self.h, *[_dptr(x) for x in a]), "nemo_set_state")
+
+    def set_grid(self, pt, e1t, e2t, e1u, e2u, e1v, e2v, gphiu, gphiv, ht=None, hu=None, hv=None):
+        """General grid (nemo_set_grid): arrays of shape (jpj+2, jpi+2) over
+        (0:jpi+1, 0:jpj+1); depths None keep the current ones.  Steps then
+        run the per-routine kernels."""
+        shape = (self.jpj + 2, self.jpi + 2)
+        p = np.ascontiguousarray(pt, dtype=np.int32)
+        assert p.shape == shape
+        a = [None if x is None else np.ascontiguousarray(x, dtype=np.float64)
+             for x in (e1t, e2t, e1u, e2u, e1v, e2v, gphiu, gphiv, ht, hu, hv)]
+        assert all(x is None or x.shape == shape for x in a)
+        g = Grid(p.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                 *[ctypes.POINTER(ctypes.c_double)() if x is None else _dptr(x) for x in a])
+        check(self.lib.nemo_set_grid(self.h, ctypes.byref(g)), "nemo_set_grid")
 
     def autotune(self, steps=5):
         sch = Schedule()

@@ -132,6 +132,40 @@ static void bathymetry(oracle_model* m) {
 
 static double* zalloc(long n) { return (double*)calloc((size_t)n, sizeof(double)); }
 
+/* initialisation of sshn_u/sshn_v, :337-353 (min/max-clamped averages) */
+static void init_sshn_uv(oracle_model* m) {
+  const int jpi = m->jpi, jpj = m->jpj;
+  for (int ji = 0; ji <= jpi; ++ji)
+    for (int jj = 1; jj <= jpj; ++jj) {
+      int i1 = ji + 1 < jpi ? ji + 1 : jpi;
+      int i2 = ji > 1 ? ji : 1;
+      double r = m->e12t[I(i1, jj)] * m->sshn[I(i1, jj)] + m->e12t[I(i2, jj)] * m->sshn[I(i2, jj)];
+      m->sshn_u[I(ji, jj)] = 0.5 * r / m->e12u[I(ji, jj)];
+    }
+  for (int ji = 1; ji <= jpi; ++ji)
+    for (int jj = 0; jj <= jpj; ++jj) {
+      int j1 = jj + 1 < jpj ? jj + 1 : jpj;
+      int j2 = jj > 1 ? jj : 1;
+      double r = m->e12t[I(ji, j1)] * m->sshn[I(ji, j1)] + m->e12t[I(ji, j2)] * m->sshn[I(ji, j2)];
+      m->sshn_v[I(ji, jj)] = 0.5 * r / m->e12v[I(ji, jj)];
+    }
+}
+
+/* cell areas over the ranges :263-279 fill; zero elsewhere */
+static void cell_areas(oracle_model* m) {
+  const int jpi = m->jpi, jpj = m->jpj;
+  const size_t n = (size_t)(jpi + 2) * (jpj + 2);
+  memset(m->e12t, 0, n * sizeof(double));
+  memset(m->e12u, 0, n * sizeof(double));
+  memset(m->e12v, 0, n * sizeof(double));
+  for (int jj = 1; jj <= jpj; ++jj)
+    for (int ji = 1; ji <= jpi; ++ji) m->e12t[I(ji, jj)] = m->e1t[I(ji, jj)] * m->e2t[I(ji, jj)];
+  for (int jj = 1; jj <= jpj; ++jj)
+    for (int ji = 0; ji <= jpi; ++ji) m->e12u[I(ji, jj)] = m->e1u[I(ji, jj)] * m->e2u[I(ji, jj)];
+  for (int jj = 0; jj <= jpj; ++jj)
+    for (int ji = 1; ji <= jpi; ++ji) m->e12v[I(ji, jj)] = m->e1v[I(ji, jj)] * m->e2v[I(ji, jj)];
+}
+
 oracle_model* oracle_create(const oracle_params* p) {
   if (p->jpi < 2 || p->jpj < 2) return NULL;
   oracle_model* m = (oracle_model*)calloc(1, sizeof(oracle_model));
@@ -190,30 +224,12 @@ oracle_model* oracle_create(const oracle_params* p) {
     bathymetry(m);
   }
   /* :263-279 cell areas */
-  for (int jj = 1; jj <= jpj; ++jj)
-    for (int ji = 1; ji <= jpi; ++ji) m->e12t[I(ji, jj)] = m->e1t[I(ji, jj)] * m->e2t[I(ji, jj)];
-  for (int jj = 1; jj <= jpj; ++jj)
-    for (int ji = 0; ji <= jpi; ++ji) m->e12u[I(ji, jj)] = m->e1u[I(ji, jj)] * m->e2u[I(ji, jj)];
-  for (int jj = 0; jj <= jpj; ++jj)
-    for (int ji = 1; ji <= jpi; ++ji) m->e12v[I(ji, jj)] = m->e1v[I(ji, jj)] * m->e2v[I(ji, jj)];
+  cell_areas(m);
 
   /* initialisation, :331-365 */
   for (int ji = 1; ji <= jpi; ++ji)
     for (int jj = 1; jj <= jpj; ++jj) m->sshn[I(ji, jj)] = 0.0;
-  for (int ji = 0; ji <= jpi; ++ji)
-    for (int jj = 1; jj <= jpj; ++jj) {
-      int i1 = ji + 1 < jpi ? ji + 1 : jpi;
-      int i2 = ji > 1 ? ji : 1;
-      double r = m->e12t[I(i1, jj)] * m->sshn[I(i1, jj)] + m->e12t[I(i2, jj)] * m->sshn[I(i2, jj)];
-      m->sshn_u[I(ji, jj)] = 0.5 * r / m->e12u[I(ji, jj)];
-    }
-  for (int ji = 1; ji <= jpi; ++ji)
-    for (int jj = 0; jj <= jpj; ++jj) {
-      int j1 = jj + 1 < jpj ? jj + 1 : jpj;
-      int j2 = jj > 1 ? jj : 1;
-      double r = m->e12t[I(ji, j1)] * m->sshn[I(ji, j1)] + m->e12t[I(ji, j2)] * m->sshn[I(ji, j2)];
-      m->sshn_v[I(ji, jj)] = 0.5 * r / m->e12v[I(ji, jj)];
-    }
+  init_sshn_uv(m);
   for (int jj = 1; jj <= jpj; ++jj)
     for (int ji = 0; ji <= jpi; ++ji) m->un[I(ji, jj)] = 0.0;
   for (int jj = 0; jj <= jpj; ++jj)
@@ -590,6 +606,23 @@ int oracle_set_state(oracle_model* m, const double* sshn, const double* un,
   for (int jj = 0; jj <= jpj; ++jj)
     for (int ji = 1; ji <= jpi; ++ji) m->vn[I(ji, jj)] = vn[k++];
   derive_sshn_uv(m);
+  return 0;
+}
+
+int oracle_set_grid(oracle_model* m, const int* pt, const double* e1t, const double* e2t,
+                    const double* e1u, const double* e2u, const double* e1v, const double* e2v,
+                    const double* gphiu, const double* gphiv, const double* ht, const double* hu,
+                    const double* hv) {
+  const size_t n = (size_t)(m->jpi + 2) * (m->jpj + 2);
+  for (size_t k = 0; k < n; ++k)
+    if (pt[k] < -1 || pt[k] > 1) return -1;
+  memcpy(m->pt, pt, n * sizeof(int));
+  const double* src[] = {e1t, e2t, e1u, e2u, e1v, e2v, gphiu, gphiv, ht, hu, hv};
+  double* dst[] = {m->e1t, m->e2t, m->e1u, m->e2u, m->e1v, m->e2v, m->gphiu, m->gphiv, m->ht, m->hu, m->hv};
+  for (int k = 0; k < 11; ++k)
+    if (src[k]) memcpy(dst[k], src[k], n * sizeof(double));
+  cell_areas(m);
+  init_sshn_uv(m);
   return 0;
 }
 

@@ -85,6 +85,19 @@ long oracle_get_field(const oracle_model* m, int field, double* out);
 int oracle_set_state(oracle_model* m, const double* sshn, const double* un,
                      const double* vn);
 
+/* Replace the grid of original/nemolite2d.f90's `grid` routine (:145-281)
+ * by general arrays, each over (0:jpi+1, 0:jpj+1), column-major, ld jpi+2:
+ * the mask pt (1 water, 0 land, -1 open water outside the domain), the scale
+ * factors e1t..e2v, the latitudes gphiu/gphiv (degrees) and, when not NULL,
+ * the depths ht/hu/hv.  The cell areas are re-formed over the ranges :263-279
+ * fill (zero elsewhere, as allocated), and sshn_u/sshn_v are re-initialised
+ * from the current sshn (:337-353).  Returns -1 for a pt value outside
+ * {-1, 0, 1}. */
+int oracle_set_grid(oracle_model* m, const int* pt, const double* e1t, const double* e2t,
+                    const double* e1u, const double* e2u, const double* e1v, const double* e2v,
+                    const double* gphiu, const double* gphiv, const double* ht, const double* hu,
+                    const double* hv);
+
 /* SUM(ABS(f(1:jpi,1:jpj))) in the reference's column-major order
  * (field_mod.f90:951). */
 double oracle_checksum_seq(const oracle_model* m, int field);

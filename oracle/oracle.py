@@ -65,6 +65,7 @@ def lib():
         L.oracle_get_field.argtypes = [vp, ctypes.c_int, dp]
         L.oracle_get_field.restype = ctypes.c_long
         L.oracle_set_state.argtypes = [vp, dp, dp, dp]
+        L.oracle_set_grid.argtypes = [vp, ctypes.POINTER(ctypes.c_int)] + [dp] * 11
         L.oracle_checksum_seq.argtypes = [vp, ctypes.c_int]
         L.oracle_checksum_seq.restype = ctypes.c_double
         L.oracle_checksum_tree.argtypes = [vp, ctypes.c_int]
@@ -159,6 +160,20 @@ class Model:
     def set_state(self, sshn, un, vn):
         a = [np.ascontiguousarray(x, dtype=np.float64) for x in (sshn, un, vn)]
         lib().oracle_set_state(self.h, *[_dptr(x) for x in a])
+
+    def set_grid(self, pt, e1t, e2t, e1u, e2u, e1v, e2v, gphiu, gphiv, ht=None, hu=None, hv=None):
+        """General grid (oracle_set_grid): arrays of shape (jpj+2, jpi+2) over
+        (0:jpi+1, 0:jpj+1); depths None keep the current ones."""
+        shape = (self.jpj + 2, self.jpi + 2)
+        p = np.ascontiguousarray(pt, dtype=np.int32)
+        assert p.shape == shape
+        a = [None if x is None else np.ascontiguousarray(x, dtype=np.float64)
+             for x in (e1t, e2t, e1u, e2u, e1v, e2v, gphiu, gphiv, ht, hu, hv)]
+        assert all(x is None or x.shape == shape for x in a)
+        ptrs = [ctypes.POINTER(ctypes.c_double)() if x is None else _dptr(x) for x in a]
+        rc = lib().oracle_set_grid(self.h, p.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), *ptrs)
+        if rc != 0:
+            raise ValueError("oracle_set_grid: mask values must be -1, 0 or 1")
 
     def checksum(self, f, order="seq"):
         if order == "seq":

@@ -359,3 +359,80 @@ def test_invalid_arguments_fail_loudly(nb):
         m.step_n(1, -1)
     with pytest.raises(nb.NemoError):
         m.checksum(nb.XT)
+
+
+def _general_models(nb, oracle_mod, strict, seed=3, jpi=150, jpj=97):
+    from gridcases import NAMES, random_grid
+    kw = dict(jpi=jpi, jpj=jpj, rdt=10.0, cbfr=0.00015, visc=0.1, amp_tide=0.3)
+    pt, g = random_grid(seed, jpi, jpj)
+    m = nb.Model(strict=strict, **kw)
+    o = oracle_mod.Model(**kw)
+    m.set_grid(pt, *[g[n] for n in NAMES])
+    o.set_grid(pt, *[g[n] for n in NAMES])
+    return m, o
+
+
+def test_strict_general_grid_matches_oracle_routine_by_routine(nb, oracle_mod):
+    """A general grid (open water on all four borders, islands, per-point
+    scale factors, latitudes and depths): every routine of the strict build
+    equals the oracle bit for bit, including the Flather condition on u."""
+    m, o = _general_models(nb, oracle_mod, True)
+    for name, fid in ALL:
+        np.testing.assert_array_equal(bits(m.field(fid)), bits(o.field(fid)), err_msg="set_grid: " + name)
+    for istp in range(1, 4):
+        rtime = istp * 10.0
+        for label, fn in [("continuity", lambda: (m.continuity(), o.continuity())),
+                          ("momentum_u", lambda: (m.momentum_u(), o.momentum_u())),
+                          ("momentum_v", lambda: (m.momentum_v(), o.momentum_v())),
+                          ("bc_ssh", lambda: (m.bc_ssh(rtime), o.bc_ssh(rtime))),
+                          ("bc_solid_u", lambda: (m.bc_solid_u(), o.bc_solid_u())),
+                          ("bc_solid_v", lambda: (m.bc_solid_v(), o.bc_solid_v())),
+                          ("bc_flather_u", lambda: (m.bc_flather_u(), o.bc_flather_u())),
+                          ("bc_flather_v", lambda: (m.bc_flather_v(), o.bc_flather_v())),
+                          ("next", lambda: (m.next(), o.next()))]:
+            fn()
+            for name, fid in ALL:
+                np.testing.assert_array_equal(bits(m.field(fid)), bits(o.field(fid)),
+                                              err_msg="step %d after %s: %s" % (istp, label, name))
+
+
+def test_strict_general_grid_step_n_matches_oracle(nb, oracle_mod):
+    """nemo_step_n on a general grid runs the routine sequence: bitwise with
+    the oracle after 150 steps; the fused schedules' autotuner is refused."""
+    m, o = _general_models(nb, oracle_mod, True, seed=11, jpi=131, jpj=140)
+    m.step_n(1, 150)
+    o.run(1, 150)
+    for name, fid in ALL:
+        np.testing.assert_array_equal(bits(m.field(fid)), bits(o.field(fid)), err_msg=name)
+    ck = m.checksums()
+    assert ck[1] == o.checksum(oracle_mod.UN, "tree")
+    with pytest.raises(nb.NemoError):
+        m.autotune(2)
+
+
+def test_default_grid_through_set_grid_is_the_built_in_grid(nb):
+    """The reference's grid passed as arrays gives, in the strict build, the
+    same bits as the built-in grid (routine path and fused path)."""
+    from gridcases import NAMES, default_grid
+    kw = dict(jpi=77, jpj=64, rdt=20.0, cbfr=0.00015, visc=0.1, amp_tide=0.4)
+    pt, g = default_grid(77, 64)
+    a = nb.Model(strict=True, **kw)
+    b = nb.Model(strict=True, **kw)
+    c = nb.Model(strict=True, **kw)
+    b.set_grid(pt, *[g[n] for n in NAMES])
+    for istp in range(1, 41):
+        a.step(istp)
+    b.step_n(1, 40)
+    c.step_n(1, 40)
+    for name, fid in STATE:
+        np.testing.assert_array_equal(bits(a.field(fid)), bits(b.field(fid)), err_msg=name)
+        np.testing.assert_array_equal(bits(c.field(fid)), bits(b.field(fid)), err_msg=name)
+
+
+def test_default_build_general_grid_within_tolerance(nb, oracle_mod):
+    m, o = _general_models(nb, oracle_mod, False, seed=5)
+    for rec in range(4):
+        m.step_n(1 + 100 * rec, 100)
+        o.run(1 + 100 * rec, 100)
+        for name, fid in STATE:
+            assert relerr(m.field(fid), o.field(fid)) <= TOL, (rec, name)
