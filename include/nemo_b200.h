@@ -350,8 +350,10 @@ typedef struct nemo_hyb_config {
   int rewind;        /* 1: a member quarantined right after a window the
                         surrogate advanced restarts from its FP64 state at
                         that window's start, the solver re-running the
-                        window; so does a member the last window's calls
-                        left non-finite (keeps one saved state per member
+                        window; after the last window a member left
+                        non-finite or with |ssh| above 10 times its tidal
+                        amplitude goes back one window (two when the solver
+                        ran its last one) (keeps one saved state per member
                         and window parity: 2 x 3 fields per member) (1) */
 } nemo_hyb_config;
 

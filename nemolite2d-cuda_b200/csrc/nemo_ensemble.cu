@@ -764,6 +764,8 @@ int ens_step_subset(nemo_ens* e, int istp0, int n, const char* sel) {
 cudaStream_t ens_stream(nemo_ens* e) { return e->stream; }
 int ens_device(nemo_ens* e) { return e->device; }
 
+double ens_amp(nemo_ens* e, int m) { return fabs(e->mem[m].amp_tide); }
+
 double ens_tide(nemo_ens* e, int m, int istp) {
   const double omega_tide = 2.0 * 3.14159 / (12.42 * 3600.0);
   const double rtime = (double)istp * e->common.rdt;

@@ -67,4 +67,6 @@ cudaStream_t ens_stream(nemo_ens* e);
 int ens_device(nemo_ens* e);
 // Tidal SSH a member's boundary row holds after step istp.
 double ens_tide(nemo_ens* e, int m, int istp);
+// A member's tidal amplitude.
+double ens_amp(nemo_ens* e, int m);
 }  // namespace nemo

@@ -449,17 +449,17 @@ cudaError_t launch_apply(nemo_sur* s, int m0, int n, const float* out) {
   return cudaGetLastError();
 }
 
-// flag[m] = 1 when member m (of those with sel[m] != 0) holds a non-finite
-// sshn, un or vn value anywhere in its storage (grid x: chunks of the
+// flag[m] = 1 when member m holds a non-finite sshn, un or vn value, or an
+// |sshn| above ssh_limit[m], anywhere in its storage (grid x: chunks of the
 // storage, grid y: members).
-__global__ void k_nonfinite(const MemberState* __restrict__ ms, const char* __restrict__ sel, int* flag) {
+__global__ void k_diverged(const MemberState* __restrict__ ms, const double* __restrict__ ssh_limit, int* flag) {
   const int m = blockIdx.y;
-  if (!sel[m]) return;
   const MemberState M = ms[m];
+  const double lim = ssh_limit[m];
   const long n = (long)(M.jpj + 3) * M.pitch;
   bool bad = false;
   for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
-    bad |= !isfinite(M.sshn[i]) | !isfinite(M.un[i]) | !isfinite(M.vn[i]);
+    bad |= !(fabs(M.sshn[i]) <= lim) | !isfinite(M.un[i]) | !isfinite(M.vn[i]);
   if (__syncthreads_or(bad) && threadIdx.x == 0) flag[m] = 1;
 }
 
@@ -992,6 +992,7 @@ int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, 
   auto saved_field = [&](int parity, int m, int f) {
     return saved + (((size_t)parity * nm + m) * 3 + f) * field_elems;
   };
+  std::vector<int> saved_at(2 * nm, -1);  // window whose start each saved slot holds
   const long long launches0 = s->nlaunch;
   long long solver_launches = 0;  // one persistent ensemble launch per solver step
   const auto t_start = std::chrono::steady_clock::now();
@@ -1009,6 +1010,7 @@ int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, 
         for (int f = 0; f < 3 && rc == NEMO_OK; ++f)
           rc = status_of(cudaMemcpyAsync(saved_field(w & 1, m, f), src[f], field_elems * sizeof(double),
                                          cudaMemcpyDeviceToDevice, s->stream));
+        saved_at[2 * m + (w & 1)] = w;
       }
       if (rc != NEMO_OK) break;
     }
@@ -1098,49 +1100,70 @@ int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, 
     }
     istp += rest;
   }
-  // The last window's surrogate calls meet no later shadow check: a member
-  // they left non-finite goes back to that window's start and the solver
-  // runs the window.
+  // The last window meets no later shadow check.  A member it left diverged
+  // (a non-finite value, or |ssh| above 10 times its tidal amplitude) goes
+  // back: to the window's start when the surrogate advanced it there, else
+  // (the solver ran it, from a state earlier surrogate calls may have led
+  // astray) to the previous window's start; the solver runs the windows from
+  // there.
   if (rc == NEMO_OK && saved && nsteps > 0) {
     const int wl = nsteps / c->anchor - 1;
     int* d_flag = nullptr;
-    char* d_sel = nullptr;
+    double* d_lim = nullptr;
     std::vector<int> flag(nm, 0);
-    cudaError_t fe = cudaMalloc(&d_flag, nm * sizeof(int) + nm);
+    std::vector<double> lim(nm);
+    for (int m = 0; m < nm; ++m) {  // no tide: only non-finite values count
+      const double a = nemo::ens_amp(e, m);
+      lim[m] = a > 0.0 ? 10.0 * a : INFINITY;
+    }
+    cudaError_t fe = cudaMalloc(&d_lim, nm * (sizeof(double) + sizeof(int)));
     if (fe == cudaSuccess) {
-      d_sel = reinterpret_cast<char*>(d_flag + nm);
+      d_flag = reinterpret_cast<int*>(d_lim + nm);
       fe = join(nemo::ens_stream(e), s->stream) == NEMO_OK ? cudaSuccess : cudaErrorUnknown;
     }
     if (fe == cudaSuccess) fe = cudaMemsetAsync(d_flag, 0, nm * sizeof(int), s->stream);
     if (fe == cudaSuccess)
-      fe = cudaMemcpyAsync(d_sel, pass.data(), nm, cudaMemcpyHostToDevice, s->stream);
+      fe = cudaMemcpyAsync(d_lim, lim.data(), nm * sizeof(double), cudaMemcpyHostToDevice, s->stream);
     if (fe == cudaSuccess) {
-      k_nonfinite<<<dim3(64, (unsigned)nm), 256, 0, s->stream>>>(s->d_ms, d_sel, d_flag);
+      k_diverged<<<dim3(64, (unsigned)nm), 256, 0, s->stream>>>(s->d_ms, d_lim, d_flag);
       s->nlaunch += 1;
       fe = cudaGetLastError();
     }
     if (fe == cudaSuccess) fe = cudaMemcpyAsync(flag.data(), d_flag, nm * sizeof(int), cudaMemcpyDeviceToHost, s->stream);
     if (fe == cudaSuccess) fe = cudaStreamSynchronize(s->stream);
-    if (d_flag) cudaFree(d_flag);
+    if (d_lim) cudaFree(d_lim);
     if (fe != cudaSuccess) rc = status_of(fe);
-    int nbad = 0;
+    std::vector<char> back2(nm, 0);  // members going back two windows
+    int n1 = 0, n2 = 0;
     for (int m = 0; m < nm && rc == NEMO_OK; ++m) {
-      rew[m] = pass[m] && flag[m];
-      if (!rew[m]) continue;
-      ++nbad;
+      rew[m] = 0;
+      if (!flag[m]) continue;
+      int depth = 0;
+      if (pass[m] && saved_at[2 * m + (wl & 1)] == wl)
+        depth = 1;
+      else if (wl >= 1 && saved_at[2 * m + ((wl - 1) & 1)] == wl - 1)
+        depth = 2;
+      if (!depth) continue;  // nothing saved to go back to: stays as it is
+      (depth == 1 ? rew[m] : back2[m]) = 1;
+      (depth == 1 ? n1 : n2) += 1;
       double* dst[3] = {ms[m].sshn, ms[m].un, ms[m].vn};
       for (int f = 0; f < 3 && rc == NEMO_OK; ++f)
-        rc = status_of(cudaMemcpyAsync(dst[f], saved_field(wl & 1, m, f), field_elems * sizeof(double),
-                                       cudaMemcpyDeviceToDevice, s->stream));
+        rc = status_of(cudaMemcpyAsync(dst[f], saved_field((wl - depth + 1) & 1, m, f),
+                                       field_elems * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
+      if (depth == 1) st.sur_steps -= (long long)(c->anchor - c->k);
     }
-    if (rc == NEMO_OK && nbad > 0) {
-      rc = join(s->stream, nemo::ens_stream(e));
-      if (rc == NEMO_OK) rc = nemo::ens_step_subset(e, istp - c->anchor + 1, c->anchor, rew.data());
+    if (rc == NEMO_OK && n1 + n2 > 0) rc = join(s->stream, nemo::ens_stream(e));
+    if (rc == NEMO_OK && n1 > 0) {
+      rc = nemo::ens_step_subset(e, istp - c->anchor + 1, c->anchor, rew.data());
       solver_launches += c->anchor;
-      st.solver_steps += (long long)c->anchor * nbad;
-      st.sur_steps -= (long long)(c->anchor - c->k) * nbad;
-      st.rewound += nbad;
+      st.solver_steps += (long long)c->anchor * n1;
     }
+    if (rc == NEMO_OK && n2 > 0) {
+      rc = nemo::ens_step_subset(e, istp - 2 * c->anchor + 1, 2 * c->anchor, back2.data());
+      solver_launches += 2 * c->anchor;
+      st.solver_steps += (long long)2 * c->anchor * n2;
+    }
+    st.rewound += n1 + n2;
   }
   cudaError_t ce = cudaStreamSynchronize(nemo::ens_stream(e));
   if (ce == cudaSuccess) ce = cudaStreamSynchronize(s->stream);
