@@ -71,6 +71,9 @@ def test_null_handles_are_rejected_without_a_gpu(built):
     assert lib.nemo_continuity(None) == 4
     assert lib.nemo_create(None, None) == 1
     assert lib.nemo_destroy(None) == 1
+    assert lib.nemo_set_grid(None, None) == 1
+    assert lib.nemo_record(None, None) == 1
+    assert lib.nemo_record_wait(None) == 1
 
 
 def test_field_shapes_follow_fortran_bounds(built):
