@@ -74,6 +74,7 @@ def parse():
     ap.add_argument("--batch", type=int, default=64, help="images per conv call (conv workload)")
     ap.add_argument("--train-iters", type=int, default=6000)
     ap.add_argument("--nblocks", type=int, default=2, help="residual blocks of the hybrid's network")
+    ap.add_argument("--k", type=int, default=10, help="model steps per surrogate call (hybrid)")
     ap.add_argument("--n", type=int, default=N,
                     help="grid side (profiling of smaller cases only; the bench line is 4096)")
     return ap.parse_args()
@@ -463,7 +464,7 @@ def run_hybrid(args):
     trainer = sm.Surrogate(nblocks=args.nblocks, batch=64, height=ts, width=ts, seed=1234, device=0, patch=P)
     t_gen = time.time()
     snaps, tides = tr.generate_runs(trainer, seed=7000, nmem=args.train_runs, side=ts,
-                                    steps=args.train_steps, pair_stride=50)
+                                    steps=args.train_steps, every=args.k, pair_stride=50)
     t_gen = time.time() - t_gen
     norm = tr.compute_norm(snaps, paired=True)
     trainer.set_norm(*norm)
@@ -515,7 +516,7 @@ def run_hybrid(args):
     clocks = ClockSampler(0)
     clocks.start()
     ev[2].record(stream)
-    st = sm.hyb_run(inf, hyb, 0, nsteps, k=10, anchor=100, tol=0.01)
+    st = sm.hyb_run(inf, hyb, 0, nsteps, k=args.k, anchor=100, tol=0.01)
     ev[3].record(stream)
     torch.cuda.synchronize()
     t_hyb = ev[2].elapsed_time(ev[3]) / 1e3
@@ -529,8 +530,8 @@ def run_hybrid(args):
             "value": v_hyb, "unit": "cell-steps/s", "n_gpus": 1, "steps": 1, "warmup": 0,
             "ms_per_step": t_hyb * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "bf16+f64", "data": "synthetic",
-            "config": {"workload": "%d members 2048x2048, %d steps, surrogate k=10, re-anchor 100, "
-                                   "tol 1%% relative SSH L2 vs shadow FP64 step" % (nm, nsteps),
+            "config": {"workload": "%d members 2048x2048, %d steps, surrogate k=%d, re-anchor 100, "
+                                   "tol 1%% relative SSH L2 vs shadow FP64 step" % (nm, nsteps, args.k),
                        "candidates": len(cands), "screened_out": len(cands) - len(ok),
                        "patch": P, "nblocks": args.nblocks, "train_side": ts, "train_steps": args.train_steps,
                        "train_runs": args.train_runs, "fallback": "per member",

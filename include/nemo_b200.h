@@ -332,15 +332,17 @@ int nemo_sur_train_step(nemo_sur* s, const float* snap0, const float* snap1, con
 /* Snapshot of every ensemble member (all must be height x width). */
 int nemo_sur_pack_ens(nemo_sur* s, nemo_ens* e, float* snap);
 /* One surrogate call: every member advances from its current state (after
- * step istp_end - 10) to step istp_end; the boundary row takes the exact
- * tidal SSH, the walls keep zero normal velocity. */
+ * step istp_end - k, k the step count the network was trained to advance,
+ * 10 in the bundled recipe) to step istp_end; the boundary row takes the
+ * exact tidal SSH, the walls keep zero normal velocity. */
 int nemo_sur_advance_ens(nemo_sur* s, nemo_ens* e, int istp_end);
 /* out[3*m + f]: relative L2 difference of member m's ssh, u, v (f) in a
  * against ref. */
 int nemo_ens_compare(nemo_ens* a, nemo_ens* ref, double* out);
 
 typedef struct nemo_hyb_config {
-  int k;          /* steps per surrogate call (10) */
+  int k;          /* steps per surrogate call: the step count the network
+                     was trained to advance (10) */
   int anchor;     /* FP64 re-anchor interval (100) */
   double tol;     /* fallback threshold on relative SSH L2 error (0.01) */
   int per_member; /* 1: each member falls back on its own (anchor - k even);

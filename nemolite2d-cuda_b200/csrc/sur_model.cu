@@ -955,7 +955,7 @@ int nemo_hyb_default_config(nemo_hyb_config* c) {
 // for the window.  Statistics count member-windows and member-steps.
 int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, int nsteps,
                  nemo_hyb_stats* stats) {
-  if (!s || !e || !c || c->k != 10 || c->anchor < c->k || c->anchor % c->k || nsteps % c->anchor ||
+  if (!s || !e || !c || c->k < 1 || c->anchor < c->k || c->anchor % c->k || nsteps % c->anchor ||
       !(c->tol > 0) || (c->per_member && (c->anchor - c->k) % 2 != 0))
     return NEMO_ERR_INVALID;
   SCK(set_dev(s));
