@@ -700,62 +700,49 @@ int nemo_set_grid(nemo_ctx* c, const nemo_grid* g) {
   int st = set_device(c); if (st) return st;
   CK(cudaStreamSynchronize(c->stream));  // queued steps may still read the depths
   const size_t fe = (size_t)c->L.elems();
-  // host images in the fields' layout: (ji, jj) of the reference's
-  // (0:jpi+1, 0:jpj+1) arrays at L.idx(ji, jj); everything else zero
-  auto put = [&](const double* src, std::vector<double>& dst) {
-    for (int jj = 0; jj <= jpj + 1; ++jj)
-      for (int ji = 0; ji <= jpi + 1; ++ji) dst[c->L.idx(ji, jj)] = src[jj * ld + ji];
-  };
   enum { E1T, E2T, E1U, E2U, E1V, E2V, E12T, E12U, E12V, FCU, FCV, NA };
-  std::vector<std::vector<double>> h(NA, std::vector<double>(fe, 0.0));
-  for (int k = 0; k < 6; ++k) put(in[k], h[k]);
-  // cell areas over the ranges original/nemolite2d.f90:263-279 fills
-  for (int jj = 1; jj <= jpj; ++jj)
-    for (int ji = 1; ji <= jpi; ++ji) {
-      const long q = c->L.idx(ji, jj);
-      h[E12T][q] = h[E1T][q] * h[E2T][q];
-    }
-  for (int jj = 1; jj <= jpj; ++jj)
-    for (int ji = 0; ji <= jpi; ++ji) {
-      const long q = c->L.idx(ji, jj);
-      h[E12U][q] = h[E1U][q] * h[E2U][q];
-    }
-  for (int jj = 0; jj <= jpj; ++jj)
-    for (int ji = 1; ji <= jpi; ++ji) {
-      const long q = c->L.idx(ji, jj);
-      h[E12V][q] = h[E1V][q] * h[E2V][q];
-    }
-  // Coriolis parameters, as the momentum loops form them (:503, :594)
-  const double d2r = kPi / 180.0;
-  for (int jj = 0; jj <= jpj + 1; ++jj)
-    for (int ji = 0; ji <= jpi + 1; ++ji) {
-      const long q = c->L.idx(ji, jj);
-      h[FCU][q] = 2.0 * kOmega * sin(g->gphiu[jj * ld + ji] * d2r);
-      h[FCV][q] = 2.0 * kOmega * sin(g->gphiv[jj * ld + ji] * d2r);
-    }
-  std::vector<signed char> hp(fe, 0);
-  for (int jj = 0; jj <= jpj + 1; ++jj)
-    for (int ji = 0; ji <= jpi + 1; ++ji) hp[c->L.idx(ji, jj)] = (signed char)g->pt[jj * ld + ji];
   if (!c->gslab) {
     cudaError_t e = cudaMalloc(&c->gslab, NA * fe * sizeof(double) + fe);
     if (e != cudaSuccess) { c->gslab = nullptr; cudaGetLastError(); return NEMO_ERR_ALLOC; }
   }
   double* base = static_cast<double*>(c->gslab);
-  for (int k = 0; k < NA; ++k)
-    CK(cudaMemcpy(base + k * fe, h[k].data(), fe * sizeof(double), cudaMemcpyHostToDevice));
+  // one host image in the fields' layout at a time: (ji, jj) of the
+  // reference's (0:jpi+1, 0:jpj+1) arrays at L.idx(ji, jj), the rest zero
+  std::vector<double> img(fe);
+  auto upload = [&](int k, auto value, int ji0, int ji1, int jj0, int jj1) -> int {
+    std::fill(img.begin(), img.end(), 0.0);
+    for (int jj = jj0; jj <= jj1; ++jj)
+      for (int ji = ji0; ji <= ji1; ++ji) img[c->L.idx(ji, jj)] = value(jj * ld + ji);
+    CK(cudaMemcpy(base + k * fe, img.data(), fe * sizeof(double), cudaMemcpyHostToDevice));
+    return NEMO_OK;
+  };
+  for (int k = 0; k < 6 && !st; ++k)
+    st = upload(k, [&](long q) { return in[k][q]; }, 0, jpi + 1, 0, jpj + 1);
+  // cell areas over the ranges original/nemolite2d.f90:263-279 fills
+  if (!st) st = upload(E12T, [&](long q) { return g->e1t[q] * g->e2t[q]; }, 1, jpi, 1, jpj);
+  if (!st) st = upload(E12U, [&](long q) { return g->e1u[q] * g->e2u[q]; }, 0, jpi, 1, jpj);
+  if (!st) st = upload(E12V, [&](long q) { return g->e1v[q] * g->e2v[q]; }, 1, jpi, 0, jpj);
+  // Coriolis parameters, as the momentum loops form them (:503, :594)
+  const double d2r = kPi / 180.0;
+  if (!st) st = upload(FCU, [&](long q) { return 2.0 * kOmega * sin(g->gphiu[q] * d2r); }, 0, jpi + 1, 0, jpj + 1);
+  if (!st) st = upload(FCV, [&](long q) { return 2.0 * kOmega * sin(g->gphiv[q] * d2r); }, 0, jpi + 1, 0, jpj + 1);
+  if (st) return st;
+  std::vector<signed char> hp(fe, 0);
+  for (int jj = 0; jj <= jpj + 1; ++jj)
+    for (int ji = 0; ji <= jpi + 1; ++ji) hp[c->L.idx(ji, jj)] = (signed char)g->pt[jj * ld + ji];
   signed char* pt = reinterpret_cast<signed char*>(base + NA * fe);
   CK(cudaMemcpy(pt, hp.data(), fe, cudaMemcpyHostToDevice));
   c->grid = GridDev{pt, base + E1T * fe, base + E2T * fe, base + E1U * fe, base + E2U * fe, base + E1V * fe,
                     base + E2V * fe, base + E12T * fe, base + E12U * fe, base + E12V * fe, base + FCU * fe,
                     base + FCV * fe};
-  // depths, when given
+  // depths, when given (the rest of each depth array is kept)
   double* hd[3] = {c->ht, c->hu, c->hv};
-  std::vector<double> tmp(fe);
   for (int k = 0; k < 3; ++k) {
     if (!in[8 + k]) continue;
-    CK(cudaMemcpy(tmp.data(), hd[k], fe * sizeof(double), cudaMemcpyDeviceToHost));
-    put(in[8 + k], tmp);
-    CK(cudaMemcpy(hd[k], tmp.data(), fe * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(img.data(), hd[k], fe * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int jj = 0; jj <= jpj + 1; ++jj)
+      for (int ji = 0; ji <= jpi + 1; ++ji) img[c->L.idx(ji, jj)] = in[8 + k][jj * ld + ji];
+    CK(cudaMemcpy(hd[k], img.data(), fe * sizeof(double), cudaMemcpyHostToDevice));
   }
   c->general = true;
   // the a-fields stay as they are; sshn_u/sshn_v restart from the current

@@ -56,13 +56,14 @@ struct ArrGrid {
   __device__ double fcv(int a, int b) const { return d.fcv[L.idx(a, b)]; }
 };
 
-// Launches kernel K with the accessor of grid g (null: the uniform grid).
-#define WITH_GRID(K, grid, block, L, C, g, ...)                                        \
-  do {                                                                                 \
-    if (g)                                                                             \
-      K<ArrGrid><<<(grid), (block), 0, s>>>(L, ArrGrid{L, *(g)}, __VA_ARGS__);         \
-    else                                                                               \
-      K<UniGrid><<<(grid), (block), 0, s>>>(L, UniGrid{C, L.jpi, L.jpj}, __VA_ARGS__); \
+// Launches kernel K on stream st with the accessor of grid g (null: the
+// uniform grid).
+#define WITH_GRID(K, grid, block, st, L, C, g, ...)                                     \
+  do {                                                                                  \
+    if (g)                                                                              \
+      K<ArrGrid><<<(grid), (block), 0, (st)>>>(L, ArrGrid{L, *(g)}, __VA_ARGS__);       \
+    else                                                                                \
+      K<UniGrid><<<(grid), (block), 0, (st)>>>(L, UniGrid{C, L.jpi, L.jpj}, __VA_ARGS__); \
   } while (0)
 
 // Seeded bathymetry (no reference counterpart): depth at half-grid point
@@ -431,57 +432,57 @@ cudaError_t launch_record(const Layout& L, const double* sshn, const double* un,
 
 cudaError_t launch_init_sshn_uv(const Layout& L, const Consts& C, const double* sshn,
                                 double* sshn_u, double* sshn_v, cudaStream_t s, const GridDev* g) {
-  WITH_GRID(k_init_sshn_uv, grid_for(L.jpi + 1, L.jpj + 1), dim3(BX, BY), L, C, g, sshn, sshn_u, sshn_v);
+  WITH_GRID(k_init_sshn_uv, grid_for(L.jpi + 1, L.jpj + 1), dim3(BX, BY), s, L, C, g, sshn, sshn_u, sshn_v);
   return cudaGetLastError();
 }
 
 cudaError_t launch_continuity(const Layout& L, const Consts& C, const RoutinePtrs& p,
                               cudaStream_t s, const GridDev* g) {
-  WITH_GRID(k_continuity, grid_for(L.jpi, L.jpj), dim3(BX, BY), L, C, g, C, p);
+  WITH_GRID(k_continuity, grid_for(L.jpi, L.jpj), dim3(BX, BY), s, L, C, g, C, p);
   return cudaGetLastError();
 }
 
 cudaError_t launch_momentum_u(const Layout& L, const Consts& C, const RoutinePtrs& p,
                               cudaStream_t s, const GridDev* g) {
   if (L.jpi < 2) return cudaSuccess;
-  WITH_GRID(k_momentum_u, grid_for(L.jpi - 1, L.jpj), dim3(BX, BY), L, C, g, C, p);
+  WITH_GRID(k_momentum_u, grid_for(L.jpi - 1, L.jpj), dim3(BX, BY), s, L, C, g, C, p);
   return cudaGetLastError();
 }
 
 cudaError_t launch_momentum_v(const Layout& L, const Consts& C, const RoutinePtrs& p,
                               cudaStream_t s, const GridDev* g) {
   if (L.jpj < 2) return cudaSuccess;
-  WITH_GRID(k_momentum_v, grid_for(L.jpi, L.jpj - 1), dim3(BX, BY), L, C, g, C, p);
+  WITH_GRID(k_momentum_v, grid_for(L.jpi, L.jpj - 1), dim3(BX, BY), s, L, C, g, C, p);
   return cudaGetLastError();
 }
 
 cudaError_t launch_bc_ssh(const Layout& L, double value, double* ssha, cudaStream_t s, const GridDev* g) {
   const Consts C{};  // the uniform grid's mask needs no constants
-  WITH_GRID(k_bc_ssh, grid_for(L.jpi, L.jpj), dim3(BX, BY), L, C, g, value, ssha);
+  WITH_GRID(k_bc_ssh, grid_for(L.jpi, L.jpj), dim3(BX, BY), s, L, C, g, value, ssha);
   return cudaGetLastError();
 }
 
 cudaError_t launch_bc_solid_u(const Layout& L, double* ua, cudaStream_t s, const GridDev* g) {
   const Consts C{};
-  WITH_GRID(k_bc_solid_u, grid_for(L.jpi + 1, L.jpj), dim3(BX, BY), L, C, g, ua);
+  WITH_GRID(k_bc_solid_u, grid_for(L.jpi + 1, L.jpj), dim3(BX, BY), s, L, C, g, ua);
   return cudaGetLastError();
 }
 
 cudaError_t launch_bc_solid_v(const Layout& L, double* va, cudaStream_t s, const GridDev* g) {
   const Consts C{};
-  WITH_GRID(k_bc_solid_v, grid_for(L.jpi, L.jpj + 1), dim3(BX, BY), L, C, g, va);
+  WITH_GRID(k_bc_solid_v, grid_for(L.jpi, L.jpj + 1), dim3(BX, BY), s, L, C, g, va);
   return cudaGetLastError();
 }
 
 cudaError_t launch_bc_flather_u(const Layout& L, const RoutinePtrs& p, cudaStream_t s, const GridDev* g) {
   const Consts C{};
-  WITH_GRID(k_bc_flather_u, (L.jpj + 127) / 128, 128, L, C, g, p);
+  WITH_GRID(k_bc_flather_u, (L.jpj + 127) / 128, 128, s, L, C, g, p);
   return cudaGetLastError();
 }
 
 cudaError_t launch_bc_flather_v(const Layout& L, const RoutinePtrs& p, cudaStream_t s, const GridDev* g) {
   const Consts C{};
-  WITH_GRID(k_bc_flather_v, (L.jpi + 127) / 128, 128, L, C, g, p);
+  WITH_GRID(k_bc_flather_v, (L.jpi + 127) / 128, 128, s, L, C, g, p);
   return cudaGetLastError();
 }
 
@@ -492,7 +493,7 @@ cudaError_t launch_copy_next(const Layout& L, const RoutinePtrs& p, cudaStream_t
 
 cudaError_t launch_derive_sshn_uv(const Layout& L, const Consts& C, const double* sshn,
                                   double* sshn_u, double* sshn_v, cudaStream_t s, const GridDev* g) {
-  WITH_GRID(k_derive_sshn_uv, grid_for(L.jpi + 1, L.jpj + 1), dim3(BX, BY), L, C, g, sshn, sshn_u, sshn_v);
+  WITH_GRID(k_derive_sshn_uv, grid_for(L.jpi + 1, L.jpj + 1), dim3(BX, BY), s, L, C, g, sshn, sshn_u, sshn_v);
   return cudaGetLastError();
 }
 
