@@ -456,14 +456,18 @@ __device__ __forceinline__ void run_strip_ring(const Layout& L, const Consts& C,
   constexpr int RING = ring_slots<NR>(), AHEAD = RING - 1, RS = ring_row<NR>();
 
   const long pitch = L.pitch;
-  const long o_last = L.idx(cl, jpj + 1);
   // rows J0+1 .. J0+AHEAD-1 into the ring, and row J0 when its stored
   // reciprocal depths are read from there (rows J0-1 and J0 are loaded
-  // directly below; rows past jpj+1 read row jpj+1 again)
+  // directly below).  Rows past J1+1, which no iteration reads, are not
+  // copied: their copy group stays empty, so the group counts of the waits
+  // hold.
+  const int r_stop = J1 + 1;
 #pragma unroll
   for (int r = NR ? 1 : 0; r < AHEAD; ++r) {
-    const long o = L.idx(cl, J0 + r);
-    ring_issue<NR>(my + ((J0 + r) % RING) * RS, A, o < o_last ? o : o_last);
+    if (J0 + r <= r_stop)
+      ring_issue<NR>(my + ((J0 + r) % RING) * RS, A, L.idx(cl, J0 + r));
+    else
+      cp_commit();
   }
 
   Cell p, cur, nx;
@@ -487,7 +491,10 @@ __device__ __forceinline__ void run_strip_ring(const Layout& L, const Consts& C,
   for (int j = J0; j <= J1; ++j) {
     const int slot_n = slot_j == RING - 1 ? 0 : slot_j + 1;  // row j+1
     const int slot_f = slot_j == 0 ? RING - 1 : slot_j - 1;  // row j+AHEAD (was row j-1)
-    ring_issue<NR>(my + slot_f * RS, A, o_ld < o_last ? o_ld : o_last);
+    if (j + AHEAD <= r_stop)
+      ring_issue<NR>(my + slot_f * RS, A, o_ld);
+    else
+      cp_commit();
     o_ld += pitch;
     cp_wait<AHEAD - 1>();  // rows <= j+1 have landed
     ring_cell(nx, my + slot_n * RS);
