@@ -995,6 +995,27 @@ int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, 
   std::vector<int> saved_at(2 * nm, -1);  // window whose start each saved slot holds
   const long long launches0 = s->nlaunch;
   long long solver_launches = 0;  // one persistent ensemble launch per solver step
+  // Members with sel[m] go back to the state saved in slot `parity` (the
+  // start of step istp_from + 1) and the solver runs them n steps (n even,
+  // so their state buffers keep their parity).
+  auto rewind_to = [&](int parity, const char* sel, int istp_from, int n, int count) -> int {
+    for (int m = 0; m < nm; ++m) {
+      if (!sel[m]) continue;
+      double* dst[3] = {ms[m].sshn, ms[m].un, ms[m].vn};
+      for (int f = 0; f < 3; ++f) {
+        const int r = status_of(cudaMemcpyAsync(dst[f], saved_field(parity, m, f), field_elems * sizeof(double),
+                                                cudaMemcpyDeviceToDevice, s->stream));
+        if (r != NEMO_OK) return r;
+      }
+    }
+    int r = join(s->stream, nemo::ens_stream(e));
+    if (r == NEMO_OK) r = nemo::ens_step_subset(e, istp_from + 1, n, sel);
+    if (r != NEMO_OK) return r;
+    solver_launches += n;
+    st.solver_steps += (long long)n * count;
+    st.rewound += count;
+    return NEMO_OK;
+  };
   const auto t_start = std::chrono::steady_clock::now();
   int istp = istp0;
   int rc = NEMO_OK;
@@ -1048,24 +1069,10 @@ int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, 
       nfail += fail[m];
       if (!(r <= worst)) worst = r;  // NaN propagates
     }
-    if (nrew > 0) {
-      // back to the previous window's start (istp - anchor), then the solver
-      // re-runs that window and this window's first k steps (an even count,
-      // so the member's state buffers keep their parity)
-      for (int m = 0; m < nm && rc == NEMO_OK; ++m) {
-        if (!rew[m]) continue;
-        double* dst[3] = {ms[m].sshn, ms[m].un, ms[m].vn};
-        for (int f = 0; f < 3 && rc == NEMO_OK; ++f)
-          rc = status_of(cudaMemcpyAsync(dst[f], saved_field((w - 1) & 1, m, f), field_elems * sizeof(double),
-                                         cudaMemcpyDeviceToDevice, s->stream));
-      }
-      if (rc == NEMO_OK) rc = join(s->stream, nemo::ens_stream(e));
-      if (rc == NEMO_OK) rc = nemo::ens_step_subset(e, istp - c->anchor + 1, c->anchor + c->k, rew.data());
-      if (rc != NEMO_OK) break;
-      solver_launches += c->anchor + c->k;
-      st.solver_steps += (long long)(c->anchor + c->k) * nrew;
-      st.rewound += nrew;
-    }
+    // back to the previous window's start; the solver re-runs that window
+    // and this window's first k steps
+    if (nrew > 0 && (rc = rewind_to((w - 1) & 1, rew.data(), istp - c->anchor, c->anchor + c->k, nrew)))
+      break;
     if (!c->per_member && nfail > 0) {
       for (int m = 0; m < nm; ++m) fail[m] = 1;
       nfail = nm;
@@ -1138,32 +1145,17 @@ int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, 
     for (int m = 0; m < nm && rc == NEMO_OK; ++m) {
       rew[m] = 0;
       if (!flag[m]) continue;
-      int depth = 0;
-      if (pass[m] && saved_at[2 * m + (wl & 1)] == wl)
-        depth = 1;
-      else if (wl >= 1 && saved_at[2 * m + ((wl - 1) & 1)] == wl - 1)
-        depth = 2;
-      if (!depth) continue;  // nothing saved to go back to: stays as it is
-      (depth == 1 ? rew[m] : back2[m]) = 1;
-      (depth == 1 ? n1 : n2) += 1;
-      double* dst[3] = {ms[m].sshn, ms[m].un, ms[m].vn};
-      for (int f = 0; f < 3 && rc == NEMO_OK; ++f)
-        rc = status_of(cudaMemcpyAsync(dst[f], saved_field((wl - depth + 1) & 1, m, f),
-                                       field_elems * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
-      if (depth == 1) st.sur_steps -= (long long)(c->anchor - c->k);
+      if (pass[m] && saved_at[2 * m + (wl & 1)] == wl) {
+        rew[m] = 1;
+        ++n1;
+        st.sur_steps -= (long long)(c->anchor - c->k);
+      } else if (wl >= 1 && saved_at[2 * m + ((wl - 1) & 1)] == wl - 1) {
+        back2[m] = 1;
+        ++n2;
+      }  // else nothing saved to go back to: it stays as it is
     }
-    if (rc == NEMO_OK && n1 + n2 > 0) rc = join(s->stream, nemo::ens_stream(e));
-    if (rc == NEMO_OK && n1 > 0) {
-      rc = nemo::ens_step_subset(e, istp - c->anchor + 1, c->anchor, rew.data());
-      solver_launches += c->anchor;
-      st.solver_steps += (long long)c->anchor * n1;
-    }
-    if (rc == NEMO_OK && n2 > 0) {
-      rc = nemo::ens_step_subset(e, istp - 2 * c->anchor + 1, 2 * c->anchor, back2.data());
-      solver_launches += 2 * c->anchor;
-      st.solver_steps += (long long)2 * c->anchor * n2;
-    }
-    st.rewound += n1 + n2;
+    if (rc == NEMO_OK && n1 > 0) rc = rewind_to(wl & 1, rew.data(), istp - c->anchor, c->anchor, n1);
+    if (rc == NEMO_OK && n2 > 0) rc = rewind_to((wl - 1) & 1, back2.data(), istp - 2 * c->anchor, 2 * c->anchor, n2);
   }
   cudaError_t ce = cudaStreamSynchronize(nemo::ens_stream(e));
   if (ce == cudaSuccess) ce = cudaStreamSynchronize(s->stream);
