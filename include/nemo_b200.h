@@ -349,17 +349,19 @@ typedef struct nemo_hyb_config {
                      0: any failing member sends the whole ensemble back (1) */
   double quarantine; /* shadow error beyond which a member stays on the FP64
                         solver for the rest of the run; 0: never (0.05) */
-  int rewind;        /* 1: a member quarantined right after a window the
-                        surrogate advanced restarts from its FP64 state at
-                        that window's start, the solver re-running the
-                        window; after the last window a member left
-                        non-finite or with |ssh| above 10 times its tidal
-                        amplitude goes back one window (two when the solver
-                        ran its last one) (keeps one saved state per member
-                        and window parity: 2 x 3 fields per member) (1) */
+  int rewind;        /* 1: a quarantined member restarts from its FP64 state
+                        at the start of the latest of the two previous
+                        windows the surrogate advanced it in, the solver
+                        re-running from there; after the last window a
+                        member left non-finite or with |ssh| above 10 times
+                        its tidal amplitude goes back to the start of the
+                        latest of the last three windows the surrogate
+                        advanced it in (keeps the states of the last three
+                        window starts: 3 x 3 fields per member) (1) */
 } nemo_hyb_config;
 
 typedef struct nemo_hyb_stats {
+  /* step counts are work done, windows a rewind discarded included */
   long long sur_calls;     /* surrogate calls (each advances its members k steps) */
   long long sur_steps;     /* member-steps advanced by the surrogate */
   long long solver_steps;  /* member-steps advanced by the FP64 solver */

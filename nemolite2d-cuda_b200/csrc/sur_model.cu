@@ -947,10 +947,10 @@ int nemo_hyb_default_config(nemo_hyb_config* c) {
 // advance by surrogate calls, k steps each.  A member whose shadow error
 // exceeds `quarantine` stays on the solver for the rest of the run (errors
 // that large precede the corner instability the surrogate's perturbations
-// can excite).  With `rewind`, such a member whose current state came from
-// the previous window's surrogate calls is first restored to its FP64 state
-// at that window's start (saved at every window start) and the solver re-runs
-// the window, anchor + k steps, so the unchecked calls leave no trace.  With
+// can excite).  With `rewind`, such a member is first restored to its FP64
+// state at the start of the latest of the two previous windows the surrogate
+// advanced it in (saved at every window start, three per member) and the
+// solver re-runs from there, so those unchecked calls leave no trace.  With
 // per_member = 0 one failing member sends the whole ensemble to the solver
 // for the window.  Statistics count member-windows and member-steps.
 int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, int nsteps,
@@ -976,14 +976,15 @@ int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, 
     out_all = own + (size_t)nm * hw * 4;
   }
   std::vector<double> tide(nm), acc(6 * nm);
-  std::vector<char> pass(nm), fail(nm), quar(nm, 0), prev_pass(nm, 0), rew(nm);
-  // saved FP64 states (sshn, un, vn) of every member at the last two window
+  std::vector<char> pass(nm), fail(nm), quar(nm, 0);
+  // saved FP64 states (sshn, un, vn) of every member at the last NS window
   // starts, for rewinding
+  constexpr int NS = 3;
   const size_t field_elems = (size_t)(ms.empty() ? 0 : (long)(ms[0].jpj + 3) * ms[0].pitch);
   double* saved = nullptr;
   const bool rewind = c->rewind && c->quarantine > 0 && c->per_member;
   if (rewind && nm > 0) {
-    cudaError_t ae = cudaMalloc(&saved, 2 * (size_t)nm * 3 * field_elems * sizeof(double));
+    cudaError_t ae = cudaMalloc(&saved, (size_t)NS * nm * 3 * field_elems * sizeof(double));
     if (ae != cudaSuccess) {
       if (own) cudaFree(own);
       return status_of(ae);
@@ -992,7 +993,19 @@ int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, 
   auto saved_field = [&](int parity, int m, int f) {
     return saved + (((size_t)parity * nm + m) * 3 + f) * field_elems;
   };
-  std::vector<int> saved_at(2 * nm, -1);  // window whose start each saved slot holds
+  // per member and slot: the window whose start the slot holds, and the
+  // window (if it is the same one) the surrogate advanced the member in
+  std::vector<int> saved_at(NS * nm, -1), accepted_at(NS * nm, -1);
+  // latest window x in [w - d_hi, w - d_lo] the surrogate advanced member m
+  // in whose start is saved, as w - x; -1 when none
+  auto back_to = [&](int m, int w, int d_lo, int d_hi) {
+    for (int d = d_lo; d <= d_hi; ++d) {
+      const int x = w - d;
+      if (x < 0) break;
+      if (saved_at[NS * m + x % NS] == x && accepted_at[NS * m + x % NS] == x) return d;
+    }
+    return -1;
+  };
   const long long launches0 = s->nlaunch;
   long long solver_launches = 0;  // one persistent ensemble launch per solver step
   // Members with sel[m] go back to the state saved in slot `parity` (the
@@ -1031,7 +1044,7 @@ int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, 
         for (int f = 0; f < 3 && rc == NEMO_OK; ++f)
           rc = status_of(cudaMemcpyAsync(saved_field(w & 1, m, f), src[f], field_elems * sizeof(double),
                                          cudaMemcpyDeviceToDevice, s->stream));
-        saved_at[2 * m + (w & 1)] = w;
+        saved_at[NS * m + w % NS] = w;
       }
       if (rc != NEMO_OK) break;
     }
@@ -1055,29 +1068,36 @@ int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, 
     if ((rc = check_err(s)) != NEMO_OK) break;
     // a non-finite error (a member whose state blew up) counts as a failure
     double worst = 0.0;
-    int nfail = 0, nrew = 0;
+    int nfail = 0;
+    std::vector<char> back[NS];
+    int nback[NS] = {0};
+    for (int d = 1; d < NS; ++d) back[d].assign(nm, 0);
     for (int m = 0; m < nm; ++m) {
       const double r = acc[6 * m + 1] > 0 ? sqrt(acc[6 * m] / acc[6 * m + 1]) : sqrt(acc[6 * m]);
-      rew[m] = 0;
       if (c->quarantine > 0 && !quar[m] && !(r <= c->quarantine)) {
         quar[m] = 1;  // far off: the solver keeps this member from now on
         st.quarantined += 1;
-        rew[m] = saved && w > 0 && prev_pass[m];  // its state came from surrogate calls
-        nrew += rew[m];
+        // back to the start of the latest window the surrogate advanced it in
+        const int d = saved ? back_to(m, w, 1, NS - 1) : -1;
+        if (d > 0) back[d][m] = 1, nback[d] += 1;
       }
       fail[m] = quar[m] || !(r <= c->tol);
       nfail += fail[m];
       if (!(r <= worst)) worst = r;  // NaN propagates
     }
-    // back to the previous window's start; the solver re-runs that window
-    // and this window's first k steps
-    if (nrew > 0 && (rc = rewind_to((w - 1) & 1, rew.data(), istp - c->anchor, c->anchor + c->k, nrew)))
-      break;
+    // the solver re-runs the windows from there and this window's first k steps
+    for (int d = 1; d < NS && rc == NEMO_OK; ++d)
+      if (nback[d] > 0)
+        rc = rewind_to((w - d) % NS, back[d].data(), istp - d * c->anchor, d * c->anchor + c->k, nback[d]);
+    if (rc != NEMO_OK) break;
     if (!c->per_member && nfail > 0) {
       for (int m = 0; m < nm; ++m) fail[m] = 1;
       nfail = nm;
     }
-    for (int m = 0; m < nm; ++m) pass[m] = prev_pass[m] = !fail[m];
+    for (int m = 0; m < nm; ++m) {
+      pass[m] = !fail[m];
+      accepted_at[NS * m + w % NS] = pass[m] ? w : -1;
+    }
     st.last_shadow_err = worst;
     if (!(worst <= st.max_shadow_err)) st.max_shadow_err = worst;
     st.windows += nm;
@@ -1140,22 +1160,19 @@ int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, 
     if (fe == cudaSuccess) fe = cudaStreamSynchronize(s->stream);
     if (d_lim) cudaFree(d_lim);
     if (fe != cudaSuccess) rc = status_of(fe);
-    std::vector<char> back2(nm, 0);  // members going back two windows
-    int n1 = 0, n2 = 0;
-    for (int m = 0; m < nm && rc == NEMO_OK; ++m) {
-      rew[m] = 0;
+    // back to the start of the latest window the surrogate advanced the
+    // member in (the last one included); with none saved it stays as it is
+    std::vector<char> back[NS];
+    int nback[NS] = {0};
+    for (int d = 0; d < NS; ++d) back[d].assign(nm, 0);
+    for (int m = 0; m < nm; ++m) {
       if (!flag[m]) continue;
-      if (pass[m] && saved_at[2 * m + (wl & 1)] == wl) {
-        rew[m] = 1;
-        ++n1;
-        st.sur_steps -= (long long)(c->anchor - c->k);
-      } else if (wl >= 1 && saved_at[2 * m + ((wl - 1) & 1)] == wl - 1) {
-        back2[m] = 1;
-        ++n2;
-      }  // else nothing saved to go back to: it stays as it is
+      const int d = back_to(m, wl, 0, NS - 1);
+      if (d >= 0) back[d][m] = 1, nback[d] += 1;
     }
-    if (rc == NEMO_OK && n1 > 0) rc = rewind_to(wl & 1, rew.data(), istp - c->anchor, c->anchor, n1);
-    if (rc == NEMO_OK && n2 > 0) rc = rewind_to((wl - 1) & 1, back2.data(), istp - 2 * c->anchor, 2 * c->anchor, n2);
+    for (int d = 0; d < NS && rc == NEMO_OK; ++d)
+      if (nback[d] > 0)
+        rc = rewind_to((wl - d) % NS, back[d].data(), istp - (d + 1) * c->anchor, (d + 1) * c->anchor, nback[d]);
   }
   cudaError_t ce = cudaStreamSynchronize(nemo::ens_stream(e));
   if (ce == cudaSuccess) ce = cudaStreamSynchronize(s->stream);
