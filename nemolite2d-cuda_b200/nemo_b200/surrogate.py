@@ -197,9 +197,9 @@ def hyb_run(sur, ens, istp0, nsteps, k=10, anchor=100, tol=0.01, per_member=True
             rewind=True):
     """Hybrid run (nemo_hyb_run); returns the statistics as a dict (counts of
     member-windows and member-steps).  quarantine: shadow error beyond which a
-    member stays on the FP64 solver (0: never); rewind: such a member whose
-    state came from the previous window's surrogate calls restarts from that
-    window's FP64 starting state."""
+    member stays on the FP64 solver (0: never); rewind: such a member (and,
+    after the last window, a diverged one) restarts from its FP64 state at the
+    start of the latest recent window the surrogate advanced it in."""
     c = HybConfig(k, anchor, tol, int(bool(per_member)), quarantine, int(bool(rewind)))
     st = HybStats()
     check(sur.lib.nemo_hyb_run(sur.h, ens.h, ctypes.byref(c), istp0, nsteps, ctypes.byref(st)),
