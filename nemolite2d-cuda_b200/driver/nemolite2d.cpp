@@ -33,6 +33,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cctype>
 #include <chrono>
 #include <condition_variable>
@@ -507,6 +508,8 @@ int main(int argc, char** argv) {
            fortran_E(ck[0], 16, 8).c_str(), fortran_E(ck[1], 16, 8).c_str(),
            fortran_E(ck[2], 16, 8).c_str());
     if (csv) fprintf(csv, "%ld,%.17e,%.17e,%.17e\n", istp, ck[0], ck[1], ck[2]);
+    if (!(std::isfinite(ck[0]) && std::isfinite(ck[1]) && std::isfinite(ck[2])))
+      fprintf(stderr, "warning: non-finite checksum at istp=%ld (the state has diverged)\n", istp);
     if (writer) writer->record((int)istp);
   };
 
