@@ -333,6 +333,23 @@ class Model:
             assert x.shape == field_shape(f, self.jpi, self.jpj), (f, x.shape)
         check(self.lib.nemo_set_state(self.h, *[_dptr(x) for x in a]), "nemo_set_state")
 
+    def save_checkpoint(self, path, istp):
+        """Write the state after step istp (sshn, un, vn in Fortran bounds,
+        FP64) to an .npz file.  Every step derives the rest of the state from
+        these three fields, so load_checkpoint followed by steps istp+1... gives
+        the uninterrupted run bit for bit (the reference writes no restart
+        files; this is the build's own format)."""
+        np.savez(path, istp=np.int64(istp), jpi=np.int64(self.jpi), jpj=np.int64(self.jpj),
+                 sshn=self.field(SSHN), un=self.field(UN), vn=self.field(VN))
+
+    def load_checkpoint(self, path):
+        """Restore a save_checkpoint file; returns the step it was taken after."""
+        with np.load(path) as z:
+            if int(z["jpi"]) != self.jpi or int(z["jpj"]) != self.jpj:
+                raise ValueError("checkpoint is for a %dx%d grid" % (int(z["jpi"]), int(z["jpj"])))
+            self.set_state(z["sshn"], z["un"], z["vn"])
+            return int(z["istp"])
+
     def set_grid(self, pt, e1t, e2t, e1u, e2u, e1v, e2v, gphiu, gphiv, ht=None, hu=None, hv=None):
         """General grid (nemo_set_grid): arrays of shape (jpj+2, jpi+2) over
         (0:jpi+1, 0:jpj+1); depths None keep the current ones.  Steps then

@@ -436,3 +436,24 @@ def test_default_build_general_grid_within_tolerance(nb, oracle_mod):
         o.run(1 + 100 * rec, 100)
         for name, fid in STATE:
             assert relerr(m.field(fid), o.field(fid)) <= TOL, (rec, name)
+
+
+def test_checkpoint_restart_is_bit_exact(nb, tmp_path):
+    """save_checkpoint after step 60, restart in a fresh context, steps 61..120:
+    the same bits as the uninterrupted run (default build, fused path)."""
+    kw = dict(jpi=150, jpj=97, rdt=20.0, cbfr=0.00015, visc=0.1, amp_tide=0.4, nbump=6,
+              seed=8, bump_amp=20.0, bump_wmin=5e3, bump_wmax=40e3)
+    a = nb.Model(strict=False, **kw)
+    a.step_n(1, 60)
+    path = str(tmp_path / "ck.npz")
+    a.save_checkpoint(path, 60)
+    a.step_n(61, 60)
+    b = nb.Model(strict=False, **kw)
+    istp = b.load_checkpoint(path)
+    assert istp == 60
+    b.step_n(istp + 1, 60)
+    for name, fid in STATE:
+        np.testing.assert_array_equal(bits(a.field(fid)), bits(b.field(fid)), err_msg=name)
+    c = nb.Model(strict=False, **dict(kw, jpi=151))
+    with pytest.raises(ValueError):
+        c.load_checkpoint(path)
