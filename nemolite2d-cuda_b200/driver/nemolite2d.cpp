@@ -252,6 +252,13 @@ bool setup(const std::string& path, Setup& s) {
   s.nit000 = nl.integer("nit000", 1);
   s.nitend = nl.integer("nitend", 1000);
   s.irecord = nl.integer("irecord", 1);
+  if (s.irecord < 1) {
+    // the step loop takes MOD(istp, irecord) (original/nemolite2d.f90:384),
+    // which has no value for irecord <= 0
+    fprintf(stderr, "irecord = %ld: the output interval must be at least 1\n", s.irecord);
+    printf("err found in reading namelist file\n");
+    return false;
+  }
   s.rdt = nl.real("rdt", 10.0);
   s.cbfr = nl.real("cbfr", 0.001);
   s.visc = nl.real("visc", 100.0);

@@ -20,7 +20,8 @@ and the gnuplot `output` routine are skipped (fields are snapshotted at each
 `irecord` step instead).  Only this script reads the reference source; the
 fixtures it writes (tests/golden/*.npz) are plain numbers.
 
-Usage: python tests/golden/make_golden.py [--src PATH] [--out DIR]
+Usage: python tests/golden/make_golden.py --src <reference>/original/nemolite2d.f90 [--out DIR]
+(or set NEMOLITE2D_F90 to that path instead of --src)
 """
 import argparse
 import math
@@ -30,7 +31,8 @@ import sys
 
 import numpy as np
 
-DEFAULT_SRC = "/root/reference/original/nemolite2d.f90"
+# the reference source: --src, else the NEMOLITE2D_F90 environment variable
+DEFAULT_SRC = os.environ.get("NEMOLITE2D_F90")
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 # Cases: namelist values (jpiglo/jpjglo include the 2 boundary rows, as the
@@ -695,6 +697,9 @@ def main():
     ap.add_argument("--cases", nargs="*", default=list(CASES))
     ap.add_argument("--dump", action="store_true", help="print the translated program")
     a = ap.parse_args()
+    if not a.src:
+        ap.error("name the reference's original/nemolite2d.f90 with --src "
+                 "(or the NEMOLITE2D_F90 environment variable)")
     with open(a.src) as fh:
         text = fh.read()
     pysrc, _ = build_program(text)

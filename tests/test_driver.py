@@ -105,6 +105,17 @@ def test_bad_namelist_stops_with_reference_message(driver, tmp_path):
     assert r.returncode != 0 and "err found in reading namelist file" in r.stdout
 
 
+@pytest.mark.parametrize("irecord", [0, -5])
+def test_nonpositive_irecord_is_a_namelist_error(driver, tmp_path, irecord):
+    """MOD(istp, irecord) has no value for irecord <= 0: the driver stops with
+    a namelist error before touching the device instead of dividing by zero."""
+    write_nl(str(tmp_path), irecord=irecord)
+    r = run(driver, str(tmp_path))
+    assert r.returncode not in (0, -8), r.stdout + r.stderr  # -8: SIGFPE
+    assert "err found in reading namelist file" in r.stdout
+    assert "irecord" in r.stderr
+
+
 def test_grid_from_file_is_refused_like_reference(driver, tmp_path):
     write_nl(str(tmp_path), jphgr=0)
     r = run(driver, str(tmp_path))

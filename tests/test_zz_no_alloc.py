@@ -38,8 +38,9 @@ def test_noalloc_checksums_match_allocating_entry_point_twice():
         assert st == 0, "call %d status %d" % (call, st)
         torch.cuda.synchronize()
         got = out.cpu().numpy()
-        np.testing.assert_allclose(got, ref, rtol=1e-15, atol=0.0,
-                                   err_msg="call %d" % call)
+        # same fixed reduction order as nemo_checksums: the same bits
+        np.testing.assert_array_equal(got.view(np.int64), ref.view(np.int64),
+                                      err_msg="call %d" % call)
         assert np.all(got > 0)
 
 
