@@ -45,7 +45,7 @@ EXPORTED = [
     "nemo_sur_get_norm", "nemo_sur_predict", "nemo_sur_loss_grad", "nemo_sur_adamw",
     "nemo_sur_train_step", "nemo_sur_pack_ens", "nemo_sur_advance_ens", "nemo_ens_compare",
     "nemo_hyb_default_config", "nemo_hyb_run", "nemo_conv3x3_fwd", "nemo_conv3x3_wgrad",
-    "nemo_conv3x3_fwd_variant", "nemo_conv3x3_wgrad_variant",
+    "nemo_conv3x3_fwd_variant", "nemo_conv3x3_wgrad_variant", "nemo_debug_fail_alloc",
     "cuda_setup_model_params_", "cuda_initialise_grid_", "cuda_continuity_", "cuda_momentum_",
     "cuda_boundary_conditions_", "cuda_next_", "cuda_retrieve_grid_constants_",
     "cuda_retrieve_results_", "cuda_finalise_", "nemo_compat_last_status", "nemo_compat_context",
@@ -147,6 +147,7 @@ def load(strict=False):
     L.nemo_checksums_noalloc.argtypes = [P(ctypes.c_void_p), ip, ip, ip, ctypes.c_long,
                                          ctypes.c_void_p, ctypes.c_void_p]
     L.nemo_autotune.argtypes = [vp, ip, P(Schedule), P(dp)]
+    L.nemo_debug_fail_alloc.argtypes = [ip]
     L.nemo_ens_generate.argtypes = [ctypes.c_uint64, ip, ip, ip, dp, P(Member)]
     L.nemo_ens_create.argtypes = [P(Params), P(Member), ip, P(vp)]
     L.nemo_ens_destroy.argtypes = [vp]
@@ -333,20 +334,57 @@ class Model:
             assert x.shape == field_shape(f, self.jpi, self.jpj), (f, x.shape)
         check(self.lib.nemo_set_state(self.h, *[_dptr(x) for x in a]), "nemo_set_state")
 
+    # parameters that change the arithmetic of a step; a checkpoint records
+    # them and a restart into a model that differs in any of them is refused
+    _CHECKPOINT_PARAMS = ("dx", "dy", "dep_const", "rdt", "cbfr", "visc", "amp_tide",
+                          "tide_phase", "lat", "nbump", "seed", "bump_amp", "bump_wmin",
+                          "bump_wmax", "hmin", "hmax")
+
+    def _geometry_digest(self):
+        """SHA-256 over the device depths ht, hu, hv and the arrays of the last
+        set_grid call (mask, scale factors, latitudes), if any."""
+        import hashlib
+        h = hashlib.sha256()
+        for f in (HT, HU, HV):
+            h.update(np.ascontiguousarray(self.field(f)).tobytes())
+        h.update(getattr(self, "_grid_digest", b""))
+        return h.hexdigest()
+
     def save_checkpoint(self, path, istp):
         """Write the state after step istp (sshn, un, vn in Fortran bounds,
-        FP64) to an .npz file.  Every step derives the rest of the state from
-        these three fields, so load_checkpoint followed by steps istp+1... gives
-        the uninterrupted run bit for bit (the reference writes no restart
-        files; this is the build's own format)."""
-        np.savez(path, istp=np.int64(istp), jpi=np.int64(self.jpi), jpj=np.int64(self.jpj),
-                 sshn=self.field(SSHN), un=self.field(UN), vn=self.field(VN))
+        FP64) to an .npz file, with the model parameters and a digest of the
+        geometry (depths and any set_grid arrays).  Every step derives the rest
+        of the state from these three fields, so load_checkpoint followed by
+        steps istp+1... gives the uninterrupted run bit for bit (the reference
+        writes no restart files; this is the build's own format).  The file is
+        written beside `path` first and renamed over it, so a crash during the
+        write leaves any previous checkpoint at `path` intact."""
+        params = np.array([float(getattr(self.p, k)) for k in self._CHECKPOINT_PARAMS])
+        tmp = path + ".tmp"
+        with open(tmp, "wb") as fh:
+            np.savez(fh, istp=np.int64(istp), jpi=np.int64(self.jpi), jpj=np.int64(self.jpj),
+                     params=params, param_names=np.array(self._CHECKPOINT_PARAMS),
+                     geometry=np.array(self._geometry_digest()),
+                     sshn=self.field(SSHN), un=self.field(UN), vn=self.field(VN))
+            fh.flush()
+            os.fsync(fh.fileno())
+        os.replace(tmp, path)
 
     def load_checkpoint(self, path):
-        """Restore a save_checkpoint file; returns the step it was taken after."""
+        """Restore a save_checkpoint file; returns the step it was taken after.
+        Raises ValueError when the file was written by a model with another
+        grid size, other parameters or another geometry."""
         with np.load(path) as z:
             if int(z["jpi"]) != self.jpi or int(z["jpj"]) != self.jpj:
                 raise ValueError("checkpoint is for a %dx%d grid" % (int(z["jpi"]), int(z["jpj"])))
+            names = [str(x) for x in z["param_names"]]
+            mine = {k: float(getattr(self.p, k)) for k in self._CHECKPOINT_PARAMS}
+            for k, v in zip(names, z["params"]):
+                if k not in mine or mine[k] != float(v):
+                    raise ValueError("checkpoint parameter %s = %r, this model has %r"
+                                     % (k, float(v), mine.get(k)))
+            if str(z["geometry"]) != self._geometry_digest():
+                raise ValueError("checkpoint was written on another geometry (depths or grid arrays)")
             self.set_state(z["sshn"], z["un"], z["vn"])
             return int(z["istp"])
 
@@ -363,6 +401,11 @@ class Model:
         g = Grid(p.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
                  *[ctypes.POINTER(ctypes.c_double)() if x is None else _dptr(x) for x in a])
         check(self.lib.nemo_set_grid(self.h, ctypes.byref(g)), "nemo_set_grid")
+        import hashlib
+        h = hashlib.sha256(p.tobytes())
+        for x in a[:8]:
+            h.update(x.tobytes())
+        self._grid_digest = h.digest()
 
     def autotune(self, steps=5):
         sch = Schedule()

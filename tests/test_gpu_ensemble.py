@@ -64,6 +64,65 @@ def test_strict_ensemble_members_match_oracle_bitwise(nb, oracle_mod, graph, sch
             assert list(ck[k]) == tree
 
 
+# Eight members of the 256-member batched benchmark draw (seed 2026, sides
+# log-uniform in [64, 1024], tidal amplitudes 0.2 x U[0.5, 1.5] m): the two
+# largest (1012 x 1643 and 919 x 1255 T-points: many strips and row blocks,
+# the persistent loop's later work items), 687 x 967, two mid-sized, a
+# 65-column member (three strips for 65 columns) and the two smallest.  All
+# eight stay finite over the 500 steps (checked on the oracle).
+CONFIG2_PICK = (89, 207, 20, 78, 52, 106, 165, 228)
+
+
+def test_config2_members_match_oracle_every_record(nb, oracle_mod):
+    """Config-2-sized members through 500 steps with a record every 100: the
+    strict build is bit-identical to the oracle per member (fields and
+    tree-order checksums) on its default schedule and on a 4-warp, 32-row one;
+    the default build stays within 1e-12 relative max-norm on both."""
+    import os
+    allm = nb.generate_members(2026, 256, 64, 1024, amp_scale=0.2)
+    members = [allm[k] for k in CONFIG2_PICK]
+    assert max(max(m.jpi, m.jpj) for m in members) >= 900
+    runs = []
+    for strict in (True, False):
+        for sched in (None, (4, None, 32, 1)):
+            e = nb.Ensemble(members, strict=strict, **COMMON)
+            if sched is not None:
+                e.set_schedule(*sched)
+                sched = e.get_schedule()
+            runs.append((strict, sched, e))
+    oracle_mod.set_threads(max(1, len(os.sched_getaffinity(0))))
+    orc = [oracle_member(oracle_mod, m) for m in members]
+    worst = 0.0
+    try:
+        for rec in range(5):
+            istp0 = 1 + 100 * rec
+            for _, _, e in runs:
+                e.step_n(istp0, 100)
+            for o in orc:
+                o.run(istp0, 100)
+            cks = [e.checksums() for _, _, e in runs]
+            for k, o in enumerate(orc):
+                refs = [o.field(fid) for _, fid in STATE]
+                tree = [o.checksum(f, "tree") for f in (oracle_mod.SSHN, oracle_mod.UN, oracle_mod.VN)]
+                assert np.all(np.isfinite(tree))
+                for (strict, sched, e), ck in zip(runs, cks):
+                    where = "step %d member %d (%dx%d) strict=%s sched=%s" % (
+                        istp0 + 99, CONFIG2_PICK[k], members[k].jpi, members[k].jpj, strict, sched)
+                    for (name, fid), ref in zip(STATE, refs):
+                        got = e.field(k, fid)
+                        if strict:
+                            np.testing.assert_array_equal(bits(got), bits(ref), err_msg=where + " " + name)
+                        else:
+                            err = relerr(got, ref)
+                            worst = max(worst, err)
+                            assert err <= TOL, "%s %s rel err %.3e" % (where, name, err)
+                    if strict:
+                        assert list(ck[k]) == tree, where
+    finally:
+        oracle_mod.set_threads(1)
+    print("config 2 members, 500 steps: worst default-build relative max-norm error %.3e" % worst)
+
+
 def test_default_ensemble_matches_single_grids(nb):
     members = nb.generate_members(11, 10, side_min=30, side_max=300, amp_scale=0.2)
     common = nb.default_params(**COMMON)

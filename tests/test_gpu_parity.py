@@ -273,31 +273,53 @@ def test_schedule_does_not_change_results(nb, sched):
                 assert relerr(a, b) <= TOL, name
 
 
-def test_config1_size_against_openmp_oracle(nb, oracle_mod):
-    """4096^2 with 32 seeded bumps: strict bitwise and default within tolerance."""
-    kw = dict(jpi=4096, jpj=4096, rdt=20.0, cbfr=0.00015, visc=0.1, amp_tide=0.2, nbump=32,
-              seed=1234, bump_amp=40.0, bump_wmin=20e3, bump_wmax=200e3, hmin=10.0)
+CONFIG1 = dict(jpi=4096, jpj=4096, rdt=20.0, cbfr=0.00015, visc=0.1, amp_tide=0.2, nbump=32,
+               seed=1234, bump_amp=40.0, bump_wmin=20e3, bump_wmax=200e3, hmin=10.0)
+
+
+def test_config1_full_run_every_record_against_openmp_oracle(nb, oracle_mod):
+    """The benchmarked configuration end to end: 4096^2, 32 seeded bumps
+    (seed 1234), 1000 steps from rest, a record every 100 steps
+    (original/nemolite2d.f90:74-85, :384).  At every record the full sshn,
+    un and vn fields of the strict build equal the oracle's bit for bit and
+    its checksums equal the oracle's tree-order sums; the default build, on
+    the schedule the bench runs, stays within 1e-12 relative max-norm and its
+    checksums within 1e-11 of the oracle's sequential sums."""
     import os
     oracle_mod.set_threads(max(1, len(os.sched_getaffinity(0))))
-    o = oracle_mod.Model(**kw)
-    o.run(1, 12)
-    oracle_mod.set_threads(1)
-    s = nb.Model(strict=True, **kw)
-    s.step_n(1, 12)
-    d = nb.Model(strict=False, **kw)
-    d.step_n(1, 12)
-    for name, fid in STATE:
-        ref = o.field(fid)
-        np.testing.assert_array_equal(bits(s.field(fid)), bits(ref), err_msg=name)
-        assert relerr(d.field(fid), ref) <= TOL
-    del s
+    o = oracle_mod.Model(**CONFIG1)
+    s = nb.Model(strict=True, **CONFIG1)
+    d = nb.Model(strict=False, **CONFIG1)
+    worst = {}
+    try:
+        for rec in range(10):
+            istp0 = 1 + 100 * rec
+            s.step_n(istp0, 100)
+            d.step_n(istp0, 100)
+            o.run(istp0, 100)
+            step = istp0 + 99
+            for name, fid in STATE:
+                ref = o.field(fid)
+                np.testing.assert_array_equal(bits(s.field(fid)), bits(ref),
+                                              err_msg="step %d %s" % (step, name))
+                e = relerr(d.field(fid), ref)
+                worst[name] = max(worst.get(name, 0.0), e)
+                assert e <= TOL, "default build step %d %s rel err %.3e" % (step, name, e)
+            cs, cd = s.checksums(), d.checksums()
+            tree = [o.checksum(f, "tree") for f in (oracle_mod.SSHN, oracle_mod.UN, oracle_mod.VN)]
+            seq = [o.checksum(f, "seq") for f in (oracle_mod.SSHN, oracle_mod.UN, oracle_mod.VN)]
+            assert list(cs) == tree, "step %d strict checksums" % step
+            np.testing.assert_allclose(cd, seq, rtol=1e-11, err_msg="step %d" % step)
+            assert np.all(np.isfinite(cs)) and np.all(cs > 0)
+    finally:
+        oracle_mod.set_threads(1)
+    print("config 1, 1000 steps: worst default-build relative max-norm error per field "
+          + ", ".join("%s %.3e" % kv for kv in worst.items()))
 
 
 def test_long_run_properties_at_4096(nb):
     """1000 fused steps at 4096^2: finite, walls exactly zero, clamped row exact."""
-    kw = dict(jpi=4096, jpj=4096, rdt=20.0, cbfr=0.00015, visc=0.1, amp_tide=0.2, nbump=32,
-              seed=1234, bump_amp=40.0, bump_wmin=20e3, bump_wmax=200e3, hmin=10.0)
-    m = nb.Model(strict=False, **kw)
+    m = nb.Model(strict=False, **CONFIG1)
     m.step_n(1, 1000)
     ck = m.checksums()
     assert np.all(np.isfinite(ck)) and np.all(ck > 0)
@@ -438,22 +460,71 @@ def test_default_build_general_grid_within_tolerance(nb, oracle_mod):
             assert relerr(m.field(fid), o.field(fid)) <= TOL, (rec, name)
 
 
-def test_checkpoint_restart_is_bit_exact(nb, tmp_path):
+def _advance(m, istp0, n, path):
+    if path == "fused":
+        m.step_n(istp0, n)
+        return
+    for istp in range(istp0, istp0 + n):
+        m.continuity()
+        m.momentum()
+        m.bc(istp * m.p.rdt)
+        m.next()
+
+
+@pytest.mark.parametrize("strict", [True, False])
+@pytest.mark.parametrize("path", ["fused", "routines"])
+@pytest.mark.parametrize("grid", ["built-in", "set_grid"])
+def test_checkpoint_restart_is_bit_exact(nb, tmp_path, strict, path, grid):
     """save_checkpoint after step 60, restart in a fresh context, steps 61..120:
-    the same bits as the uninterrupted run (default build, fused path)."""
+    the same bits as the uninterrupted run, in both builds, through the fused
+    path and through the continuity/momentum/bc/next calls, on the built-in
+    grid and on a general grid."""
+    from gridcases import NAMES, random_grid
     kw = dict(jpi=150, jpj=97, rdt=20.0, cbfr=0.00015, visc=0.1, amp_tide=0.4, nbump=6,
               seed=8, bump_amp=20.0, bump_wmin=5e3, bump_wmax=40e3)
-    a = nb.Model(strict=False, **kw)
-    a.step_n(1, 60)
-    path = str(tmp_path / "ck.npz")
-    a.save_checkpoint(path, 60)
-    a.step_n(61, 60)
-    b = nb.Model(strict=False, **kw)
-    istp = b.load_checkpoint(path)
+    if grid == "set_grid":
+        kw["rdt"] = 10.0
+        pt, g = random_grid(4, 150, 97)
+
+    def make(**over):
+        m = nb.Model(strict=strict, **dict(kw, **over))
+        if grid == "set_grid":
+            m.set_grid(pt, *[g[n] for n in NAMES])
+        return m
+
+    a = make()
+    _advance(a, 1, 60, path)
+    ck = str(tmp_path / "ck.npz")
+    a.save_checkpoint(ck, 60)
+    assert not (tmp_path / "ck.npz.tmp").exists()
+    _advance(a, 61, 60, path)
+    b = make()
+    istp = b.load_checkpoint(ck)
     assert istp == 60
-    b.step_n(istp + 1, 60)
+    _advance(b, istp + 1, 60, path)
     for name, fid in STATE:
         np.testing.assert_array_equal(bits(a.field(fid)), bits(b.field(fid)), err_msg=name)
-    c = nb.Model(strict=False, **dict(kw, jpi=151))
+
+
+def test_checkpoint_refuses_another_model(nb, tmp_path):
+    """A checkpoint restarts only a model of the same size, parameters and
+    geometry; anything else raises instead of silently computing another run."""
+    from gridcases import NAMES, random_grid
+    kw = dict(jpi=150, jpj=97, rdt=20.0, cbfr=0.00015, visc=0.1, amp_tide=0.4, nbump=6,
+              seed=8, bump_amp=20.0, bump_wmin=5e3, bump_wmax=40e3)
+    a = nb.Model(**kw)
+    a.step_n(1, 10)
+    ck = str(tmp_path / "ck.npz")
+    a.save_checkpoint(ck, 10)
+    for over in (dict(jpi=151), dict(seed=9), dict(rdt=10.0), dict(visc=0.2), dict(amp_tide=0.3),
+                 dict(cbfr=0.001), dict(tide_phase=0.1)):
+        c = nb.Model(**dict(kw, **over))
+        with pytest.raises(ValueError):
+            c.load_checkpoint(ck)
+    pt, g = random_grid(4, 150, 97)
+    d = nb.Model(**kw)
+    d.set_grid(pt, *[g[n] for n in NAMES])
     with pytest.raises(ValueError):
-        c.load_checkpoint(path)
+        d.load_checkpoint(ck)
+    e = nb.Model(**kw)
+    assert e.load_checkpoint(ck) == 10
