@@ -17,8 +17,17 @@ checksums; two contexts alternate so that one's transfers overlap the
 other's steps.  `--impl reference` times the CPU restatement of the reference
 (oracle/, OpenMP over all host cores) on the same grid.
 
+The default line also carries, measured on the same GPU after the timed
+region: `ensemble` (the 256-member batched configuration, its 500-step run
+from rest, graph-replayed persistent launches, with its own roofline and
+clocks), `conv` (the surrogate's forward and weight-gradient convolution
+kernels at 64 x 256 x 256, TFLOP/s against the measured BF16 peak) and
+`cpu_baseline` (the oracle on the host cores: OpenMP over every core and
+serial on one pinned core at the bench grid, and config 0 both ways).
+
 Multi-GPU (torchrun): independent replicas, one per GPU (the stepper does not
-shard); value = all ranks' cell-steps / max-over-ranks time.
+shard); value = all ranks' cell-steps / max-over-ranks time.  The ensemble,
+convolution and CPU legs run at N = 1 only.
 """
 import argparse
 import json
@@ -41,9 +50,11 @@ WORKLOAD = dict(jpi=N, jpj=N, dx=1000.0, dy=1000.0, dep_const=100.0, rdt=20.0, c
                 bump_wmin=20e3, bump_wmax=200e3, hmin=10.0)
 BYTES_PER_CELL_STEP = 72  # read sshn, un, vn, ht, hu, hv; write sshn, un, vn (FP64)
 METRIC = "cell-steps/s at 4096^2 FP64 (% of HBM peak)"
-CONFIG = {"workload": "plain fused FP64 stepper, one 4096x4096 instance per GPU, seeded "
-                      "32-bump bathymetry, 1000 steps from rest, checksums every 100 steps",
-          "grid": [N, N], "steps_per_bench_step": STEPS_PER_ITER, "dtype": "f64",
+CONFIG = {"workload": "plain FP64 stepper, one 4096x4096 instance per GPU, seeded 32-bump "
+                      "bathymetry (seed 1234), 1000 steps from rest, checksums every 100 steps, "
+                      "tidal amplitude 0.2 m (the reference's hard-coded value; 1 m diverges "
+                      "in the reference scheme)",
+          "grid": [N, N], "dtype": "f64",
           "l2": "inputs larger than L2 (1.2 GB touched per model step)"}
 
 
@@ -55,9 +66,13 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true",
+                    help="leave out the 256-member ensemble leg of the default line")
+    ap.add_argument("--no-conv", action="store_true",
+                    help="leave out the convolution leg of the default line")
     ap.add_argument("--schedule", type=str, default="",
                     help="warps,occupancy,rows of the fused kernel (default: tuned)")
-    ap.add_argument("--workload", choices=["grid", "ensemble", "surrogate", "hybrid", "conv"],
+    ap.add_argument("--workload", choices=["grid", "ensemble", "surrogate", "hybrid", "conv", "general"],
                     default="grid",
                     help="grid: the 4096^2 line (default); ensemble: the 256-member batch")
     ap.add_argument("--hyb-steps", type=int, default=5000)
@@ -75,6 +90,13 @@ def parse():
     ap.add_argument("--train-iters", type=int, default=6000)
     ap.add_argument("--nblocks", type=int, default=2, help="residual blocks of the hybrid's network")
     ap.add_argument("--k", type=int, default=10, help="model steps per surrogate call (hybrid)")
+    ap.add_argument("--anchor", type=int, default=100, help="FP64 re-anchor interval (hybrid)")
+    ap.add_argument("--tol", type=float, default=0.01, help="fallback tolerance (hybrid)")
+    ap.add_argument("--quarantine", type=float, default=0.05, help="quarantine threshold (hybrid)")
+    ap.add_argument("--sweep", type=str, default="",
+                    help="hybrid points anchor:tol:quarantine,... run after one training")
+    ap.add_argument("--repeats", type=int, default=1, help="hybrid runs per point (median reported)")
+    ap.add_argument("--candidates", type=int, default=128, help="hybrid member candidates")
     ap.add_argument("--n", type=int, default=N,
                     help="grid side (profiling of smaller cases only; the bench line is 4096)")
     return ap.parse_args()
@@ -138,12 +160,13 @@ class ClockSampler:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", "bench_clocks_%d.csv" % index)
+        self.path = None
 
     def start(self):
-        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        import tempfile
         try:
-            self.fh = open(self.path, "w")
+            fd, self.path = tempfile.mkstemp(prefix="nemo_clocks_%d_" % self.index, suffix=".csv")
+            self.fh = os.fdopen(fd, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
                  "--format=csv,noheader,nounits", "-lms", "200"],
@@ -175,34 +198,87 @@ class ClockSampler:
                 for k, n in enumerate(names):
                     if f[5 + k].lower() == "active":
                         reasons.add(n)
+        try:
+            os.remove(self.path)
+        except OSError:
+            pass
         if not sm:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "samples": len(sm),
                 "reasons": sorted(reasons)}
 
 
-def cpu_oracle_rate(budget_s=12.0, max_steps=8):
-    """Oracle (OpenMP, all host cores) on the bench grid: (cell-steps/s, steps, threads)."""
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def _timed_oracle_steps(m, istp0, n):
+    t0 = time.perf_counter()
+    m.run(istp0, n)
+    return time.perf_counter() - t0
+
+
+def cpu_baselines(omp_steps=20, serial_steps=20):
+    """The oracle (the CPU restatement of original/nemolite2d.f90) on the
+    host cores: config 1 (the bench grid) with OpenMP over every core and
+    serial on one pinned core (the reference's own benchmark mode, one
+    process on one core), and config 0 (128^2, 2000 steps) both ways.
+    One untimed step first; the serial runs continue the OpenMP run's state
+    (the arithmetic per step does not depend on the values)."""
     from oracle import oracle
     th = host_cores()
-    oracle.set_threads(th)
-    okw = dict(WORKLOAD)
-    m = oracle.Model(**okw)
-    t0 = time.perf_counter()
-    m.step(1)
-    t1 = time.perf_counter()
-    per = t1 - t0
-    n = max(1, min(max_steps, int(budget_s / max(per, 1e-3))))
-    t0 = time.perf_counter()
-    m.run(2, n)
-    dt = time.perf_counter() - t0
-    m.close()
-    oracle.set_threads(1)
-    return cells() * n / dt, n, th
+    keep = os.sched_getaffinity(0)
+    pin = max(keep)
+    out = {}
+    try:
+        oracle.set_threads(th)
+        m = oracle.Model(**WORKLOAD)
+        m.run(1, 1)
+        dt = _timed_oracle_steps(m, 2, omp_steps)
+        out["omp"] = (cells() * omp_steps / dt, dt)
+        oracle.set_threads(1)
+        os.sched_setaffinity(0, {pin})
+        dt = _timed_oracle_steps(m, 2 + omp_steps, serial_steps)
+        out["serial"] = (cells() * serial_steps / dt, dt)
+        m.close()
+        c0 = dict(jpi=128, jpj=128, rdt=20.0, cbfr=0.00015, visc=0.1, amp_tide=0.2)
+        m = oracle.Model(**c0)
+        out["c0_serial"] = 128 * 128 * 2000 / _timed_oracle_steps(m, 1, 2000)
+        m.close()
+        os.sched_setaffinity(0, keep)
+        oracle.set_threads(th)
+        m = oracle.Model(**c0)
+        out["c0_omp"] = 128 * 128 * 2000 / _timed_oracle_steps(m, 1, 2000)
+        m.close()
+    finally:
+        os.sched_setaffinity(0, keep)
+        oracle.set_threads(1)
+    return {"value": out["omp"][0], "unit": "cell-steps/s", "cores": th, "kind": "port",
+            "sample": "%d model steps (2..%d) of the 4096^2 bench grid, oracle port of "
+                      "original/nemolite2d.f90, OpenMP %d threads" % (omp_steps, omp_steps + 1, th),
+            "cpu_model": cpu_model(),
+            "serial": {"value": out["serial"][0], "cores": 1, "pinned_core": pin,
+                       "steps": serial_steps, "seconds": out["serial"][1],
+                       "sample": "steps %d..%d of the same run on one pinned core (the "
+                                 "reference's benchmark mode)" % (2 + omp_steps,
+                                                                  1 + omp_steps + serial_steps)},
+            "config0": {"grid": [128, 128], "steps": 2000, "serial": out["c0_serial"],
+                        "openmp": out["c0_omp"], "openmp_cores": th,
+                        "sample": "the whole 2000-step 128^2 run from rest, amplitude 0.2 m"}}
 
 
 def run_reference(args, rank):
-    """CPU restatement of original/nemolite2d.f90 (the reference's CPU path)."""
+    """CPU restatement of original/nemolite2d.f90 (the reference's CPU path),
+    OpenMP over every host core, on the bench's workload and config: `warmup`
+    untimed model steps, then `steps` timed model steps (each bench step of
+    this arm is one model step; the metric, cell-steps/s, is the same)."""
     if rank != 0:
         return
     from oracle import oracle
@@ -226,47 +302,54 @@ def run_reference(args, rank):
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1000.0 * dt / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": dict(CONFIG, bench_step="1 model time step"),
+            "config": dict(CONFIG), "bench_step": "1 model time step",
             "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": th, "kind": "port",
-                             "sample": sample},
+                             "sample": sample, "cpu_model": cpu_model()},
             "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
-def run_ensemble(args):
-    """256 members (sides log-uniform 64..1024, aspect 0.5..2, seeded 50-150 m
-    bathymetry, random tidal phase), 500 steps per bench step split in records
-    of 100 with per-member checksums, one persistent launch per step replayed
-    from a CUDA graph, schedule from the autotuner.  Tidal amplitudes are the
-    reference's 0.2 m scaled by U[0.5, 1.5]; the scheme diverges for the 1 m
-    class of amplitudes with a random phase, and throughput does not depend on
-    the amplitude."""
+ENS_METRIC = "ensemble cell-steps/s (256 members, 500 steps, FP64)"
+
+
+def ensemble_leg(device, warmup, reps, tune_steps=3):
+    """The batched configuration: 256 members of the recipe (seed 2026, sides
+    log-uniform 64..1024, aspect 0.5..2, seeded 50-150 m bathymetry, random
+    tidal phase), the 500-step run from rest with per-member checksums every
+    100 steps, one persistent launch per step replayed from a CUDA graph,
+    schedule from the autotuner; `reps` timed runs after `warmup` untimed
+    ones.  Tidal amplitudes are the reference's 0.2 m scaled by U[0.5, 1.5]
+    (the 1 m class diverges with a random phase; throughput does not depend
+    on the amplitude)."""
+    import numpy as np
     import torch
     import nemo_b200
-    torch.cuda.set_device(0)
     stream = torch.cuda.Stream()
     members = nemo_b200.generate_members(2026, 256, 64, 1024, amp_scale=0.2)
     common = nemo_b200.default_params(dx=1000.0, dy=1000.0, rdt=20.0, cbfr=0.00015, visc=0.1,
-                                      stream=stream.cuda_stream, device=0)
+                                      stream=stream.cuda_stream, device=device)
     e = nemo_b200.Ensemble(members, common=common)
     nmem, ncell = e.info()
-    sched, tuned_ms = e.autotune(steps=3)
+    sched, tuned_ms = e.autotune(steps=tune_steps)
     rest = [(np.zeros((m.jpj, m.jpi)), np.zeros((m.jpj, m.jpi + 1)), np.zeros((m.jpj + 1, m.jpi)))
             for m in members]
-    for w in range(args.warmup):
+    for w in range(warmup):
         for r in range(5):
             e.step_n(1 + 100 * r, 100)
-        e.checksums()
+            e.checksums()
     for k, st in enumerate(rest):
         e.set_state(k, *st)
     torch.cuda.synchronize()
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
-    clocks = ClockSampler(0)
+    clocks = ClockSampler(device)
     clocks.start()
     t0.record(stream)
-    for it in range(args.steps):
+    for it in range(reps):
+        if it:
+            for k, st in enumerate(rest):
+                e.set_state(k, *st)
         for r in range(5):
             e.step_n(1 + 100 * r, 100)
             ck = e.checksums()
@@ -274,23 +357,63 @@ def run_ensemble(args):
     torch.cuda.synchronize()
     clk = clocks.stop()
     ms = t0.elapsed_time(t1)
-    value = ncell * 500 * args.steps / (ms / 1e3)
-    finite = int(np.isfinite(ck).all(axis=1).sum())
-    line = {"metric": "ensemble cell-steps/s (256 members, 500 steps, FP64)", "value": value,
-            "unit": "cell-steps/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "batched ensemble: %d members, %d cells, 500 steps, checksums "
-                                   "per member every 100 steps" % (nmem, ncell),
-                       "schedule": {"warps": sched[0], "occupancy": sched[1], "rows": sched[2],
-                                    "order": sched[3]},
-                       "graph": True, "l2": "inputs larger than L2"},
-            "roofline": {"bound": "hbm", "achieved": BYTES_PER_CELL_STEP * value / 1e9,
-                         "peak": load_peaks()[0], "unit": "GB/s",
-                         "frac": BYTES_PER_CELL_STEP * value / 1e9 / load_peaks()[0]},
-            "finite_members": finite, "gpu_launches": args.steps * (500 + 10), "clocks": clk}
-    print(json.dumps(line), flush=True)
     e.close()
+    value = ncell * 500 * reps / (ms / 1e3)
+    peak = load_peaks()
+    return {"metric": ENS_METRIC, "value": value, "unit": "cell-steps/s", "members": nmem,
+            "cells": ncell, "steps": 500, "reps": reps, "ms_per_rep": ms / reps,
+            "schedule": {"warps": sched[0], "occupancy": sched[1], "rows": sched[2],
+                         "order": sched[3]},
+            "graph": True, "finite_members": int(np.isfinite(ck).all(axis=1).sum()),
+            "roofline": {"bound": "hbm", "kernel": "k_ens_step",
+                         "achieved": BYTES_PER_CELL_STEP * value / 1e9, "peak": peak[0],
+                         "unit": "GB/s", "frac": BYTES_PER_CELL_STEP * value / 1e9 / peak[0],
+                         "peak_source": peak[1]},
+            "gpu_launches": reps * (500 + 10), "clocks": clk}
+
+
+def conv_leg(device, batch=64, reps=200, warm=3):
+    """The surrogate's two convolution kernels alone (64 -> 64 channels, 3x3,
+    batch x 256 x 256 BF16 NHWC, FP32 accumulation): forward with the bias +
+    ReLU epilogue and weight gradient with the bias gradient, `reps` timed
+    launches each."""
+    import torch
+    import nemo_b200
+    from nemo_b200 import surrogate as sm
+    stream = torch.cuda.Stream()
+    S = 256
+    clocks = ClockSampler(device)
+    clocks.start()
+    rates = conv_kernel_rates(sm, nemo_b200.load(False), batch, S, S, reps, stream.cuda_stream,
+                              warm=warm)
+    clk = clocks.stop()
+    flop = 2 * 9 * 64 * 64 * batch * S * S
+    peak = load_peaks_tensor()
+    out = {"batch": batch, "grid": [S, S], "flop_per_launch": flop, "launches": reps,
+           "peak": peak[0], "peak_source": peak[1], "unit": "TFLOP/s", "clocks": clk,
+           "gpu_launches": 2 * (reps + warm)}
+    for k, name in (("fwd", "k_conv_fwd_tri"), ("wgrad", "k_conv_wgrad_tri")):
+        tf = flop / rates[k] / 1e12
+        out[k] = {"kernel": name, "tflops": tf, "frac": tf / peak[0], "us": rates[k] * 1e6}
+    return out
+
+
+def run_ensemble(args):
+    """The batched configuration alone (see ensemble_leg): one bench step is
+    the 500-step run of all 256 members."""
+    import torch
+    torch.cuda.set_device(0)
+    leg = ensemble_leg(0, args.warmup, args.steps)
+    line = {"metric": ENS_METRIC, "value": leg["value"], "unit": "cell-steps/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": leg["ms_per_rep"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": "batched ensemble: %d members, %d cells, 500 steps, checksums "
+                                   "per member every 100 steps" % (leg["members"], leg["cells"]),
+                       "schedule": leg["schedule"], "graph": True, "l2": "inputs larger than L2"},
+            "roofline": leg["roofline"], "finite_members": leg["finite_members"],
+            "gpu_launches": leg["gpu_launches"], "clocks": leg["clocks"]}
+    print(json.dumps(line), flush=True)
 
 
 def conv_kernel_rates(sur_mod, lib, n, h, w, reps, stream, warm=3):
@@ -494,9 +617,10 @@ def run_hybrid(args):
     # end, the rule the training data follow) are the workload
     stream = torch.cuda.Stream()
     common = dict(tr.COMMON, stream=stream.cuda_stream, device=0)
-    cands = tr.square_members(4242, 64, side, 0.2)
-    ok = tr.bounded_members(cands, nsteps, common)
+    cands = tr.square_members(4242, args.candidates, side, 0.2)
+    ok = tr.bounded_members(cands, nsteps, common, want=nm)
     members = [cands[i] for i in ok[:nm]]
+    screened = min(len(cands), 64 * ((ok[nm - 1] // 64) + 1)) if len(ok) >= nm else len(cands)
     nm = len(members)
     plain = nemo_b200.Ensemble(members, **common)
     hyb = nemo_b200.Ensemble(members, **common)
@@ -505,52 +629,173 @@ def run_hybrid(args):
     inf.set_params(params)
     inf.set_norm(*norm)
     cells = nm * side * side
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
-    torch.cuda.synchronize()
-    ev[0].record(stream)
-    plain.step_n(1, nsteps)
-    ev[1].record(stream)
+    rest = [(np.zeros((m.jpj, m.jpi)), np.zeros((m.jpj, m.jpi + 1)), np.zeros((m.jpj + 1, m.jpi)))
+            for m in members]
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        out = fn()
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        return ev[0].elapsed_time(ev[1]) / 1e3, out
+
+    t_plain = []
+    for r in range(args.repeats):
+        if r:
+            for k, st0 in enumerate(rest):
+                plain.set_state(k, *st0)
+        t_plain.append(timed(lambda: plain.step_n(1, nsteps))[0])
     plain.checksums()
+    v_plain = cells * nsteps / statistics.median(t_plain)
+    points = [(args.anchor, args.tol, args.quarantine)]
+    if args.sweep:
+        points = [tuple(float(x) for x in p.split(":")) for p in args.sweep.split(",")]
+    for anchor, tol, quar in points:
+        anchor = int(anchor)
+        runs = []
+        for r in range(args.repeats):
+            for k, st0 in enumerate(rest):
+                hyb.set_state(k, *st0)
+            clocks = ClockSampler(0)
+            clocks.start()
+            t_hyb, st = timed(lambda: sm.hyb_run(inf, hyb, 0, nsteps, k=args.k, anchor=anchor, tol=tol,
+                                                 quarantine=quar))
+            clk = clocks.stop()
+            err = sm.ens_compare(hyb, plain)
+            finite = np.isfinite(err).all(axis=1)
+            ef = err[finite] if finite.any() else np.full((1, 3), np.nan)
+            runs.append({"seconds": t_hyb, "hybrid_over_plain": (cells * nsteps / t_hyb) / v_plain,
+                         "stats": st, "clocks": clk,
+                         "err": {"ssh_max": float(ef[:, 0].max()), "ssh_mean": float(ef[:, 0].mean()),
+                                 "u_max": float(ef[:, 1].max()), "v_max": float(ef[:, 2].max()),
+                                 "u_mean": float(ef[:, 1].mean()), "v_mean": float(ef[:, 2].mean()),
+                                 "members_nonfinite": int((~finite).sum())}})
+        med = sorted(runs, key=lambda x: x["seconds"])[len(runs) // 2]
+        st = med["stats"]
+        v_hyb = cells * nsteps / med["seconds"]
+        line = {"metric": "hybrid vs plain ensemble cell-steps/s (32 x 2048^2, 5000 steps, <=1% SSH err)",
+                "value": v_hyb, "unit": "cell-steps/s", "n_gpus": 1, "steps": args.repeats, "warmup": 0,
+                "ms_per_step": med["seconds"] * 1e3, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "bf16+f64", "data": "synthetic",
+                "config": {"workload": "%d members 2048x2048, %d steps, surrogate k=%d, re-anchor %d, "
+                                       "tol %g relative SSH L2 vs shadow FP64 step, quarantine %g"
+                                       % (nm, nsteps, args.k, anchor, tol, quar),
+                           "anchor": anchor, "tol": tol, "quarantine": quar, "k": args.k,
+                           "candidates": len(cands), "candidates_screened": screened,
+                           "screened_out": screened - len(ok),
+                           "patch": P, "nblocks": args.nblocks, "train_side": ts,
+                           "train_steps": args.train_steps, "train_runs": args.train_runs,
+                           "fallback": "per member", "train_input_noise": args.noise,
+                           "finetune_iters": args.finetune_iters,
+                           "train_iters": args.train_iters, "train_s": t_train, "datagen_s": t_gen,
+                           "train_runs_dropped": tr.generate_runs.dropped},
+                "plain_value": v_plain, "plain_seconds": t_plain,
+                "hybrid_over_plain": v_hyb / v_plain,
+                "hybrid_over_plain_runs": [x["hybrid_over_plain"] for x in runs],
+                "hybrid_stats": st,
+                "surrogate_share": st["sur_steps"] / max(1, st["sur_steps"] + st["solver_steps"]),
+                "err_vs_fp64": med["err"], "err_vs_fp64_runs": [x["err"] for x in runs],
+                "loss_first": losses[0], "loss_last": losses[-1], "clocks": med["clocks"],
+                "gpu_launches": st["launches"]}
+        print(json.dumps(line), flush=True)
+
+
+GEN_BYTES_PER_CELL_STEP = 137  # 113 read (6 state/depth + 8 metric fields, int8 mask), 24 written
+
+
+def general_grid(jpi, jpj, seed=3, dx=1000.0, dy=1000.0):
+    """A general grid as nemo_set_grid takes it ((jpj+2, jpi+2) arrays over
+    (0:jpi+1, 0:jpj+1)): open water on parts of all four borders, 64 land
+    islands, scale factors within 15% of dx, dy and latitudes 30-60 degrees
+    varying smoothly per point, one smooth bathymetry of 25-75 m."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    shape = (jpj + 2, jpi + 2)
+    pt = np.ones(shape, np.int32)
+    pt[:, 0] = pt[:, jpi + 1] = pt[0, :] = pt[jpj + 1, :] = 0
+    pt[0, jpi // 8: jpi // 2] = -1
+    pt[jpj + 1, jpi // 3: 2 * jpi // 3] = -1
+    pt[jpj // 4: jpj // 2, 0] = -1
+    pt[jpj // 2: 3 * jpj // 4, jpi + 1] = -1
+    for _ in range(64):
+        y0, x0 = int(rng.integers(3, jpj - 40)), int(rng.integers(3, jpi - 40))
+        pt[y0:y0 + int(rng.integers(1, 32)), x0:x0 + int(rng.integers(1, 32))] = 0
+    jj, ji = np.mgrid[0:jpj + 2, 0:jpi + 2].astype(np.float64)
+    pos = {"t": (ji, jj), "u": (ji + 0.5, jj), "v": (ji, jj + 0.5)}
+
+    def smooth(at, amp):
+        kx, ky = rng.uniform(0.5, 2.0, 2)
+        p1, p2 = rng.uniform(0.0, 2.0 * np.pi, 2)
+        x, y = pos[at]
+        return amp * np.sin(2 * np.pi * kx * x / jpi + p1) * np.cos(2 * np.pi * ky * y / jpj + p2)
+
+    g = {}
+    for name, base, at in (("e1t", dx, "t"), ("e2t", dy, "t"), ("e1u", dx, "u"), ("e2u", dy, "u"),
+                           ("e1v", dx, "v"), ("e2v", dy, "v")):
+        g[name] = base * (1.0 + smooth(at, 0.15))
+    g["gphiu"] = 45.0 + smooth("u", 15.0)
+    g["gphiv"] = 45.0 + smooth("v", 15.0)
+    kx, ky = rng.uniform(0.5, 2.0, 2)
+    p1, p2 = rng.uniform(0.0, 2.0 * np.pi, 2)
+    for name, at in (("ht", "t"), ("hu", "u"), ("hv", "v")):
+        x, y = pos[at]
+        g[name] = 50.0 + 25.0 * np.sin(2 * np.pi * kx * x / jpi + p1) * np.cos(2 * np.pi * ky * y / jpj + p2)
+    return pt, g
+
+
+def run_general(args):
+    """The fused step on a general grid (nemo_set_grid) at 4096^2: every step
+    is the general kernel plus the Flather chains; one bench step = 100 model
+    steps + checksums; `steps` timed after `warmup`, from rest."""
+    import numpy as np
+    import torch
+    import nemo_b200
+    torch.cuda.set_device(0)
+    n = args.n
+    stream = torch.cuda.Stream()
+    m = nemo_b200.Model(strict=False, stream=stream.cuda_stream, device=0, jpi=n, jpj=n, rdt=10.0,
+                        cbfr=0.00015, visc=0.1, amp_tide=0.3)
+    pt, g = general_grid(n, n)
+    names = ("e1t", "e2t", "e1u", "e2u", "e1v", "e2v", "gphiu", "gphiv", "ht", "hu", "hv")
+    m.set_grid(pt, *[g[k] for k in names])
+    del g
+    rest = (np.zeros((n, n)), np.zeros((n, n + 1)), np.zeros((n + 1, n)))
+    for w in range(args.warmup):
+        m.step_n(1 + 100 * w, 100)
+        m.checksums()
+    m.set_state(*rest)
     torch.cuda.synchronize()
-    t_plain = ev[0].elapsed_time(ev[1]) / 1e3
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
     clocks = ClockSampler(0)
     clocks.start()
-    ev[2].record(stream)
-    st = sm.hyb_run(inf, hyb, 0, nsteps, k=args.k, anchor=100, tol=0.01)
-    ev[3].record(stream)
+    ev[0].record(stream)
+    for k in range(args.steps):
+        m.step_n(1 + 100 * k, 100)
+        ck = m.checksums()
+    ev[1].record(stream)
     torch.cuda.synchronize()
-    t_hyb = ev[2].elapsed_time(ev[3]) / 1e3
     clk = clocks.stop()
-    err = sm.ens_compare(hyb, plain)
-    finite = np.isfinite(err).all(axis=1)
-    ef = err[finite] if finite.any() else np.full((1, 3), np.nan)
-    v_plain = cells * nsteps / t_plain
-    v_hyb = cells * nsteps / t_hyb
-    line = {"metric": "hybrid vs plain ensemble cell-steps/s (32 x 2048^2, 5000 steps, <=1% SSH err)",
-            "value": v_hyb, "unit": "cell-steps/s", "n_gpus": 1, "steps": 1, "warmup": 0,
-            "ms_per_step": t_hyb * 1e3, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "bf16+f64", "data": "synthetic",
-            "config": {"workload": "%d members 2048x2048, %d steps, surrogate k=%d, re-anchor 100, "
-                                   "tol 1%% relative SSH L2 vs shadow FP64 step" % (nm, nsteps, args.k),
-                       "candidates": len(cands), "screened_out": len(cands) - len(ok),
-                       "patch": P, "nblocks": args.nblocks, "train_side": ts, "train_steps": args.train_steps,
-                       "train_runs": args.train_runs, "fallback": "per member",
-                       "train_input_noise": args.noise,
-                       "rollout_runs": args.rollout_runs, "rollout_windows": args.rollout_windows,
-                       "rollout_runs_dropped": tr.rollout_runs.dropped,
-                       "finetune_iters": args.finetune_iters,
-                       "train_iters": args.train_iters, "train_s": t_train, "datagen_s": t_gen,
-                       "train_runs_dropped": tr.generate_runs.dropped},
-            "plain_value": v_plain, "hybrid_over_plain": v_hyb / v_plain,
-            "hybrid_stats": st,
-            "surrogate_share": st["sur_steps"] / max(1, st["sur_steps"] + st["solver_steps"]),
-            "err_vs_fp64": {"ssh_max": float(ef[:, 0].max()), "ssh_mean": float(ef[:, 0].mean()),
-                            "u_max": float(ef[:, 1].max()), "v_max": float(ef[:, 2].max()),
-                            "u_mean": float(ef[:, 1].mean()), "v_mean": float(ef[:, 2].mean()),
-                            "members_nonfinite": int((~finite).sum())},
-            "loss_first": losses[0], "loss_last": losses[-1], "clocks": clk,
-            "gpu_launches": st["launches"]}
+    ms = ev[0].elapsed_time(ev[1])
+    value = n * n * 100 * args.steps / (ms / 1e3)
+    peak, kind = load_peaks()
+    achieved = GEN_BYTES_PER_CELL_STEP * value / 1e9
+    line = {"metric": "general-grid cell-steps/s at %d^2 FP64" % n, "value": value,
+            "unit": "cell-steps/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "general grid %dx%d: open water on all four borders, 64 islands, "
+                                   "per-point scale factors, latitudes and depths; 100 model steps + "
+                                   "checksums per bench step" % (n, n),
+                       "l2": "inputs larger than L2"},
+            "roofline": {"bound": "hbm", "kernel": "k_fused_general", "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": kind,
+                         "algorithmic_bytes_per_cell_step": GEN_BYTES_PER_CELL_STEP},
+            "checksums_last": [float(x) for x in ck],
+            "gpu_launches": args.steps * (2 * 100 + 2), "clocks": clk}
     print(json.dumps(line), flush=True)
+    m.close()
 
 
 def main():
@@ -565,6 +810,8 @@ def main():
         return run_hybrid(args)
     if args.workload == "conv":
         return run_conv(args)
+    if args.workload == "general":
+        return run_general(args)
     if args.n != N:
         WORKLOAD["jpi"] = WORKLOAD["jpj"] = args.n
         CONFIG["grid"] = [args.n, args.n]
@@ -682,22 +929,28 @@ def main():
                "steps": k_e2e, "contexts": 2}
         m2.close()
 
+    sched = m.get_schedule()
+    m.close()
+
+    # ---- the other two kernels families on the same box (one GPU only) -----
+    ens = conv = None
+    if world == 1 and not args.no_ensemble:
+        ens = ensemble_leg(local, warmup=1, reps=1)
+    if world == 1 and not args.no_conv:
+        conv = conv_leg(local)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        rate, n, th = cpu_oracle_rate()
-        cpu = {"value": rate, "unit": "cell-steps/s", "cores": th, "kind": "port",
-               "sample": "%d model steps (2..%d) of the 4096^2 bench grid, oracle port of "
-                         "original/nemolite2d.f90, OpenMP %d threads" % (n, n + 1, th)}
+        cpu = cpu_baselines()
 
     if rank == 0:
-        sched = m.get_schedule()
         line = {"metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f64", "data": "synthetic",
-                "config": dict(CONFIG, parallelism="replicas x%d" % world,
-                               schedule={"warps": sched[0], "occupancy": sched[1],
-                                         "rows": sched[2]}),
+                "dtype": "f64", "data": "synthetic", "config": dict(CONFIG),
+                "bench_step": "%d model steps + device checksums of sshn, u, v" % STEPS_PER_ITER,
+                "parallelism": "replicas x%d" % world,
+                "schedule": {"warps": sched[0], "occupancy": sched[1], "rows": sched[2]},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
                              "unit": "GB/s", "frac": achieved / peak,
                              "peak_source": peak_kind, "traffic": traffic,
@@ -705,9 +958,9 @@ def main():
                              "algorithmic_bytes_per_launch": BYTES_PER_CELL_STEP * cells()},
                 "gpu_launches": args.steps * (STEPS_PER_ITER + 2),
                 "checksums_last": [float(x) for x in records[-1]],
-                "clocks": clk, "e2e": e2e, "cpu_baseline": cpu}
+                "clocks": clk, "e2e": e2e, "cpu_baseline": cpu,
+                "ensemble": ens, "conv": conv}
         print(json.dumps(line), flush=True)
-    m.close()
     if dist is not None:
         dist.destroy_process_group()
 

@@ -142,7 +142,10 @@ int nemo_host_free(void* ptr);
 /* Overwrites sshn, un, vn (dense, Fortran extents) and re-derives
  * sshn_u/sshn_v with the post-`next` interpolation (:736-764); the
  * open-boundary row sshn_v(:,0), which the reference never updates after
- * initialisation, keeps its value. */
+ * initialisation, keeps its value.  The result is the state as after a
+ * complete step: ssha, ua, va equal the new sshn, un, vn, as `next`
+ * (:712-732) leaves them, so points that no routine of a step writes (a u
+ * point between two open cells of a general grid) carry the given value. */
 int nemo_set_state(nemo_ctx* ctx, const double* sshn, const double* un,
                    const double* vn);
 
@@ -401,10 +404,40 @@ int nemo_conv3x3_wgrad(const void* x, const void* dz, float* dw, float* db, int 
  * window per tap.  Returns the previous variant; values out of range change
  * nothing. */
 int nemo_conv3x3_fwd_variant(int variant, int rows);
-/* Process-wide weight-gradient kernel: 1 (default) multiplies the x windows of
- * two horizontal taps with the dz windows of three rows (six taps per N = 192
- * MMA); 0 pairs taps with N = 64 MMAs.  Returns the previous variant. */
+/* Process-wide weight-gradient kernel: 2 (default) gives each CTA all nine
+ * taps and the bias over a range of column-strip rows (one x window per row
+ * read at three shifts, each dz row loaded once into a mirrored ring) and adds
+ * the CTAs' partial sums in a fixed order afterwards, so results are
+ * bit-identical from call to call; it keeps one scratch array per device for
+ * nemo_conv3x3_wgrad (calls that overlap on the GPU race on it; a surrogate
+ * has its own).  1 multiplies the x windows of two horizontal taps with the
+ * dz windows of three rows (six taps per N = 192 MMA); 0 pairs taps with
+ * N = 64 MMAs; both add partial results with atomics.  Returns the previous
+ * variant; values out of range change nothing. */
 int nemo_conv3x3_wgrad_variant(int variant);
+
+/* ---- allocation-failure injection (tests of the error paths) ---------------
+ * No counterpart in the reference, which stops the program when an ALLOCATE
+ * fails (original/nemolite2d.f90:308).  Every device and page-locked
+ * allocation of this library counts down from n: the n-th one from this call
+ * on reports failure without allocating (n = 1: the next one), after which
+ * the countdown is off again; n = 0 turns it off.  Returns the countdown's
+ * previous value (so nemo_debug_fail_alloc(0) after a call tells whether the
+ * failure fired: 0 yes, > 0 not reached), or -1 for n < 0.  Process-wide;
+ * meant for tests, which check that every create call then returns
+ * NEMO_ERR_ALLOC, sets no handle and leaves no device memory behind. */
+int nemo_debug_fail_alloc(int n);
+
+/* Test of the convolution kernels' failure path (no counterpart in the
+ * reference).  The default forward kernel's main waits (operand rows, the
+ * accumulator hand-over) give up after wait_ns nanoseconds of wall time
+ * (0: the default, 2 s); the drains before exit keep 2 s.  The next
+ * skip_launches forward launches leave out CTA 0's first input-row load, so
+ * that the waits for that row run out: the kernel records an error code,
+ * lets its copies and MMAs finish, frees its tensor memory and returns, and
+ * the surrogate call reports NEMO_ERR_TIMEOUT.  Nothing faults and the
+ * context stays usable.  Process-wide. */
+int nemo_debug_conv_wait(unsigned long long wait_ns, int skip_launches);
 
 /* ---- drop-in symbols (cuda/cuda_nemolite2d.cu:234-270) --------------------
  * One default context.  Errors are printed to stderr and kept in a sticky

@@ -6,6 +6,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <atomic>
 #include <cmath>
 #include <fstream>
 #include <new>
@@ -41,6 +42,8 @@ struct nemo_ctx {
   bool general = false;
   void* gslab = nullptr;
   GridDev grid{};
+  int4* gchains = nullptr;   // Flather chains of the general grid
+  int n_gchains = 0;
   // output records (nemo_record): staging buffer, side stream and events
   double* rec_dev = nullptr;
   cudaStream_t rec_stream = nullptr;
@@ -287,6 +290,20 @@ void tune_store(const nemo_ctx* c, const nemo_schedule& s, double ms) {
 
 }  // namespace
 
+namespace nemo {
+// Countdown of nemo_debug_fail_alloc: 0 is off; n > 0 makes the n-th
+// allocation from now fail.
+static std::atomic<int> g_alloc_countdown{0};
+
+bool alloc_should_fail() {
+  int c = g_alloc_countdown.load(std::memory_order_relaxed);
+  while (c > 0) {
+    if (g_alloc_countdown.compare_exchange_weak(c, c - 1, std::memory_order_relaxed)) return c == 1;
+  }
+  return false;
+}
+}  // namespace nemo
+
 extern "C" {
 
 int nemo_default_params(nemo_params* p) {
@@ -332,6 +349,7 @@ int nemo_destroy(nemo_ctx* c) {
   if (c->rec_copied) cudaEventDestroy(c->rec_copied);
   if (c->rec_stream) cudaStreamDestroy(c->rec_stream);
   if (c->gslab) cudaFree(c->gslab);
+  if (c->gchains) cudaFree(c->gchains);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return NEMO_OK;
@@ -368,9 +386,9 @@ int nemo_create(const nemo_params* p, nemo_ctx** out) {
   const size_t fe = (size_t)c->L.elems();
   const size_t ck = 4 * (size_t)p->jpj + 4;
   const size_t total = 13 * fe + ck;
-  e = cudaMalloc(&c->slab, total * sizeof(double));
+  e = nemo::dev_alloc(&c->slab, total * sizeof(double));
   if (e != cudaSuccess) { c->slab = nullptr; nemo_destroy(c); cudaGetLastError(); return NEMO_ERR_ALLOC; }
-  e = cudaMallocHost(&c->ck_host, 4 * sizeof(double));
+  e = nemo::host_alloc(&c->ck_host, 4 * sizeof(double));
   if (e != cudaSuccess) { c->ck_host = nullptr; nemo_destroy(c); cudaGetLastError(); return NEMO_ERR_ALLOC; }
   double* q = c->slab;
   for (int s = 0; s < 2; ++s) {
@@ -400,7 +418,7 @@ int nemo_create(const nemo_params* p, nemo_ctx** out) {
     const size_t nax = (size_t)p->nbump * (2 * p->jpi + 2), ngy = (size_t)p->nbump * (2 * p->jpj + 2);
     std::vector<double> h(nax + ngy);
     depth_tables(*p, h.data(), h.data() + nax);
-    e = cudaMalloc(&tab, (nax + ngy) * sizeof(double));
+    e = nemo::dev_alloc(&tab, (nax + ngy) * sizeof(double));
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(tab, h.data(), (nax + ngy) * sizeof(double), cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess)
@@ -533,9 +551,27 @@ int nemo_step_n(nemo_ctx* c, int istp0, int n) {
   if (n < 0) return NEMO_ERR_INVALID;
   if (n == 0) return NEMO_OK;
   int st = set_device(c); if (st) return st;
-  if (c->general) {  // the fused kernel holds the reference's grid: the routine sequence
-    for (int k = 0; k < n; ++k)
-      if ((st = nemo_step(c, istp0 + k))) return st;
+  if (c->general) {  // the general grid's fused kernel and its Flather chains
+    for (int k = 0; k < n; ++k) {
+      GenArgs a;
+      a.sshn = nset(c).ssh;
+      a.un = nset(c).u;
+      a.vn = nset(c).v;
+      a.ht = c->ht;
+      a.hu = c->hu;
+      a.hv = c->hv;
+      a.su_st = c->sshn_u;
+      a.sv_st = c->sshn_v;
+      a.ssha = aset(c).ssh;
+      a.ua = aset(c).u;
+      a.va = aset(c).v;
+      a.tide = tide_value(c->p, istp0 + k);
+      a.g = c->grid;
+      CK(launch_fused_general(c->L, c->C, a, c->gchains, c->n_gchains, 32, c->stream));
+      c->n_idx = 1 - c->n_idx;
+    }
+    c->a_mirrors_n = true;
+    c->uv_stale = true;
     return NEMO_OK;
   }
   for (int k = 0; k < n; ++k) {
@@ -591,7 +627,7 @@ int nemo_record(nemo_ctx* c, double* host) {
   if (!c || !host) return NEMO_ERR_INVALID;
   int st = set_device(c); if (st) return st;
   if (!c->rec_dev) {
-    CK(cudaMalloc(&c->rec_dev, 3 * (size_t)c->L.jpi * c->L.jpj * sizeof(double)));
+    CK(nemo::dev_alloc(&c->rec_dev, 3 * (size_t)c->L.jpi * c->L.jpj * sizeof(double)));
     CK(cudaStreamCreateWithFlags(&c->rec_stream, cudaStreamNonBlocking));
     CK(cudaEventCreateWithFlags(&c->rec_state, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&c->rec_staged, cudaEventDisableTiming));
@@ -614,7 +650,7 @@ int nemo_record(nemo_ctx* c, double* host) {
 int nemo_host_alloc(size_t bytes, void** ptr) {
   if (!ptr || bytes == 0) return NEMO_ERR_INVALID;
   *ptr = nullptr;
-  cudaError_t e = cudaMallocHost(ptr, bytes);
+  cudaError_t e = nemo::host_alloc(ptr, bytes);
   if (e != cudaSuccess) {
     cudaGetLastError();
     *ptr = nullptr;
@@ -680,6 +716,9 @@ int nemo_set_state(nemo_ctx* c, const double* sshn, const double* un, const doub
   CK(launch_derive_sshn_uv(L, c->C, nset(c).ssh, c->sshn_u, c->sshn_v, c->stream, gridp(c)));
   CK(cudaStreamSynchronize(c->stream));
   c->uv_stale = false;
+  // the state as after a complete step: `next` has made the a-fields equal
+  // to these (they are materialised before a routine next writes them)
+  c->a_mirrors_n = true;
   return NEMO_OK;
 }
 
@@ -702,7 +741,7 @@ int nemo_set_grid(nemo_ctx* c, const nemo_grid* g) {
   const size_t fe = (size_t)c->L.elems();
   enum { E1T, E2T, E1U, E2U, E1V, E2V, E12T, E12U, E12V, FCU, FCV, NA };
   if (!c->gslab) {
-    cudaError_t e = cudaMalloc(&c->gslab, NA * fe * sizeof(double) + fe);
+    cudaError_t e = nemo::dev_alloc(&c->gslab, NA * fe * sizeof(double) + fe);
     if (e != cudaSuccess) { c->gslab = nullptr; cudaGetLastError(); return NEMO_ERR_ALLOC; }
   }
   double* base = static_cast<double*>(c->gslab);
@@ -732,6 +771,20 @@ int nemo_set_grid(nemo_ctx* c, const nemo_grid* g) {
     for (int ji = 0; ji <= jpi + 1; ++ji) hp[c->L.idx(ji, jj)] = (signed char)g->pt[jj * ld + ji];
   signed char* pt = reinterpret_cast<signed char*>(base + NA * fe);
   CK(cudaMemcpy(pt, hp.data(), fe, cudaMemcpyHostToDevice));
+  // Flather points of the mask, as chains in the sweeps' order
+  std::vector<int4> chains;
+  flather_chains(g->pt, jpi, jpj, chains);
+  if (c->gchains) {
+    cudaFree(c->gchains);
+    c->gchains = nullptr;
+    c->n_gchains = 0;
+  }
+  if (!chains.empty()) {
+    cudaError_t e = nemo::dev_alloc(&c->gchains, chains.size() * sizeof(int4));
+    if (e != cudaSuccess) { c->gchains = nullptr; cudaGetLastError(); return NEMO_ERR_ALLOC; }
+    CK(cudaMemcpy(c->gchains, chains.data(), chains.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    c->n_gchains = (int)chains.size();
+  }
   c->grid = GridDev{pt, base + E1T * fe, base + E2T * fe, base + E1U * fe, base + E2U * fe, base + E1V * fe,
                     base + E2V * fe, base + E12T * fe, base + E12U * fe, base + E12V * fe, base + FCU * fe,
                     base + FCV * fe};
@@ -802,7 +855,7 @@ int nemo_autotune(nemo_ctx* c, int steps, nemo_schedule* best, double* best_ms) 
   // both state sets and the bookkeeping are restored afterwards
   const size_t fe = (size_t)c->L.elems();
   double* backup = nullptr;
-  CK(cudaMalloc(&backup, 6 * fe * sizeof(double)));
+  CK(nemo::dev_alloc(&backup, 6 * fe * sizeof(double)));
   const int n_save = c->n_idx;
   const bool a_save = c->a_mirrors_n, uv_save = c->uv_stale;
   cudaError_t er = cudaSuccess;
@@ -863,6 +916,11 @@ int nemo_autotune(nemo_ctx* c, int steps, nemo_schedule* best, double* best_ms) 
   if (best) *best = c->sched;
   if (best_ms) *best_ms = bms;
   return NEMO_OK;
+}
+
+int nemo_debug_fail_alloc(int n) {
+  if (n < 0) return -1;
+  return nemo::g_alloc_countdown.exchange(n, std::memory_order_relaxed);
 }
 
 const char* nemo_status_string(int s) {

@@ -270,7 +270,7 @@ int build_work(nemo_ens* e) {
   if ((int)w.size() > e->work_cap) {
     if (e->d_work) cudaFree(e->d_work);
     e->d_work = nullptr;
-    ECK(cudaMalloc(&e->d_work, w.size() * sizeof(int4)));
+    ECK(nemo::dev_alloc(&e->d_work, w.size() * sizeof(int4)));
     e->work_cap = (int)w.size();
   }
   ECK(cudaMemcpyAsync(e->d_work, w.data(), w.size() * sizeof(int4), cudaMemcpyHostToDevice, e->stream));
@@ -288,8 +288,8 @@ int ensure_tide(nemo_ens* e, int n) {
   e->d_tide = nullptr;
   e->h_tide = nullptr;
   const size_t cnt = (size_t)n * e->mem.size();
-  ECK(cudaMalloc(&e->d_tide, cnt * sizeof(double)));
-  ECK(cudaMallocHost(&e->h_tide, cnt * sizeof(double)));
+  ECK(nemo::dev_alloc(&e->d_tide, cnt * sizeof(double)));
+  ECK(nemo::host_alloc(&e->h_tide, cnt * sizeof(double)));
   e->tide_cap = n;
   drop_graphs(e);  // graphs hold the old table address
   return NEMO_OK;
@@ -424,7 +424,7 @@ int nemo_ens_create(const nemo_params* common, const nemo_member* members, int n
     e->cells += (long long)L.jpi * L.jpj;
     e->nrows += L.jpj;
   }
-  err = cudaMalloc(&e->slab, total * sizeof(double));
+  err = nemo::dev_alloc(&e->slab, total * sizeof(double));
   if (err != cudaSuccess) { e->slab = nullptr; cudaGetLastError(); nemo_ens_destroy(e); return NEMO_ERR_ALLOC; }
   err = cudaMemsetAsync(e->slab, 0, total * sizeof(double), e->stream);
   if (err != cudaSuccess) { nemo_ens_destroy(e); return status_of(err); }
@@ -434,7 +434,7 @@ int nemo_ens_create(const nemo_params* common, const nemo_member* members, int n
   double* tab = nullptr;
   size_t tab_cap = 0;
   int* d_bad = nullptr;  // depths whose in-kernel reciprocal differs from RN(1/h)
-  err = cudaMalloc(&d_bad, sizeof(int));
+  err = nemo::dev_alloc(&d_bad, sizeof(int));
   if (err == cudaSuccess) err = cudaMemsetAsync(d_bad, 0, sizeof(int), e->stream);
   for (int m = 0; m < nmem && err == cudaSuccess; ++m) {
     MemberDev& d = e->hmem[m];
@@ -466,7 +466,7 @@ int nemo_ens_create(const nemo_params* common, const nemo_member* members, int n
         err = cudaStreamSynchronize(e->stream);
         if (tab) cudaFree(tab);
         tab = nullptr;
-        if (err == cudaSuccess) err = cudaMalloc(&tab, (nax + ngy) * sizeof(double));
+        if (err == cudaSuccess) err = nemo::dev_alloc(&tab, (nax + ngy) * sizeof(double));
         tab_cap = nax + ngy;
       }
       if (err == cudaSuccess)
@@ -498,13 +498,13 @@ int nemo_ens_create(const nemo_params* common, const nemo_member* members, int n
   if (!e->recip_nr_ok) e->sched.occupancy = 116;
   if (err != cudaSuccess) { nemo_ens_destroy(e); return status_of(err); }
   const size_t nm = (size_t)nmem;
-  err = cudaMalloc(&e->d_mem, nm * sizeof(MemberDev));
-  if (err == cudaSuccess) err = cudaMalloc(&e->d_rows, rows.size() * sizeof(int2));
-  if (err == cudaSuccess) err = cudaMalloc(&e->d_row_off, nm * sizeof(int));
-  if (err == cudaSuccess) err = cudaMalloc(&e->d_row_cnt, nm * sizeof(int));
-  if (err == cudaSuccess) err = cudaMalloc(&e->d_partial, 3 * rows.size() * sizeof(double));
-  if (err == cudaSuccess) err = cudaMalloc(&e->d_ck, 3 * nm * sizeof(double));
-  if (err == cudaSuccess) err = cudaMallocHost(&e->h_ck, 3 * nm * sizeof(double));
+  err = nemo::dev_alloc(&e->d_mem, nm * sizeof(MemberDev));
+  if (err == cudaSuccess) err = nemo::dev_alloc(&e->d_rows, rows.size() * sizeof(int2));
+  if (err == cudaSuccess) err = nemo::dev_alloc(&e->d_row_off, nm * sizeof(int));
+  if (err == cudaSuccess) err = nemo::dev_alloc(&e->d_row_cnt, nm * sizeof(int));
+  if (err == cudaSuccess) err = nemo::dev_alloc(&e->d_partial, 3 * rows.size() * sizeof(double));
+  if (err == cudaSuccess) err = nemo::dev_alloc(&e->d_ck, 3 * nm * sizeof(double));
+  if (err == cudaSuccess) err = nemo::host_alloc(&e->h_ck, 3 * nm * sizeof(double));
   if (err == cudaSuccess) err = cudaEventCreateWithFlags(&e->tide_ev, cudaEventDisableTiming);
   if (err == cudaSuccess)
     err = cudaMemcpyAsync(e->d_mem, e->hmem.data(), nm * sizeof(MemberDev), cudaMemcpyHostToDevice, e->stream);
@@ -646,7 +646,7 @@ int nemo_ens_autotune(nemo_ens* e, int steps, nemo_ens_schedule* best, double* b
   size_t tot = 0;
   for (auto& d : e->hmem) tot += 3 * (size_t)d.L.elems();
   double* backup = nullptr;
-  ECK(cudaMalloc(&backup, tot * sizeof(double)));
+  ECK(nemo::dev_alloc(&backup, tot * sizeof(double)));
   const int p_save = e->parity;
   auto copy_state = [&](bool save) -> cudaError_t {
     size_t o = 0;
@@ -749,7 +749,7 @@ int ens_step_subset(nemo_ens* e, int istp0, int n, const char* sel) {
     if (e->d_work_sub) cudaFree(e->d_work_sub);
     e->d_work_sub = nullptr;
     e->sub_cap = 0;
-    ECK(cudaMalloc(&e->d_work_sub, w.size() * sizeof(int4)));
+    ECK(nemo::dev_alloc(&e->d_work_sub, w.size() * sizeof(int4)));
     e->sub_cap = (int)w.size();
   }
   // pageable source: the copy is staged before the call returns

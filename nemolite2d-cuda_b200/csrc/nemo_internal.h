@@ -3,6 +3,9 @@
 
 #include <cuda_runtime.h>
 
+#include <vector>
+
+#include "nemo_alloc.h"
 #include "nemo_b200.h"
 #include "nemo_common.cuh"
 
@@ -76,6 +79,22 @@ cudaError_t launch_fused_step(const Layout& L, const Consts& C, const FusedArgs&
                               int occ, int tile_y, cudaStream_t s);
 // nr_ok: the grid's depths passed launch_recip's check (variants 216, 220).
 bool fused_variant_ok(int warps, int occ, bool nr_ok);
+
+// Fused step of a general grid (nemo_fused_general.cu).  su_st, sv_st: the
+// stored sshn_u / sshn_v, read where `next` leaves them unchanged.
+struct GenArgs {
+  const double *sshn, *un, *vn, *ht, *hu, *hv;
+  const double *su_st, *sv_st;
+  double *ssha, *ua, *va;
+  double tide;
+  GridDev g;
+};
+// One step: the fused kernel, then the Flather chains (flather_chains).
+cudaError_t launch_fused_general(const Layout& L, const Consts& C, const GenArgs& a, const int4* chains,
+                                 int nchains, int tile_y, cudaStream_t s);
+// Flather points of the mask pt ((0:jpi+1, 0:jpj+1), leading dimension
+// jpi+2) as independent chains: {ji, jj, kind, continues}.
+void flather_chains(const int* pt, int jpi, int jpj, std::vector<int4>& out);
 
 // Sums |f(1:jpi,1:jpj)| of nf fields into out[0..nf-1] (device), fixed order.
 // row_partials: nf*jpj doubles of scratch.

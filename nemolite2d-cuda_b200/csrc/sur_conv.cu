@@ -29,6 +29,9 @@
 #include <stdint.h>
 #include <stdio.h>
 
+#include <atomic>
+#include <mutex>
+
 #include "sur_internal.h"
 
 namespace sur {
@@ -76,19 +79,19 @@ __device__ __forceinline__ uint64_t gtimer() {
   asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
   return t;
 }
-// Bounded wait for the phase with the given parity; false after WAIT_NS of
-// wall time without completion.
-__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity) {
+// Bounded wait for the phase with the given parity; false after `limit` ns
+// (WAIT_NS by default) of wall time without completion.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, uint64_t limit = WAIT_NS) {
   if (mbar_try(b, parity)) return true;
   const uint64_t t0 = gtimer();
   for (uint32_t i = 1;; ++i) {
     if (mbar_try(b, parity)) return true;
-    if ((i & 255u) == 0 && gtimer() - t0 > WAIT_NS) return false;
+    if ((i & 255u) == 0 && gtimer() - t0 > limit) return false;
   }
 }
 // The same, agreed across the warp (for .sync.aligned tcgen05 instructions).
-__device__ __forceinline__ bool mbar_wait_warp(uint64_t* b, uint32_t parity) {
-  return __all_sync(0xffffffffu, mbar_wait(b, parity)) != 0;
+__device__ __forceinline__ bool mbar_wait_warp(uint64_t* b, uint32_t parity, uint64_t limit = WAIT_NS) {
+  return __all_sync(0xffffffffu, mbar_wait(b, parity, limit)) != 0;
 }
 __device__ __forceinline__ void fence_barrier_init() {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -581,6 +584,8 @@ k_conv_fwd_tri(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = S.tmem_base;
+  // main waits (operands, accumulator hand-over); the drains keep WAIT_NS
+  const uint64_t LIM = E.wait_ns ? (uint64_t)E.wait_ns : WAIT_NS;
   if (warp >= 2) {  // every accumulator block starts at zero
     const uint32_t tl = tmem + ((uint32_t)(32 * (warp & 3)) << 16);
     for (int c = 0; c < 64 * TBLK; c += 32) tmem_zero32(tl + (uint32_t)c);
@@ -597,20 +602,25 @@ k_conv_fwd_tri(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
       tma_load_2d(S.w + ((tap % 3) * 3 + tap / 3) * WT_BYTES, &tmW, &S.wbar, 0, tap * CH);
     uint32_t L = 0;  // loads issued
     bool ok = true;
+    // test of the failure path: the first load is never issued, so the waits
+    // for its row run out (the load is left out, not broken)
+    const bool skip_first = E.skip_load && blockIdx.x == 0;
     for (int st = blockIdx.x; st < nstrip && ok; st += gridDim.x) {
       const int ys = st % ystrips, r0 = st / ystrips, xt = r0 % xtiles, n = r0 / xtiles;
       const int y0 = ys * R, y1 = min(y0 + R, E.H) - 1;
       for (int r = y0 - 1; r <= y1 + 1; ++r, ++L) {
         const int slot = (int)(L % NSLOT_T);
         const uint32_t ph = (L / NSLOT_T) & 1;
-        if (!mbar_wait(&S.empty[slot], ph ^ 1)) { fail(E.err, 31); ok = false; break; }
+        if (!mbar_wait(&S.empty[slot], ph ^ 1, LIM)) { fail(E.err, 31); ok = false; break; }
+        if (skip_first && L == 0) continue;
         mbar_expect_tx(&S.full[slot], RW_BYTES);
         tma_load_4d(S.slot[slot], &tmA, &S.full[slot], 0, xt * TM - 8, r, n);
       }
     }
-    // every armed load lands before the CTA may exit
+    // every armed load lands before the CTA may exit (the omitted one is not armed)
     for (int s = 0; s < NSLOT_T; ++s) {
       const uint32_t armed = L / NSLOT_T + ((uint32_t)s < L % NSLOT_T ? 1u : 0u);
+      if (skip_first && s == 0 && armed == 1) continue;
       if (armed) mbar_wait(&S.full[s], (armed - 1) & 1);
     }
     mbar_wait(&S.wbar, 0);
@@ -632,9 +642,9 @@ k_conv_fwd_tri(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         const int slot = (int)(ld % NSLOT_T);
         if (t <= rows - 1) {  // output row t starts here: its block must be drained and zeroed
           const uint32_t g = g0 + (uint32_t)t;
-          if (!mbar_wait(&S.tempty[tblk(g)], ((g / TBLK) & 1) ^ 1)) { fail(E.err, 33); ok = false; break; }
+          if (!mbar_wait(&S.tempty[tblk(g)], ((g / TBLK) & 1) ^ 1, LIM)) { fail(E.err, 33); ok = false; break; }
         }
-        if (!mbar_wait(&S.full[slot], (ld / NSLOT_T) & 1)) { fail(E.err, 34); ok = false; break; }
+        if (!mbar_wait(&S.full[slot], (ld / NSLOT_T) & 1, LIM)) { fail(E.err, 34); ok = false; break; }
         tc_fence_after();
         const int nout = o_hi - o_lo + 1;
         const uint32_t dfirst = tblk(g0 + (uint32_t)o_hi);
@@ -674,7 +684,7 @@ k_conv_fwd_tri(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
       const int y0 = ys * R, y1 = min(y0 + R, E.H) - 1;
       for (int y = y0; y <= y1; ++y, ++g) {
         const uint32_t b = tblk(g);
-        if (!mbar_wait_warp(&S.tfull[b], (g / TBLK) & 1)) { fail(E.err, 35); ok = false; break; }
+        if (!mbar_wait_warp(&S.tfull[b], (g / TBLK) & 1, LIM)) { fail(E.err, 35); ok = false; break; }
         tc_fence_after();
         float v[64];
         const uint32_t ta = tmem + b * 64 + ((uint32_t)(32 * q) << 16);
@@ -957,6 +967,231 @@ k_conv_wgrad_tri(const __grid_constant__ CUtensorMap tmX, const __grid_constant_
   }
 }
 
+// ---- weight gradient over column strips, all taps per CTA (default) ---------------
+// dw[dy,dx][co][ci] = sum_q x[q + (0,dx)][ci] dz[q - (dy,0)][co] as above, but one
+// CTA computes all nine taps and the bias gradient: its accumulator holds
+// group A = [x(dx=-1) | x(dx=0)]^T [dz(y+1) | dz(y) | dz(y-1)] in TMEM columns
+// 0..191 and group B = [x(dx=+1) | ones]^T [...] in columns 256..447 (the ones
+// half yields the bias gradient in its dy = 0 block).  The CTA owns a
+// contiguous range of (image, 64-pixel column chunk, row) units ordered so
+// that consecutive units march down the rows of one column strip:
+//  * x row y: ONE load of the 80-pixel window x0-8 .. x0+71 (zero outside the
+//    image); the operand is MN-major, one pixel per 128-byte K row, so the
+//    horizontal taps are descriptors shifted by one pixel (128 bytes), and the
+//    two M halves of group A, one pixel apart, are one descriptor with a
+//    leading byte offset of 128;
+//  * dz rows: each is loaded once into a ring of WS_KZ rows and once into the
+//    ring's mirror (slot + WS_KZ).  Row loads take slots in descending order,
+//    so rows y+1, y, y-1 always sit at three consecutive slots and each N block
+//    of the accumulator always receives the same dy.
+// Per unit: one 10 KiB x window, two 8 KiB dz copies and 8 MMAs of
+// 128 x 192 x 16 (the earlier kernels move 40 KiB per 4 MMAs).  At the end the
+// CTA writes its 9 x 64 x 64 + 64 sums to its own row of a scratch array and
+// k_wgrad_reduce adds the rows in a fixed order into dw and db, so the result
+// does not depend on timing (no atomics).
+constexpr int WS_XPIX = 80;                  // x window pixels: x0-8 .. x0+71
+constexpr int WS_XBYTES = WS_XPIX * CH * 2;  // 10 KiB
+constexpr int WS_KX = 4;                     // x window slots
+constexpr int WS_KZ = 6;                     // dz ring rows (12 slots with the mirrors)
+static_assert(WS_NPART == 9 * CH * CH + CH, "one CTA's partial dw and db");
+
+struct WsSmem {
+  uint8_t x[WS_KX][WS_XBYTES];
+  uint8_t z[2 * WS_KZ][WG_TILE];
+  uint8_t ones[WG_TILE];
+  uint64_t xfull[WS_KX], xempty[WS_KX], zfull[WS_KZ], zempty[WS_KZ];
+  uint64_t done;
+  uint32_t tmem_base;
+};
+
+// Ring slot of the l-th dz row load: consecutive loads take descending slots.
+__device__ __forceinline__ uint32_t ws_zslot(uint32_t l) { return (WS_KZ - l % WS_KZ) % WS_KZ; }
+// Loads among the first n whose slot is s (the ring visits each slot once per WS_KZ loads).
+__device__ __forceinline__ uint32_t ws_zcount(uint32_t n, uint32_t s) {
+  const uint32_t j = (WS_KZ - s) % WS_KZ;
+  return n / WS_KZ + (j < n % WS_KZ ? 1u : 0u);
+}
+
+__global__ void __launch_bounds__(THREADS, 1)
+k_conv_wgrad_strip(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmZ,
+                   WgradArgs G) {
+  extern __shared__ uint8_t smem_raw[];
+  WsSmem& S = *reinterpret_cast<WsSmem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int xch = G.W / WG_PIX;
+  const long nunit = (long)G.N * xch * G.H;
+  const long u_begin = nunit * blockIdx.x / gridDim.x;
+  const long u_end = nunit * (blockIdx.x + 1) / gridDim.x;
+  const bool have = u_end > u_begin;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < WS_KX; ++s) {
+      mbar_init(&S.xfull[s], 1);
+      mbar_init(&S.xempty[s], 1);
+    }
+    for (int s = 0; s < WS_KZ; ++s) {
+      mbar_init(&S.zfull[s], 1);
+      mbar_init(&S.zempty[s], 1);
+    }
+    mbar_init(&S.done, 1);
+    fence_barrier_init();
+  }
+  if (warp >= 2) {  // the all-ones half of group B's A operand
+    const uint4 ones = make_uint4(0x3F803F80u, 0x3F803F80u, 0x3F803F80u, 0x3F803F80u);
+    uint4* d = reinterpret_cast<uint4*>(S.ones);
+    for (int i = threadIdx.x - 64; i < WG_TILE / 16; i += THREADS - 64) d[i] = ones;
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 1) tmem_alloc(&S.tmem_base, 512);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = S.tmem_base;
+
+  if (warp == 0 && lane == 0) {
+    // ---- TMA producer: per unit the next dz row and the x window ----
+    uint32_t lx = 0, lz = 0;
+    bool ok = true;
+    for (long u = u_begin; u < u_end && ok; ++u) {
+      const int y = (int)(u % G.H);
+      const long t = u / G.H;
+      const int x0 = (int)(t % xch) * WG_PIX, n = (int)(t / xch);
+      // a strip starts at the range's first unit or at row 0: rows y-1 and y first
+      for (int dr = (u == u_begin || y == 0) ? -1 : 1; dr <= 1 && ok; ++dr) {
+        const uint32_t s = ws_zslot(lz);
+        if (!mbar_wait(&S.zempty[s], ((lz / WS_KZ) & 1) ^ 1)) { ok = false; break; }
+        mbar_expect_tx(&S.zfull[s], 2 * WG_TILE);
+        tma_load_4d(S.z[s], &tmZ, &S.zfull[s], 0, x0, y + dr, n);
+        tma_load_4d(S.z[s + WS_KZ], &tmZ, &S.zfull[s], 0, x0, y + dr, n);
+        ++lz;
+      }
+      if (!ok) break;
+      const uint32_t s = lx % WS_KX;
+      if (!mbar_wait(&S.xempty[s], ((lx / WS_KX) & 1) ^ 1)) { ok = false; break; }
+      mbar_expect_tx(&S.xfull[s], WS_XBYTES);
+      tma_load_4d(S.x[s], &tmX, &S.xfull[s], 0, x0 - 8, y, n);
+      ++lx;
+    }
+    if (!ok) fail(G.err, 51);
+    // every armed load lands before the CTA may exit
+    for (uint32_t s = 0; s < WS_KX; ++s) {
+      const uint32_t armed = lx / WS_KX + (s < lx % WS_KX ? 1u : 0u);
+      if (armed) mbar_wait(&S.xfull[s], (armed - 1) & 1);
+    }
+    for (uint32_t s = 0; s < WS_KZ; ++s) {
+      const uint32_t armed = ws_zcount(lz, s);
+      if (armed) mbar_wait(&S.zfull[s], (armed - 1) & 1);
+    }
+  } else if (warp == 1 && lane == 0) {
+    // ---- MMA issuer ----
+    const uint32_t ID = idesc(128, 192, 1, 1);
+    const uint32_t ones = smem_u32(S.ones);
+    uint32_t lx = 0, lz = 0;
+    bool ok = true, first = true;
+    for (long u = u_begin; u < u_end; ++u) {
+      const int y = (int)(u % G.H);
+      const bool start = (u == u_begin) || y == 0;
+      const bool last = (u + 1 == u_end) || ((u + 1) % G.H == 0);
+      if (start) lz += 2;
+      const uint32_t l1 = lz++;  // dz row y+1; rows y and y-1 are loads l1-1 and l1-2
+      for (uint32_t l = start ? l1 - 2 : l1; l <= l1 && ok; ++l)
+        ok = mbar_wait(&S.zfull[ws_zslot(l)], (l / WS_KZ) & 1);
+      const uint32_t xsl = lx % WS_KX;
+      if (ok) ok = mbar_wait(&S.xfull[xsl], (lx / WS_KX) & 1);
+      if (!ok) break;
+      ++lx;
+      tc_fence_after();
+      const uint32_t xs = smem_u32(S.x[xsl]);
+      const uint32_t zb = smem_u32(S.z[ws_zslot(l1)]);
+      const uint32_t lbo_ones = ones - (xs + 9u * 128u);
+#pragma unroll
+      for (int k = 0; k < WG_PIX / 16; ++k) {
+        const uint64_t bd = sdesc(zb + 2048u * k, WG_TILE, 1024);
+        const uint32_t acc = (first && k == 0) ? 0u : 1u;
+        mma_bf16(tmem, sdesc(xs + (7u + 16u * k) * 128u, 128, 1024), bd, ID, acc);
+        mma_bf16(tmem + 256, sdesc(xs + (9u + 16u * k) * 128u, lbo_ones, 1024), bd, ID, acc);
+      }
+      first = false;
+      mma_commit(&S.xempty[xsl]);
+      mma_commit(&S.zempty[ws_zslot(l1 - 2)]);  // row y-1 has had its last use
+      if (last) {                                // so have rows y and y+1 at a strip's end
+        mma_commit(&S.zempty[ws_zslot(l1 - 1)]);
+        mma_commit(&S.zempty[ws_zslot(l1)]);
+      }
+    }
+    if (!ok) fail(G.err, 52);
+    mma_commit(&S.done);  // completes once every MMA issued above has finished
+    if (!mbar_wait(&S.done, 0)) fail(G.err, 53);
+  }
+  if (warp >= 2) {
+    // ---- this CTA's partial sums -> its row of the scratch array ----
+    const int q = warp & 3;
+    const int row = 32 * q + lane;  // TMEM lane: (M half, ci)
+    const int half = row >> 6, ci = row & 63;
+    float* part = G.partial + (long)blockIdx.x * WS_NPART;
+    bool ok = true;
+    if (have) {
+      ok = mbar_wait_warp(&S.done, 0);
+      if (!ok) fail(G.err, 54);
+      tc_fence_after();
+    }
+    for (int grp = 0; grp < 2; ++grp) {
+      for (int j = 0; j < 3; ++j) {  // dy = j - 1
+        float v[64];
+        if (have && ok) {
+          const uint32_t ta = tmem + (uint32_t)(256 * grp + 64 * j) + ((uint32_t)(32 * q) << 16);
+          tmem_ld32(ta, v);
+          tmem_ld32(ta + 32, v + 32);
+        } else {
+#pragma unroll
+          for (int c = 0; c < 64; ++c) v[c] = 0.0f;
+        }
+        if (grp == 0 || half == 0) {
+          const int dx = grp == 1 ? 1 : (half == 0 ? -1 : 0);
+          float* d = part + (long)(3 * j + dx + 1) * CH * CH + ci;
+#pragma unroll
+          for (int co = 0; co < 64; ++co) d[co * CH] = v[co];
+        } else if (j == 1 && ci == 0) {
+#pragma unroll
+          for (int co = 0; co < 64; ++co) part[9 * CH * CH + co] = v[co];
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    __syncwarp();
+    tc_fence_after();
+    tmem_dealloc(tmem, 512);
+  }
+}
+
+// dw[i] += sum_b part[b][i] (i < 9*64*64), db[i - 9*64*64] += ... (the rest),
+// b = 0 .. nblk-1 in a fixed tree: 8 segments of consecutive rows summed in
+// order, then the segment sums in order.  A block serves 32 consecutive i.
+__global__ void __launch_bounds__(256)
+k_wgrad_reduce(const float* __restrict__ part, int nblk, float* dw, float* db) {
+  __shared__ float seg[8][32];
+  const int i = blockIdx.x * 32 + (threadIdx.x & 31);
+  const int g = threadIdx.x >> 5;
+  const int b0 = nblk * g / 8, b1 = nblk * (g + 1) / 8;
+  float s = 0.0f;
+  if (i < WS_NPART) {
+#pragma unroll 4
+    for (int b = b0; b < b1; ++b) s += part[(long)b * WS_NPART + i];
+  }
+  seg[g][threadIdx.x & 31] = s;
+  __syncthreads();
+  if (g == 0 && i < WS_NPART) {
+    float t = seg[0][threadIdx.x];
+#pragma unroll
+    for (int k = 1; k < 8; ++k) t += seg[k][threadIdx.x];
+    if (i < 9 * CH * CH) dw[i] += t;
+    else if (db) db[i - 9 * CH * CH] += t;
+  }
+}
+
 // ---- tensor maps ---------------------------------------------------------------
 PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
 
@@ -999,7 +1234,16 @@ bool g_attr[64];
 int g_fwd_variant = 2;  // 2: three output rows per MMA (k_conv_fwd_tri), 1: row ring
                         // (k_conv_fwd_rows), 0: a TMA window per tap (k_conv_fwd)
 int g_fwd_rows = 16;    // rows per strip of the row-ring kernel
-int g_wgrad_variant = 1;  // 1: three vertical taps per MMA (k_conv_wgrad_tri), 0: tap pairs
+int g_wgrad_variant = 2;  // 2: all taps per CTA over column strips (k_conv_wgrad_strip),
+                          // 1: three vertical taps per MMA (k_conv_wgrad_tri), 0: tap pairs
+// Scratch of k_conv_wgrad_strip for callers that pass none: one array per
+// device, grown on demand and kept until the process exits.
+// Test settings of the forward kernel's failure path (set_test_wait).
+std::atomic<unsigned long long> g_test_wait_ns{0};
+std::atomic<int> g_test_skip{0};
+std::mutex g_part_mu;
+float* g_part[64];
+int g_part_blocks[64];
 
 // SM count of the current device; opts the kernels into their shared memory.
 cudaError_t prepare_device(int* sms) {
@@ -1016,6 +1260,9 @@ cudaError_t prepare_device(int* sms) {
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k_conv_wgrad_tri, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)(sizeof(WtSmem) + 1024));
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_conv_wgrad_strip, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(sizeof(WsSmem) + 1024));
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k_conv_fwd_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)(sizeof(RowSmem) + 1024));
@@ -1050,7 +1297,14 @@ cudaError_t conv_fwd(const __nv_bfloat16* x, const __nv_bfloat16* w, const ConvE
     const int R = g_fwd_rows;
     const long nstrip = (long)epi.N * (epi.W / TM) * ((epi.H + R - 1) / R);
     const int grid = (int)(nstrip < sms ? nstrip : sms);
-    k_conv_fwd_tri<<<grid, THREADS, sizeof(TriSmem) + 1024, s>>>(ta, tw, epi, R);
+    ConvEpi E = epi;
+    E.wait_ns = g_test_wait_ns.load();
+    int k = g_test_skip.load();
+    E.skip_load = 0;
+    while (k > 0 && !g_test_skip.compare_exchange_weak(k, k - 1)) {
+    }
+    if (k > 0) E.skip_load = 1;
+    k_conv_fwd_tri<<<grid, THREADS, sizeof(TriSmem) + 1024, s>>>(ta, tw, E, R);
     return cudaGetLastError();
   }
   if (g_fwd_variant == 1) {
@@ -1070,8 +1324,15 @@ cudaError_t conv_fwd(const __nv_bfloat16* x, const __nv_bfloat16* w, const ConvE
 
 int set_wgrad_variant(int variant) {
   const int prev = g_wgrad_variant;
-  if (variant == 0 || variant == 1) g_wgrad_variant = variant;
+  if (variant >= 0 && variant <= 2) g_wgrad_variant = variant;
   return prev;
+}
+
+int wgrad_kernels() { return g_wgrad_variant == 2 ? 2 : 1; }
+
+unsigned long long set_test_wait(unsigned long long wait_ns, int skip_launches) {
+  g_test_skip.store(skip_launches > 0 ? skip_launches : 0);
+  return g_test_wait_ns.exchange(wait_ns);
 }
 
 int set_fwd_variant(int variant, int rows) {
@@ -1091,8 +1352,40 @@ cudaError_t conv_wgrad(const __nv_bfloat16* x, const __nv_bfloat16* dz, const Wg
   int sms = 0;
   if ((e = prepare_device(&sms)) != cudaSuccess) return e;
   CUtensorMap tx, tz;
-  if ((e = act_map(&tx, x, g.N, g.H, g.W, WG_PIX)) != cudaSuccess) return e;
   if ((e = act_map(&tz, dz, g.N, g.H, g.W, WG_PIX)) != cudaSuccess) return e;
+  if (g_wgrad_variant == 2) {
+    if ((e = act_map(&tx, x, g.N, g.H, g.W, WS_XPIX)) != cudaSuccess) return e;
+    const long nunit = (long)g.N * g.H * (g.W / WG_PIX);
+    long gx = ctas > 0 ? ctas : sms;  // one CTA per SM (shared and tensor memory)
+    if (gx > nunit) gx = nunit;
+    WgradArgs a = g;
+    if (!a.partial) {
+      int dev = 0;
+      if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+      std::lock_guard<std::mutex> lock(g_part_mu);
+      const int want = (int)(gx > sms ? gx : sms);
+      if (g_part_blocks[dev] < want) {
+        float* p = nullptr;
+        if ((e = nemo::dev_alloc(&p, (size_t)want * WS_NPART * sizeof(float))) != cudaSuccess) return e;
+        if (g_part[dev]) {
+          // the old array may still be read by work queued on another stream
+          cudaDeviceSynchronize();
+          cudaFree(g_part[dev]);
+        }
+        g_part[dev] = p;
+        g_part_blocks[dev] = want;
+      }
+      a.partial = g_part[dev];
+      a.partial_blocks = g_part_blocks[dev];
+    }
+    if (gx > a.partial_blocks) gx = a.partial_blocks;
+    if (gx < 1) return cudaErrorInvalidValue;
+    k_conv_wgrad_strip<<<(unsigned)gx, THREADS, sizeof(WsSmem) + 1024, s>>>(tx, tz, a);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    k_wgrad_reduce<<<(WS_NPART + 31) / 32, 256, 0, s>>>(a.partial, (int)gx, g.dw, g.db);
+    return cudaGetLastError();
+  }
+  if ((e = act_map(&tx, x, g.N, g.H, g.W, WG_PIX)) != cudaSuccess) return e;
   if (g_wgrad_variant == 1) {
     // one CTA per SM: one wave of the 2 tap groups
     int gx = ctas > 0 ? ctas : sms / 2;

@@ -5,6 +5,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include "nemo_alloc.h"
 #include "nemo_b200.h"
 
 namespace sur {
@@ -24,14 +25,31 @@ struct ConvEpi {
   int N, H, W;
   int* err;  // device flag, first failing wait's code
   int out32_ch;
+  // set by conv_fwd from the process-wide test settings (set_test_wait):
+  unsigned long long wait_ns;  // limit of the main waits; 0: the default 2 s
+  int skip_load;               // 1: CTA 0 omits its first input-row load
 };
 
+// Test settings of the forward kernel's failure path: the next conv_fwd
+// launches use `wait_ns` for their main waits (0: the default 2 s), and the
+// next `skip_launches` of them have CTA 0 omit one input-row load, so that a
+// wait for it runs out without any fault.  Returns the previous wait limit.
+unsigned long long set_test_wait(unsigned long long wait_ns, int skip_launches);
+
 // dw[tap][co][ci] += sum_p dz[p][co] x[p + off(tap)][ci]; db[co] += sum_p dz[p][co].
+// One CTA's partial weight and bias gradient in the default (strip) kernel.
+constexpr int WS_NPART = 9 * 64 * 64 + 64;
+
 struct WgradArgs {
   float* dw;
   float* db;
   int N, H, W;
   int* err;
+  // scratch of the default kernel: partial_blocks rows of WS_NPART floats, one
+  // per CTA, summed in a fixed order afterwards; null: a scratch array the
+  // library keeps per device (calls that overlap on the GPU then race on it)
+  float* partial;
+  int partial_blocks;
 };
 
 // W % 128 == 0, x and w 16-byte aligned; w = [9][64 out][64 in] BF16.
@@ -41,9 +59,13 @@ cudaError_t conv_fwd(const __nv_bfloat16* x, const __nv_bfloat16* w, const ConvE
 // ring kernels.  Returns the previous variant; out-of-range values leave the
 // setting unchanged.
 int set_fwd_variant(int variant, int rows);
-// Process-wide choice of the weight-gradient kernel: 1 = three vertical taps
-// per MMA (default), 0 = tap pairs.  Returns the previous variant.
+// Process-wide choice of the weight-gradient kernel: 2 = all taps per CTA over
+// column strips, summed in a fixed order (default, deterministic), 1 = three
+// vertical taps per MMA, 0 = tap pairs (1 and 0 add with atomics).  Returns the
+// previous variant.
 int set_wgrad_variant(int variant);
+// Kernels one conv_wgrad call launches with the current variant.
+int wgrad_kernels();
 // W % 64 == 0.  ctas <= 0 picks the count from the SM count.
 cudaError_t conv_wgrad(const __nv_bfloat16* x, const __nv_bfloat16* dz, const WgradArgs& g, int ctas,
                        cudaStream_t s);

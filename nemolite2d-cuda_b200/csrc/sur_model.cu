@@ -373,6 +373,8 @@ struct nemo_sur {
   int ms_cap = 0;
   double* d_acc = nullptr;
   int acc_cap = 0;
+  float* wpart = nullptr;        // weight-gradient partial sums, one row per CTA
+  int wpart_blocks = 0;
   long adam_t = 0;
   long long nlaunch = 0;  // kernels this surrogate has launched
 };
@@ -399,9 +401,9 @@ int conv(nemo_sur* s, const __nv_bfloat16* x, const __nv_bfloat16* w, const floa
 }
 
 int wgrad(nemo_sur* s, const __nv_bfloat16* x, const __nv_bfloat16* dz, int l, int n) {
-  sur::WgradArgs a{dW_of(s, l), dB_of(s, l), n, s->Hn, s->Wn, s->err};
+  sur::WgradArgs a{dW_of(s, l), dB_of(s, l), n, s->Hn, s->Wn, s->err, s->wpart, s->wpart_blocks};
   ECK(sur::conv_wgrad(x, dz, a, 0, s->stream));
-  s->nlaunch += 1;
+  s->nlaunch += sur::wgrad_kernels();
   return NEMO_OK;
 }
 
@@ -560,16 +562,16 @@ int ensure_members(nemo_sur* s, nemo_ens* e, std::vector<MemberState>& ms, Membe
     s->d_ms = s->d_ms2 = nullptr;
     s->tide_d = nullptr;
     s->ms_cap = 0;
-    ECK(cudaMalloc(&s->d_ms, nm * sizeof(MemberState)));
-    ECK(cudaMalloc(&s->d_ms2, nm * sizeof(MemberState)));
-    ECK(cudaMalloc(&s->tide_d, nm * sizeof(double)));
+    ECK(nemo::dev_alloc(&s->d_ms, nm * sizeof(MemberState)));
+    ECK(nemo::dev_alloc(&s->d_ms2, nm * sizeof(MemberState)));
+    ECK(nemo::dev_alloc(&s->tide_d, nm * sizeof(double)));
     s->ms_cap = nm;
   }
   if (6 * nm > s->acc_cap) {
     cudaFree(s->d_acc);
     s->d_acc = nullptr;
     s->acc_cap = 0;
-    ECK(cudaMalloc(&s->d_acc, 6 * nm * sizeof(double)));
+    ECK(nemo::dev_alloc(&s->d_acc, 6 * nm * sizeof(double)));
     s->acc_cap = 6 * nm;
   }
   MemberState* d = dst ? *dst : s->d_ms;
@@ -672,6 +674,7 @@ int nemo_sur_destroy(nemo_sur* s) {
   cudaFree(s->d_ms);
   cudaFree(s->d_ms2);
   cudaFree(s->d_acc);
+  cudaFree(s->wpart);
   if (s->h_loss) cudaFreeHost(s->h_loss);
   if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
   delete s;
@@ -715,16 +718,16 @@ int nemo_sur_create(const nemo_sur_config* c, nemo_sur** out) {
     s->own_stream = true;
   }
   const size_t pb = s->np * sizeof(float);
-  if (cudaMalloc(&s->p, pb) || cudaMalloc(&s->g, pb) || cudaMalloc(&s->wbf, s->nw * 2) ||
-      cudaMalloc(&s->wt, s->nw * 2) || cudaMalloc(&s->loss, sizeof(double)) || cudaMalloc(&s->err, sizeof(int)) ||
-      cudaMallocHost(&s->h_loss, sizeof(double)))
+  if (nemo::dev_alloc(&s->p, pb) || nemo::dev_alloc(&s->g, pb) || nemo::dev_alloc(&s->wbf, s->nw * 2) ||
+      nemo::dev_alloc(&s->wt, s->nw * 2) || nemo::dev_alloc(&s->loss, sizeof(double)) || nemo::dev_alloc(&s->err, sizeof(int)) ||
+      nemo::host_alloc(&s->h_loss, sizeof(double)))
     return fail(NEMO_ERR_ALLOC);
-  if (c->train && (cudaMalloc(&s->m, pb) || cudaMalloc(&s->v, pb))) return fail(NEMO_ERR_ALLOC);
+  if (c->train && (nemo::dev_alloc(&s->m, pb) || nemo::dev_alloc(&s->v, pb))) return fail(NEMO_ERR_ALLOC);
   const size_t ab = (size_t)s->nnet * CH * 2;
   const int nact = c->train ? 1 + (c->nblocks + 1) + c->nblocks + 4 : 4;
   for (int i = 0; i < nact; ++i) {
     __nv_bfloat16* a = nullptr;
-    if (cudaMalloc(&a, ab)) return fail(NEMO_ERR_ALLOC);
+    if (nemo::dev_alloc(&a, ab)) return fail(NEMO_ERR_ALLOC);
     s->act.push_back(a);
   }
   s->x0 = s->act[0];
@@ -737,10 +740,17 @@ int nemo_sur_create(const nemo_sur_config* c, nemo_sur** out) {
     s->g1 = s->act[k++];
     s->dt = s->act[k++];
   }
-  if (cudaMalloc(&s->out32, s->nnet * s->NO * sizeof(float)) || cudaMalloc(&s->snap, s->npix * 16) ||
-      cudaMalloc(&s->tide_f, c->batch * sizeof(float)))
+  if (nemo::dev_alloc(&s->out32, s->nnet * s->NO * sizeof(float)) || nemo::dev_alloc(&s->snap, s->npix * 16) ||
+      nemo::dev_alloc(&s->tide_f, c->batch * sizeof(float)))
     return fail(NEMO_ERR_ALLOC);
-  if (c->train && cudaMalloc(&s->tgt, s->npix * 16)) return fail(NEMO_ERR_ALLOC);
+  if (c->train && nemo::dev_alloc(&s->tgt, s->npix * 16)) return fail(NEMO_ERR_ALLOC);
+  if (c->train) {  // the weight gradient's per-CTA partial sums (one CTA per SM)
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev))
+      return fail(NEMO_ERR_CUDA);
+    if (nemo::dev_alloc(&s->wpart, (size_t)sms * sur::WS_NPART * sizeof(float))) return fail(NEMO_ERR_ALLOC);
+    s->wpart_blocks = sms;
+  }
   if (cudaMemsetAsync(s->err, 0, sizeof(int), s->stream) || cudaMemsetAsync(s->g, 0, pb, s->stream) ||
       (c->train && (cudaMemsetAsync(s->m, 0, pb, s->stream) || cudaMemsetAsync(s->v, 0, pb, s->stream))))
     return fail(NEMO_ERR_CUDA);
@@ -897,9 +907,9 @@ int nemo_ens_compare(nemo_ens* a, nemo_ens* ref, double* out) {
   SCK(join(nemo::ens_stream(ref), st));
   MemberState *da = nullptr, *dr = nullptr;
   double* acc = nullptr;
-  cudaError_t e = cudaMalloc(&da, nm * sizeof(MemberState));
-  if (e == cudaSuccess) e = cudaMalloc(&dr, nm * sizeof(MemberState));
-  if (e == cudaSuccess) e = cudaMalloc(&acc, 6 * nm * sizeof(double));
+  cudaError_t e = nemo::dev_alloc(&da, nm * sizeof(MemberState));
+  if (e == cudaSuccess) e = nemo::dev_alloc(&dr, nm * sizeof(MemberState));
+  if (e == cudaSuccess) e = nemo::dev_alloc(&acc, 6 * nm * sizeof(double));
   if (e == cudaSuccess) e = cudaMemcpyAsync(da, ma.data(), nm * sizeof(MemberState), cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(dr, mr.data(), nm * sizeof(MemberState), cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(acc, 0, 6 * nm * sizeof(double), st);
@@ -971,7 +981,7 @@ int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, 
   float* own = nullptr;
   const size_t out_per = (size_t)s->Hn * s->Wn * s->NO;  // FP32 outputs per member
   if (nm > s->cfg.batch) {
-    ECK(cudaMalloc(&own, (size_t)nm * (hw * 4 + out_per) * sizeof(float)));
+    ECK(nemo::dev_alloc(&own, (size_t)nm * (hw * 4 + out_per) * sizeof(float)));
     snap_all = own;
     out_all = own + (size_t)nm * hw * 4;
   }
@@ -984,7 +994,7 @@ int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, 
   double* saved = nullptr;
   const bool rewind = c->rewind && c->quarantine > 0 && c->per_member;
   if (rewind && nm > 0) {
-    cudaError_t ae = cudaMalloc(&saved, (size_t)NS * nm * 3 * field_elems * sizeof(double));
+    cudaError_t ae = nemo::dev_alloc(&saved, (size_t)NS * nm * 3 * field_elems * sizeof(double));
     if (ae != cudaSuccess) {
       if (own) cudaFree(own);
       return status_of(ae);
@@ -1143,7 +1153,7 @@ int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, 
       const double a = nemo::ens_amp(e, m);
       lim[m] = a > 0.0 ? 10.0 * a : INFINITY;
     }
-    cudaError_t fe = cudaMalloc(&d_lim, nm * (sizeof(double) + sizeof(int)));
+    cudaError_t fe = nemo::dev_alloc(&d_lim, nm * (sizeof(double) + sizeof(int)));
     if (fe == cudaSuccess) {
       d_flag = reinterpret_cast<int*>(d_lim + nm);
       fe = join(nemo::ens_stream(e), s->stream) == NEMO_OK ? cudaSuccess : cudaErrorUnknown;
@@ -1200,10 +1210,16 @@ int nemo_conv3x3_fwd_variant(int variant, int rows) { return sur::set_fwd_varian
 
 int nemo_conv3x3_wgrad_variant(int variant) { return sur::set_wgrad_variant(variant); }
 
+int nemo_debug_conv_wait(unsigned long long wait_ns, int skip_launches) {
+  if (skip_launches < 0) return NEMO_ERR_INVALID;
+  sur::set_test_wait(wait_ns, skip_launches);
+  return NEMO_OK;
+}
+
 int nemo_conv3x3_wgrad(const void* x, const void* dz, float* dw, float* db, int n, int h, int wd, int ctas,
                        int* err, void* stream) {
   if (!x || !dz || !dw || !err) return NEMO_ERR_INVALID;
-  sur::WgradArgs a{dw, db, n, h, wd, err};
+  sur::WgradArgs a{dw, db, n, h, wd, err, nullptr, 0};
   ECK(sur::conv_wgrad((const __nv_bfloat16*)x, (const __nv_bfloat16*)dz, a, ctas, (cudaStream_t)stream));
   return NEMO_OK;
 }

@@ -46,6 +46,7 @@ EXPORTED = [
     "nemo_sur_train_step", "nemo_sur_pack_ens", "nemo_sur_advance_ens", "nemo_ens_compare",
     "nemo_hyb_default_config", "nemo_hyb_run", "nemo_conv3x3_fwd", "nemo_conv3x3_wgrad",
     "nemo_conv3x3_fwd_variant", "nemo_conv3x3_wgrad_variant", "nemo_debug_fail_alloc",
+    "nemo_debug_conv_wait",
     "cuda_setup_model_params_", "cuda_initialise_grid_", "cuda_continuity_", "cuda_momentum_",
     "cuda_boundary_conditions_", "cuda_next_", "cuda_retrieve_grid_constants_",
     "cuda_retrieve_results_", "cuda_finalise_", "nemo_compat_last_status", "nemo_compat_context",
@@ -148,6 +149,7 @@ def load(strict=False):
                                          ctypes.c_void_p, ctypes.c_void_p]
     L.nemo_autotune.argtypes = [vp, ip, P(Schedule), P(dp)]
     L.nemo_debug_fail_alloc.argtypes = [ip]
+    L.nemo_debug_conv_wait.argtypes = [ctypes.c_ulonglong, ip]
     L.nemo_ens_generate.argtypes = [ctypes.c_uint64, ip, ip, ip, dp, P(Member)]
     L.nemo_ens_create.argtypes = [P(Params), P(Member), ip, P(vp)]
     L.nemo_ens_destroy.argtypes = [vp]

@@ -89,25 +89,32 @@ def generate_runs(sur, seed, nmem, side, steps, every=10, amp_scale=0.2, strict=
 generate_runs.dropped = 0
 
 
-def bounded_members(members, steps, common, bound=2.5, checks=2):
+def bounded_members(members, steps, common, bound=2.5, checks=2, batch=64, want=None):
     """Indices of the members whose FP64 run from rest stays bounded: finite
     and max |ssh| <= bound x the member's tidal amplitude at `checks` evenly
-    spaced points of the run (the last at `steps`)."""
-    ens = Ensemble(members, **common)
-    alive = list(range(len(members)))
-    done = 0
-    for k in range(1, checks + 1):
-        to = steps * k // checks
-        ens.step_n(done + 1, to - done)
-        done = to
-        keep = []
-        for i in alive:
-            ssh = ens.field(i, SSHN)
-            if np.isfinite(ssh).all() and np.abs(ssh).max() <= bound * members[i].amp_tide:
-                keep.append(i)
-        alive = keep
-    ens.close()
-    return alive
+    spaced points of the run (the last at `steps`).  Screens `batch` members
+    per ensemble and stops once `want` members passed (None: screen all)."""
+    out = []
+    for b0 in range(0, len(members), batch):
+        if want is not None and len(out) >= want:
+            break
+        idx = list(range(b0, min(b0 + batch, len(members))))
+        ens = Ensemble([members[i] for i in idx], **common)
+        alive = list(range(len(idx)))
+        done = 0
+        for k in range(1, checks + 1):
+            to = steps * k // checks
+            ens.step_n(done + 1, to - done)
+            done = to
+            keep = []
+            for i in alive:
+                ssh = ens.field(i, SSHN)
+                if np.isfinite(ssh).all() and np.abs(ssh).max() <= bound * members[idx[i]].amp_tide:
+                    keep.append(i)
+            alive = keep
+        ens.close()
+        out += [idx[i] for i in alive]
+    return out
 
 
 def compute_norm(snaps, paired=False):

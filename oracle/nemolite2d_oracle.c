@@ -605,6 +605,14 @@ int oracle_set_state(oracle_model* m, const double* sshn, const double* un,
   k = 0;
   for (int jj = 0; jj <= jpj; ++jj)
     for (int ji = 1; ji <= jpi; ++ji) m->vn[I(ji, jj)] = vn[k++];
+  /* the state as after a complete step, where `next` (:712-732) has made the
+   * after-step fields equal to the current ones */
+  for (int jj = 1; jj <= jpj; ++jj)
+    for (int ji = 1; ji <= jpi; ++ji) m->ssha[I(ji, jj)] = m->sshn[I(ji, jj)];
+  for (int jj = 1; jj <= jpj; ++jj)
+    for (int ji = 0; ji <= jpi; ++ji) m->ua[I(ji, jj)] = m->un[I(ji, jj)];
+  for (int jj = 0; jj <= jpj; ++jj)
+    for (int ji = 1; ji <= jpi; ++ji) m->va[I(ji, jj)] = m->vn[I(ji, jj)];
   derive_sshn_uv(m);
   return 0;
 }

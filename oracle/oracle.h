@@ -80,8 +80,10 @@ void oracle_run(oracle_model* m, int istp0, int nsteps);
 /* Copy a field's Fortran-bounded region into a dense column-major array.
  * Extents: T (jpi,jpj), U (jpi+1,jpj), V (jpi,jpj+1).  Returns count or -1. */
 long oracle_get_field(const oracle_model* m, int field, double* out);
-/* Replace sshn/un/vn (dense, same extents) and re-derive sshn_u/sshn_v with
- * the post-`next` interpolation (:736-764). */
+/* Replace sshn/un/vn (dense, same extents), set ssha/ua/va to the same
+ * values (the state as after a complete step, where `next` has copied them,
+ * :712-732) and re-derive sshn_u/sshn_v with the post-`next` interpolation
+ * (:736-764). */
 int oracle_set_state(oracle_model* m, const double* sshn, const double* un,
                      const double* vn);
 

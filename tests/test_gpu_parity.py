@@ -432,6 +432,58 @@ def test_strict_general_grid_step_n_matches_oracle(nb, oracle_mod):
         m.autotune(2)
 
 
+def _channel_grid(seed, jpi, jpj):
+    """random_grid plus open cells inside the domain that form one-cell water
+    channels between two open cells along x and along y (the only places where
+    the reference's in-place Flather sweeps chain two updates), and an open
+    cell next to an island."""
+    from gridcases import random_grid
+    pt, g = random_grid(seed, jpi, jpj)
+    for jj in (20, 21, 40):
+        pt[jj, 30] = -1
+        pt[jj, 31] = 1
+        pt[jj, 32] = -1
+    for ji in (60, 61):
+        pt[50, ji] = -1
+        pt[51, ji] = 1
+        pt[52, ji] = -1
+    pt[70, 90] = -1
+    pt[70, 91] = 0
+    return pt, g
+
+
+@pytest.mark.parametrize("strict", [True, False])
+def test_general_fused_step_equals_routines_with_flather_chains(nb, oracle_mod, strict):
+    """The general grid's fused step (one kernel plus the Flather chains)
+    against the per-routine kernels and the oracle, from a random state, on a
+    mask with interior open cells and one-cell channels in both directions:
+    bitwise in the strict build, within 1e-12 in the default build."""
+    from gridcases import NAMES
+    jpi, jpj = 150, 97
+    kw = dict(jpi=jpi, jpj=jpj, rdt=10.0, cbfr=0.00015, visc=0.1, amp_tide=0.3)
+    pt, g = _channel_grid(8, jpi, jpj)
+    rng = np.random.default_rng(3)
+    st = (rng.normal(0, 0.05, (jpj, jpi)), rng.normal(0, 0.1, (jpj, jpi + 1)),
+          rng.normal(0, 0.1, (jpj + 1, jpi)))
+    fused = nb.Model(strict=strict, **kw)
+    routine = nb.Model(strict=strict, **kw)
+    o = oracle_mod.Model(**kw)
+    for m in (fused, routine, o):
+        m.set_grid(pt, *[g[n] for n in NAMES])
+        m.set_state(*st)
+    fused.step_n(1, 6)
+    for istp in range(1, 7):
+        routine.step(istp)
+        o.step(istp)
+    for name, fid in STATE:
+        a, b, r = fused.field(fid), routine.field(fid), o.field(fid)
+        if strict:
+            np.testing.assert_array_equal(bits(a), bits(r), err_msg="fused " + name)
+            np.testing.assert_array_equal(bits(b), bits(r), err_msg="routines " + name)
+        else:
+            assert relerr(a, r) <= TOL and relerr(b, r) <= TOL, name
+
+
 def test_default_grid_through_set_grid_is_the_built_in_grid(nb):
     """The reference's grid passed as arrays gives, in the strict build, the
     same bits as the built-in grid (routine path and fused path)."""

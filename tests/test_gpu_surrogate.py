@@ -115,10 +115,10 @@ def test_dgrad_with_flipped_weights_matches_oracle(env, variant):
     assert np.abs(o32 - ref[..., :4]).max() <= 1e-4 * np.abs(ref[..., :4]).max()
 
 
-@pytest.fixture(params=[1, 0], ids=["wg-tri", "wg-pairs"])
+@pytest.fixture(params=[2, 1, 0], ids=["wg-strip", "wg-tri", "wg-pairs"])
 def wvariant(request, env):
-    """Each weight-gradient kernel (six taps per MMA, tap pairs), restored to
-    the default afterwards."""
+    """Each weight-gradient kernel (all taps per CTA with a fixed-order sum,
+    six taps per MMA, tap pairs), restored to the default afterwards."""
     torch, nb, sm = env
     lib = nb.load(False)
     prev = sm.conv3x3_wgrad_variant(lib, request.param)
@@ -147,6 +147,54 @@ def test_wgrad_and_bias_grad_match_oracle(env, wvariant, shape, ctas):
     gb = db.cpu().numpy() + 1.0
     assert np.abs(gw - rw).max() <= 1e-4 * np.abs(rw).max()
     assert np.abs(gb - rb).max() <= 1e-4 * np.abs(rb).max()
+
+
+@pytest.mark.parametrize("shape,ctas", [((4, 33, 256), 0), ((2, 9, 128), 7)])
+def test_default_wgrad_is_bitwise_repeatable(env, shape, ctas):
+    """The default weight gradient sums per-CTA partials in a fixed order: the
+    same inputs give the same bits on every call (the atomic variants do not
+    promise that)."""
+    torch, nb, sm = env
+    lib = nb.load(False)
+    assert sm.conv3x3_wgrad_variant(lib, -1) == 2  # the default
+    N, H, W = shape
+    g = torch.Generator(device="cuda").manual_seed(5)
+    x = torch.randn((N, H, W, 64), device="cuda", generator=g).to(torch.bfloat16)
+    dz = torch.randn((N, H, W, 64), device="cuda", generator=g).to(torch.bfloat16)
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    outs = []
+    for _ in range(3):
+        dw = torch.zeros((9, 64, 64), dtype=torch.float32, device="cuda")
+        db = torch.zeros(64, dtype=torch.float32, device="cuda")
+        sm.conv3x3_wgrad(lib, x.data_ptr(), dz.data_ptr(), dw.data_ptr(), N, H, W, err.data_ptr(),
+                         db=db.data_ptr(), ctas=ctas, stream=torch.cuda.current_stream().cuda_stream)
+        outs.append((dw.cpu().numpy().view(np.int32), db.cpu().numpy().view(np.int32)))
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    for dw, db in outs[1:]:
+        np.testing.assert_array_equal(dw, outs[0][0])
+        np.testing.assert_array_equal(db, outs[0][1])
+
+
+def test_training_is_reproducible(env):
+    """Two surrogates with the same seed trained on the same batches end with
+    bit-identical parameters: every kernel of the training step, the weight
+    gradient included, is free of order-dependent sums."""
+    torch, nb, sm = env
+    N, H, W = 4, 16, 128
+    rng = np.random.default_rng(12)
+    snap0, snap1, tide, norm, d = random_setup(rng, torch, N, H, W)
+    hp = sm.adamw(lr=2e-3, weight_decay=1e-4)
+    params = []
+    for _ in range(2):
+        s = sm.Surrogate(nblocks=2, batch=N, height=H, width=W, seed=31)
+        s.set_norm(*norm)
+        for _ in range(5):
+            s.train_step(d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), N, hp)
+        torch.cuda.synchronize()
+        params.append(s.params())
+        s.close()
+    np.testing.assert_array_equal(params[0].view(np.int32), params[1].view(np.int32))
 
 
 def test_conv_rejects_unsupported_shapes(env):
