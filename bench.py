@@ -97,6 +97,7 @@ def parse():
                     help="hybrid points anchor:tol:quarantine,... run after one training")
     ap.add_argument("--repeats", type=int, default=1, help="hybrid runs per point (median reported)")
     ap.add_argument("--candidates", type=int, default=128, help="hybrid member candidates")
+    ap.add_argument("--strict", action="store_true", help="time the -fmad=false library (general)")
     ap.add_argument("--n", type=int, default=N,
                     help="grid side (profiling of smaller cases only; the bench line is 4096)")
     return ap.parse_args()
@@ -755,7 +756,7 @@ def run_general(args):
     torch.cuda.set_device(0)
     n = args.n
     stream = torch.cuda.Stream()
-    m = nemo_b200.Model(strict=False, stream=stream.cuda_stream, device=0, jpi=n, jpj=n, rdt=10.0,
+    m = nemo_b200.Model(strict=args.strict, stream=stream.cuda_stream, device=0, jpi=n, jpj=n, rdt=10.0,
                         cbfr=0.00015, visc=0.1, amp_tide=0.3)
     pt, g = general_grid(n, n)
     names = ("e1t", "e2t", "e1u", "e2u", "e1v", "e2v", "gphiu", "gphiv", "ht", "hu", "hv")
@@ -792,7 +793,7 @@ def run_general(args):
             "roofline": {"bound": "hbm", "kernel": "k_fused_general", "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": kind,
                          "algorithmic_bytes_per_cell_step": GEN_BYTES_PER_CELL_STEP},
-            "checksums_last": [float(x) for x in ck],
+            "checksums_last": [float(x) for x in ck], "build": "strict" if args.strict else "default",
             "gpu_launches": args.steps * (2 * 100 + 2), "clocks": clk}
     print(json.dumps(line), flush=True)
     m.close()

@@ -33,7 +33,13 @@
 // where the reference masks the two uses differently (the slip-wall forms)
 // each use has its own value.  e12t, e12u, e12v are formed in the kernel as
 // the products the reference stores (:263-279), zero outside their ranges.
-// Quotients are IEEE divisions in both builds.
+// Quotients: IEEE division in the -fmad=false build (bit-exact with the
+// oracle).  The default build, which the reference's 1e-12 tolerance governs,
+// multiplies by Newton reciprocals of the scale factors (the grid-constant
+// sites of the uniform kernel's default build), and keeps the two quotients
+// that scale the new velocities every step rounded as that build does: the
+// depth by the corrected quotient, the friction factor by the two-part
+// reciprocal.
 #include "nemo_step_dev.cuh"
 
 namespace nemo {
@@ -43,6 +49,28 @@ using stepdev::FULL;
 using stepdev::dn;
 using stepdev::up;
 using stepdev::upw;
+
+using stepdev::kRoundedQuotients;
+
+// a / b for a scale-factor divisor.
+__device__ __forceinline__ double qm(double a, double b) {
+  if (kRoundedQuotients) return a / b;
+  return a * recip_nr(b);
+}
+// a / h for a static depth h: the corrected quotient from a one-step Newton
+// reciprocal in the default build (the rounded quotient except within about
+// 2^-39 ulp of a rounding boundary).
+__device__ __forceinline__ double qh(double a, double h) {
+  if (kRoundedQuotients) return a / h;
+  bool bad = false;
+  return stepdev::qdiv<false>(a, h, recip_nr1(h), bad);
+}
+// a / cfric
+__device__ __forceinline__ double qf(double a, const Consts& C) {
+  if (kRoundedQuotients) return a / C.cfric;
+  bool bad = false;
+  return stepdev::qdiv_fric<false>(a, C, bad);
+}
 
 __device__ __forceinline__ int dni(int x) { return __shfl_down_sync(FULL, x, 1); }
 __device__ __forceinline__ int upi(int x) { return __shfl_up_sync(FULL, x, 1); }
@@ -92,7 +120,7 @@ __device__ __forceinline__ double sshn_u_at(const GNext& x, int c, int r, int jp
   const double t0 = e12t_at(x, c, r, jpi, jpj);
   const double t1 = dn(t0);
   if (a + b > 0) {
-    if (a * b > 0) return 0.5 * (t0 * x.s + t1 * s1) / (x.e1u * x.e2u);
+    if (a * b > 0) return qm(0.5 * (t0 * x.s + t1 * s1), x.e1u * x.e2u);
     if (a <= 0) return s1;
     return x.s;
   }
@@ -106,7 +134,7 @@ __device__ __forceinline__ double sshn_v_at(const GNext& x, const GOwn& w, const
   if (a + b > 0) {
     if (a * b > 0) {
       const double t0 = e12t_at(x, c, j, jpi, jpj), t1 = e12t_at(y, c, j + 1, jpi, jpj);
-      return 0.5 * (t0 * x.s + t1 * y.s) / (w.e1v * w.e2v);
+      return qm(0.5 * (t0 * x.s + t1 * y.s), w.e1v * w.e2v);
     }
     if (a <= 0) return y.s;
     return x.s;
@@ -163,12 +191,12 @@ k_fused_general(Layout L, Consts C, GenArgs A, int tile_y) {
     const bool ms = p.pt <= 0 || dni(p.pt) <= 0;  // pt(ji,jj-1), pt(ji+1,jj-1) of u(c, J0)
     k.Fuy_s = (ms ? upwind_hi_only(vfl, cur.u) : upw(vfl, p.u, cur.u)) * vfl * depc;
     k.vnc_s = vnc;
-    k.dudy_s = ms ? 0.0 : (cur.u - p.u) / (cur.e2u + p.e2u) * (cur.hu + k.su + p.hu + su_p);
+    k.dudy_s = ms ? 0.0 : qm(cur.u - p.u, cur.e2u + p.e2u) * (cur.hu + k.su + p.hu + su_p);
     // T(c, J0): the south face of v(c, J0)
     const double vs = 0.5 * (cur.v + p.v) * cur.e1t;
     const double deps = cur.ht + cur.s;
     k.Fvy_s = upw(vs, p.v, cur.v) * vs * deps;
-    k.Dvy_s = (cur.v - p.v) / cur.e2t * deps;
+    k.Dvy_s = qm(cur.v - p.v, cur.e2t) * deps;
     k.pt_s = p.pt;
     if (J0 == 1 && store) {
       // v(c, 0): outside the momentum loop (:520); solid wall (:656-660) or
@@ -196,7 +224,7 @@ k_fused_general(Layout L, Consts C, GenArgs A, int tile_y) {
     const double r1 = (k.su + cur.hu) * cur.u;
     const double r2 = up(r1);
     const double r3 = (sv + w.hv) * cur.v;
-    double ssha = cur.s + (r2 - r1 + k.cf_s - r3) * C.rdt / e12t_at(cur, c, j, jpi, jpj);
+    double ssha = cur.s + qm((r2 - r1 + k.cf_s - r3) * C.rdt, e12t_at(cur, c, j, jpi, jpj));
     if (cur.pt > 0 && (k.pt_s < 0 || nx.pt < 0 || pt_e < 0 || pt_w < 0)) ssha = A.tide;
 
     // ---- x-face at T(c,j), between u(c-1,j) and u(c,j) ----
@@ -204,7 +232,7 @@ k_fused_general(Layout L, Consts C, GenArgs A, int tile_y) {
     const double uw = 0.5 * (cur.u + u_wn) * cur.e2t;
     const double dep = cur.ht + cur.s;
     const double Fx = upw(uw, u_wn, cur.u) * uw * dep;
-    const double Dx = (cur.u - u_wn) / cur.e1t * dep;
+    const double Dx = qm(cur.u - u_wn, cur.e1t) * dep;
 
     // ---- corner (c,j): north face of u(c,j) / south face of u(c,j+1) ----
     const double v_e = dn(cur.v);
@@ -216,7 +244,7 @@ k_fused_general(Layout L, Consts C, GenArgs A, int tile_y) {
     const double Fuy_full = upw(vfl, cur.u, nx.u) * vfl * depc;
     const double Fuy_n = mn ? upwind_lo_only(vfl, cur.u) * vfl * depc : Fuy_full;
     const double Fuy_s_next = ms ? upwind_hi_only(vfl, nx.u) * vfl * depc : Fuy_full;
-    const double Gy = (nx.u - cur.u) / (cur.e2u + nx.e2u);
+    const double Gy = qm(nx.u - cur.u, cur.e2u + nx.e2u);
     const double dudy_n = mn ? 0.0 : Gy * (cur.hu + k.su + nx.hu + su_n);
     const double dudy_s_next = ms ? 0.0 : Gy * (nx.hu + su_n + cur.hu + k.su);
     // ---- corner (c,j): east face of v(c,j) / west face of v(c+1,j) ----
@@ -229,14 +257,14 @@ k_fused_general(Layout L, Consts C, GenArgs A, int tile_y) {
     const double Fvx_e = me ? upwind_lo_only(ufl, cur.v) * ufl * depcu : Fvx_full;
     const double Fvx_w_next = mw_next ? upwind_hi_only(ufl, v_e) * ufl * depcu : Fvx_full;
     const double hv_e = dn(w.hv), sv_e = dn(sv);
-    const double Gx = (v_e - cur.v) / (w.e1v + dn(w.e1v));
+    const double Gx = qm(v_e - cur.v, w.e1v + dn(w.e1v));
     const double dvdx_e = me ? 0.0 : Gx * (w.hv + sv + hv_e + sv_e);
     const double dvdx_w_next = mw_next ? 0.0 : Gx * (hv_e + sv_e + w.hv + sv);
     // ---- y-face at T(c,j+1), between v(c,j) and v(c,j+1) ----
     const double vfn = 0.5 * (cur.v + nx.v) * nx.e1t;
     const double depn = nx.ht + nx.s;
     const double Fvy_n = upw(vfn, cur.v, nx.v) * vfn * depn;
-    const double Dvy_n = (nx.v - cur.v) / nx.e2t * depn;
+    const double Dvy_n = qm(nx.v - cur.v, nx.e2t) * depn;
 
     // ---- u equation at u(c,j) (:431-517), solid walls (:648-652) ----
     const double Fx_e = dn(Fx), Dx_e = dn(Dx);
@@ -249,7 +277,7 @@ k_fused_general(Layout L, Consts C, GenArgs A, int tile_y) {
       const double e12u = cur.e1u * cur.e2u;
       const double cor = 0.5 * (w.fcu * (k.vnc_s + vnc)) * e12u * Hu;
       const double hpg = -(C.g * Hu * cur.e2u * (s_e - cur.s));
-      ua = (cur.u * Hu + C.rdt * (adv + vis + cor + hpg) / e12u) / (cur.hu + 0.0) / C.cfric;
+      ua = qf(qh(cur.u * Hu + qm(C.rdt * (adv + vis + cor + hpg), e12u), cur.hu + 0.0), C);
     } else {
       ua = (cur.pt * pt_e == 0) ? 0.0 : cur.u;
     }
@@ -265,7 +293,7 @@ k_fused_general(Layout L, Consts C, GenArgs A, int tile_y) {
       const double e12v = w.e1v * w.e2v;
       const double cor = -(0.5 * (w.fcv * (uec + uec_w)) * e12v * Hv);
       const double hpg = -(C.g * Hv * w.e1v * (nx.s - cur.s));
-      va = (cur.v * Hv + C.rdt * (adv + vis + cor + hpg) / e12v) / (w.hv + 0.0) / C.cfric;
+      va = qf(qh(cur.v * Hv + qm(C.rdt * (adv + vis + cor + hpg), e12v), w.hv + 0.0), C);
     } else {
       va = (cur.pt * nx.pt == 0) ? 0.0 : cur.v;
     }
