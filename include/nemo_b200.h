@@ -228,9 +228,14 @@ typedef struct nemo_ens nemo_ens;
 typedef struct nemo_ens_schedule {
   int warps;      /* warps per CTA: 2 or 4 */
   int occupancy;  /* as nemo_schedule.occupancy: 116, 120 (2 warps), 116 (4
-                     warps), 20, 24, -20, -24 (2 warps), 20, 24, -20 (4) */
+                     warps), 20, 24, -20, -24 (2 warps), 20, 24, -20 (4);
+                     212, 216, 220 (2 warps) and 212, 216 (4 warps) stage rows
+                     through shared memory with in-kernel reciprocal depths
+                     at a budget of 12, 16, 20 resident warps per SM */
   int rows;       /* rows per work item */
-  int order;      /* work-list order: 0 member by member, 1 largest member first */
+  int order;      /* work-list order: 0 member by member, 1 largest member first,
+                     2 dynamic: warps take the next item as they finish one,
+                     items largest first (suits tall row blocks, e.g. 128) */
   int ctas;       /* persistent grid size; 0: every resident CTA slot */
 } nemo_ens_schedule;
 

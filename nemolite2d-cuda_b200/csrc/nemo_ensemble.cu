@@ -36,13 +36,27 @@ struct MemberDev {
   const double *rhu, *rhv;
 };
 
+// Next work item of a warp under the dynamic schedule: one atomic per item.
+__device__ __forceinline__ int ens_fetch(int* counter, int lane) {
+  int w = 0;
+  if (lane == 0) w = atomicAdd(counter, 1);
+  return __shfl_sync(0xffffffffu, w, 0);
+}
+
+// counter == nullptr: warp w takes items w, w + W, w + 2W, ... (W warps in
+// the grid).  Otherwise the dynamic schedule: warps take the next item of the
+// list from counter[parity] as they finish one (the list is ordered largest
+// first), and the launch resets counter[parity ^ 1] for the next launch,
+// whose buffer parity is the other one.
 template <int NW, int MB, int PF>
 __global__ void __launch_bounds__(32 * NW, MB)
 k_ens_step(const MemberDev* __restrict__ mem, const int4* __restrict__ work, int nwork, Consts C,
-           const double* __restrict__ tide, int parity) {
+           const double* __restrict__ tide, int parity, int* counter) {
   const int lane = threadIdx.x & 31;
   const int nw = (int)gridDim.x * NW;
-  for (int w = (int)blockIdx.x * NW + (int)(threadIdx.x >> 5); w < nwork; w += nw) {
+  if (counter && blockIdx.x == 0 && threadIdx.x == 0) counter[parity ^ 1] = 0;
+  for (int w = counter ? ens_fetch(counter + parity, lane) : (int)blockIdx.x * NW + (int)(threadIdx.x >> 5);
+       w < nwork; w = counter ? ens_fetch(counter + parity, lane) : w + nw) {
     const int4 it = work[w];  // member, c0, J0, J1
     const MemberDev* M = mem + it.x;
     FusedArgs A;
@@ -121,7 +135,7 @@ __global__ void __launch_bounds__(CT) k_ens_cols(const int* __restrict__ row_off
 
 template <int NW, int MB, int PF>
 cudaError_t launch_ens_variant(const MemberDev* mem, const int4* work, int nwork, const Consts& C,
-                               const double* tide, int parity, int ctas, cudaStream_t s) {
+                               const double* tide, int parity, int ctas, int* counter, cudaStream_t s) {
   if (ctas <= 0) {
     static int slots = 0;
     if (slots == 0) {
@@ -136,16 +150,17 @@ cudaError_t launch_ens_variant(const MemberDev* mem, const int4* work, int nwork
   const int need = (nwork + NW - 1) / NW;
   if (ctas > need) ctas = need;
   if (ctas < 1) ctas = 1;
-  k_ens_step<NW, MB, PF><<<ctas, 32 * NW, 0, s>>>(mem, work, nwork, C, tide, parity);
+  k_ens_step<NW, MB, PF><<<ctas, 32 * NW, 0, s>>>(mem, work, nwork, C, tide, parity, counter);
   return cudaGetLastError();
 }
 
 cudaError_t launch_ens(int warps, int occ, const MemberDev* mem, const int4* work, int nwork,
-                       const Consts& C, const double* tide, int parity, int ctas,
+                       const Consts& C, const double* tide, int parity, int ctas, int* counter,
                        cudaStream_t s) {
-#define ENS(NW, MB, PF) launch_ens_variant<NW, MB, PF>(mem, work, nwork, C, tide, parity, ctas, s)
+#define ENS(NW, MB, PF) launch_ens_variant<NW, MB, PF>(mem, work, nwork, C, tide, parity, ctas, counter, s)
   if (warps == 2) {
     switch (occ) {
+      case 212: return ENS(2, 6, 3);
       case 216: return ENS(2, 8, 3);
       case 220: return ENS(2, 10, 3);
       case 116: return ENS(2, 8, 2);
@@ -157,6 +172,7 @@ cudaError_t launch_ens(int warps, int occ, const MemberDev* mem, const int4* wor
     }
   } else if (warps == 4) {
     switch (occ) {
+      case 212: return ENS(4, 3, 3);
       case 216: return ENS(4, 4, 3);
       case 116: return ENS(4, 4, 2);
       case -20: return ENS(4, 5, 0);
@@ -169,8 +185,8 @@ cudaError_t launch_ens(int warps, int occ, const MemberDev* mem, const int4* wor
 }
 
 bool ens_variant_ok(int warps, int occ, bool nr_ok) {
-  if (warps == 2 && (occ == 216 || occ == 220)) return nr_ok;
-  if (warps == 4 && occ == 216) return nr_ok;
+  if (warps == 2 && (occ == 212 || occ == 216 || occ == 220)) return nr_ok;
+  if (warps == 4 && (occ == 212 || occ == 216)) return nr_ok;
   if (warps == 2) return occ == -24 || occ == -20 || occ == 20 || occ == 24 || occ == 116 || occ == 120;
   if (warps == 4) return occ == -20 || occ == 20 || occ == 24 || occ == 116;
   return false;
@@ -227,6 +243,7 @@ struct nemo_ens {
   std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
   long long cells = 0;
   int4* d_work_sub = nullptr;  // work list of a member subset (ens_step_subset)
+  int* d_counter = nullptr;    // dynamic schedule: [main parity 0, 1, subset parity 0, 1]
   int sub_cap = 0;
   bool recip_nr_ok = false;    // every member's depths pass launch_recip's check
 };
@@ -247,11 +264,13 @@ void drop_graphs(nemo_ens* e) {
 // schedule's order: row blocks of `rows` rows, each split into 30-column
 // strips, neighbouring strips of one row block consecutive so concurrently
 // running warps share halo rows in L2.
+// Order 2 (the dynamic schedule) lists the same items largest first: the
+// members by size, then every item of R rows before the shorter last blocks.
 std::vector<int4> work_items(const nemo_ens* e, const char* sel) {
   const int R = e->sched.rows;
   std::vector<int> order(e->mem.size());
   for (size_t m = 0; m < order.size(); ++m) order[m] = (int)m;
-  if (e->sched.order == 1)
+  if (e->sched.order >= 1)
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
       return (long)e->mem[a].jpi * e->mem[a].jpj > (long)e->mem[b].jpi * e->mem[b].jpj;
     });
@@ -262,7 +281,13 @@ std::vector<int4> work_items(const nemo_ens* e, const char* sel) {
     for (int J0 = 1; J0 <= jpj; J0 += R)
       for (int c0 = 1; c0 <= jpi; c0 += 30) w.push_back(make_int4(m, c0, J0, std::min(J0 + R - 1, jpj)));
   }
+  if (e->sched.order == 2)
+    std::stable_sort(w.begin(), w.end(), [](const int4& a, const int4& b) { return a.w - a.z > b.w - b.z; });
   return w;
+}
+
+int* counter_of(nemo_ens* e, bool subset) {
+  return e->sched.order == 2 ? e->d_counter + (subset ? 2 : 0) : nullptr;
 }
 
 int build_work(nemo_ens* e) {
@@ -317,7 +342,8 @@ int launch_steps(nemo_ens* e, int n, int p0) {
   const size_t nm = e->mem.size();
   for (int k = 0; k < n; ++k)
     ECK(launch_ens(e->sched.warps, e->sched.occupancy, e->d_mem, e->d_work, e->nwork, e->C,
-                   e->d_tide + (size_t)k * nm, (p0 + k) & 1, e->sched.ctas, e->stream));
+                   e->d_tide + (size_t)k * nm, (p0 + k) & 1, e->sched.ctas, counter_of(e, false),
+                   e->stream));
   return NEMO_OK;
 }
 
@@ -366,6 +392,7 @@ int nemo_ens_destroy(nemo_ens* e) {
   cudaFree(e->d_row_cnt);
   cudaFree(e->d_partial);
   cudaFree(e->d_ck);
+  cudaFree(e->d_counter);
   cudaFree(e->d_tide);
   if (e->h_ck) cudaFreeHost(e->h_ck);
   if (e->h_tide) cudaFreeHost(e->h_tide);
@@ -504,6 +531,8 @@ int nemo_ens_create(const nemo_params* common, const nemo_member* members, int n
   if (err == cudaSuccess) err = nemo::dev_alloc(&e->d_row_cnt, nm * sizeof(int));
   if (err == cudaSuccess) err = nemo::dev_alloc(&e->d_partial, 3 * rows.size() * sizeof(double));
   if (err == cudaSuccess) err = nemo::dev_alloc(&e->d_ck, 3 * nm * sizeof(double));
+  if (err == cudaSuccess) err = nemo::dev_alloc(&e->d_counter, 4 * sizeof(int));
+  if (err == cudaSuccess) err = cudaMemsetAsync(e->d_counter, 0, 4 * sizeof(int), e->stream);
   if (err == cudaSuccess) err = nemo::host_alloc(&e->h_ck, 3 * nm * sizeof(double));
   if (err == cudaSuccess) err = cudaEventCreateWithFlags(&e->tide_ev, cudaEventDisableTiming);
   if (err == cudaSuccess)
@@ -611,12 +640,14 @@ int nemo_ens_set_state(nemo_ens* e, int member, const double* sshn, const double
 int nemo_ens_set_schedule(nemo_ens* e, const nemo_ens_schedule* s) {
   if (!e) return NEMO_ERR_STATE;
   if (!s || !ens_variant_ok(s->warps, s->occupancy, e->recip_nr_ok) || s->rows < 1 || s->rows > 65536 ||
-      s->order < 0 || s->order > 1 || s->ctas < 0)
+      s->order < 0 || s->order > 2 || s->ctas < 0)
     return NEMO_ERR_INVALID;
   int st = set_dev(e); if (st) return st;
   const bool rebuild = s->rows != e->sched.rows || s->order != e->sched.order;
   e->sched = *s;
   drop_graphs(e);
+  // the dynamic schedule's counters start from zero whatever ran before
+  ECK(cudaMemsetAsync(e->d_counter, 0, 4 * sizeof(int), e->stream));
   return rebuild ? build_work(e) : NEMO_OK;
 }
 
@@ -668,16 +699,17 @@ int nemo_ens_autotune(nemo_ens* e, int steps, nemo_ens_schedule* best, double* b
   e->use_graph = false;
   nemo_ens_schedule bsched = keep;
   double bms = 1e300;
-  const int warps_occ[][2] = {{2, 216}, {2, 220}, {4, 216}, {2, 116}, {2, 120}, {4, 116}, {2, -24},
+  const int warps_occ[][2] = {{2, 216}, {2, 220}, {4, 216}, {2, 212}, {4, 212}, {2, 116}, {2, 120}, {4, 116}, {2, -24},
                               {2, -20}, {2, 20}, {2, 24}, {4, -20}, {4, 20}, {4, 24}};
-  const int rows_c[] = {8, 16, 32};
+  const int rows_c[] = {8, 16, 32, 64, 128};
   cudaEvent_t t0 = nullptr, t1 = nullptr;
   if (er == cudaSuccess) er = cudaEventCreate(&t0);
   if (er == cudaSuccess) er = cudaEventCreate(&t1);
   for (const auto& wo : warps_occ) {
     if (!ens_variant_ok(wo[0], wo[1], e->recip_nr_ok)) continue;
     for (int rows : rows_c) {
-      for (int order = 0; order <= 1 && er == cudaSuccess; ++order) {
+      for (int order = 0; order <= 2 && er == cudaSuccess; ++order) {
+        if ((rows > 32) != (order == 2)) continue;  // tall blocks need the dynamic schedule
         nemo_ens_schedule c{wo[0], wo[1], rows, order, 0};
         if ((st = nemo_ens_set_schedule(e, &c))) break;
         nemo_ens_step_n(e, 1, 1);  // warm
@@ -758,7 +790,8 @@ int ens_step_subset(nemo_ens* e, int istp0, int n, const char* sel) {
   const size_t nm = e->mem.size();
   for (int k = 0; k < n; ++k)
     ECK(launch_ens(e->sched.warps, e->sched.occupancy, e->d_mem, e->d_work_sub, (int)w.size(), e->C,
-                   e->d_tide + (size_t)k * nm, (e->parity + k) & 1, e->sched.ctas, e->stream));
+                   e->d_tide + (size_t)k * nm, (e->parity + k) & 1, e->sched.ctas, counter_of(e, true),
+                   e->stream));
   return NEMO_OK;
 }
 cudaStream_t ens_stream(nemo_ens* e) { return e->stream; }

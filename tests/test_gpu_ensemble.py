@@ -42,7 +42,7 @@ def oracle_member(oracle_mod, m):
 @pytest.mark.parametrize("graph", [True, False])
 @pytest.mark.parametrize("sched", [(2, 216, 16, 1), (4, 216, 7, 0), (2, 220, 3, 0), (2, 116, 16, 1),
                                    (4, 116, 7, 0), (2, 120, 3, 1), (2, -24, 16, 1), (4, 20, 8, 0),
-                                   (2, 24, 5, 0)])
+                                   (2, 24, 5, 0), (4, 216, 128, 2), (2, 212, 64, 2), (4, 212, 9, 2)])
 def test_strict_ensemble_members_match_oracle_bitwise(nb, oracle_mod, graph, sched):
     members = nb.generate_members(7, 6, side_min=20, side_max=90, amp_scale=0.2)
     e = nb.Ensemble(members, strict=True, **COMMON)
@@ -76,15 +76,16 @@ CONFIG2_PICK = (89, 207, 20, 78, 52, 106, 165, 228)
 def test_config2_members_match_oracle_every_record(nb, oracle_mod):
     """Config-2-sized members through 500 steps with a record every 100: the
     strict build is bit-identical to the oracle per member (fields and
-    tree-order checksums) on its default schedule and on a 4-warp, 32-row one;
-    the default build stays within 1e-12 relative max-norm on both."""
+    tree-order checksums) on its default schedule, on a 4-warp, 32-row one and
+    on the dynamic schedule with 128-row blocks; the default build stays within
+    1e-12 relative max-norm on all three."""
     import os
     allm = nb.generate_members(2026, 256, 64, 1024, amp_scale=0.2)
     members = [allm[k] for k in CONFIG2_PICK]
     assert max(max(m.jpi, m.jpj) for m in members) >= 900
     runs = []
     for strict in (True, False):
-        for sched in (None, (4, None, 32, 1)):
+        for sched in (None, (4, None, 32, 1), (4, None, 128, 2)):
             e = nb.Ensemble(members, strict=strict, **COMMON)
             if sched is not None:
                 e.set_schedule(*sched)
@@ -154,6 +155,29 @@ def test_ensemble_set_state_and_graph_replay_agree(nb):
     for k in range(len(members)):
         for name, fid in STATE:
             np.testing.assert_array_equal(bits(a.field(k, fid)), bits(b.field(k, fid)))
+
+
+def test_dynamic_schedule_survives_switches_and_graph_replays(nb):
+    """The dynamic schedule's work counters: graph replays of every length and
+    parity, switches to the static schedule and back, and odd step counts give
+    the same bits as a static schedule of the same compiled variant."""
+    members = nb.generate_members(21, 9, side_min=40, side_max=300, amp_scale=0.2)
+    a = nb.Ensemble(members, **COMMON)
+    b = nb.Ensemble(members, **COMMON)
+    a.set_schedule(4, None, 128, 2)
+    b.set_schedule(4, None, 16, 1)
+    istp = 1
+    for n, switch in [(7, None), (4, (4, None, 16, 0)), (6, (4, None, 64, 2)), (5, None), (5, None),
+                      (3, None), (2, (4, None, 128, 2)), (7, None)]:
+        if switch:
+            a.set_schedule(*switch)
+        a.step_n(istp, n)
+        b.step_n(istp, n)
+        istp += n
+    assert a.get_schedule()[3] == 2
+    for k in range(len(members)):
+        for name, fid in STATE:
+            np.testing.assert_array_equal(bits(a.field(k, fid)), bits(b.field(k, fid)), err_msg=name)
 
 
 def test_ensemble_autotune_keeps_state(nb):
