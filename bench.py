@@ -98,6 +98,8 @@ def parse():
     ap.add_argument("--repeats", type=int, default=1, help="hybrid runs per point (median reported)")
     ap.add_argument("--candidates", type=int, default=128, help="hybrid member candidates")
     ap.add_argument("--strict", action="store_true", help="time the -fmad=false library (general)")
+    ap.add_argument("--ens-schedule", type=str, default="",
+                    help="warps,occupancy,rows,order of the ensemble workload (default: autotuned)")
     ap.add_argument("--n", type=int, default=N,
                     help="grid side (profiling of smaller cases only; the bench line is 4096)")
     return ap.parse_args()
@@ -314,7 +316,7 @@ def run_reference(args, rank):
 ENS_METRIC = "ensemble cell-steps/s (256 members, 500 steps, FP64)"
 
 
-def ensemble_leg(device, warmup, reps, tune_steps=3):
+def ensemble_leg(device, warmup, reps, tune_steps=3, schedule=None):
     """The batched configuration: 256 members of the recipe (seed 2026, sides
     log-uniform 64..1024, aspect 0.5..2, seeded 50-150 m bathymetry, random
     tidal phase), the 500-step run from rest with per-member checksums every
@@ -332,7 +334,11 @@ def ensemble_leg(device, warmup, reps, tune_steps=3):
                                       stream=stream.cuda_stream, device=device)
     e = nemo_b200.Ensemble(members, common=common)
     nmem, ncell = e.info()
-    sched, tuned_ms = e.autotune(steps=tune_steps)
+    if schedule:  # a fixed schedule (profiling), else the autotuner's choice
+        e.set_schedule(*schedule)
+        sched = e.get_schedule()
+    else:
+        sched, tuned_ms = e.autotune(steps=tune_steps)
     rest = [(np.zeros((m.jpj, m.jpi)), np.zeros((m.jpj, m.jpi + 1)), np.zeros((m.jpj + 1, m.jpi)))
             for m in members]
     for w in range(warmup):
@@ -404,7 +410,8 @@ def run_ensemble(args):
     the 500-step run of all 256 members."""
     import torch
     torch.cuda.set_device(0)
-    leg = ensemble_leg(0, args.warmup, args.steps)
+    fixed = tuple(int(x) for x in args.ens_schedule.split(",")) if args.ens_schedule else None
+    leg = ensemble_leg(0, args.warmup, args.steps, schedule=fixed)
     line = {"metric": ENS_METRIC, "value": leg["value"], "unit": "cell-steps/s", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": leg["ms_per_rep"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
