@@ -119,27 +119,19 @@ __device__ __forceinline__ double sshn_u_at(const GNext& x, int c, int r, int jp
   const double s1 = dn(x.s);
   const double t0 = e12t_at(x, c, r, jpi, jpj);
   const double t1 = dn(t0);
-  if (a + b > 0) {
-    if (a * b > 0) return qm(0.5 * (t0 * x.s + t1 * s1), x.e1u * x.e2u);
-    if (a <= 0) return s1;
-    return x.s;
-  }
-  return __ldg(stored + o);
+  const double avg = qm(0.5 * (t0 * x.s + t1 * s1), x.e1u * x.e2u);
+  const double st = (a + b > 0) ? 0.0 : __ldg(stored + o);
+  return (a + b > 0) ? ((a * b > 0) ? avg : ((a <= 0) ? s1 : x.s)) : st;
 }
 
 // sshn_v at (c, j) after `next` (:751-764) from rows j (x, own) and j+1 (y).
 __device__ __forceinline__ double sshn_v_at(const GNext& x, const GOwn& w, const GNext& y, int c, int j,
                                             int jpi, int jpj, const double* stored, long o) {
   const int a = x.pt, b = y.pt;
-  if (a + b > 0) {
-    if (a * b > 0) {
-      const double t0 = e12t_at(x, c, j, jpi, jpj), t1 = e12t_at(y, c, j + 1, jpi, jpj);
-      return qm(0.5 * (t0 * x.s + t1 * y.s), w.e1v * w.e2v);
-    }
-    if (a <= 0) return y.s;
-    return x.s;
-  }
-  return __ldg(stored + o);
+  const double t0 = e12t_at(x, c, j, jpi, jpj), t1 = e12t_at(y, c, j + 1, jpi, jpj);
+  const double avg = qm(0.5 * (t0 * x.s + t1 * y.s), w.e1v * w.e2v);
+  const double st = (a + b > 0) ? 0.0 : __ldg(stored + o);
+  return (a + b > 0) ? ((a * b > 0) ? avg : ((a <= 0) ? y.s : x.s)) : st;
 }
 
 // Values carried from row j-1 to row j for one column.
@@ -188,7 +180,10 @@ k_fused_general(Layout L, Consts C, GenArgs A, int tile_y) {
     const double vnc = 0.5 * (p.v + dn(p.v));
     const double vfl = 0.5 * vnc * (pw.e1v + dn(pw.e1v));
     const double depc = 0.5 * (pw.hv + sv_p + dn(pw.hv) + dn(sv_p));
-    const bool ms = p.pt <= 0 || dni(p.pt) <= 0;  // pt(ji,jj-1), pt(ji+1,jj-1) of u(c, J0)
+    // every lane shuffles (a shuffle inside the short-circuit would leave out
+    // the lanes whose own cell is land or open)
+    const int ppt_e = dni(p.pt);
+    const bool ms = p.pt <= 0 || ppt_e <= 0;  // pt(ji,jj-1), pt(ji+1,jj-1) of u(c, J0)
     k.Fuy_s = (ms ? upwind_hi_only(vfl, cur.u) : upw(vfl, p.u, cur.u)) * vfl * depc;
     k.vnc_s = vnc;
     k.dudy_s = ms ? 0.0 : qm(cur.u - p.u, cur.e2u + p.e2u) * (cur.hu + k.su + p.hu + su_p);
@@ -267,9 +262,15 @@ k_fused_general(Layout L, Consts C, GenArgs A, int tile_y) {
     const double Dvy_n = qm(nx.v - cur.v, nx.e2t) * depn;
 
     // ---- u equation at u(c,j) (:431-517), solid walls (:648-652) ----
+    // Both equations are evaluated in every lane and the result selected
+    // afterwards: a lane outside an equation's mask still takes part in the
+    // shuffles its neighbours' results need (a shuffle whose source lane has
+    // branched away returns an undefined value), and the values it computes
+    // for itself (quotients by the zero scale factors of the border ring
+    // included) are discarded.
     const double Fx_e = dn(Fx), Dx_e = dn(Dx);
     double ua;
-    if (c >= 1 && c <= jpi - 1 && cur.pt > 0 && pt_e > 0) {
+    {
       const double Hu = cur.hu + k.su;
       const double adv = Fx - Fx_e + k.Fuy_s - Fuy_n;
       double vis = (Dx_e - Dx) * cur.e2u + (dudy_n - k.dudy_s) * cur.e1u * 0.5;
@@ -277,15 +278,15 @@ k_fused_general(Layout L, Consts C, GenArgs A, int tile_y) {
       const double e12u = cur.e1u * cur.e2u;
       const double cor = 0.5 * (w.fcu * (k.vnc_s + vnc)) * e12u * Hu;
       const double hpg = -(C.g * Hu * cur.e2u * (s_e - cur.s));
-      ua = qf(qh(cur.u * Hu + qm(C.rdt * (adv + vis + cor + hpg), e12u), cur.hu + 0.0), C);
-    } else {
-      ua = (cur.pt * pt_e == 0) ? 0.0 : cur.u;
+      const double um = qf(qh(cur.u * Hu + qm(C.rdt * (adv + vis + cor + hpg), e12u), cur.hu + 0.0), C);
+      const bool mom = c >= 1 && c <= jpi - 1 && cur.pt > 0 && pt_e > 0;
+      ua = mom ? um : ((cur.pt * pt_e == 0) ? 0.0 : cur.u);
     }
 
     // ---- v equation at v(c,j) (:520-609), solid walls (:656-660) ----
     const double Fvx_w = up(Fvx_w_next), dvdx_w = up(dvdx_w_next), uec_w = up(uec);
     double va;
-    if (j <= jpj - 1 && !(cur.pt + pt_e <= 0) && cur.pt > 0 && nx.pt > 0) {
+    {
       const double Hv = w.hv + sv;
       const double adv = Fvx_w - Fvx_e + k.Fvy_s - Fvy_n;
       double vis = (Dvy_n - k.Dvy_s) * w.e1v + (dvdx_e - dvdx_w) * w.e2v * 0.5;
@@ -293,9 +294,9 @@ k_fused_general(Layout L, Consts C, GenArgs A, int tile_y) {
       const double e12v = w.e1v * w.e2v;
       const double cor = -(0.5 * (w.fcv * (uec + uec_w)) * e12v * Hv);
       const double hpg = -(C.g * Hv * w.e1v * (nx.s - cur.s));
-      va = qf(qh(cur.v * Hv + qm(C.rdt * (adv + vis + cor + hpg), e12v), w.hv + 0.0), C);
-    } else {
-      va = (cur.pt * nx.pt == 0) ? 0.0 : cur.v;
+      const double vm = qf(qh(cur.v * Hv + qm(C.rdt * (adv + vis + cor + hpg), e12v), w.hv + 0.0), C);
+      const bool mom = j <= jpj - 1 && !(cur.pt + pt_e <= 0) && cur.pt > 0 && nx.pt > 0;
+      va = mom ? vm : ((cur.pt * nx.pt == 0) ? 0.0 : cur.v);
     }
 
     if (store) {

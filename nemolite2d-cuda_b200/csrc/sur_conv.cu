@@ -991,8 +991,8 @@ k_conv_wgrad_tri(const __grid_constant__ CUtensorMap tmX, const __grid_constant_
 // does not depend on timing (no atomics).
 constexpr int WS_XPIX = 80;                  // x window pixels: x0-8 .. x0+71
 constexpr int WS_XBYTES = WS_XPIX * CH * 2;  // 10 KiB
-constexpr int WS_KX = 4;                     // x window slots
-constexpr int WS_KZ = 6;                     // dz ring rows (12 slots with the mirrors)
+constexpr int WS_KX = 6;                     // x window slots
+constexpr int WS_KZ = 8;                     // dz ring rows (16 slots with the mirrors)
 static_assert(WS_NPART == 9 * CH * CH + CH, "one CTA's partial dw and db");
 
 struct WsSmem {
