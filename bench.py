@@ -102,6 +102,8 @@ def parse():
                     help="ensemble members (profiling of smaller cases only; the line is 256)")
     ap.add_argument("--ens-schedule", type=str, default="",
                     help="warps,occupancy,rows,order of the ensemble workload (default: autotuned)")
+    ap.add_argument("--gen-schedule", type=str, default="",
+                    help="ring,rows of the general grid's kernel (ring 0, 3 or 4; default 3,32)")
     ap.add_argument("--n", type=int, default=N,
                     help="grid side (profiling of smaller cases only; the bench line is 4096)")
     return ap.parse_args()
@@ -771,6 +773,9 @@ def run_general(args):
     names = ("e1t", "e2t", "e1u", "e2u", "e1v", "e2v", "gphiu", "gphiv", "ht", "hu", "hv")
     m.set_grid(pt, *[g[k] for k in names])
     del g
+    if args.gen_schedule:
+        ring, rows = (int(x) for x in args.gen_schedule.split(","))
+        m.set_schedule(2, ring, rows)
     rest = (np.zeros((n, n)), np.zeros((n, n + 1)), np.zeros((n + 1, n)))
     for w in range(args.warmup):
         m.step_n(1 + 100 * w, 100)
@@ -789,6 +794,7 @@ def run_general(args):
     clk = clocks.stop()
     ms = ev[0].elapsed_time(ev[1])
     value = n * n * 100 * args.steps / (ms / 1e3)
+    sch = m.get_schedule()
     peak, kind = load_peaks()
     achieved = GEN_BYTES_PER_CELL_STEP * value / 1e9
     line = {"metric": "general-grid cell-steps/s at %d^2 FP64" % n, "value": value,
@@ -803,6 +809,7 @@ def run_general(args):
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": kind,
                          "algorithmic_bytes_per_cell_step": GEN_BYTES_PER_CELL_STEP},
             "checksums_last": [float(x) for x in ck], "build": "strict" if args.strict else "default",
+            "schedule": {"warps": sch[0], "ring": sch[1], "rows": sch[2]},
             "gpu_launches": args.steps * (2 * 100 + 2), "clocks": clk}
     print(json.dumps(line), flush=True)
     m.close()

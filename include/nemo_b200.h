@@ -186,7 +186,11 @@ int nemo_device_field(nemo_ctx* ctx, int field, double** ptr, long* pitch);
  * (the default, 2 warps, 116, 16 rows); 0 (compiler's choice), 16, 20, 24
  * prefetch the next row into registers (8-warp CTAs take 0, 16 or 24); -16,
  * -20, -24 for 2-warp and -20 for 4-warp CTAs load each row one step ahead.
- * In the -fmad=false build every schedule gives bit-identical results. */
+ * In the -fmad=false build every schedule gives bit-identical results.
+ * After nemo_set_grid the context keeps a separate schedule for the general
+ * grid's fused kernel: warps 2, occupancy 3 or 4 (rows staged through a
+ * shared-memory ring of that many slots; 3 is the default) or 0 (each row
+ * loaded where it is used), rows 1..65536 per CTA (default 32). */
 typedef struct nemo_schedule {
   int warps;
   int occupancy;

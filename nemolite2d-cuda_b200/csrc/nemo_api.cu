@@ -44,6 +44,9 @@ struct nemo_ctx {
   GridDev grid{};
   int4* gchains = nullptr;   // Flather chains of the general grid
   int n_gchains = 0;
+  // the general grid's fused kernel: warps 2, occupancy = ring slots (0, 3, 4),
+  // rows per CTA
+  nemo_schedule gsched{2, 3, 32};
   // output records (nemo_record): staging buffer, side stream and events
   double* rec_dev = nullptr;
   cudaStream_t rec_stream = nullptr;
@@ -567,7 +570,8 @@ int nemo_step_n(nemo_ctx* c, int istp0, int n) {
       a.va = aset(c).v;
       a.tide = tide_value(c->p, istp0 + k);
       a.g = c->grid;
-      CK(launch_fused_general(c->L, c->C, a, c->gchains, c->n_gchains, 32, c->stream));
+      CK(launch_fused_general(c->L, c->C, a, c->gchains, c->n_gchains, c->gsched.occupancy, c->gsched.rows,
+                              c->stream));
       c->n_idx = 1 - c->n_idx;
     }
     c->a_mirrors_n = true;
@@ -836,6 +840,13 @@ int nemo_device_field(nemo_ctx* c, int field, double** ptr, long* pitch) {
 
 int nemo_set_schedule(nemo_ctx* c, const nemo_schedule* s) {
   if (!c) return NEMO_ERR_STATE;
+  if (c->general) {
+    if (!s || s->warps != 2 || (s->occupancy != 0 && s->occupancy != 3 && s->occupancy != 4) || s->rows < 1 ||
+        s->rows > 65536)
+      return NEMO_ERR_INVALID;
+    c->gsched = *s;
+    return NEMO_OK;
+  }
   if (!s || !fused_variant_ok(s->warps, s->occupancy, c->recip_nr_ok) || s->rows < 0 || s->rows > 65536)
     return NEMO_ERR_INVALID;
   c->sched = *s;
@@ -844,7 +855,7 @@ int nemo_set_schedule(nemo_ctx* c, const nemo_schedule* s) {
 
 int nemo_get_schedule(nemo_ctx* c, nemo_schedule* s) {
   if (!c || !s) return NEMO_ERR_INVALID;
-  *s = c->sched;
+  *s = c->general ? c->gsched : c->sched;
   return NEMO_OK;
 }
 

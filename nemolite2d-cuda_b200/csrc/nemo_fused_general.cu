@@ -52,18 +52,33 @@ using stepdev::upw;
 
 using stepdev::kRoundedQuotients;
 
-// a / b for a scale-factor divisor.
-__device__ __forceinline__ double qm(double a, double b) {
-  if (kRoundedQuotients) return a / b;
-  return a * recip_nr(b);
+// The default build's reciprocal of a scale factor or depth: the FP64
+// approximate reciprocal (one special-function operation, no conversions)
+// refined by two Newton-Raphson steps, y <- y + y(1 - b y), each of which
+// squares the relative error; the result is within a few units in the last
+// place.  b = 0 gives NaN, in lanes whose results are discarded.
+__device__ __forceinline__ double grecip(double b) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
+  y = fma(y, fma(-b, y, 1.0), y);
+  return fma(y, fma(-b, y, 1.0), y);
 }
-// a / h for a static depth h: the corrected quotient from a one-step Newton
-// reciprocal in the default build (the rounded quotient except within about
-// 2^-39 ulp of a rounding boundary).
+// a / b: the rounded quotient in the -fmad=false build; a * rb in the default
+// build, rb a reciprocal of b (grecip(b), or for a factor b of a product
+// b*d, d * grecip(b*d)), which the strict build never forms.
+__device__ __forceinline__ double qr(double a, double b, double rb) {
+  if (kRoundedQuotients) return a / b;
+  return a * rb;
+}
+// a / b for a scale-factor divisor.
+__device__ __forceinline__ double qm(double a, double b) { return qr(a, b, grecip(b)); }
+// a / h for a static depth h: in the default build the quotient corrected by
+// one residual step, q + (a - q h) r, which is the rounded quotient except
+// within a tiny fraction of an ulp of a rounding boundary.
 __device__ __forceinline__ double qh(double a, double h) {
   if (kRoundedQuotients) return a / h;
   bool bad = false;
-  return stepdev::qdiv<false>(a, h, recip_nr1(h), bad);
+  return stepdev::qdiv<false>(a, h, grecip(h), bad);
 }
 // a / cfric
 __device__ __forceinline__ double qf(double a, const Consts& C) {
@@ -113,23 +128,25 @@ __device__ __forceinline__ double e12t_at(const GNext& x, int c, int r, int jpi,
 // sshn_u at (c, r) after `next` (:736-749); every lane of the warp calls it
 // (shuffles).  e12u is e1u*e2u of (c, r), inside its range (0:jpi, 1:jpj)
 // wherever the branch that uses it is taken.
+// ru: the default build's reciprocal of e1u*e2u at (c, r).
 __device__ __forceinline__ double sshn_u_at(const GNext& x, int c, int r, int jpi, int jpj,
-                                            const double* stored, long o) {
+                                            const double* stored, long o, double ru) {
   const int a = x.pt, b = dni(x.pt);
   const double s1 = dn(x.s);
   const double t0 = e12t_at(x, c, r, jpi, jpj);
   const double t1 = dn(t0);
-  const double avg = qm(0.5 * (t0 * x.s + t1 * s1), x.e1u * x.e2u);
+  const double avg = qr(0.5 * (t0 * x.s + t1 * s1), x.e1u * x.e2u, ru);
   const double st = (a + b > 0) ? 0.0 : __ldg(stored + o);
   return (a + b > 0) ? ((a * b > 0) ? avg : ((a <= 0) ? s1 : x.s)) : st;
 }
 
-// sshn_v at (c, j) after `next` (:751-764) from rows j (x, own) and j+1 (y).
+// sshn_v at (c, j) after `next` (:751-764) from rows j (x, own) and j+1 (y);
+// rv: the default build's reciprocal of e1v*e2v at (c, j).
 __device__ __forceinline__ double sshn_v_at(const GNext& x, const GOwn& w, const GNext& y, int c, int j,
-                                            int jpi, int jpj, const double* stored, long o) {
+                                            int jpi, int jpj, const double* stored, long o, double rv) {
   const int a = x.pt, b = y.pt;
   const double t0 = e12t_at(x, c, j, jpi, jpj), t1 = e12t_at(y, c, j + 1, jpi, jpj);
-  const double avg = qm(0.5 * (t0 * x.s + t1 * y.s), w.e1v * w.e2v);
+  const double avg = qr(0.5 * (t0 * x.s + t1 * y.s), w.e1v * w.e2v, rv);
   const double st = (a + b > 0) ? 0.0 : __ldg(stored + o);
   return (a + b > 0) ? ((a * b > 0) ? avg : ((a <= 0) ? y.s : x.s)) : st;
 }
@@ -146,8 +163,61 @@ struct GCarry {
   int pt_s;       // pt(c, j-1)
 };
 
-__global__ void __launch_bounds__(64)
+// Rows staged through a per-warp ring in shared memory: RG slots, each row
+// issued RG-1 rows ahead of its use by cp.async, every lane copying its own
+// column of each field (8 bytes).  A slot holds the 14 fields of one row (the
+// 9 of GNext and the 5 of GOwn) field-major, 32 doubles per field with lane
+// l's column at l; the int8 mask is loaded one row ahead into a register.
+// RG = 0: every row is loaded at the top of the iteration that needs it.
+constexpr int GF = 14;
+
+__device__ __forceinline__ void ring_issue_g(double* my, const GenArgs& A, long o) {
+  using stepdev::cp_async8;
+  cp_async8(my + 0 * 32, A.sshn + o);
+  cp_async8(my + 1 * 32, A.un + o);
+  cp_async8(my + 2 * 32, A.vn + o);
+  cp_async8(my + 3 * 32, A.ht + o);
+  cp_async8(my + 4 * 32, A.hu + o);
+  cp_async8(my + 5 * 32, A.g.e1t + o);
+  cp_async8(my + 6 * 32, A.g.e2t + o);
+  cp_async8(my + 7 * 32, A.g.e1u + o);
+  cp_async8(my + 8 * 32, A.g.e2u + o);
+  cp_async8(my + 9 * 32, A.hv + o);
+  cp_async8(my + 10 * 32, A.g.e1v + o);
+  cp_async8(my + 11 * 32, A.g.e2v + o);
+  cp_async8(my + 12 * 32, A.g.fcu + o);
+  cp_async8(my + 13 * 32, A.g.fcv + o);
+  stepdev::cp_commit();
+}
+__device__ __forceinline__ void ring_next(GNext& x, const double* my, int pt) {
+  x.s = my[0 * 32];
+  x.u = my[1 * 32];
+  x.v = my[2 * 32];
+  x.ht = my[3 * 32];
+  x.hu = my[4 * 32];
+  x.e1t = my[5 * 32];
+  x.e2t = my[6 * 32];
+  x.e1u = my[7 * 32];
+  x.e2u = my[8 * 32];
+  x.pt = pt;
+}
+__device__ __forceinline__ void ring_own(GOwn& w, const double* my) {
+  w.hv = my[9 * 32];
+  w.e1v = my[10 * 32];
+  w.e2v = my[11 * 32];
+  w.fcu = my[12 * 32];
+  w.fcv = my[13 * 32];
+}
+__device__ __forceinline__ int ring_step(int s, int rg) { return s + 1 == rg ? 0 : s + 1; }
+
+#ifndef NEMO_GEN_MINB
+#define NEMO_GEN_MINB 8  // resident CTAs per SM the register budget is fitted to
+#endif
+template <int RG>
+__global__ void __launch_bounds__(64, NEMO_GEN_MINB)
 k_fused_general(Layout L, Consts C, GenArgs A, int tile_y) {
+  constexpr int AHEAD = RG > 0 ? RG - 1 : 0;
+  __shared__ double ring_all[RG > 0 ? 2 * RG * GF * 32 : 1];
   const int lane = threadIdx.x & 31;
   const int warp = (int)(blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5));
   const int c0 = 1 + COLS_PER_WARP * warp;
@@ -164,17 +234,38 @@ k_fused_general(Layout L, Consts C, GenArgs A, int tile_y) {
   const bool store_u = store || (c == 0);
   const long pitch = L.pitch;
 
+  // ---- the ring: rows J0 .. J1+1 (row J0-1 is loaded directly); row J0+i
+  // goes to slot i mod RG ----
+  double* my = ring_all + (threadIdx.x >> 5) * (RG > 0 ? RG * GF * 32 : 0) + lane;
+  const int r_stop = J1 + 1;  // the last row any iteration reads
+  if constexpr (RG > 0) {
+#pragma unroll
+    for (int r = 0; r < AHEAD; ++r) {
+      if (J0 + r <= r_stop) ring_issue_g(my + r * GF * 32, A, L.idx(cl, J0 + r));
+      else stepdev::cp_commit();
+    }
+  }
+
   // ---- prologue: rows J0-1 (p) and J0 (q) ----
   GNext p, cur;
   GOwn pw;
   load_next(p, A, L.idx(cl, J0 - 1));
   load_own(pw, A, L.idx(cl, J0 - 1));
-  load_next(cur, A, L.idx(cl, J0));
+  int pt1 = 0;  // RG > 0: the mask of the next row to take out of the ring
+  if constexpr (RG > 0) {
+    const int pt0 = A.g.pt[L.idx(cl, J0)];
+    pt1 = A.g.pt[L.idx(cl, J0 + 1)];
+    stepdev::cp_wait<AHEAD - 1>();  // row J0 has landed in slot 0
+    ring_next(cur, my, pt0);
+  } else {
+    load_next(cur, A, L.idx(cl, J0));
+  }
   GCarry k;
   {
-    const double su_p = sshn_u_at(p, c, J0 - 1, jpi, jpj, A.su_st, L.idx(cl, J0 - 1));
-    k.su = sshn_u_at(cur, c, J0, jpi, jpj, A.su_st, L.idx(cl, J0));
-    const double sv_p = sshn_v_at(p, pw, cur, c, J0 - 1, jpi, jpj, A.sv_st, L.idx(cl, J0 - 1));
+    const double su_p = sshn_u_at(p, c, J0 - 1, jpi, jpj, A.su_st, L.idx(cl, J0 - 1), grecip(p.e1u * p.e2u));
+    k.su = sshn_u_at(cur, c, J0, jpi, jpj, A.su_st, L.idx(cl, J0), grecip(cur.e1u * cur.e2u));
+    const double sv_p = sshn_v_at(p, pw, cur, c, J0 - 1, jpi, jpj, A.sv_st, L.idx(cl, J0 - 1),
+                                  grecip(pw.e1v * pw.e2v));
     k.cf_s = (sv_p + pw.hv) * p.v;
     // corner (c, J0-1): the south face of u(c, J0)
     const double vnc = 0.5 * (p.v + dn(p.v));
@@ -200,26 +291,46 @@ k_fused_general(Layout L, Consts C, GenArgs A, int tile_y) {
     }
   }
 
+  // slots of rows j, j+1 and j+AHEAD (= the slot of row j-1)
+  int s_w = 0, s_n = RG > 1 ? 1 : 0, s_i = RG > 0 ? RG - 1 : 0;
   long o_st = L.idx(c, J0);
 #pragma unroll 1
   for (int j = J0; j <= J1; ++j) {
     GNext nx;
     GOwn w;
-    load_next(nx, A, L.idx(cl, j + 1));  // row j+1 <= jpj+1
-    load_own(w, A, L.idx(cl, j));
+    if constexpr (RG > 0) {
+      // row j+AHEAD into the slot of row j-1, the mask of row j+2 ahead
+      if (j + AHEAD <= r_stop) ring_issue_g(my + s_i * GF * 32, A, L.idx(cl, j + AHEAD));
+      else stepdev::cp_commit();
+      const int pt2 = (j + 2 <= L.jpj + 1) ? A.g.pt[L.idx(cl, j + 2)] : 0;
+      stepdev::cp_wait<AHEAD - 1>();  // rows <= j+1 have landed
+      ring_next(nx, my + s_n * GF * 32, pt1);
+      ring_own(w, my + s_w * GF * 32);
+      pt1 = pt2;
+      s_w = s_n;
+      s_n = ring_step(s_n, RG);
+      s_i = ring_step(s_i, RG);
+    } else {
+      load_next(nx, A, L.idx(cl, j + 1));  // row j+1 <= jpj+1
+      load_own(w, A, L.idx(cl, j));
+    }
     const int pt_e = dni(cur.pt), pt_w = upi(cur.pt);
     const int ptn_e = dni(nx.pt), ptn_w = upi(nx.pt);
     const double s_e = dn(cur.s);
+    // default build: reciprocals of e1v*e2v and e1t*e2t at (c, j) (the
+    // latter gives 1/e1t as e2t/(e1t*e2t))
+    const double rv = grecip(w.e1v * w.e2v);
+    const double rt = grecip(cur.e1t * cur.e2t);
 
     // sshn_v at (c, j), sshn_u at (c, j+1)
-    const double sv = sshn_v_at(cur, w, nx, c, j, jpi, jpj, A.sv_st, L.idx(cl, j));
-    const double su_n = sshn_u_at(nx, c, j + 1, jpi, jpj, A.su_st, L.idx(cl, j + 1));
+    const double sv = sshn_v_at(cur, w, nx, c, j, jpi, jpj, A.sv_st, L.idx(cl, j), rv);
+    const double su_n = sshn_u_at(nx, c, j + 1, jpi, jpj, A.su_st, L.idx(cl, j + 1), grecip(nx.e1u * nx.e2u));
 
     // ---- continuity (:397-405) and the clamped SSH (:631-644) ----
     const double r1 = (k.su + cur.hu) * cur.u;
     const double r2 = up(r1);
     const double r3 = (sv + w.hv) * cur.v;
-    double ssha = cur.s + qm((r2 - r1 + k.cf_s - r3) * C.rdt, e12t_at(cur, c, j, jpi, jpj));
+    double ssha = cur.s + qr((r2 - r1 + k.cf_s - r3) * C.rdt, e12t_at(cur, c, j, jpi, jpj), rt);
     if (cur.pt > 0 && (k.pt_s < 0 || nx.pt < 0 || pt_e < 0 || pt_w < 0)) ssha = A.tide;
 
     // ---- x-face at T(c,j), between u(c-1,j) and u(c,j) ----
@@ -227,7 +338,7 @@ k_fused_general(Layout L, Consts C, GenArgs A, int tile_y) {
     const double uw = 0.5 * (cur.u + u_wn) * cur.e2t;
     const double dep = cur.ht + cur.s;
     const double Fx = upw(uw, u_wn, cur.u) * uw * dep;
-    const double Dx = qm(cur.u - u_wn, cur.e1t) * dep;
+    const double Dx = qr(cur.u - u_wn, cur.e1t, cur.e2t * rt) * dep;
 
     // ---- corner (c,j): north face of u(c,j) / south face of u(c,j+1) ----
     const double v_e = dn(cur.v);
@@ -294,7 +405,7 @@ k_fused_general(Layout L, Consts C, GenArgs A, int tile_y) {
       const double e12v = w.e1v * w.e2v;
       const double cor = -(0.5 * (w.fcv * (uec + uec_w)) * e12v * Hv);
       const double hpg = -(C.g * Hv * w.e1v * (nx.s - cur.s));
-      const double vm = qf(qh(cur.v * Hv + qm(C.rdt * (adv + vis + cor + hpg), e12v), w.hv + 0.0), C);
+      const double vm = qf(qh(cur.v * Hv + qr(C.rdt * (adv + vis + cor + hpg), e12v, rv), w.hv + 0.0), C);
       const bool mom = j <= jpj - 1 && !(cur.pt + pt_e <= 0) && cur.pt > 0 && nx.pt > 0;
       va = mom ? vm : ((cur.pt * nx.pt == 0) ? 0.0 : cur.v);
     }
@@ -316,6 +427,7 @@ k_fused_general(Layout L, Consts C, GenArgs A, int tile_y) {
     k.pt_s = cur.pt;
     cur = nx;
   }
+  if constexpr (RG > 0) asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
 // One Flather chain (see the file comment): x = ji, y = jj, z = kind (0: u,
@@ -383,12 +495,17 @@ __global__ void k_flather_general(Layout L, GenArgs A, const int4* __restrict__ 
 }  // namespace
 
 cudaError_t launch_fused_general(const Layout& L, const Consts& C, const GenArgs& a, const int4* chains,
-                                 int nchains, int tile_y, cudaStream_t s) {
+                                 int nchains, int ring, int tile_y, cudaStream_t s) {
   constexpr int NW = 2;
   const int cols_per_cta = COLS_PER_WARP * NW;
   if (tile_y < 1) tile_y = 32;
   dim3 grid((unsigned)((L.jpi + cols_per_cta - 1) / cols_per_cta), (unsigned)((L.jpj + tile_y - 1) / tile_y));
-  k_fused_general<<<grid, 32 * NW, 0, s>>>(L, C, a, tile_y);
+  switch (ring) {
+    case 0: k_fused_general<0><<<grid, 32 * NW, 0, s>>>(L, C, a, tile_y); break;
+    case 3: k_fused_general<3><<<grid, 32 * NW, 0, s>>>(L, C, a, tile_y); break;
+    case 4: k_fused_general<4><<<grid, 32 * NW, 0, s>>>(L, C, a, tile_y); break;
+    default: return cudaErrorInvalidValue;
+  }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess || nchains == 0) return e;
   k_flather_general<<<(nchains + 127) / 128, 128, 0, s>>>(L, a, chains, nchains);

@@ -90,8 +90,10 @@ struct GenArgs {
   GridDev g;
 };
 // One step: the fused kernel, then the Flather chains (flather_chains).
+// ring: 0 (rows loaded where used), 3 or 4 (rows staged through a shared-memory
+// ring of that many slots); tile_y: rows per CTA.
 cudaError_t launch_fused_general(const Layout& L, const Consts& C, const GenArgs& a, const int4* chains,
-                                 int nchains, int tile_y, cudaStream_t s);
+                                 int nchains, int ring, int tile_y, cudaStream_t s);
 // Flather points of the mask pt ((0:jpi+1, 0:jpj+1), leading dimension
 // jpi+2) as independent chains: {ji, jj, kind, continues}.
 void flather_chains(const int* pt, int jpi, int jpj, std::vector<int4>& out);

@@ -32,6 +32,7 @@
 #include <atomic>
 #include <mutex>
 
+#include "nemo_mbar.cuh"
 #include "sur_internal.h"
 
 namespace sur {
@@ -51,50 +52,20 @@ constexpr int WG_PIX = 64;                 // pixels per wgrad K chunk
 constexpr int WG_TILE = WG_PIX * CH * 2;   // 8 KiB
 
 // ---- PTX wrappers ------------------------------------------------------------
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
-}
-__device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-      " selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(ok)
-      : "r"(smem_u32(b)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-__device__ __forceinline__ uint64_t gtimer() {
-  uint64_t t;
-  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
-  return t;
-}
+using devsync::fence_barrier_init;
+using devsync::mbar_arrive;
+using devsync::mbar_expect_tx;
+using devsync::mbar_init;
+using devsync::mbar_try;
+using devsync::smem_u32;
 // Bounded wait for the phase with the given parity; false after `limit` ns
 // (WAIT_NS by default) of wall time without completion.
 __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, uint64_t limit = WAIT_NS) {
-  if (mbar_try(b, parity)) return true;
-  const uint64_t t0 = gtimer();
-  for (uint32_t i = 1;; ++i) {
-    if (mbar_try(b, parity)) return true;
-    if ((i & 255u) == 0 && gtimer() - t0 > limit) return false;
-  }
+  return devsync::mbar_wait(b, parity, limit);
 }
 // The same, agreed across the warp (for .sync.aligned tcgen05 instructions).
 __device__ __forceinline__ bool mbar_wait_warp(uint64_t* b, uint32_t parity, uint64_t limit = WAIT_NS) {
   return __all_sync(0xffffffffu, mbar_wait(b, parity, limit)) != 0;
-}
-__device__ __forceinline__ void fence_barrier_init() {
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* tm, uint64_t* bar, int c0,
                                             int c1) {

@@ -277,7 +277,9 @@ class Model:
 
     def set_schedule(self, warps=2, occupancy=None, rows=32):
         """occupancy None: the context's default staging (216 when the in-kernel
-        reciprocal depths passed their check, else 116)."""
+        reciprocal depths passed their check, else 116).  After set_grid the
+        general grid's kernel takes warps 2, occupancy 3 or 4 (ring slots) or 0
+        (rows loaded where used), rows >= 1."""
         if occupancy is None:
             occupancy = 216 if self.recip_in_kernel() else 116
         s = Schedule(warps, occupancy, rows)

@@ -175,3 +175,4 @@ def test_convolution_wait_runs_out_and_the_surrogate_recovers(nb):
     a, b = (o.cpu().numpy() for o in outs)
     assert np.all(np.isfinite(a)) and np.any(a)
     np.testing.assert_array_equal(a.view(np.int32), b.view(np.int32))
+

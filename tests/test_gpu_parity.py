@@ -453,11 +453,14 @@ def _channel_grid(seed, jpi, jpj):
 
 
 @pytest.mark.parametrize("strict", [True, False])
-def test_general_fused_step_equals_routines_with_flather_chains(nb, oracle_mod, strict):
+@pytest.mark.parametrize("gsched", [None, (2, 0, 32), (2, 4, 7), (2, 3, 1), (2, 3, 200)])
+def test_general_fused_step_equals_routines_with_flather_chains(nb, oracle_mod, strict, gsched):
     """The general grid's fused step (one kernel plus the Flather chains)
     against the per-routine kernels and the oracle, from a random state, on a
     mask with interior open cells and one-cell channels in both directions:
-    bitwise in the strict build, within 1e-12 in the default build."""
+    bitwise in the strict build, within 1e-12 in the default build.  Every
+    schedule of the general kernel (rows loaded where used, or staged through
+    a ring of 3 or 4 slots; 1 row to the whole grid per CTA) gives these."""
     from gridcases import NAMES
     jpi, jpj = 150, 97
     kw = dict(jpi=jpi, jpj=jpj, rdt=10.0, cbfr=0.00015, visc=0.1, amp_tide=0.3)
@@ -471,6 +474,14 @@ def test_general_fused_step_equals_routines_with_flather_chains(nb, oracle_mod, 
     for m in (fused, routine, o):
         m.set_grid(pt, *[g[n] for n in NAMES])
         m.set_state(*st)
+    if gsched is not None:
+        fused.set_schedule(*gsched)
+        assert fused.get_schedule() == gsched
+    else:
+        assert fused.get_schedule() == (2, 3, 32)
+        for bad in ((2, 216, 32), (4, 3, 32), (2, 5, 32), (2, 3, 0)):
+            with pytest.raises(nb.NemoError):
+                fused.set_schedule(*bad)
     fused.step_n(1, 6)
     for istp in range(1, 7):
         routine.step(istp)
