@@ -1019,14 +1019,19 @@ k_conv_wgrad_strip(const __grid_constant__ CUtensorMap tmX, const __grid_constan
   tc_fence_after();
   const uint32_t tmem = S.tmem_base;
 
+  // unit u = (n * xch + column chunk) * H + y: the coordinates of the range's
+  // first unit, then stepped per unit (a 64-bit division per unit would cost
+  // the single producer and MMA threads more than the unit's MMAs take)
+  const int y_begin = have ? (int)(u_begin % G.H) : 0;
+  const long t_begin = have ? u_begin / G.H : 0;
+  const int xc_begin = (int)(t_begin % xch), n_begin = (int)(t_begin / xch);
   if (warp == 0 && lane == 0) {
     // ---- TMA producer: per unit the next dz row and the x window ----
     uint32_t lx = 0, lz = 0;
     bool ok = true;
+    int y = y_begin, xc = xc_begin, n = n_begin;
     for (long u = u_begin; u < u_end && ok; ++u) {
-      const int y = (int)(u % G.H);
-      const long t = u / G.H;
-      const int x0 = (int)(t % xch) * WG_PIX, n = (int)(t / xch);
+      const int x0 = xc * WG_PIX;
       // a strip starts at the range's first unit or at row 0: rows y-1 and y first
       for (int dr = (u == u_begin || y == 0) ? -1 : 1; dr <= 1 && ok; ++dr) {
         const uint32_t s = ws_zslot(lz);
@@ -1042,6 +1047,10 @@ k_conv_wgrad_strip(const __grid_constant__ CUtensorMap tmX, const __grid_constan
       mbar_expect_tx(&S.xfull[s], WS_XBYTES);
       tma_load_4d(S.x[s], &tmX, &S.xfull[s], 0, x0 - 8, y, n);
       ++lx;
+      if (++y == G.H) {
+        y = 0;
+        if (++xc == xch) { xc = 0; ++n; }
+      }
     }
     if (!ok) fail(G.err, 51);
     // every armed load lands before the CTA may exit
@@ -1059,10 +1068,10 @@ k_conv_wgrad_strip(const __grid_constant__ CUtensorMap tmX, const __grid_constan
     const uint32_t ones = smem_u32(S.ones);
     uint32_t lx = 0, lz = 0;
     bool ok = true, first = true;
-    for (long u = u_begin; u < u_end; ++u) {
-      const int y = (int)(u % G.H);
+    int y = y_begin;
+    for (long u = u_begin; u < u_end; ++u, y = (y + 1 == G.H) ? 0 : y + 1) {
       const bool start = (u == u_begin) || y == 0;
-      const bool last = (u + 1 == u_end) || ((u + 1) % G.H == 0);
+      const bool last = (u + 1 == u_end) || (y + 1 == G.H);
       if (start) lz += 2;
       const uint32_t l1 = lz++;  // dz row y+1; rows y and y-1 are loads l1-1 and l1-2
       for (uint32_t l = start ? l1 - 2 : l1; l <= l1 && ok; ++l)
