@@ -413,13 +413,14 @@ int nemo_conv3x3_wgrad(const void* x, const void* dz, float* dw, float* db, int 
  * window per tap.  Returns the previous variant; values out of range change
  * nothing. */
 int nemo_conv3x3_fwd_variant(int variant, int rows);
-/* Process-wide weight-gradient kernel: 2 (default) gives each CTA all nine
+/* Process-wide weight-gradient kernel: 2 gives each CTA all nine
  * taps and the bias over a range of column-strip rows (one x window per row
- * read at three shifts, each dz row loaded once into a mirrored ring) and adds
- * the CTAs' partial sums in a fixed order afterwards, so results are
+ * read at three shifts, each dz row loaded once into a ring) and adds the
+ * CTAs' partial sums in a fixed order afterwards, so results are
  * bit-identical from call to call; it keeps one scratch array per device for
  * nemo_conv3x3_wgrad (calls that overlap on the GPU race on it; a surrogate
- * has its own).  1 multiplies the x windows of two horizontal taps with the
+ * has its own).  3 (default) is the same with 128-pixel column chunks instead
+ * of 64 where the width is a multiple of 128 (else 2).  1 multiplies the x windows of two horizontal taps with the
  * dz windows of three rows (six taps per N = 192 MMA); 0 pairs taps with
  * N = 64 MMAs; both add partial results with atomics.  Returns the previous
  * variant; values out of range change nothing. */

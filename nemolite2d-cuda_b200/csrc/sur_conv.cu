@@ -951,56 +951,66 @@ k_conv_wgrad_tri(const __grid_constant__ CUtensorMap tmX, const __grid_constant_
 //    horizontal taps are descriptors shifted by one pixel (128 bytes), and the
 //    two M halves of group A, one pixel apart, are one descriptor with a
 //    leading byte offset of 128;
-//  * dz rows: each is loaded once into a ring of WS_KZ rows and once into the
-//    ring's mirror (slot + WS_KZ).  Row loads take slots in descending order,
-//    so rows y+1, y, y-1 always sit at three consecutive slots and each N block
-//    of the accumulator always receives the same dy.
-// Per unit: one 10 KiB x window, two 8 KiB dz copies and 8 MMAs of
-// 128 x 192 x 16 (the earlier kernels move 40 KiB per 4 MMAs).  At the end the
-// CTA writes its 9 x 64 x 64 + 64 sums to its own row of a scratch array and
+//  * dz rows: each is loaded once into a ring of KZ rows.  Row loads take slots
+//    in descending order, so rows y+1, y, y-1 sit at three consecutive slots
+//    (one descriptor, leading byte offset = one slot) and each N block of the
+//    accumulator always receives the same dy.  The descriptor of the top slot
+//    reads two slots past the ring, so rows landing in slots 0 and 1 are
+//    loaded a second time into slots KZ and KZ+1 (2 of every KZ rows).
+// Per unit (PIX = 64): one 10 KiB x window, 8 KiB of dz (plus the occasional
+// second copy) and 8 MMAs of 128 x 192 x 16 (the earlier kernels move 40 KiB
+// per 4 MMAs); PIX = 128 doubles the unit, halving the per-unit waits and
+// commits of the single producer and MMA threads.  At the end the CTA writes
+// its 9 x 64 x 64 + 64 sums to its own row of a scratch array and
 // k_wgrad_reduce adds the rows in a fixed order into dw and db, so the result
 // does not depend on timing (no atomics).
-constexpr int WS_XPIX = 80;                  // x window pixels: x0-8 .. x0+71
-constexpr int WS_XBYTES = WS_XPIX * CH * 2;  // 10 KiB
-constexpr int WS_KX = 6;                     // x window slots
-constexpr int WS_KZ = 8;                     // dz ring rows (16 slots with the mirrors)
 static_assert(WS_NPART == 9 * CH * CH + CH, "one CTA's partial dw and db");
 
+template <int PIX, int KX, int KZ>
 struct WsSmem {
-  uint8_t x[WS_KX][WS_XBYTES];
-  uint8_t z[2 * WS_KZ][WG_TILE];
-  uint8_t ones[WG_TILE];
-  uint64_t xfull[WS_KX], xempty[WS_KX], zfull[WS_KZ], zempty[WS_KZ];
+  static constexpr int XPIX = PIX + 16;            // x window pixels: x0-8 .. x0+PIX+7
+  static constexpr int XBYTES = XPIX * CH * 2;     // 10 KiB at PIX = 64
+  static constexpr int ZBYTES = PIX * CH * 2;      // 8 KiB at PIX = 64
+  uint8_t x[KX][XBYTES];
+  uint8_t z[KZ + 2][ZBYTES];
+  uint8_t ones[16 * 128];  // 16 pixel rows of ones: the second M half of group B's A operand
+  uint64_t xfull[KX], xempty[KX], zfull[KZ], zempty[KZ];
   uint64_t done;
   uint32_t tmem_base;
 };
 
 // Ring slot of the l-th dz row load: consecutive loads take descending slots.
-__device__ __forceinline__ uint32_t ws_zslot(uint32_t l) { return (WS_KZ - l % WS_KZ) % WS_KZ; }
-// Loads among the first n whose slot is s (the ring visits each slot once per WS_KZ loads).
+template <int KZ>
+__device__ __forceinline__ uint32_t ws_zslot(uint32_t l) { return (KZ - l % KZ) % KZ; }
+// Loads among the first n whose slot is s (the ring visits each slot once per KZ loads).
+template <int KZ>
 __device__ __forceinline__ uint32_t ws_zcount(uint32_t n, uint32_t s) {
-  const uint32_t j = (WS_KZ - s) % WS_KZ;
-  return n / WS_KZ + (j < n % WS_KZ ? 1u : 0u);
+  const uint32_t j = (KZ - s) % KZ;
+  return n / KZ + (j < n % KZ ? 1u : 0u);
 }
 
+template <int PIX, int KX, int KZ>
 __global__ void __launch_bounds__(THREADS, 1)
 k_conv_wgrad_strip(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmZ,
                    WgradArgs G) {
+  using Smem = WsSmem<PIX, KX, KZ>;
+  static_assert(Smem::XBYTES % 1024 == 0 && Smem::ZBYTES % 1024 == 0, "128-byte swizzle atoms");
+  static_assert(KZ >= 4 && KX >= 2, "ring depths");
   extern __shared__ uint8_t smem_raw[];
-  WsSmem& S = *reinterpret_cast<WsSmem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  Smem& S = *reinterpret_cast<Smem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int xch = G.W / WG_PIX;
+  const int xch = G.W / PIX;
   const long nunit = (long)G.N * xch * G.H;
   const long u_begin = nunit * blockIdx.x / gridDim.x;
   const long u_end = nunit * (blockIdx.x + 1) / gridDim.x;
   const bool have = u_end > u_begin;
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < WS_KX; ++s) {
+    for (int s = 0; s < KX; ++s) {
       mbar_init(&S.xfull[s], 1);
       mbar_init(&S.xempty[s], 1);
     }
-    for (int s = 0; s < WS_KZ; ++s) {
+    for (int s = 0; s < KZ; ++s) {
       mbar_init(&S.zfull[s], 1);
       mbar_init(&S.zempty[s], 1);
     }
@@ -1010,7 +1020,7 @@ k_conv_wgrad_strip(const __grid_constant__ CUtensorMap tmX, const __grid_constan
   if (warp >= 2) {  // the all-ones half of group B's A operand
     const uint4 ones = make_uint4(0x3F803F80u, 0x3F803F80u, 0x3F803F80u, 0x3F803F80u);
     uint4* d = reinterpret_cast<uint4*>(S.ones);
-    for (int i = threadIdx.x - 64; i < WG_TILE / 16; i += THREADS - 64) d[i] = ones;
+    for (int i = threadIdx.x - 64; i < 16 * 128 / 16; i += THREADS - 64) d[i] = ones;
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
   if (warp == 1) tmem_alloc(&S.tmem_base, 512);
@@ -1031,20 +1041,20 @@ k_conv_wgrad_strip(const __grid_constant__ CUtensorMap tmX, const __grid_constan
     bool ok = true;
     int y = y_begin, xc = xc_begin, n = n_begin;
     for (long u = u_begin; u < u_end && ok; ++u) {
-      const int x0 = xc * WG_PIX;
+      const int x0 = xc * PIX;
       // a strip starts at the range's first unit or at row 0: rows y-1 and y first
       for (int dr = (u == u_begin || y == 0) ? -1 : 1; dr <= 1 && ok; ++dr) {
-        const uint32_t s = ws_zslot(lz);
-        if (!mbar_wait(&S.zempty[s], ((lz / WS_KZ) & 1) ^ 1)) { ok = false; break; }
-        mbar_expect_tx(&S.zfull[s], 2 * WG_TILE);
+        const uint32_t s = ws_zslot<KZ>(lz);
+        if (!mbar_wait(&S.zempty[s], ((lz / KZ) & 1) ^ 1)) { ok = false; break; }
+        mbar_expect_tx(&S.zfull[s], (s < 2 ? 2 : 1) * Smem::ZBYTES);
         tma_load_4d(S.z[s], &tmZ, &S.zfull[s], 0, x0, y + dr, n);
-        tma_load_4d(S.z[s + WS_KZ], &tmZ, &S.zfull[s], 0, x0, y + dr, n);
+        if (s < 2) tma_load_4d(S.z[s + KZ], &tmZ, &S.zfull[s], 0, x0, y + dr, n);
         ++lz;
       }
       if (!ok) break;
-      const uint32_t s = lx % WS_KX;
-      if (!mbar_wait(&S.xempty[s], ((lx / WS_KX) & 1) ^ 1)) { ok = false; break; }
-      mbar_expect_tx(&S.xfull[s], WS_XBYTES);
+      const uint32_t s = lx % KX;
+      if (!mbar_wait(&S.xempty[s], ((lx / KX) & 1) ^ 1)) { ok = false; break; }
+      mbar_expect_tx(&S.xfull[s], Smem::XBYTES);
       tma_load_4d(S.x[s], &tmX, &S.xfull[s], 0, x0 - 8, y, n);
       ++lx;
       if (++y == G.H) {
@@ -1054,12 +1064,12 @@ k_conv_wgrad_strip(const __grid_constant__ CUtensorMap tmX, const __grid_constan
     }
     if (!ok) fail(G.err, 51);
     // every armed load lands before the CTA may exit
-    for (uint32_t s = 0; s < WS_KX; ++s) {
-      const uint32_t armed = lx / WS_KX + (s < lx % WS_KX ? 1u : 0u);
+    for (uint32_t s = 0; s < (uint32_t)KX; ++s) {
+      const uint32_t armed = lx / KX + (s < lx % KX ? 1u : 0u);
       if (armed) mbar_wait(&S.xfull[s], (armed - 1) & 1);
     }
-    for (uint32_t s = 0; s < WS_KZ; ++s) {
-      const uint32_t armed = ws_zcount(lz, s);
+    for (uint32_t s = 0; s < (uint32_t)KZ; ++s) {
+      const uint32_t armed = ws_zcount<KZ>(lz, s);
       if (armed) mbar_wait(&S.zfull[s], (armed - 1) & 1);
     }
   } else if (warp == 1 && lane == 0) {
@@ -1075,28 +1085,28 @@ k_conv_wgrad_strip(const __grid_constant__ CUtensorMap tmX, const __grid_constan
       if (start) lz += 2;
       const uint32_t l1 = lz++;  // dz row y+1; rows y and y-1 are loads l1-1 and l1-2
       for (uint32_t l = start ? l1 - 2 : l1; l <= l1 && ok; ++l)
-        ok = mbar_wait(&S.zfull[ws_zslot(l)], (l / WS_KZ) & 1);
-      const uint32_t xsl = lx % WS_KX;
-      if (ok) ok = mbar_wait(&S.xfull[xsl], (lx / WS_KX) & 1);
+        ok = mbar_wait(&S.zfull[ws_zslot<KZ>(l)], (l / KZ) & 1);
+      const uint32_t xsl = lx % KX;
+      if (ok) ok = mbar_wait(&S.xfull[xsl], (lx / KX) & 1);
       if (!ok) break;
       ++lx;
       tc_fence_after();
       const uint32_t xs = smem_u32(S.x[xsl]);
-      const uint32_t zb = smem_u32(S.z[ws_zslot(l1)]);
-      const uint32_t lbo_ones = ones - (xs + 9u * 128u);
+      const uint32_t zb = smem_u32(S.z[ws_zslot<KZ>(l1)]);
 #pragma unroll
-      for (int k = 0; k < WG_PIX / 16; ++k) {
-        const uint64_t bd = sdesc(zb + 2048u * k, WG_TILE, 1024);
+      for (int k = 0; k < PIX / 16; ++k) {
+        const uint64_t bd = sdesc(zb + 2048u * k, Smem::ZBYTES, 1024);
         const uint32_t acc = (first && k == 0) ? 0u : 1u;
+        const uint32_t xb = xs + (9u + 16u * k) * 128u;  // x(+1) rows of this K step
         mma_bf16(tmem, sdesc(xs + (7u + 16u * k) * 128u, 128, 1024), bd, ID, acc);
-        mma_bf16(tmem + 256, sdesc(xs + (9u + 16u * k) * 128u, lbo_ones, 1024), bd, ID, acc);
+        mma_bf16(tmem + 256, sdesc(xb, ones - xb, 1024), bd, ID, acc);  // ones lie after the x ring
       }
       first = false;
       mma_commit(&S.xempty[xsl]);
-      mma_commit(&S.zempty[ws_zslot(l1 - 2)]);  // row y-1 has had its last use
-      if (last) {                                // so have rows y and y+1 at a strip's end
-        mma_commit(&S.zempty[ws_zslot(l1 - 1)]);
-        mma_commit(&S.zempty[ws_zslot(l1)]);
+      mma_commit(&S.zempty[ws_zslot<KZ>(l1 - 2)]);  // row y-1 has had its last use
+      if (last) {                                    // so have rows y and y+1 at a strip's end
+        mma_commit(&S.zempty[ws_zslot<KZ>(l1 - 1)]);
+        mma_commit(&S.zempty[ws_zslot<KZ>(l1)]);
       }
     }
     if (!ok) fail(G.err, 52);
@@ -1146,6 +1156,14 @@ k_conv_wgrad_strip(const __grid_constant__ CUtensorMap tmX, const __grid_constan
     tmem_dealloc(tmem, 512);
   }
 }
+
+// The strip kernel's configurations: unit width and ring depths.
+using WsA = WsSmem<64, 8, 12>;   // wgrad variant 2
+#ifndef NEMO_WS_WIDE_KX
+#define NEMO_WS_WIDE_KX 5
+#endif
+using WsB = WsSmem<128, NEMO_WS_WIDE_KX, 6>;  // wgrad variant 3, the default (WsA unless W % 128 == 0)
+static_assert(sizeof(WsA) + 1024 <= 232448 && sizeof(WsB) + 1024 <= 232448, "shared memory per CTA");
 
 // dw[i] += sum_b part[b][i] (i < 9*64*64), db[i - 9*64*64] += ... (the rest),
 // b = 0 .. nblk-1 in a fixed tree: 8 segments of consecutive rows summed in
@@ -1214,8 +1232,10 @@ bool g_attr[64];
 int g_fwd_variant = 2;  // 2: three output rows per MMA (k_conv_fwd_tri), 1: row ring
                         // (k_conv_fwd_rows), 0: a TMA window per tap (k_conv_fwd)
 int g_fwd_rows = 16;    // rows per strip of the row-ring kernel
-int g_wgrad_variant = 2;  // 2: all taps per CTA over column strips (k_conv_wgrad_strip),
-                          // 1: three vertical taps per MMA (k_conv_wgrad_tri), 0: tap pairs
+int g_wgrad_variant = 3;  // 3: all taps per CTA over column strips (k_conv_wgrad_strip)
+                          // in 128-pixel units where the width allows, else as 2;
+                          // 2: the same in 64-pixel units; 1: three vertical taps per MMA
+                          // (k_conv_wgrad_tri), 0: tap pairs
 // Scratch of k_conv_wgrad_strip for callers that pass none: one array per
 // device, grown on demand and kept until the process exits.
 // Test settings of the forward kernel's failure path (set_test_wait).
@@ -1241,8 +1261,11 @@ cudaError_t prepare_device(int* sms) {
     e = cudaFuncSetAttribute(k_conv_wgrad_tri, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)(sizeof(WtSmem) + 1024));
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_conv_wgrad_strip, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)(sizeof(WsSmem) + 1024));
+    e = cudaFuncSetAttribute(k_conv_wgrad_strip<64, 8, 12>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(sizeof(WsA) + 1024));
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_conv_wgrad_strip<128, NEMO_WS_WIDE_KX, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(sizeof(WsB) + 1024));
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k_conv_fwd_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)(sizeof(RowSmem) + 1024));
@@ -1304,11 +1327,11 @@ cudaError_t conv_fwd(const __nv_bfloat16* x, const __nv_bfloat16* w, const ConvE
 
 int set_wgrad_variant(int variant) {
   const int prev = g_wgrad_variant;
-  if (variant >= 0 && variant <= 2) g_wgrad_variant = variant;
+  if (variant >= 0 && variant <= 3) g_wgrad_variant = variant;
   return prev;
 }
 
-int wgrad_kernels() { return g_wgrad_variant == 2 ? 2 : 1; }
+int wgrad_kernels() { return g_wgrad_variant >= 2 ? 2 : 1; }
 
 unsigned long long set_test_wait(unsigned long long wait_ns, int skip_launches) {
   g_test_skip.store(skip_launches > 0 ? skip_launches : 0);
@@ -1332,10 +1355,12 @@ cudaError_t conv_wgrad(const __nv_bfloat16* x, const __nv_bfloat16* dz, const Wg
   int sms = 0;
   if ((e = prepare_device(&sms)) != cudaSuccess) return e;
   CUtensorMap tx, tz;
-  if ((e = act_map(&tz, dz, g.N, g.H, g.W, WG_PIX)) != cudaSuccess) return e;
-  if (g_wgrad_variant == 2) {
-    if ((e = act_map(&tx, x, g.N, g.H, g.W, WS_XPIX)) != cudaSuccess) return e;
-    const long nunit = (long)g.N * g.H * (g.W / WG_PIX);
+  if (g_wgrad_variant >= 2) {
+    const bool wide = g_wgrad_variant == 3 && g.W % 128 == 0;
+    const int pix = wide ? 128 : 64;
+    if ((e = act_map(&tz, dz, g.N, g.H, g.W, pix)) != cudaSuccess) return e;
+    if ((e = act_map(&tx, x, g.N, g.H, g.W, pix + 16)) != cudaSuccess) return e;
+    const long nunit = (long)g.N * g.H * (g.W / pix);
     long gx = ctas > 0 ? ctas : sms;  // one CTA per SM (shared and tensor memory)
     if (gx > nunit) gx = nunit;
     WgradArgs a = g;
@@ -1360,11 +1385,15 @@ cudaError_t conv_wgrad(const __nv_bfloat16* x, const __nv_bfloat16* dz, const Wg
     }
     if (gx > a.partial_blocks) gx = a.partial_blocks;
     if (gx < 1) return cudaErrorInvalidValue;
-    k_conv_wgrad_strip<<<(unsigned)gx, THREADS, sizeof(WsSmem) + 1024, s>>>(tx, tz, a);
+    if (wide)
+      k_conv_wgrad_strip<128, NEMO_WS_WIDE_KX, 6><<<(unsigned)gx, THREADS, sizeof(WsB) + 1024, s>>>(tx, tz, a);
+    else
+      k_conv_wgrad_strip<64, 8, 12><<<(unsigned)gx, THREADS, sizeof(WsA) + 1024, s>>>(tx, tz, a);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     k_wgrad_reduce<<<(WS_NPART + 31) / 32, 256, 0, s>>>(a.partial, (int)gx, g.dw, g.db);
     return cudaGetLastError();
   }
+  if ((e = act_map(&tz, dz, g.N, g.H, g.W, WG_PIX)) != cudaSuccess) return e;
   if ((e = act_map(&tx, x, g.N, g.H, g.W, WG_PIX)) != cudaSuccess) return e;
   if (g_wgrad_variant == 1) {
     // one CTA per SM: one wave of the 2 tap groups

@@ -222,7 +222,8 @@ def conv3x3_fwd_variant(lib, variant, rows=0):
 
 def conv3x3_wgrad_variant(lib, variant):
     """Select the weight-gradient kernel process-wide (2: all taps per CTA with
-    a fixed-order sum of the CTAs' partials, the default; 1: three vertical
+    a fixed-order sum of the CTAs' partials; 3, the default: the same with
+    128-pixel column chunks where the width allows; 1: three vertical
     taps per MMA; 0: tap pairs); returns the previous variant (-1 only
     queries)."""
     return lib.nemo_conv3x3_wgrad_variant(variant)

@@ -115,10 +115,11 @@ def test_dgrad_with_flipped_weights_matches_oracle(env, variant):
     assert np.abs(o32 - ref[..., :4]).max() <= 1e-4 * np.abs(ref[..., :4]).max()
 
 
-@pytest.fixture(params=[2, 1, 0], ids=["wg-strip", "wg-tri", "wg-pairs"])
+@pytest.fixture(params=[2, 3, 1, 0], ids=["wg-strip", "wg-strip128", "wg-tri", "wg-pairs"])
 def wvariant(request, env):
-    """Each weight-gradient kernel (all taps per CTA with a fixed-order sum,
-    six taps per MMA, tap pairs), restored to the default afterwards."""
+    """Each weight-gradient kernel (all taps per CTA with a fixed-order sum, in
+    64- and 128-pixel column chunks; six taps per MMA; tap pairs), restored to
+    the default afterwards."""
     torch, nb, sm = env
     lib = nb.load(False)
     prev = sm.conv3x3_wgrad_variant(lib, request.param)
@@ -126,7 +127,8 @@ def wvariant(request, env):
     sm.conv3x3_wgrad_variant(lib, prev)
 
 
-@pytest.mark.parametrize("shape,ctas", [((2, 5, 128), 0), ((1, 7, 192), 3), ((3, 2, 64), 1), ((1, 1, 64), 0)])
+@pytest.mark.parametrize("shape,ctas", [((2, 5, 128), 0), ((1, 7, 192), 3), ((3, 2, 64), 1), ((1, 1, 64), 0),
+                                        ((2, 13, 256), 5), ((1, 3, 384), 0)])
 def test_wgrad_and_bias_grad_match_oracle(env, wvariant, shape, ctas):
     torch, nb, sm = env
     N, H, W = shape
@@ -156,7 +158,7 @@ def test_default_wgrad_is_bitwise_repeatable(env, shape, ctas):
     promise that)."""
     torch, nb, sm = env
     lib = nb.load(False)
-    assert sm.conv3x3_wgrad_variant(lib, -1) == 2  # the default
+    assert sm.conv3x3_wgrad_variant(lib, -1) == 3  # the default
     N, H, W = shape
     g = torch.Generator(device="cuda").manual_seed(5)
     x = torch.randn((N, H, W, 64), device="cuda", generator=g).to(torch.bfloat16)
