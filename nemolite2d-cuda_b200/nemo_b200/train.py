@@ -49,7 +49,7 @@ def snapshot_steps(steps, every=10, pair_stride=None):
 
 
 def generate_runs(sur, seed, nmem, side, steps, every=10, amp_scale=0.2, strict=False,
-                  bound=2.5, pair_stride=None):
+                  bound=2.5, pair_stride=None, members=None):
     """Runs nmem members from rest for `steps` steps and returns (snaps, tides)
     of the members whose run stays bounded (finite, max |ssh| <= bound x the
     member's tidal amplitude; the reference scheme lets a tide that starts
@@ -57,9 +57,12 @@ def generate_runs(sur, seed, nmem, side, steps, every=10, amp_scale=0.2, strict=
     snaps [S][kept][side][side][4] float32 on the device at the steps of
     snapshot_steps(steps, every, pair_stride), tides [S][kept] float32 (the
     boundary SSH at each snapshot's step).  The number of members dropped is
-    in generate_runs.dropped."""
+    in generate_runs.dropped.  `members` (a list of side x side members)
+    replaces the seeded draw of nmem members."""
     torch = _torch()
-    members = square_members(seed, nmem, side, amp_scale)
+    if members is None:
+        members = square_members(seed, nmem, side, amp_scale)
+    nmem = len(members)
     ens = Ensemble(members, strict=strict, **COMMON)
     at = snapshot_steps(steps, every, pair_stride)
     ns = len(at)
@@ -87,6 +90,26 @@ def generate_runs(sur, seed, nmem, side, steps, every=10, amp_scale=0.2, strict=
 
 
 generate_runs.dropped = 0
+
+
+def generate_dataset(sur, seed, nruns, side, steps, every=10, chunk=256, amp_scale=0.2, bound=2.5):
+    """A training set of `nruns` seeded runs of the batched recipe at a fixed
+    side (the surrogate-training configuration: 2048 runs of 256 x 256, 500
+    steps, snapshots every 10 steps, about 100 GiB of FP32 snapshots),
+    generated `chunk` runs at a time, one ensemble per chunk, and kept as one
+    snapshot tensor per chunk, so that generation never holds more than one
+    chunk twice.  Returns (chunks, dropped): chunks is a list of the
+    (snaps, tides) pairs generate_runs returns, dropped the number of runs
+    that left the bound."""
+    members = square_members(seed, nruns, side, amp_scale)
+    chunks, dropped = [], 0
+    for c0 in range(0, nruns, chunk):
+        snaps, tides = generate_runs(sur, seed, 0, side, steps, every, amp_scale, bound=bound,
+                                     members=members[c0:c0 + chunk])
+        dropped += generate_runs.dropped
+        if snaps.shape[1]:
+            chunks.append((snaps, tides))
+    return chunks, dropped
 
 
 def bounded_members(members, steps, common, bound=2.5, checks=2, batch=64, want=None):
@@ -163,6 +186,47 @@ class PairSampler:
         s0 = self.snaps[k, m].contiguous()
         s1 = self.snaps[k + 1, m].contiguous()
         t1 = self.tides[k + 1, m].contiguous()
+        torch.cuda.synchronize()
+        self.s0, self.s1, self.t1 = s0, s1, t1  # keep alive while the library reads
+        return s0, s1, t1
+
+
+class ChunkPairSampler:
+    """Random (snapshot k, snapshot k+1) pairs drawn from a data set held as
+    several snapshot tensors (generate_dataset's chunks), gathered into one
+    contiguous device batch."""
+
+    def __init__(self, chunks, seed=0):
+        torch = _torch()
+        self.chunks = chunks
+        self.pairs = [(c, k, m) for c, (sn, _) in enumerate(chunks)
+                      for k in range(sn.shape[0] - 1) for m in range(sn.shape[1])]
+        self.rng = np.random.default_rng(seed)
+        self.order = []
+        self.s0 = self.s1 = self.t1 = None
+        self._torch = torch
+
+    def __len__(self):
+        return len(self.pairs)
+
+    def batch(self, n):
+        torch = self._torch
+        if len(self.order) < n:
+            self.order = list(self.rng.permutation(len(self.pairs)))
+        idx = [self.pairs[self.order.pop()] for _ in range(n)]
+        parts0, parts1, partt = [], [], []
+        for c, (sn, td) in enumerate(self.chunks):
+            sel = [(k, m) for cc, k, m in idx if cc == c]
+            if not sel:
+                continue
+            k = torch.tensor([i[0] for i in sel], device="cuda")
+            m = torch.tensor([i[1] for i in sel], device="cuda")
+            parts0.append(sn[k, m])
+            parts1.append(sn[k + 1, m])
+            partt.append(td[k + 1, m])
+        s0 = torch.cat(parts0).contiguous()
+        s1 = torch.cat(parts1).contiguous()
+        t1 = torch.cat(partt).contiguous()
         torch.cuda.synchronize()
         self.s0, self.s1, self.t1 = s0, s1, t1  # keep alive while the library reads
         return s0, s1, t1

@@ -633,3 +633,30 @@ def test_training_beats_persistence_on_held_out_runs(env):
     print("ssh rel err: persistence %.4f untrained %.4f trained %.4f" % (pers, untrained, trained))
     assert trained < 0.5 * pers
     assert trained < untrained
+
+
+def test_chunked_data_set_holds_the_runs_of_one_ensemble(env):
+    """generate_dataset (the 2048-run training set, generated a chunk of runs
+    at a time) holds exactly the snapshots one ensemble of all the runs gives,
+    and ChunkPairSampler draws (snapshot k, snapshot k+1) pairs of one run with
+    the boundary SSH of the later one."""
+    torch, nb, sm = env
+    from nemo_b200 import train as tr
+    side = 128
+    s = sm.Surrogate(nblocks=1, batch=4, height=side, width=side, seed=2)
+    chunks, dropped = tr.generate_dataset(s, seed=31, nruns=7, side=side, steps=60, chunk=3)
+    whole, tides = tr.generate_runs(s, seed=31, nmem=7, side=side, steps=60)
+    assert dropped == tr.generate_runs.dropped
+    assert sum(c[0].shape[1] for c in chunks) == whole.shape[1] == 7 - dropped
+    assert torch.equal(torch.cat([c[0] for c in chunks], 1), whole)
+    assert torch.equal(torch.cat([c[1] for c in chunks], 1), tides)
+    sampler = tr.ChunkPairSampler(chunks, seed=5)
+    assert len(sampler) == (whole.shape[0] - 1) * whole.shape[1]
+    s0, s1, t1 = sampler.batch(9)
+    assert s0.shape == (9, side, side, 4) and s1.shape == s0.shape and t1.shape == (9,)
+    S, M = whole.shape[0], whole.shape[1]
+    for i in range(9):
+        hits = [(k, m) for k in range(S - 1) for m in range(M)
+                if torch.equal(whole[k, m], s0[i]) and torch.equal(whole[k + 1, m], s1[i])]
+        assert hits, "sampled pair %d is not two consecutive snapshots of one run" % i
+        assert any(float(tides[k + 1, m]) == float(t1[i]) for k, m in hits)
