@@ -1000,8 +1000,9 @@ int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, 
       return status_of(ae);
     }
   }
-  auto saved_field = [&](int parity, int m, int f) {
-    return saved + (((size_t)parity * nm + m) * 3 + f) * field_elems;
+  // slot x % NS holds the start of window x
+  auto saved_field = [&](int slot, int m, int f) {
+    return saved + (((size_t)slot * nm + m) * 3 + f) * field_elems;
   };
   // per member and slot: the window whose start the slot holds, and the
   // window (if it is the same one) the surrogate advanced the member in
@@ -1018,15 +1019,15 @@ int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, 
   };
   const long long launches0 = s->nlaunch;
   long long solver_launches = 0;  // one persistent ensemble launch per solver step
-  // Members with sel[m] go back to the state saved in slot `parity` (the
-  // start of step istp_from + 1) and the solver runs them n steps (n even,
-  // so their state buffers keep their parity).
-  auto rewind_to = [&](int parity, const char* sel, int istp_from, int n, int count) -> int {
+  // Members with sel[m] go back to the state saved in `slot` (the start of
+  // step istp_from + 1) and the solver runs them n steps (n even, so their
+  // state buffers keep their parity).
+  auto rewind_to = [&](int slot, const char* sel, int istp_from, int n, int count) -> int {
     for (int m = 0; m < nm; ++m) {
       if (!sel[m]) continue;
       double* dst[3] = {ms[m].sshn, ms[m].un, ms[m].vn};
       for (int f = 0; f < 3; ++f) {
-        const int r = status_of(cudaMemcpyAsync(dst[f], saved_field(parity, m, f), field_elems * sizeof(double),
+        const int r = status_of(cudaMemcpyAsync(dst[f], saved_field(slot, m, f), field_elems * sizeof(double),
                                                 cudaMemcpyDeviceToDevice, s->stream));
         if (r != NEMO_OK) return r;
       }
@@ -1052,7 +1053,7 @@ int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, 
         if (quar[m]) continue;
         double* src[3] = {ms[m].sshn, ms[m].un, ms[m].vn};
         for (int f = 0; f < 3 && rc == NEMO_OK; ++f)
-          rc = status_of(cudaMemcpyAsync(saved_field(w & 1, m, f), src[f], field_elems * sizeof(double),
+          rc = status_of(cudaMemcpyAsync(saved_field(w % NS, m, f), src[f], field_elems * sizeof(double),
                                          cudaMemcpyDeviceToDevice, s->stream));
         saved_at[NS * m + w % NS] = w;
       }

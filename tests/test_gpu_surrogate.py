@@ -6,6 +6,8 @@ Tolerances: BF16 outputs within 1 BF16 ulp of the oracle rounded to BF16
 1e-4 of the output's max-norm; whole-network gradients within 2e-2 normwise
 per layer (BF16 activations and gradients in both, FP32 vs FP64 sums).
 """
+import math
+
 import numpy as np
 import pytest
 
@@ -660,3 +662,55 @@ def test_chunked_data_set_holds_the_runs_of_one_ensemble(env):
                 if torch.equal(whole[k, m], s0[i]) and torch.equal(whole[k + 1, m], s1[i])]
         assert hits, "sampled pair %d is not two consecutive snapshots of one run" % i
         assert any(float(tides[k + 1, m]) == float(t1[i]) for k, m in hits)
+
+
+def test_rewind_from_the_fourth_window_restores_the_third_windows_start(env):
+    """The window starts are kept in three slots (slot x mod 3 holds window
+    x): a member accepted in window 2 and quarantined in window 3 restarts
+    from window 2's start, so its run equals two hybrid windows followed by
+    the plain solver, bit for bit.  The network (no residual blocks) passes
+    only the boundary row's tide input, less a threshold set between the
+    tides windows 2 and 3 predict (times the boundary flag), through a ReLU:
+    windows 0-2 see a zero output (persistence, accepted), window 3's
+    prediction adds inf to u (its FP32 quotient by an output scale of 1e-35
+    overflows), so its shadow error is not finite.  The start step is the
+    first at which the tide rises through the four windows."""
+    torch, nb, sm = env
+    from nemo_b200 import train as tr
+    side, n = 128, 1
+    member = tr.square_members(61, n, side, 0.2)[0]
+
+    def tides(i0):
+        return [tr.tide_of(member, i0 + 100 * w + 10) for w in range(4)]
+
+    istp0 = next(i for i in range(0, 2300, 10)
+                 if all(b - a > 0.05 * member.amp_tide for a, b in zip(tides(i), tides(i)[1:])))
+    t = tides(istp0)
+    theta = 0.5 * (t[2] + t[3])
+    s = sm.Surrogate(nblocks=0, batch=n, height=side, width=side, train=False, seed=4)
+    p = np.zeros_like(s.params())
+    wl = 9 * 64 * 64
+    big = 2.0 ** 33
+    centre = 4 * 64 * 64                         # tap (0, 0), [out channel][in channel]
+    p[0 * wl + centre + 0 * 64 + 5] = big        # tide input (channel 5) -> channel 0
+    p[0 * wl + centre + 0 * 64 + 4] = -big * theta  # boundary flag (channel 4) -> channel 0
+    p[1 * wl + centre + 1 * 64 + 0] = 1.0        # channel 0 -> u output
+    s.set_params(p)
+    s.set_norm([1.0] * 4, [0.0] * 4, [1.0, 1e-35, 1.0])
+
+    def developed():
+        e = small_ensemble(nb, 61, n, side)
+        if istp0 > 0:
+            e.step_n(1, istp0)
+        return e
+
+    ref = developed()
+    st = sm.hyb_run(s, ref, istp0, 200, tol=1e300, quarantine=1e100)
+    assert st["fallbacks"] == 0 and st["quarantined"] == 0 and st["sur_steps"] == 180, st
+    ref.step_n(istp0 + 201, 200)
+    a = developed()
+    st = sm.hyb_run(s, a, istp0, 400, tol=1e300, quarantine=1e100)
+    assert st["quarantined"] == 1 and st["rewound"] == 1 and st["fallbacks"] == 1, st
+    assert st["sur_steps"] == 270 and st["solver_steps"] == 4 * 10 + 110 + 90, st
+    for f in (nb.SSHN, nb.UN, nb.VN):
+        np.testing.assert_array_equal(a.field(0, f), ref.field(0, f))
