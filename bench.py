@@ -95,8 +95,10 @@ def parse():
     ap.add_argument("--anchor", type=int, default=100, help="FP64 re-anchor interval (hybrid)")
     ap.add_argument("--tol", type=float, default=0.01, help="fallback tolerance (hybrid)")
     ap.add_argument("--quarantine", type=float, default=0.05, help="quarantine threshold (hybrid)")
+    ap.add_argument("--correct", type=int, default=0,
+                    help="1: accepted calls add the shadow step's correction (hybrid)")
     ap.add_argument("--sweep", type=str, default="",
-                    help="hybrid points anchor:tol:quarantine,... run after one training")
+                    help="hybrid points anchor:tol:quarantine[:correct],... run after one training")
     ap.add_argument("--repeats", type=int, default=1, help="hybrid runs per point (median reported)")
     ap.add_argument("--candidates", type=int, default=128, help="hybrid member candidates")
     ap.add_argument("--strict", action="store_true", help="time the -fmad=false library (general)")
@@ -673,11 +675,12 @@ def run_hybrid(args):
         t_plain.append(timed(lambda: plain.step_n(1, nsteps))[0])
     plain.checksums()
     v_plain = cells * nsteps / statistics.median(t_plain)
-    points = [(args.anchor, args.tol, args.quarantine)]
+    points = [(args.anchor, args.tol, args.quarantine, args.correct)]
     if args.sweep:
         points = [tuple(float(x) for x in p.split(":")) for p in args.sweep.split(",")]
-    for anchor, tol, quar in points:
-        anchor = int(anchor)
+        points = [p if len(p) == 4 else p + (args.correct,) for p in points]
+    for anchor, tol, quar, corr in points:
+        anchor, corr = int(anchor), int(corr)
         runs = []
         for r in range(args.repeats):
             for k, st0 in enumerate(rest):
@@ -685,7 +688,7 @@ def run_hybrid(args):
             clocks = ClockSampler(0)
             clocks.start()
             t_hyb, st = timed(lambda: sm.hyb_run(inf, hyb, 0, nsteps, k=args.k, anchor=anchor, tol=tol,
-                                                 quarantine=quar))
+                                                 quarantine=quar, correct=bool(corr)))
             clk = clocks.stop()
             err = sm.ens_compare(hyb, plain)
             finite = np.isfinite(err).all(axis=1)
@@ -704,9 +707,11 @@ def run_hybrid(args):
                 "ms_per_step": med["seconds"] * 1e3, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "bf16+f64", "data": "synthetic",
                 "config": {"workload": "%d members 2048x2048, %d steps, surrogate k=%d, re-anchor %d, "
-                                       "tol %g relative SSH L2 vs shadow FP64 step, quarantine %g"
-                                       % (nm, nsteps, args.k, anchor, tol, quar),
+                                       "tol %g relative SSH L2 vs shadow FP64 step, quarantine %g%s"
+                                       % (nm, nsteps, args.k, anchor, tol, quar,
+                                          ", shadow correction" if corr else ""),
                            "anchor": anchor, "tol": tol, "quarantine": quar, "k": args.k,
+                           "correct": corr,
                            "candidates": len(cands), "candidates_screened": screened,
                            "screened_out": screened - len(ok),
                            "patch": P, "nblocks": args.nblocks, "train_side": ts,

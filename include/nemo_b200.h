@@ -370,6 +370,10 @@ typedef struct nemo_hyb_config {
                         latest of the last three windows the surrogate
                         advanced it in (keeps the states of the last three
                         window starts: 3 x 3 fields per member) (1) */
+  int correct;       /* 1: every surrogate call of an accepted window also adds
+                        the difference between the window's shadow state and
+                        the surrogate's prediction of it, per cell (4 floats
+                        per cell and member of device memory) (0) */
 } nemo_hyb_config;
 
 typedef struct nemo_hyb_stats {

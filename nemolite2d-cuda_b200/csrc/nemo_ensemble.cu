@@ -761,6 +761,7 @@ int ens_member_state(nemo_ens* e, int m, MemberState* out) {
   out->jpi = d.L.jpi;
   out->jpj = d.L.jpj;
   out->pitch = d.L.pitch;
+  out->corr = nullptr;
   return NEMO_OK;
 }
 

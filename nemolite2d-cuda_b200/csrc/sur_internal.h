@@ -80,6 +80,10 @@ struct MemberState {
   const double *ht, *hv;
   const double* sshv0;  // stored sshn_v (row jj = 0: the open boundary's)
   int jpi, jpj, pitch;
+  // hybrid only: the shadow step's correction of a surrogate call, 4 floats
+  // (ssh, u, v, unused) per T-cell in row-major order, added by every call
+  // (null: none)
+  const float* corr;
 };
 int ens_member_state(nemo_ens* e, int m, MemberState* out);
 int ens_member_count(nemo_ens* e);

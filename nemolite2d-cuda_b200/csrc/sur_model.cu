@@ -247,14 +247,16 @@ __global__ void k_apply(const MemberState* __restrict__ ms, int m0, int nm, int 
     const int ji = x + 1, jj = y + 1;
     const float4 d = make_float4(out[out_index<P>(m, y, x, Hn, Wn, 0)], out[out_index<P>(m, y, x, Hn, Wn, 1)],
                                  out[out_index<P>(m, y, x, Hn, Wn, 2)], 0.0f);
+    float4 c = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (M.corr) c = reinterpret_cast<const float4*>(M.corr)[(long)y * W + x];
     double* s = M.sshn + gidx(M.pitch, ji, jj);
-    *s = (jj == 1) ? tide[m0 + m] : *s + (double)(d.x / nm_.out_scale[0]);
+    *s = (jj == 1) ? tide[m0 + m] : *s + (double)(d.x / nm_.out_scale[0]) + (double)c.x;
     if (ji >= 2) {
       double* u = M.un + gidx(M.pitch, ji - 1, jj);
-      *u = *u + (double)(d.y / nm_.out_scale[1]);
+      *u = *u + (double)(d.y / nm_.out_scale[1]) + (double)c.y;
     }
     double* v = M.vn + gidx(M.pitch, ji, jj - 1);
-    *v = *v + (double)(d.z / nm_.out_scale[2]);
+    *v = *v + (double)(d.z / nm_.out_scale[2]) + (double)c.z;
   }
 }
 
@@ -275,11 +277,12 @@ __global__ void k_flather(const MemberState* __restrict__ ms, int m0) {
 
 // Per member: sum (pred - ref)^2 and sum ref^2 for ssh, u, v (acc[m][6]).
 // pred = snap + delta / out_scale when out != null, else the state of `pm`.
+// With corr (and out), ref - pred per T-cell goes to corr[m][y][x].
 template <int P>
 __global__ void __launch_bounds__(256) k_err(const MemberState* __restrict__ ref, const float4* __restrict__ snap,
                                              const float* __restrict__ out, Norm nm_,
                                              const MemberState* __restrict__ pm, int m0, int H, int W,
-                                             double* __restrict__ acc) {
+                                             double* __restrict__ acc, float4* __restrict__ corr = nullptr) {
   __shared__ double sh[8];
   const int m = blockIdx.y;
   const MemberState& R = ref[m0 + m];
@@ -301,6 +304,7 @@ __global__ void __launch_bounds__(256) k_err(const MemberState* __restrict__ ref
       ps = (jj == 1) ? rs : (double)s.x + (double)(d.x / nm_.out_scale[0]);
       pu = (ji >= 2) ? (double)s.y + (double)(d.y / nm_.out_scale[1]) : 0.0;
       pv = (double)s.z + (double)(d.z / nm_.out_scale[2]);
+      if (corr) corr[p] = make_float4((float)(rs - ps), (float)(ru - pu), (float)(rv - pv), 0.0f);
     } else {
       const MemberState& Q = pm[m0 + m];
       ps = Q.sshn[gidx(Q.pitch, ji, jj)];
@@ -465,15 +469,16 @@ __global__ void k_diverged(const MemberState* __restrict__ ms, const double* __r
   if (__syncthreads_or(bad) && threadIdx.x == 0) flag[m] = 1;
 }
 
-cudaError_t launch_err(nemo_sur* s, int nm, const float* snap, const float* out) {
+cudaError_t launch_err(nemo_sur* s, int nm, const float* snap, const float* out, float* corr = nullptr) {
   s->nlaunch += 1;
   const int H = s->cfg.height, W = s->cfg.width;
   const dim3 g((unsigned)(grid_for((long)H * W, 256) / 16 + 1), (unsigned)nm);
   const float4* sp = reinterpret_cast<const float4*>(snap);
+  float4* c4 = reinterpret_cast<float4*>(corr);
   switch (s->P) {
-    case 1: k_err<1><<<g, 256, 0, s->stream>>>(s->d_ms, sp, out, s->norm, nullptr, 0, H, W, s->d_acc); break;
-    case 2: k_err<2><<<g, 256, 0, s->stream>>>(s->d_ms, sp, out, s->norm, nullptr, 0, H, W, s->d_acc); break;
-    default: k_err<4><<<g, 256, 0, s->stream>>>(s->d_ms, sp, out, s->norm, nullptr, 0, H, W, s->d_acc); break;
+    case 1: k_err<1><<<g, 256, 0, s->stream>>>(s->d_ms, sp, out, s->norm, nullptr, 0, H, W, s->d_acc, c4); break;
+    case 2: k_err<2><<<g, 256, 0, s->stream>>>(s->d_ms, sp, out, s->norm, nullptr, 0, H, W, s->d_acc, c4); break;
+    default: k_err<4><<<g, 256, 0, s->stream>>>(s->d_ms, sp, out, s->norm, nullptr, 0, H, W, s->d_acc, c4); break;
   }
   return cudaGetLastError();
 }
@@ -945,6 +950,7 @@ int nemo_hyb_default_config(nemo_hyb_config* c) {
   c->per_member = 1;
   c->quarantine = 0.05;
   c->rewind = 1;
+  c->correct = 0;
   return NEMO_OK;
 }
 
@@ -985,6 +991,15 @@ int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, 
     snap_all = own;
     out_all = own + (size_t)nm * hw * 4;
   }
+  // per-cell corrections from the shadow step (correct = 1)
+  float* corr = nullptr;
+  if (c->correct && nm > 0) {
+    cudaError_t ae = nemo::dev_alloc(&corr, (size_t)nm * hw * 4 * sizeof(float));
+    if (ae != cudaSuccess) {
+      if (own) cudaFree(own);
+      return status_of(ae);
+    }
+  }
   std::vector<double> tide(nm), acc(6 * nm);
   std::vector<char> pass(nm), fail(nm), quar(nm, 0);
   // saved FP64 states (sshn, un, vn) of every member at the last NS window
@@ -997,6 +1012,7 @@ int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, 
     cudaError_t ae = nemo::dev_alloc(&saved, (size_t)NS * nm * 3 * field_elems * sizeof(double));
     if (ae != cudaSuccess) {
       if (own) cudaFree(own);
+      if (corr) cudaFree(corr);
       return status_of(ae);
     }
   }
@@ -1072,7 +1088,7 @@ int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, 
     if (rc == NEMO_OK) rc = ensure_members(s, e, ms, nullptr);  // buffers swapped
     if (rc != NEMO_OK) break;
     cudaError_t ce = cudaMemsetAsync(s->d_acc, 0, 6 * nm * sizeof(double), s->stream);
-    if (ce == cudaSuccess) ce = launch_err(s, nm, snap_all, out_all);
+    if (ce == cudaSuccess) ce = launch_err(s, nm, snap_all, out_all, corr);
     if (ce == cudaSuccess)
       ce = cudaMemcpyAsync(acc.data(), s->d_acc, 6 * nm * sizeof(double), cudaMemcpyDeviceToHost, s->stream);
     if (ce != cudaSuccess) { rc = status_of(ce); break; }
@@ -1127,6 +1143,8 @@ int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, 
     if (nfail < nm) {
       // the accepted members' surrogate calls overlap the fallen-back
       // members' solver steps (disjoint states; the next window starts after both)
+      if (corr)
+        for (int m = 0; m < nm; ++m) ms[m].corr = corr + (size_t)m * hw * 4;
       for (int j = c->k; j < c->anchor && rc == NEMO_OK; j += c->k) {
         rc = advance_members(s, e, ms, pass.data(), istp + j);
         st.sur_calls += 1;
@@ -1189,6 +1207,7 @@ int nemo_hyb_run(nemo_sur* s, nemo_ens* e, const nemo_hyb_config* c, int istp0, 
   if (ce == cudaSuccess) ce = cudaStreamSynchronize(s->stream);
   if (own) cudaFree(own);
   if (saved) cudaFree(saved);
+  if (corr) cudaFree(corr);
   if (rc != NEMO_OK) return rc;
   ECK(ce);
   st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();

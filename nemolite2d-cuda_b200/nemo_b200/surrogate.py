@@ -25,7 +25,8 @@ class AdamW(ctypes.Structure):
 
 class HybConfig(ctypes.Structure):
     _fields_ = [("k", ctypes.c_int), ("anchor", ctypes.c_int), ("tol", ctypes.c_double),
-                ("per_member", ctypes.c_int), ("quarantine", ctypes.c_double), ("rewind", ctypes.c_int)]
+                ("per_member", ctypes.c_int), ("quarantine", ctypes.c_double), ("rewind", ctypes.c_int),
+                ("correct", ctypes.c_int)]
 
 
 class HybStats(ctypes.Structure):
@@ -194,13 +195,16 @@ def ens_compare(a, ref):
 
 
 def hyb_run(sur, ens, istp0, nsteps, k=10, anchor=100, tol=0.01, per_member=True, quarantine=0.05,
-            rewind=True):
+            rewind=True, correct=False):
     """Hybrid run (nemo_hyb_run); returns the statistics as a dict (counts of
     member-windows and member-steps).  quarantine: shadow error beyond which a
     member stays on the FP64 solver (0: never); rewind: such a member (and,
     after the last window, a diverged one) restarts from its FP64 state at the
-    start of the latest recent window the surrogate advanced it in."""
-    c = HybConfig(k, anchor, tol, int(bool(per_member)), quarantine, int(bool(rewind)))
+    start of the latest recent window the surrogate advanced it in; correct:
+    the calls of an accepted window add the shadow step's correction of the
+    window's first prediction."""
+    c = HybConfig(k, anchor, tol, int(bool(per_member)), quarantine, int(bool(rewind)),
+                  int(bool(correct)))
     st = HybStats()
     check(sur.lib.nemo_hyb_run(sur.h, ens.h, ctypes.byref(c), istp0, nsteps, ctypes.byref(st)),
           "nemo_hyb_run")

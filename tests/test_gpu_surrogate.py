@@ -714,3 +714,44 @@ def test_rewind_from_the_fourth_window_restores_the_third_windows_start(env):
     assert st["sur_steps"] == 270 and st["solver_steps"] == 4 * 10 + 110 + 90, st
     for f in (nb.SSHN, nb.UN, nb.VN):
         np.testing.assert_array_equal(a.field(0, f), ref.field(0, f))
+
+
+def test_shadow_correction_is_added_by_every_accepted_call(env):
+    """With correct=True every surrogate call of an accepted window adds,
+    per cell, the FP32 difference between the shadow state and the window's
+    first prediction.  A network with a zero output predicts no change, so
+    after the window each interior value is the shadow state plus nine times
+    (shadow - window start), the boundary row holds the tide and the open
+    boundary's v is the Flather value."""
+    torch, nb, sm = env
+    side, n = 128, 1
+    s = sm.Surrogate(nblocks=0, batch=n, height=side, width=side, train=False, seed=4)
+    s.set_params(np.zeros_like(s.params()))
+    s.set_norm([1.0] * 4, [0.0] * 4, [1.0, 1.0, 1.0])
+
+    def developed():
+        e = small_ensemble(nb, 61, n, side)
+        e.step_n(1, 300)
+        return e
+
+    ref = developed()
+    start = [ref.field(0, f).copy() for f in (nb.SSHN, nb.UN, nb.VN)]
+    ref.step_n(301, 10)  # the shadow step
+    shadow = [ref.field(0, f).copy() for f in (nb.SSHN, nb.UN, nb.VN)]
+    a = developed()
+    st = sm.hyb_run(s, a, 300, 100, tol=1e300, quarantine=1e100, correct=True)
+    assert st["fallbacks"] == 0 and st["sur_steps"] == 90, st
+    got = [a.field(0, f) for f in (nb.SSHN, nb.UN, nb.VN)]
+    want = []
+    for x0, xf in zip(start, shadow):
+        d = (xf - x0.astype(np.float32).astype(np.float64)).astype(np.float32).astype(np.float64)
+        x = xf.copy()
+        for _ in range(9):
+            x = (x + 0.0) + d
+        want.append(x)
+    np.testing.assert_array_equal(got[0][1:], want[0][1:])          # ssh below the tide row
+    np.testing.assert_array_equal(got[1][:, 1:-1], want[1][:, 1:-1])  # u between the walls
+    np.testing.assert_array_equal(got[2][1:-1], want[2][1:-1])      # v between boundary and wall
+    b = developed()
+    sm.hyb_run(s, b, 300, 100, tol=1e300, quarantine=1e100)  # without: persistence from the shadow
+    np.testing.assert_array_equal(b.field(0, nb.UN)[:, 1:-1], shadow[1][:, 1:-1])
