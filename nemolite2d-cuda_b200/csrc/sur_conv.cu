@@ -502,20 +502,21 @@ k_conv_fwd_rows(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
 // N = 64 or 128 (an edge input row feeds one or two output rows of the
 // strip).  An input row's ring slot is released as soon as its 12 MMAs are
 // issued.
-constexpr int NSLOT_T = 6;
-constexpr int TBLK = 8;  // accumulator blocks of 64 columns (512 TMEM columns)
-
+// NS input-row slots, NB accumulator blocks of 64 TMEM columns; the default
+// (6, 8) runs one CTA per SM with all 512 columns, (2, 4) two CTAs per SM.
+template <int NS, int NB>
 struct TriSmem {
-  uint8_t slot[NSLOT_T][RW_BYTES];
+  uint8_t slot[NS][RW_BYTES];
   uint8_t w[W_BYTES];  // [dx][dy][64 co][64 ci]: per dx a 192 x 64 K-major B operand
-  uint64_t full[NSLOT_T], empty[NSLOT_T];
+  uint64_t full[NS], empty[NS];
   uint64_t wbar, done;
-  uint64_t tfull[TBLK], tempty[TBLK];
+  uint64_t tfull[NB], tempty[NB];
   uint32_t tmem_base;
   float bias[CH];
 };
 
-__device__ __forceinline__ uint32_t tblk(uint32_t g) { return (TBLK - (g & (TBLK - 1))) & (TBLK - 1); }
+template <int NB>
+__device__ __forceinline__ uint32_t tblk(uint32_t g) { return (NB - (g & (NB - 1))) & (NB - 1); }
 
 __device__ __forceinline__ void tmem_zero32(uint32_t taddr) {
   asm volatile(
@@ -526,31 +527,32 @@ __device__ __forceinline__ void tmem_zero32(uint32_t taddr) {
 }
 __device__ __forceinline__ void tmem_st_wait() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
-__global__ void __launch_bounds__(THREADS, 1)
+template <int NS, int NB, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB)
 k_conv_fwd_tri(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmW,
                ConvEpi E, int R) {
   extern __shared__ uint8_t smem_raw[];
-  TriSmem& S = *reinterpret_cast<TriSmem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  TriSmem<NS, NB>& S = *reinterpret_cast<TriSmem<NS, NB>*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int xtiles = E.W / TM;
   const int ystrips = (E.H + R - 1) / R;
   const int nstrip = E.N * xtiles * ystrips;
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < NSLOT_T; ++s) {
+    for (int s = 0; s < NS; ++s) {
       mbar_init(&S.full[s], 1);
       mbar_init(&S.empty[s], 1);
     }
     mbar_init(&S.wbar, 1);
     mbar_init(&S.done, 1);
-    for (int b = 0; b < TBLK; ++b) {
+    for (int b = 0; b < NB; ++b) {
       mbar_init(&S.tfull[b], 1);
       mbar_init(&S.tempty[b], 128);
     }
     fence_barrier_init();
   }
   if (threadIdx.x < CH) S.bias[threadIdx.x] = E.bias ? E.bias[threadIdx.x] : 0.0f;
-  if (warp == 1) tmem_alloc(&S.tmem_base, 64 * TBLK);
+  if (warp == 1) tmem_alloc(&S.tmem_base, 64 * NB);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -559,7 +561,7 @@ k_conv_fwd_tri(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
   const uint64_t LIM = E.wait_ns ? (uint64_t)E.wait_ns : WAIT_NS;
   if (warp >= 2) {  // every accumulator block starts at zero
     const uint32_t tl = tmem + ((uint32_t)(32 * (warp & 3)) << 16);
-    for (int c = 0; c < 64 * TBLK; c += 32) tmem_zero32(tl + (uint32_t)c);
+    for (int c = 0; c < 64 * NB; c += 32) tmem_zero32(tl + (uint32_t)c);
     tmem_st_wait();
   }
   tc_fence_before();
@@ -580,8 +582,8 @@ k_conv_fwd_tri(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
       const int ys = st % ystrips, r0 = st / ystrips, xt = r0 % xtiles, n = r0 / xtiles;
       const int y0 = ys * R, y1 = min(y0 + R, E.H) - 1;
       for (int r = y0 - 1; r <= y1 + 1; ++r, ++L) {
-        const int slot = (int)(L % NSLOT_T);
-        const uint32_t ph = (L / NSLOT_T) & 1;
+        const int slot = (int)(L % NS);
+        const uint32_t ph = (L / NS) & 1;
         if (!mbar_wait(&S.empty[slot], ph ^ 1, LIM)) { fail(E.err, 31); ok = false; break; }
         if (skip_first && L == 0) continue;
         mbar_expect_tx(&S.full[slot], RW_BYTES);
@@ -589,8 +591,8 @@ k_conv_fwd_tri(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
       }
     }
     // every armed load lands before the CTA may exit (the omitted one is not armed)
-    for (int s = 0; s < NSLOT_T; ++s) {
-      const uint32_t armed = L / NSLOT_T + ((uint32_t)s < L % NSLOT_T ? 1u : 0u);
+    for (int s = 0; s < NS; ++s) {
+      const uint32_t armed = L / NS + ((uint32_t)s < L % NS ? 1u : 0u);
       if (skip_first && s == 0 && armed == 1) continue;
       if (armed) mbar_wait(&S.full[s], (armed - 1) & 1);
     }
@@ -610,16 +612,16 @@ k_conv_fwd_tri(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         // input row y0-1+t feeds the strip's output rows o_lo .. o_hi
         const int o_hi = min(t, rows - 1), o_lo = max(t - 2, 0);
         const uint32_t ld = L + (uint32_t)t;
-        const int slot = (int)(ld % NSLOT_T);
+        const int slot = (int)(ld % NS);
         if (t <= rows - 1) {  // output row t starts here: its block must be drained and zeroed
           const uint32_t g = g0 + (uint32_t)t;
-          if (!mbar_wait(&S.tempty[tblk(g)], ((g / TBLK) & 1) ^ 1, LIM)) { fail(E.err, 33); ok = false; break; }
+          if (!mbar_wait(&S.tempty[tblk<NB>(g)], ((g / NB) & 1) ^ 1, LIM)) { fail(E.err, 33); ok = false; break; }
         }
-        if (!mbar_wait(&S.full[slot], (ld / NSLOT_T) & 1, LIM)) { fail(E.err, 34); ok = false; break; }
+        if (!mbar_wait(&S.full[slot], (ld / NS) & 1, LIM)) { fail(E.err, 34); ok = false; break; }
         tc_fence_after();
         const int nout = o_hi - o_lo + 1;
-        const uint32_t dfirst = tblk(g0 + (uint32_t)o_hi);
-        const int n1 = min(nout, TBLK - (int)dfirst), n2 = nout - n1;
+        const uint32_t dfirst = tblk<NB>(g0 + (uint32_t)o_hi);
+        const int n1 = min(nout, NB - (int)dfirst), n2 = nout - n1;
         const int bfirst = t - o_hi;  // B block: 0 for dy = -1, 1 for 0, 2 for +1
         const uint32_t id1 = idesc(128, 64 * n1, 0, 0);
         const uint32_t id2 = idesc(128, 64 * (n2 > 0 ? n2 : 1), 0, 0);
@@ -637,7 +639,7 @@ k_conv_fwd_tri(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
           }
         }
         mma_commit(&S.empty[slot]);                         // the input row has had its last use
-        if (t >= 2) mma_commit(&S.tfull[tblk(g0 + (uint32_t)(t - 2))]);  // output row t-2 is complete
+        if (t >= 2) mma_commit(&S.tfull[tblk<NB>(g0 + (uint32_t)(t - 2))]);  // output row t-2 is complete
       }
       L += (uint32_t)rows + 2;
       g0 += (uint32_t)rows;
@@ -654,8 +656,8 @@ k_conv_fwd_tri(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
       const int ys = st % ystrips, r0 = st / ystrips, xt = r0 % xtiles, n = r0 / xtiles;
       const int y0 = ys * R, y1 = min(y0 + R, E.H) - 1;
       for (int y = y0; y <= y1; ++y, ++g) {
-        const uint32_t b = tblk(g);
-        if (!mbar_wait_warp(&S.tfull[b], (g / TBLK) & 1, LIM)) { fail(E.err, 35); ok = false; break; }
+        const uint32_t b = tblk<NB>(g);
+        if (!mbar_wait_warp(&S.tfull[b], (g / NB) & 1, LIM)) { fail(E.err, 35); ok = false; break; }
         tc_fence_after();
         float v[64];
         const uint32_t ta = tmem + b * 64 + ((uint32_t)(32 * q) << 16);
@@ -676,7 +678,7 @@ k_conv_fwd_tri(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
   if (warp == 1) {
     __syncwarp();
     tc_fence_after();
-    tmem_dealloc(tmem, 64 * TBLK);
+    tmem_dealloc(tmem, 64 * NB);
   }
 }
 
@@ -1270,8 +1272,11 @@ cudaError_t prepare_device(int* sms) {
     e = cudaFuncSetAttribute(k_conv_fwd_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)(sizeof(RowSmem) + 1024));
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_conv_fwd_tri, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)(sizeof(TriSmem) + 1024));
+    e = cudaFuncSetAttribute(k_conv_fwd_tri<6, 8, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(sizeof(TriSmem<6, 8>) + 1024));
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_conv_fwd_tri<2, 4, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(sizeof(TriSmem<2, 4>) + 1024));
     if (e != cudaSuccess) return e;
     g_attr[dev] = true;
   }
@@ -1295,11 +1300,12 @@ cudaError_t conv_fwd(const __nv_bfloat16* x, const __nv_bfloat16* w, const ConvE
   if ((e = prepare_device(&sms)) != cudaSuccess) return e;
   CUtensorMap ta, tw;
   if ((e = w_map(&tw, w)) != cudaSuccess) return e;
-  if (g_fwd_variant == 2) {
+  if (g_fwd_variant == 2 || g_fwd_variant == 3) {
     if ((e = act_map(&ta, x, epi.N, epi.H, epi.W, RW_PIX)) != cudaSuccess) return e;
     const int R = g_fwd_rows;
     const long nstrip = (long)epi.N * (epi.W / TM) * ((epi.H + R - 1) / R);
-    const int grid = (int)(nstrip < sms ? nstrip : sms);
+    const long slots = g_fwd_variant == 3 ? 2L * sms : (long)sms;  // resident CTAs
+    const int grid = (int)(nstrip < slots ? nstrip : slots);
     ConvEpi E = epi;
     E.wait_ns = g_test_wait_ns.load();
     int k = g_test_skip.load();
@@ -1307,7 +1313,10 @@ cudaError_t conv_fwd(const __nv_bfloat16* x, const __nv_bfloat16* w, const ConvE
     while (k > 0 && !g_test_skip.compare_exchange_weak(k, k - 1)) {
     }
     if (k > 0) E.skip_load = 1;
-    k_conv_fwd_tri<<<grid, THREADS, sizeof(TriSmem) + 1024, s>>>(ta, tw, E, R);
+    if (g_fwd_variant == 3)
+      k_conv_fwd_tri<2, 4, 2><<<grid, THREADS, sizeof(TriSmem<2, 4>) + 1024, s>>>(ta, tw, E, R);
+    else
+      k_conv_fwd_tri<6, 8, 1><<<grid, THREADS, sizeof(TriSmem<6, 8>) + 1024, s>>>(ta, tw, E, R);
     return cudaGetLastError();
   }
   if (g_fwd_variant == 1) {
@@ -1340,7 +1349,7 @@ unsigned long long set_test_wait(unsigned long long wait_ns, int skip_launches) 
 
 int set_fwd_variant(int variant, int rows) {
   const int prev = g_fwd_variant;
-  if (variant >= 0 && variant <= 2) g_fwd_variant = variant;
+  if (variant >= 0 && variant <= 3) g_fwd_variant = variant;
   if (rows >= 1 && rows <= 4096) g_fwd_rows = rows;
   return prev;
 }
