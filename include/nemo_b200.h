@@ -412,7 +412,8 @@ int nemo_conv3x3_wgrad(const void* x, const void* dz, float* dw, float* db, int 
                        int ctas, int* err, void* stream);
 /* Process-wide forward kernel: 2 (default) marches column strips of `rows`
  * output rows with each input row loaded once and multiplied once per
- * horizontal tap into all three output rows it feeds (N = 192 MMAs); 1 marches
+ * horizontal tap into all three output rows it feeds (N = 192 MMAs); 3 is the
+ * same with two CTAs per SM (2 input-row slots, 256 TMEM columns each); 1 marches
  * the same strips with one N = 64 MMA per tap and output row; 0 loads one TMA
  * window per tap.  Returns the previous variant; values out of range change
  * nothing. */
