@@ -410,10 +410,12 @@ int nemo_conv3x3_fwd(const void* x, const void* w, const float* bias, const void
                      int* err, void* stream);
 int nemo_conv3x3_wgrad(const void* x, const void* dz, float* dw, float* db, int n, int h, int w_,
                        int ctas, int* err, void* stream);
-/* Process-wide forward kernel: 2 (default) marches column strips of `rows`
- * output rows with each input row loaded once and multiplied once per
- * horizontal tap into all three output rows it feeds (N = 192 MMAs); 3 is the
- * same with two CTAs per SM (2 input-row slots, 256 TMEM columns each); 1 marches
+/* Process-wide forward kernel: 4 (default, with rows = 32) marches column
+ * strips of `rows` output rows with each input row loaded once and multiplied
+ * once per horizontal tap into all three output rows it feeds (N = 192 MMAs),
+ * and each epilogue warp writes its 32 pixels of an output row with one TMA
+ * store from shared memory; 2 is the same with per-thread stores; 3 is 2 with
+ * two CTAs per SM (2 input-row slots, 256 TMEM columns each); 1 marches
  * the same strips with one N = 64 MMA per tap and output row; 0 loads one TMA
  * window per tap.  Returns the previous variant; values out of range change
  * nothing. */

@@ -155,8 +155,9 @@ struct FwdSmem {
 __device__ __forceinline__ void fail(int* err, int code) { atomicCAS(err, 0, code); }
 
 // Epilogue of one 128-pixel output tile for this thread's pixel `row`:
-// v = acc (64 fp32 values) + bias, + residual, *(mask > 0), relu; stores.
-__device__ __forceinline__ void epilogue_store(const ConvEpi& E, const float* bias, float* v, long p) {
+// v = acc (64 fp32 values) + bias, + residual, *(mask > 0), relu; the FP32
+// output; the BF16 output is left to the caller.
+__device__ __forceinline__ void epilogue_math(const ConvEpi& E, const float* bias, float* v, long p) {
 #pragma unroll
   for (int c = 0; c < 64; ++c) v[c] += bias[c];
   if (E.residual) {
@@ -198,18 +199,40 @@ __device__ __forceinline__ void epilogue_store(const ConvEpi& E, const float* bi
     for (int g = 0; g < 16; ++g)
       if (g < nq) o32[g] = make_float4(v[4 * g], v[4 * g + 1], v[4 * g + 2], v[4 * g + 3]);
   }
+}
+
+// Eight 16-byte groups of BF16 channels (8 channels each) of one pixel.
+__device__ __forceinline__ uint4 bf16x8(const float* v, int g) {
+  uint4 u;
+  __nv_bfloat162* h = reinterpret_cast<__nv_bfloat162*>(&u);
+#pragma unroll
+  for (int e = 0; e < 4; ++e) h[e] = __floats2bfloat162_rn(v[8 * g + 2 * e], v[8 * g + 2 * e + 1]);
+  return u;
+}
+
+// The whole epilogue with the BF16 output stored by this thread.
+__device__ __forceinline__ void epilogue_store(const ConvEpi& E, const float* bias, float* v, long p) {
+  epilogue_math(E, bias, v, p);
   if (E.out) {
     uint4* op = reinterpret_cast<uint4*>(E.out + p * CH);
 #pragma unroll
-    for (int g = 0; g < 8; ++g) {
-      uint4 u;
-      __nv_bfloat162* h = reinterpret_cast<__nv_bfloat162*>(&u);
-#pragma unroll
-      for (int e = 0; e < 4; ++e) h[e] = __floats2bfloat162_rn(v[8 * g + 2 * e], v[8 * g + 2 * e + 1]);
-      op[g] = u;
-    }
+    for (int g = 0; g < 8; ++g) op[g] = bf16x8(v, g);
   }
 }
+
+// TMA store of a 64-channel x 32-pixel BF16 tile staged in shared memory
+// (128-byte swizzle, as the tensor map's), and the bulk-group bookkeeping.
+__device__ __forceinline__ void tma_store_4d(const CUtensorMap* tm, const void* src, int c0, int c1, int c2,
+                                             int c3) {
+  asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.bulk_group [%0, {%2, %3, %4, %5}], [%1];" ::"l"(tm),
+               "r"(smem_u32(src)), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// at most one group still reading its shared-memory source
+__device__ __forceinline__ void bulk_wait_read1() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 
 __global__ void __launch_bounds__(THREADS, 1)
@@ -504,9 +527,12 @@ k_conv_fwd_rows(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
 // issued.
 // NS input-row slots, NB accumulator blocks of 64 TMEM columns; the default
 // (6, 8) runs one CTA per SM with all 512 columns, (2, 4) two CTAs per SM.
-template <int NS, int NB>
+// OST: bytes of output staging (two 4 KiB tiles per epilogue warp when the
+// BF16 output leaves by TMA stores).
+template <int NS, int NB, int OST = 1024>
 struct TriSmem {
   uint8_t slot[NS][RW_BYTES];
+  uint8_t ost[OST];
   uint8_t w[W_BYTES];  // [dx][dy][64 co][64 ci]: per dx a 192 x 64 K-major B operand
   uint64_t full[NS], empty[NS];
   uint64_t wbar, done;
@@ -527,12 +553,16 @@ __device__ __forceinline__ void tmem_zero32(uint32_t taddr) {
 }
 __device__ __forceinline__ void tmem_st_wait() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
-template <int NS, int NB, int MINB>
+// TS: each epilogue warp stages its 32 pixels' BF16 outputs in shared memory
+// (two tiles alternating) and writes them with one TMA store per output row
+// (tensor map tmO, box 64 channels x 32 pixels) instead of per-thread stores.
+template <int NS, int NB, int MINB, bool TS>
 __global__ void __launch_bounds__(THREADS, MINB)
 k_conv_fwd_tri(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmW,
-               ConvEpi E, int R) {
+               const __grid_constant__ CUtensorMap tmO, ConvEpi E, int R) {
   extern __shared__ uint8_t smem_raw[];
-  TriSmem<NS, NB>& S = *reinterpret_cast<TriSmem<NS, NB>*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  using Smem = TriSmem<NS, NB, TS ? 8 * 4096 : 1024>;
+  Smem& S = *reinterpret_cast<Smem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int xtiles = E.W / TM;
   const int ystrips = (E.H + R - 1) / R;
@@ -602,6 +632,8 @@ k_conv_fwd_tri(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     bool ok = mbar_wait(&S.wbar, 0);
     if (!ok) fail(E.err, 32);
     const uint32_t wbase = smem_u32(S.w);
+    const uint64_t DK = sdesc(0, 16, 1024);  // K-major, 128-byte swizzle; address field zero
+    const uint32_t ID192 = idesc(128, 192, 0, 0);
     uint32_t L = 0;  // loads consumed
     uint32_t g0 = 0;  // CTA-wide index of the strip's first output row
     for (int st = blockIdx.x; st < nstrip && ok; st += gridDim.x) {
@@ -623,19 +655,35 @@ k_conv_fwd_tri(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         const uint32_t dfirst = tblk<NB>(g0 + (uint32_t)o_hi);
         const int n1 = min(nout, NB - (int)dfirst), n2 = nout - n1;
         const int bfirst = t - o_hi;  // B block: 0 for dy = -1, 1 for 0, 2 for +1
-        const uint32_t id1 = idesc(128, 64 * n1, 0, 0);
-        const uint32_t id2 = idesc(128, 64 * (n2 > 0 ? n2 : 1), 0, 0);
-        const uint32_t sbase = smem_u32(S.slot[slot]);
+        // descriptors as constant offsets (in 16-byte units) from two bases:
+        // the input row's window starting at pixel 7 and the weight block of
+        // dx = -1, dy = bfirst; dx steps 128 bytes / 3 weight blocks, k 32 bytes
+        const uint64_t A0 = DK + ((smem_u32(S.slot[slot]) + 7u * 128u) >> 4);
+        const uint64_t B0 = DK + ((wbase + (uint32_t)bfirst * WT_BYTES) >> 4);
+        if (n2 == 0 && nout == 3) {  // an interior row, no wrap: 12 MMAs of N = 192
+          const uint32_t d = tmem + dfirst * 64;
 #pragma unroll
-        for (int dx = 0; dx < 3; ++dx) {
-          const uint32_t a0 = sbase + (uint32_t)(7 + dx) * 128u;
-          const uint32_t b0 = wbase + (uint32_t)(dx * 3 + bfirst) * WT_BYTES;
+          for (int dx = 0; dx < 3; ++dx)
 #pragma unroll
-          for (int k = 0; k < 4; ++k) {
-            mma_bf16(tmem + dfirst * 64, sdesc(a0 + 32 * k, 16, 1024), sdesc(b0 + 32 * k, 16, 1024), id1, 1);
-            if (n2 > 0)
-              mma_bf16(tmem, sdesc(a0 + 32 * k, 16, 1024), sdesc(b0 + (uint32_t)n1 * WT_BYTES + 32 * k, 16, 1024),
-                       id2, 1);
+            for (int k = 0; k < 4; ++k)
+              mma_bf16(d, A0 + (uint64_t)(8 * dx + 2 * k), B0 + (uint64_t)(dx * 3 * (WT_BYTES >> 4) + 2 * k), ID192, 1u);
+        } else {
+          const uint32_t id1 = idesc(128, 64 * n1, 0, 0);
+          const uint32_t id2 = idesc(128, 64 * (n2 > 0 ? n2 : 1), 0, 0);
+          const uint64_t B1 = B0 + (uint64_t)(n1 * (WT_BYTES >> 4));
+#pragma unroll
+          for (int dx = 0; dx < 3; ++dx)
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+              mma_bf16(tmem + dfirst * 64, A0 + (uint64_t)(8 * dx + 2 * k),
+                       B0 + (uint64_t)(dx * 3 * (WT_BYTES >> 4) + 2 * k), id1, 1u);
+          if (n2 > 0) {
+#pragma unroll
+            for (int dx = 0; dx < 3; ++dx)
+#pragma unroll
+              for (int k = 0; k < 4; ++k)
+                mma_bf16(tmem, A0 + (uint64_t)(8 * dx + 2 * k), B1 + (uint64_t)(dx * 3 * (WT_BYTES >> 4) + 2 * k),
+                         id2, 1u);
           }
         }
         mma_commit(&S.empty[slot]);                         // the input row has had its last use
@@ -669,9 +717,28 @@ k_conv_fwd_tri(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         tc_fence_before();
         mbar_arrive(&S.tempty[b]);
         const long p = ((long)(n * E.H + y) * E.W + xt * TM + row);
-        epilogue_store(E, S.bias, v, p);
+        if constexpr (TS) {
+          epilogue_math(E, S.bias, v, p);
+          if (E.out) {
+            uint8_t* buf = S.ost + (q * 2 + (int)(g & 1)) * 4096;
+            if (lane == 0) bulk_wait_read1();  // the store two rows ago has read this tile
+            __syncwarp();
+#pragma unroll
+            for (int c = 0; c < 8; ++c)  // 16-byte chunk c of row `lane`, 128-byte swizzle
+              *reinterpret_cast<uint4*>(buf + lane * 128 + ((c ^ (lane & 7)) << 4)) = bf16x8(v, c);
+            fence_proxy_async();
+            __syncwarp();
+            if (lane == 0) {
+              tma_store_4d(&tmO, buf, 0, xt * TM + 32 * q, y, n);
+              bulk_commit();
+            }
+          }
+        } else {
+          epilogue_store(E, S.bias, v, p);
+        }
       }
     }
+    if (TS && lane == 0) bulk_wait_all();  // every store has landed before the CTA exits
   }
   tc_fence_before();
   __syncthreads();
@@ -1030,6 +1097,14 @@ k_conv_wgrad_strip(const __grid_constant__ CUtensorMap tmX, const __grid_constan
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = S.tmem_base;
+  if (warp >= 2) {  // every accumulator starts at zero, so every MMA accumulates
+    const uint32_t tl = tmem + ((uint32_t)(32 * (warp & 3)) << 16);
+    for (int c = 0; c < 512; c += 32) tmem_zero32(tl + (uint32_t)c);
+    tmem_st_wait();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
 
   // unit u = (n * xch + column chunk) * H + y: the coordinates of the range's
   // first unit, then stepped per unit (a 64-bit division per unit would cost
@@ -1076,39 +1151,61 @@ k_conv_wgrad_strip(const __grid_constant__ CUtensorMap tmX, const __grid_constan
     }
   } else if (warp == 1 && lane == 0) {
     // ---- MMA issuer ----
+    // A single thread issues the MMAs, so its per-unit work is kept to a few
+    // independent operations: ring slots and phases are stepped, not divided
+    // out, and the descriptors of group A and of dz are constant offsets from
+    // two bases (their address fields are addresses / 16).
     const uint32_t ID = idesc(128, 192, 1, 1);
     const uint32_t ones = smem_u32(S.ones);
-    uint32_t lx = 0, lz = 0;
-    bool ok = true, first = true;
+    const uint32_t xbase = smem_u32(S.x[0]), zbase = smem_u32(S.z[0]);
+    const uint64_t DA = sdesc(0, 128, 1024), DB = sdesc(0, Smem::ZBYTES, 1024);
+    uint32_t xsl = 0, xph = 0;   // x window slot and phase of the next unit
+    uint32_t zsl = 0, zph = 0;   // dz slot and phase of the next row load
+    uint32_t s1 = 0, s2 = 0;     // slots of rows y and y-1
+    bool ok = true;
     int y = y_begin;
+    auto zstep = [&]() {
+      zsl = zsl ? zsl - 1 : (uint32_t)KZ - 1;
+      if (zsl == 0) zph ^= 1u;
+    };
     for (long u = u_begin; u < u_end; ++u, y = (y + 1 == G.H) ? 0 : y + 1) {
       const bool start = (u == u_begin) || y == 0;
       const bool last = (u + 1 == u_end) || (y + 1 == G.H);
-      if (start) lz += 2;
-      const uint32_t l1 = lz++;  // dz row y+1; rows y and y-1 are loads l1-1 and l1-2
-      for (uint32_t l = start ? l1 - 2 : l1; l <= l1 && ok; ++l)
-        ok = mbar_wait(&S.zfull[ws_zslot<KZ>(l)], (l / KZ) & 1);
-      const uint32_t xsl = lx % KX;
-      if (ok) ok = mbar_wait(&S.xfull[xsl], (lx / KX) & 1);
+      if (start) {  // rows y-1 and y are this strip's first two loads
+        s2 = zsl;
+        ok = mbar_wait(&S.zfull[zsl], zph);
+        zstep();
+        s1 = zsl;
+        if (ok) ok = mbar_wait(&S.zfull[zsl], zph);
+        zstep();
+      }
+      const uint32_t s0 = zsl;  // row y+1
+      if (ok) ok = mbar_wait(&S.zfull[zsl], zph);
+      zstep();
+      if (ok) ok = mbar_wait(&S.xfull[xsl], xph);
       if (!ok) break;
-      ++lx;
       tc_fence_after();
-      const uint32_t xs = smem_u32(S.x[xsl]);
-      const uint32_t zb = smem_u32(S.z[ws_zslot<KZ>(l1)]);
+      const uint32_t xs = xbase + xsl * (uint32_t)Smem::XBYTES;
+      const uint64_t a1 = DA + ((xs + 7u * 128u) >> 4);                            // [x(-1) | x(0)]
+      const uint64_t bd = DB + ((zbase + s0 * (uint32_t)Smem::ZBYTES) >> 4);     // dz rows y+1, y, y-1
 #pragma unroll
       for (int k = 0; k < PIX / 16; ++k) {
-        const uint64_t bd = sdesc(zb + 2048u * k, Smem::ZBYTES, 1024);
-        const uint32_t acc = (first && k == 0) ? 0u : 1u;
+        const uint64_t dk = (uint64_t)(128 * k);  // 16 pixel rows of 128 bytes, in 16-byte units
+        mma_bf16(tmem, a1 + dk, bd + dk, ID, 1u);
         const uint32_t xb = xs + (9u + 16u * k) * 128u;  // x(+1) rows of this K step
-        mma_bf16(tmem, sdesc(xs + (7u + 16u * k) * 128u, 128, 1024), bd, ID, acc);
-        mma_bf16(tmem + 256, sdesc(xb, ones - xb, 1024), bd, ID, acc);  // ones lie after the x ring
+        mma_bf16(tmem + 256, sdesc(xb, ones - xb, 1024), bd + dk, ID, 1u);  // ones lie after the rings
       }
-      first = false;
       mma_commit(&S.xempty[xsl]);
-      mma_commit(&S.zempty[ws_zslot<KZ>(l1 - 2)]);  // row y-1 has had its last use
-      if (last) {                                    // so have rows y and y+1 at a strip's end
-        mma_commit(&S.zempty[ws_zslot<KZ>(l1 - 1)]);
-        mma_commit(&S.zempty[ws_zslot<KZ>(l1)]);
+      mma_commit(&S.zempty[s2]);  // row y-1 has had its last use
+      if (last) {                 // so have rows y and y+1 at a strip's end
+        mma_commit(&S.zempty[s1]);
+        mma_commit(&S.zempty[s0]);
+      }
+      s2 = s1;
+      s1 = s0;
+      if (++xsl == (uint32_t)KX) {
+        xsl = 0;
+        xph ^= 1u;
       }
     }
     if (!ok) fail(G.err, 52);
@@ -1231,9 +1328,10 @@ cudaError_t w_map(CUtensorMap* m, const void* base) {
 
 int g_sms[64];
 bool g_attr[64];
-int g_fwd_variant = 2;  // 2: three output rows per MMA (k_conv_fwd_tri), 1: row ring
-                        // (k_conv_fwd_rows), 0: a TMA window per tap (k_conv_fwd)
-int g_fwd_rows = 16;    // rows per strip of the row-ring kernel
+int g_fwd_variant = 4;  // 4: three output rows per MMA (k_conv_fwd_tri), outputs by TMA
+                        // stores; 2: the same with per-thread stores; 3: as 2, two CTAs
+                        // per SM; 1: row ring (k_conv_fwd_rows); 0: a TMA window per tap
+int g_fwd_rows = 32;    // rows per strip of the ring kernels
 int g_wgrad_variant = 3;  // 3: all taps per CTA over column strips (k_conv_wgrad_strip)
                           // in 128-pixel units where the width allows, else as 2;
                           // 2: the same in 64-pixel units; 1: three vertical taps per MMA
@@ -1272,10 +1370,13 @@ cudaError_t prepare_device(int* sms) {
     e = cudaFuncSetAttribute(k_conv_fwd_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)(sizeof(RowSmem) + 1024));
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_conv_fwd_tri<6, 8, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(k_conv_fwd_tri<6, 8, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)(sizeof(TriSmem<6, 8>) + 1024));
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_conv_fwd_tri<2, 4, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(k_conv_fwd_tri<6, 8, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(sizeof(TriSmem<6, 8, 8 * 4096>) + 1024));
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_conv_fwd_tri<2, 4, 2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)(sizeof(TriSmem<2, 4>) + 1024));
     if (e != cudaSuccess) return e;
     g_attr[dev] = true;
@@ -1300,7 +1401,7 @@ cudaError_t conv_fwd(const __nv_bfloat16* x, const __nv_bfloat16* w, const ConvE
   if ((e = prepare_device(&sms)) != cudaSuccess) return e;
   CUtensorMap ta, tw;
   if ((e = w_map(&tw, w)) != cudaSuccess) return e;
-  if (g_fwd_variant == 2 || g_fwd_variant == 3) {
+  if (g_fwd_variant >= 2) {
     if ((e = act_map(&ta, x, epi.N, epi.H, epi.W, RW_PIX)) != cudaSuccess) return e;
     const int R = g_fwd_rows;
     const long nstrip = (long)epi.N * (epi.W / TM) * ((epi.H + R - 1) / R);
@@ -1313,10 +1414,15 @@ cudaError_t conv_fwd(const __nv_bfloat16* x, const __nv_bfloat16* w, const ConvE
     while (k > 0 && !g_test_skip.compare_exchange_weak(k, k - 1)) {
     }
     if (k > 0) E.skip_load = 1;
-    if (g_fwd_variant == 3)
-      k_conv_fwd_tri<2, 4, 2><<<grid, THREADS, sizeof(TriSmem<2, 4>) + 1024, s>>>(ta, tw, E, R);
-    else
-      k_conv_fwd_tri<6, 8, 1><<<grid, THREADS, sizeof(TriSmem<6, 8>) + 1024, s>>>(ta, tw, E, R);
+    if (g_fwd_variant == 3) {
+      k_conv_fwd_tri<2, 4, 2, false><<<grid, THREADS, sizeof(TriSmem<2, 4>) + 1024, s>>>(ta, tw, ta, E, R);
+    } else if (g_fwd_variant == 4 && epi.out) {
+      CUtensorMap to;
+      if ((e = act_map(&to, epi.out, epi.N, epi.H, epi.W, 32)) != cudaSuccess) return e;
+      k_conv_fwd_tri<6, 8, 1, true><<<grid, THREADS, sizeof(TriSmem<6, 8, 8 * 4096>) + 1024, s>>>(ta, tw, to, E, R);
+    } else {
+      k_conv_fwd_tri<6, 8, 1, false><<<grid, THREADS, sizeof(TriSmem<6, 8>) + 1024, s>>>(ta, tw, ta, E, R);
+    }
     return cudaGetLastError();
   }
   if (g_fwd_variant == 1) {
@@ -1349,7 +1455,7 @@ unsigned long long set_test_wait(unsigned long long wait_ns, int skip_launches) 
 
 int set_fwd_variant(int variant, int rows) {
   const int prev = g_fwd_variant;
-  if (variant >= 0 && variant <= 3) g_fwd_variant = variant;
+  if (variant >= 0 && variant <= 4) g_fwd_variant = variant;
   if (rows >= 1 && rows <= 4096) g_fwd_rows = rows;
   return prev;
 }

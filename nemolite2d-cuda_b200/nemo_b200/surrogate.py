@@ -218,9 +218,10 @@ def conv3x3_fwd(lib, x, w, n, h, wd, err, bias=None, residual=None, mask=None, r
 
 
 def conv3x3_fwd_variant(lib, variant, rows=0):
-    """Select the forward kernel process-wide (2: three output rows per MMA,
-    the default; 3: the same with two CTAs per SM; 1: row ring; 0: window per
-    tap) and the rows per strip of the
+    """Select the forward kernel process-wide (4, the default: three output
+    rows per MMA with TMA stores of the outputs; 2: the same with per-thread
+    stores; 3: 2 with two CTAs per SM; 1: row ring; 0: window per tap) and the
+    rows per strip (default 32) of the
     ring kernels; returns the previous variant."""
     return lib.nemo_conv3x3_fwd_variant(variant, rows)
 

@@ -40,18 +40,20 @@ def ulp_close(got, ref):
     return bad.mean(), np.abs(got - ref).max()
 
 
-@pytest.fixture(params=[(2, 16), (2, 2), (2, 1), (2, 5), (3, 16), (3, 2), (3, 1), (1, 16), (1, 2), (0, 0)],
-                ids=["tri16", "tri2", "tri1", "tri5", "tri2cta16", "tri2cta2", "tri2cta1", "rows16",
-                     "rows2", "per-tap"])
+@pytest.fixture(params=[(2, 16), (2, 2), (2, 1), (2, 5), (3, 16), (3, 2), (3, 1), (4, 16), (4, 1), (4, 5),
+                        (1, 16), (1, 2), (0, 0)],
+                ids=["tri16", "tri2", "tri1", "tri5", "tri2cta16", "tri2cta2", "tri2cta1", "tritma16",
+                     "tritma1", "tritma5", "rows16", "rows2", "per-tap"])
 def variant(request, env):
     """Each forward kernel variant (three output rows per MMA with 16, 2, 1 or
-    5 rows per strip, the same two CTAs per SM, row ring with 16 or 2 rows per
-    strip, window per tap), restored to the default afterwards."""
+    5 rows per strip, the same two CTAs per SM, the same with TMA stores of
+    the output, row ring with 16 or 2 rows per strip, window per tap),
+    restored to the default afterwards."""
     torch, nb, sm = env
     lib = nb.load(False)
     prev = sm.conv3x3_fwd_variant(lib, *request.param)
     yield request.param
-    sm.conv3x3_fwd_variant(lib, prev, 16)  # the default, restored
+    sm.conv3x3_fwd_variant(lib, prev, 32)  # the default, restored
 
 
 def run_fwd(torch, sm, lib, x, w, bias=None, residual=None, mask=None, relu=False, out32=False):
