@@ -1261,7 +1261,10 @@ using WsA = WsSmem<64, 8, 12>;   // wgrad variant 2
 #ifndef NEMO_WS_WIDE_KX
 #define NEMO_WS_WIDE_KX 5
 #endif
-using WsB = WsSmem<128, NEMO_WS_WIDE_KX, 6>;  // wgrad variant 3, the default (WsA unless W % 128 == 0)
+#ifndef NEMO_WS_WIDE_KZ
+#define NEMO_WS_WIDE_KZ 6
+#endif
+using WsB = WsSmem<128, NEMO_WS_WIDE_KX, NEMO_WS_WIDE_KZ>;  // wgrad variant 3, the default (WsA unless W % 128 == 0)
 static_assert(sizeof(WsA) + 1024 <= 232448 && sizeof(WsB) + 1024 <= 232448, "shared memory per CTA");
 
 // dw[i] += sum_b part[b][i] (i < 9*64*64), db[i - 9*64*64] += ... (the rest),
@@ -1364,7 +1367,7 @@ cudaError_t prepare_device(int* sms) {
     e = cudaFuncSetAttribute(k_conv_wgrad_strip<64, 8, 12>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)(sizeof(WsA) + 1024));
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_conv_wgrad_strip<128, NEMO_WS_WIDE_KX, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(k_conv_wgrad_strip<128, NEMO_WS_WIDE_KX, NEMO_WS_WIDE_KZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)(sizeof(WsB) + 1024));
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k_conv_fwd_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1501,7 +1504,7 @@ cudaError_t conv_wgrad(const __nv_bfloat16* x, const __nv_bfloat16* dz, const Wg
     if (gx > a.partial_blocks) gx = a.partial_blocks;
     if (gx < 1) return cudaErrorInvalidValue;
     if (wide)
-      k_conv_wgrad_strip<128, NEMO_WS_WIDE_KX, 6><<<(unsigned)gx, THREADS, sizeof(WsB) + 1024, s>>>(tx, tz, a);
+      k_conv_wgrad_strip<128, NEMO_WS_WIDE_KX, NEMO_WS_WIDE_KZ><<<(unsigned)gx, THREADS, sizeof(WsB) + 1024, s>>>(tx, tz, a);
     else
       k_conv_wgrad_strip<64, 8, 12><<<(unsigned)gx, THREADS, sizeof(WsA) + 1024, s>>>(tx, tz, a);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
