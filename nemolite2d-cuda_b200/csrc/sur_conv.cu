@@ -20,6 +20,11 @@
 //   TMA and are read by the MMA as MN-major (channels contiguous); CTAs split
 //   the pixel range and add their partial D into an FP32 dw with atomics.
 //
+// These two are the first forms; the defaults are k_conv_fwd_tri (three output
+// rows per N = 192 MMA, outputs written by TMA stores) and k_conv_wgrad_strip
+// (all nine taps per CTA over column strips, partial sums added in a fixed
+// order by k_wgrad_reduce), described where they are defined.
+//
 // Every wait on an mbarrier is bounded; on timeout the kernel records an
 // error code, lets in-flight copies and MMAs finish (also bounded), frees its
 // tensor memory and returns.
